@@ -1,0 +1,180 @@
+// extern "C" RI-MP2 entry points: argument checks, host<->device staging and
+// precision dispatch.  Replaces the reference's device hook
+// try_spin_components_on_device / spin_components_on_device
+// (ferric-mp2/src/rimp2_gpu.rs:105-471) and the host gradient intermediates
+// x_ov / P (ferric-mp2/src/zvector.rs:651-703, oo_rimp2.rs:1170-1300).
+#include "fc_internal.cuh"
+#include "rimp2.cuh"
+
+#include <cmath>
+#include <cstdlib>
+
+using namespace fc;
+
+namespace {
+
+fc_status check_shapes(const void* b_ov, int64_t naux, int64_t nocc, int64_t nvir, const void* eo,
+                       const void* ev, int32_t precision, int32_t has_kappa, double kappa,
+                       const void* e_os, const void* e_ss) {
+    if (!e_os || !e_ss) return fail(FC_ERR_INVALID, "RI-MP2: null output pointer");
+    if (naux < 0 || nocc < 0 || nvir < 0) return fail(FC_ERR_LAYOUT, "RI-MP2: negative dimension");
+    int64_t nov, nb;
+    if (!mul_ok(nocc, nvir, &nov) || !mul_ok(nov, naux, &nb) || !mul_ok(nb, 8, &nb))
+        return fail(FC_ERR_LAYOUT, "RI-MP2: naux*nocc*nvir overflows");
+    if (nocc > 1 << 20 || nvir > 1 << 24) return fail(FC_ERR_LAYOUT, "RI-MP2: nocc/nvir out of range");
+    if (nov && naux && (!b_ov || !eo || !ev)) return fail(FC_ERR_INVALID, "RI-MP2: null input pointer");
+    if (precision < FC_PREC_F64 || precision > FC_PREC_MIXED_X6)
+        return fail(FC_ERR_INVALID, "RI-MP2: unknown precision " + std::to_string(precision));
+    if (has_kappa && precision != FC_PREC_F64)
+        return fail(FC_ERR_INVALID,
+                    "RI-MP2: kappa damping runs in FP64 only (mixed is defined without kappa)");
+    if (has_kappa && !(std::isfinite(kappa) && kappa > 0.0))
+        return fail(FC_ERR_INVALID, "RI-MP2: kappa must be finite and > 0");
+    return FC_OK;
+}
+
+int64_t chunk_budget() {
+    int64_t b = int64_t(8) << 30;
+    if (const char* s = std::getenv("FERRIC_CUDA_CHUNK_BYTES")) {
+        long long v = std::atoll(s);
+        if (v > 0) b = v;
+    }
+    Context& c = ctx();
+    if (c.pool_cap) {
+        int64_t left = (int64_t)c.pool_cap - (int64_t)(ws_bytes() + c.handle_bytes);
+        if (left / 2 < b) b = left / 2 > 0 ? left / 2 : 1;
+    }
+    return b;
+}
+
+fc_status energy_dispatch(const Rimp2Dev& d, int32_t precision, cudaStream_t st, double* e_os,
+                          double* e_ss, fc_stats* stats) {
+    if (precision == FC_PREC_F64) return rimp2_energy_f64(d, st, e_os, e_ss, stats);
+    return rimp2_energy_mixed(d, precision == FC_PREC_MIXED ? 2 : 3, st, e_os, e_ss, stats);
+}
+
+fc_status grad_dispatch(const Rimp2Dev& d, int32_t precision, cudaStream_t st, double* e_os,
+                        double* e_ss, double* gamma, double* de_docc, double* de_dvir,
+                        fc_stats* stats) {
+    if (precision == FC_PREC_F64)
+        return rimp2_grad_f64(d, st, e_os, e_ss, gamma, de_docc, de_dvir, stats);
+    return rimp2_grad_mixed(d, precision == FC_PREC_MIXED ? 2 : 3, st, e_os, e_ss, gamma, de_docc,
+                            de_dvir, stats);
+}
+
+}  // namespace
+
+extern "C" {
+
+fc_status fc_rimp2_energy_dev(const double* b_ov, int64_t naux, int64_t nocc, int64_t nvir,
+                              const double* eps_occ, const double* eps_vir, int32_t has_kappa,
+                              double kappa, int32_t precision, double* e_os, double* e_ss,
+                              void* stream, fc_stats* stats) {
+    FC_TRY(check_shapes(b_ov, naux, nocc, nvir, eps_occ, eps_vir, precision, has_kappa, kappa, e_os, e_ss));
+    FC_TRY(require_init());
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (stats) *stats = fc_stats{};
+    if (naux == 0 || nocc == 0 || nvir == 0) {
+        *e_os = 0.0;
+        *e_ss = 0.0;
+        return FC_OK;
+    }
+    Rimp2Dev d{b_ov, eps_occ, eps_vir, naux, nocc, nvir, has_kappa, kappa, chunk_budget()};
+    return energy_dispatch(d, precision, pick_stream(stream), e_os, e_ss, stats);
+}
+
+fc_status fc_rimp2_energy(const double* b_ov, int64_t naux, int64_t nocc, int64_t nvir,
+                          const double* eps_occ, const double* eps_vir, int32_t has_kappa,
+                          double kappa, int32_t precision, double* e_os, double* e_ss,
+                          fc_stats* stats) {
+    FC_TRY(check_shapes(b_ov, naux, nocc, nvir, eps_occ, eps_vir, precision, has_kappa, kappa, e_os, e_ss));
+    FC_TRY(require_init());
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (stats) *stats = fc_stats{};
+    if (naux == 0 || nocc == 0 || nvir == 0) {
+        *e_os = 0.0;
+        *e_ss = 0.0;
+        return FC_OK;
+    }
+    cudaStream_t st = ctx().stream;
+    const size_t nb = (size_t)naux * nocc * nvir * sizeof(double);
+    void *db, *de;
+    FC_TRY(ws_get(WS_B, nb, &db));
+    FC_TRY(ws_get(WS_EPS, (nocc + nvir) * sizeof(double), &de));
+    FC_CUDA(cudaMemcpyAsync(db, b_ov, nb, cudaMemcpyHostToDevice, st));
+    FC_CUDA(cudaMemcpyAsync(de, eps_occ, nocc * sizeof(double), cudaMemcpyHostToDevice, st));
+    FC_CUDA(cudaMemcpyAsync((double*)de + nocc, eps_vir, nvir * sizeof(double), cudaMemcpyHostToDevice, st));
+    Rimp2Dev d{(const double*)db, (const double*)de, (const double*)de + nocc, naux, nocc, nvir,
+               has_kappa, kappa, chunk_budget()};
+    FC_TRY(energy_dispatch(d, precision, st, e_os, e_ss, stats));
+    if (stats) stats->h2d_bytes += nb + (nocc + nvir) * sizeof(double);
+    return FC_OK;
+}
+
+fc_status fc_rimp2_energy_grad_dev(const double* b_ov, int64_t naux, int64_t nocc, int64_t nvir,
+                                   const double* eps_occ, const double* eps_vir, int32_t precision,
+                                   double* e_os, double* e_ss, double* gamma, double* de_docc,
+                                   double* de_dvir, void* stream, fc_stats* stats) {
+    FC_TRY(check_shapes(b_ov, naux, nocc, nvir, eps_occ, eps_vir, precision, 0, 0.0, e_os, e_ss));
+    if (naux && nocc && nvir && (!gamma || !de_docc || !de_dvir))
+        return fail(FC_ERR_INVALID, "RI-MP2 gradient: null output pointer");
+    FC_TRY(require_init());
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (stats) *stats = fc_stats{};
+    cudaStream_t st = pick_stream(stream);
+    if (naux == 0 || nocc == 0 || nvir == 0) {
+        *e_os = 0.0;
+        *e_ss = 0.0;
+        if (gamma && naux * nocc * nvir) FC_CUDA(cudaMemsetAsync(gamma, 0, naux * nocc * nvir * 8, st));
+        if (de_docc && nocc) FC_CUDA(cudaMemsetAsync(de_docc, 0, nocc * 8, st));
+        if (de_dvir && nvir) FC_CUDA(cudaMemsetAsync(de_dvir, 0, nvir * 8, st));
+        FC_CUDA(cudaStreamSynchronize(st));
+        return FC_OK;
+    }
+    Rimp2Dev d{b_ov, eps_occ, eps_vir, naux, nocc, nvir, 0, 0.0, chunk_budget()};
+    return grad_dispatch(d, precision, st, e_os, e_ss, gamma, de_docc, de_dvir, stats);
+}
+
+fc_status fc_rimp2_energy_grad(const double* b_ov, int64_t naux, int64_t nocc, int64_t nvir,
+                               const double* eps_occ, const double* eps_vir, int32_t precision,
+                               double* e_os, double* e_ss, double* gamma, double* de_docc,
+                               double* de_dvir, fc_stats* stats) {
+    FC_TRY(check_shapes(b_ov, naux, nocc, nvir, eps_occ, eps_vir, precision, 0, 0.0, e_os, e_ss));
+    if (naux && nocc && nvir && (!gamma || !de_docc || !de_dvir))
+        return fail(FC_ERR_INVALID, "RI-MP2 gradient: null output pointer");
+    FC_TRY(require_init());
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (stats) *stats = fc_stats{};
+    const size_t nel = (size_t)naux * nocc * nvir;
+    if (nel == 0) {
+        *e_os = 0.0;
+        *e_ss = 0.0;
+        for (size_t k = 0; gamma && k < nel; ++k) gamma[k] = 0.0;
+        for (int64_t k = 0; de_docc && k < nocc; ++k) de_docc[k] = 0.0;
+        for (int64_t k = 0; de_dvir && k < nvir; ++k) de_dvir[k] = 0.0;
+        return FC_OK;
+    }
+    cudaStream_t st = ctx().stream;
+    void *db, *de, *dg, *dd;
+    FC_TRY(ws_get(WS_B, nel * 8, &db));
+    FC_TRY(ws_get(WS_EPS, (nocc + nvir) * 8, &de));
+    FC_TRY(ws_get(WS_GAMMA, nel * 8, &dg));
+    FC_TRY(ws_get(WS_MISC, (nocc + nvir) * 8, &dd));
+    FC_CUDA(cudaMemcpyAsync(db, b_ov, nel * 8, cudaMemcpyHostToDevice, st));
+    FC_CUDA(cudaMemcpyAsync(de, eps_occ, nocc * 8, cudaMemcpyHostToDevice, st));
+    FC_CUDA(cudaMemcpyAsync((double*)de + nocc, eps_vir, nvir * 8, cudaMemcpyHostToDevice, st));
+    Rimp2Dev d{(const double*)db, (const double*)de, (const double*)de + nocc, naux, nocc, nvir,
+               0, 0.0, chunk_budget()};
+    FC_TRY(grad_dispatch(d, precision, st, e_os, e_ss, (double*)dg, (double*)dd, (double*)dd + nocc, stats));
+    FC_CUDA(cudaMemcpyAsync(gamma, dg, nel * 8, cudaMemcpyDeviceToHost, st));
+    FC_CUDA(cudaMemcpyAsync(de_docc, dd, nocc * 8, cudaMemcpyDeviceToHost, st));
+    FC_CUDA(cudaMemcpyAsync(de_dvir, (double*)dd + nocc, nvir * 8, cudaMemcpyDeviceToHost, st));
+    FC_CUDA(cudaStreamSynchronize(st));
+    if (stats) {
+        stats->h2d_bytes += nel * 8 + (nocc + nvir) * 8;
+        stats->d2h_bytes += nel * 8 + (nocc + nvir) * 8;
+    }
+    return FC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,464 @@
+// DF-J and DF-K builders behind a device-resident handle.
+//
+// DF-J (ferric-scf/src/df_j.rs:1199-1245, 1459-1572) is two GEMV passes over
+// the packed lower triangle of B, HBM-bound:
+//   pass 1  d_P = sum_k Bp[P, k] w_k      (one CTA per aux row, fixed-order sum)
+//   solve   c = V^-1 d                     (FP64 Cholesky solves, when a metric is set)
+//   pass 2  J_k = sum_P Bp[P, k] c_P       (column-parallel over k, split over P,
+//                                           fixed-order fold of the splits)
+// DF-K occupied path (ferric-scf/src/df_k.rs:1409-1520, 1575-1660):
+//   stage 1 M_Q = B_Q C_occ on the DMMA tile GEMM, written as W[mu, (Q, i)]
+//   stage 2 K = W W^T, upper tiles only, split over (Q, i), fixed-order fold
+//           that also symmetrises (the final J/K symmetrisation in FP64).
+#include "fc_internal.cuh"
+#include "dgemm_tn.cuh"
+#include "dfjk.cuh"
+
+#include <vector>
+
+using namespace fc;
+
+namespace fc {
+
+// ------------------------------------------------------------- layout --
+
+__global__ void pack_lower_kernel(const double* __restrict__ sq, int64_t n, int64_t pair,
+                                  double* __restrict__ pk) {
+    const int64_t mu = blockIdx.x, q = blockIdx.y;
+    const double* src = sq + (q * n + mu) * n;
+    double* dst = pk + q * pair + mu * (mu + 1) / 2;
+    for (int64_t nu = threadIdx.x; nu <= mu; nu += blockDim.x) dst[nu] = src[nu];
+}
+
+// Packed density weights (ferric-scf/src/df_j.rs:1134-1150).
+__global__ void density_weights_kernel(const double* __restrict__ d, int64_t n,
+                                       double* __restrict__ w) {
+    const int64_t mu = blockIdx.x;
+    double* dst = w + mu * (mu + 1) / 2;
+    for (int64_t nu = threadIdx.x; nu <= mu; nu += blockDim.x)
+        dst[nu] = nu == mu ? d[mu * n + mu] : d[mu * n + nu] + d[nu * n + mu];
+}
+
+// ---------------------------------------------------------- DF-J passes --
+
+__global__ void __launch_bounds__(256) dfj_pass1_kernel(const double* __restrict__ bp, int64_t pair,
+                                                        const double* __restrict__ w,
+                                                        double* __restrict__ dp) {
+    __shared__ double red[32];
+    const double* row = bp + (int64_t)blockIdx.x * pair;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    int64_t k = threadIdx.x;
+    for (; k + 768 < pair; k += 1024) {
+        s0 += row[k] * w[k];
+        s1 += row[k + 256] * w[k + 256];
+        s2 += row[k + 512] * w[k + 512];
+        s3 += row[k + 768] * w[k + 768];
+    }
+    for (; k < pair; k += 256) s0 += row[k] * w[k];
+    const double v = block_sum((s0 + s1) + (s2 + s3), red);
+    if (threadIdx.x == 0) dp[blockIdx.x] = v;
+}
+
+__global__ void __launch_bounds__(256) dfj_pass2_kernel(const double* __restrict__ bp, int64_t naux,
+                                                        int64_t pair, const double* __restrict__ c,
+                                                        int64_t rows_per_split,
+                                                        double* __restrict__ part) {
+    const int64_t k = (int64_t)blockIdx.x * 256 + threadIdx.x;
+    const int64_t p0 = (int64_t)blockIdx.y * rows_per_split;
+    const int64_t p1 = p0 + rows_per_split < naux ? p0 + rows_per_split : naux;
+    if (k >= pair) return;
+    double s0 = 0.0, s1 = 0.0;
+    int64_t p = p0;
+    for (; p + 1 < p1; p += 2) {
+        s0 += bp[p * pair + k] * c[p];
+        s1 += bp[(p + 1) * pair + k] * c[p + 1];
+    }
+    if (p < p1) s0 += bp[p * pair + k] * c[p];
+    part[(int64_t)blockIdx.y * pair + k] = s0 + s1;
+}
+
+__global__ void dfj_unpack_kernel(const double* __restrict__ part, int nsplit, int64_t pair, int64_t n,
+                                  double* __restrict__ j) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n * n) return;
+    const int64_t r = idx / n, c = idx % n;
+    const int64_t hi = r > c ? r : c, lo = r > c ? c : r;
+    const int64_t k = hi * (hi + 1) / 2 + lo;
+    double s = 0.0;
+    for (int sp = 0; sp < nsplit; ++sp) s += part[(int64_t)sp * pair + k];
+    j[idx] = s;
+}
+
+// c = V^-1 d with V = L L^T, L lower row-major (naux x naux); in place on x.
+// One CTA of 32 warps, blocked by 32 rows: left-looking forward solve, then
+// the backward solve with L^T.  Fixed reduction order throughout.
+__global__ void __launch_bounds__(1024) chol_solve_kernel(const double* __restrict__ L, int64_t naux,
+                                                          double* __restrict__ x) {
+    __shared__ double sh[32][33];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // forward: L y = d
+    for (int64_t kb = 0; kb < naux; kb += 32) {
+        const int nb = (int)(naux - kb < 32 ? naux - kb : 32);
+        if (warp < nb) {
+            const int64_t r = kb + warp;
+            double s = 0.0;
+            for (int64_t k = lane; k < kb; k += 32) s += L[r * naux + k] * x[k];
+            s = warp_sum(s);
+            if (lane == 0) x[r] -= s;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            double yl = lane < nb ? x[kb + lane] : 0.0;
+            for (int rr = 0; rr < nb; ++rr) {
+                const double v = lane < rr ? L[(kb + rr) * naux + kb + lane] * yl : 0.0;
+                const double s = warp_sum(v);
+                if (lane == rr) yl = (yl - s) / L[(kb + rr) * naux + kb + rr];
+            }
+            if (lane < nb) x[kb + lane] = yl;
+        }
+        __syncthreads();
+    }
+    // backward: L^T c = y
+    const int64_t nblk = (naux + 31) / 32;
+    for (int64_t bi = nblk - 1; bi >= 0; --bi) {
+        const int64_t kb = bi * 32;
+        const int nb = (int)(naux - kb < 32 ? naux - kb : 32);
+        double part = 0.0;
+        if (lane < nb)
+            for (int64_t k = kb + nb + warp; k < naux; k += 32) part += L[k * naux + kb + lane] * x[k];
+        sh[warp][lane] = part;
+        __syncthreads();
+        if (warp == 0) {
+            double s = 0.0;
+            for (int w = 0; w < 32; ++w) s += sh[w][lane];
+            double yl = lane < nb ? x[kb + lane] - s : 0.0;
+            for (int rr = nb - 1; rr >= 0; --rr) {
+                const double v = (lane > rr && lane < nb) ? L[(kb + lane) * naux + kb + rr] * yl : 0.0;
+                const double s2 = warp_sum(v);
+                if (lane == rr) yl = (yl - s2) / L[(kb + rr) * naux + kb + rr];
+            }
+            if (lane < nb) x[kb + lane] = yl;
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------- DF-K --
+
+__global__ void transpose_kernel(const double* __restrict__ a, int64_t rows, int64_t cols,
+                                 double* __restrict__ at) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= rows * cols) return;
+    const int64_t r = idx / cols, c = idx % cols;
+    at[c * rows + r] = a[idx];
+}
+
+// Stage-1 epilogue: row (Q, mu) of M = B C goes to W[mu, Q*nocc + i].
+struct EpiScatterW {
+    double* W;
+    int64_t n, naux, nocc;
+    __device__ __forceinline__ void operator()(int m, int i, double v, int) const {
+        const int64_t q = m / n, mu = m % n;
+        W[mu * (naux * nocc) + q * nocc + i] = v;
+    }
+};
+
+__global__ void dfk_fold_kernel(const double* __restrict__ part, int nsplit, int64_t n,
+                                double* __restrict__ k) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n * n) return;
+    const int64_t r = idx / n, c = idx % n;
+    const int64_t lo = r < c ? r : c, hi = r < c ? c : r;
+    double s = 0.0;
+    for (int sp = 0; sp < nsplit; ++sp) s += part[(int64_t)sp * n * n + lo * n + hi];
+    k[idx] = s;
+}
+
+static fc_status dfjk_smem_once() {
+    static bool done = false;
+    if (done) return FC_OK;
+    FC_CUDA(cudaFuncSetAttribute(dgemm_tn_kernel<EpiScatterW>, cudaFuncAttributeMaxDynamicSharedMemorySize, DG_SMEM));
+    FC_CUDA(cudaFuncSetAttribute(dgemm_tn_kernel<EpiSplit>, cudaFuncAttributeMaxDynamicSharedMemorySize, DG_SMEM));
+    done = true;
+    return FC_OK;
+}
+
+fc_status dfj_build_f64(fc_dfjk* h, const double* d, double* j, cudaStream_t st, fc_stats* stats) {
+    const int64_t naux = h->naux, n = h->n, pair = h->pair;
+    void *vw, *vdp, *vpart;
+    const int nsplit = 4;
+    FC_TRY(ws_get(WS_MISC, (pair + naux + 64) * 8, &vw));
+    FC_TRY(ws_get(WS_PART, (int64_t)nsplit * pair * 8, &vpart));
+    double* w = (double*)vw;
+    vdp = w + pair;
+    Context& c = ctx();
+    if (stats) FC_CUDA(cudaEventRecord(c.ev0, st));
+    density_weights_kernel<<<(unsigned)n, 128, 0, st>>>(d, n, w);
+    dfj_pass1_kernel<<<(unsigned)naux, 256, 0, st>>>(h->b_pk, pair, w, (double*)vdp);
+    if (h->l_chol) chol_solve_kernel<<<1, 1024, 0, st>>>(h->l_chol, naux, (double*)vdp);
+    const int64_t rps = (naux + nsplit - 1) / nsplit;
+    dim3 g2((unsigned)((pair + 255) / 256), nsplit);
+    dfj_pass2_kernel<<<g2, 256, 0, st>>>(h->b_pk, naux, pair, (const double*)vdp, rps, (double*)vpart);
+    dfj_unpack_kernel<<<(unsigned)((n * n + 255) / 256), 256, 0, st>>>((const double*)vpart, nsplit, pair, n, j);
+    FC_TRY(check_launch("DF-J kernels"));
+    if (stats) {
+        FC_CUDA(cudaEventRecord(c.ev1, st));
+        FC_CUDA(cudaEventSynchronize(c.ev1));
+        float ms = 0.f;
+        FC_CUDA(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
+        stats->kernel_ms = ms;
+        stats->flops = 4.0 * (double)naux * (double)pair;
+        stats->precision = FC_PREC_F64;
+        stats->launches += 4 + (h->l_chol ? 1 : 0);
+    }
+    return FC_OK;
+}
+
+fc_status dfk_build_f64(fc_dfjk* h, const double* c_occ, int64_t nocc, double* k, cudaStream_t st,
+                        fc_stats* stats) {
+    FC_TRY(dfjk_smem_once());
+    const int64_t naux = h->naux, n = h->n;
+    const int64_t M1 = naux * n;
+    if (M1 > INT32_MAX || (M1 + DG_BM - 1) / DG_BM > 65535)
+        return fail(FC_ERR_LAYOUT, "DF-K: naux*n too large for one stage-1 launch");
+    const int64_t kdim = naux * nocc;
+    const int tm = (int)((n + DG_BM - 1) / DG_BM), tn = (int)((n + DG_BN - 1) / DG_BN);
+    int upper = 0;
+    for (int a = 0; a < tm; ++a)
+        for (int b = 0; b < tn; ++b) upper += (a * DG_BM <= b * DG_BN + DG_BN - 1);
+    int nsplit = (1200 + upper - 1) / upper;
+    if (nsplit < 1) nsplit = 1;
+    if (nsplit > 64) nsplit = 64;
+    int64_t kps = (kdim + nsplit - 1) / nsplit;
+    kps = (kps + DG_BK - 1) / DG_BK * DG_BK;
+    nsplit = (int)((kdim + kps - 1) / kps);
+
+    void *vct, *vw, *vpart;
+    FC_TRY(ws_get(WS_MISC, nocc * n * 8, &vct));
+    FC_TRY(ws_get(WS_T, n * kdim * 8, &vw));
+    FC_TRY(ws_get(WS_PART, (int64_t)nsplit * n * n * 8, &vpart));
+    Context& c = ctx();
+    if (stats) FC_CUDA(cudaEventRecord(c.ev0, st));
+    transpose_kernel<<<(unsigned)((n * nocc + 255) / 256), 256, 0, st>>>(c_occ, n, nocc, (double*)vct);
+    {
+        dim3 g((unsigned)((nocc + DG_BN - 1) / DG_BN), (unsigned)((M1 + DG_BM - 1) / DG_BM), 1);
+        EpiScatterW epi{(double*)vw, n, naux, nocc};
+        dgemm_tn_kernel<EpiScatterW><<<g, 256, DG_SMEM, st>>>(h->b_sq, n, (const double*)vct, n, (int)M1,
+                                                               (int)nocc, n, n, 0, epi);
+    }
+    {
+        dim3 g(tn, tm, nsplit);
+        EpiSplit epi{(double*)vpart, n * n, (int)n};
+        dgemm_tn_kernel<EpiSplit><<<g, 256, DG_SMEM, st>>>((const double*)vw, kdim, (const double*)vw, kdim,
+                                                            (int)n, (int)n, kdim, kps, 1, epi);
+    }
+    dfk_fold_kernel<<<(unsigned)((n * n + 255) / 256), 256, 0, st>>>((const double*)vpart, nsplit, n, k);
+    FC_TRY(check_launch("DF-K kernels"));
+    if (stats) {
+        FC_CUDA(cudaEventRecord(c.ev1, st));
+        FC_CUDA(cudaEventSynchronize(c.ev1));
+        float ms = 0.f;
+        FC_CUDA(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
+        stats->kernel_ms = ms;
+        stats->flops = 4.0 * (double)naux * (double)n * (double)n * (double)nocc;
+        stats->precision = FC_PREC_F64;
+        stats->launches += 4;
+        stats->tile_m = DG_BM;
+        stats->tile_n = DG_BN;
+    }
+    return FC_OK;
+}
+
+}  // namespace fc
+
+// ------------------------------------------------------------------ ABI --
+
+namespace {
+
+fc_status create_common(const double* b, int64_t naux, int64_t n, int32_t layout, int32_t precision,
+                        bool host, cudaStream_t st, fc_dfjk** out) {
+    if (!out) return fail(FC_ERR_INVALID, "fc_dfjk_create: null out");
+    *out = nullptr;
+    if (naux <= 0 || n <= 0) return fail(FC_ERR_LAYOUT, "fc_dfjk_create: naux and n must be > 0");
+    if (!b) return fail(FC_ERR_INVALID, "fc_dfjk_create: null tensor");
+    if (layout != FC_LAYOUT_SQUARE && layout != FC_LAYOUT_PACKED_LOWER)
+        return fail(FC_ERR_INVALID, "fc_dfjk_create: unknown layout");
+    if (precision < FC_PREC_F64 || precision > FC_PREC_MIXED_X6)
+        return fail(FC_ERR_INVALID, "fc_dfjk_create: unknown precision");
+    int64_t nn, pair = n * (n + 1) / 2, bytes_sq = 0, bytes_pk;
+    if (!mul_ok(n, n, &nn) || !mul_ok(nn, naux, &bytes_sq) || !mul_ok(bytes_sq, 8, &bytes_sq))
+        return fail(FC_ERR_LAYOUT, "fc_dfjk_create: size overflow");
+    if (!mul_ok(pair, naux, &bytes_pk) || !mul_ok(bytes_pk, 8, &bytes_pk))
+        return fail(FC_ERR_LAYOUT, "fc_dfjk_create: size overflow");
+    if (layout == FC_LAYOUT_PACKED_LOWER) bytes_sq = 0;
+    FC_TRY(require_init());
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    const uint64_t need = (uint64_t)bytes_sq + (uint64_t)bytes_pk;
+    FC_TRY(pool_reserve(need));
+    fc_dfjk* h = new fc_dfjk{};
+    h->naux = naux;
+    h->n = n;
+    h->pair = pair;
+    h->layout = layout;
+    h->precision = precision;
+    h->bytes = need;
+    auto bail = [&](fc_status s) {
+        if (h->b_sq) cudaFree(h->b_sq);
+        if (h->b_pk) cudaFree(h->b_pk);
+        delete h;
+        return s;
+    };
+    cudaError_t e;
+    if (bytes_sq) {
+        e = cudaMalloc(&h->b_sq, bytes_sq);
+        if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(B square)"));
+    }
+    e = cudaMalloc(&h->b_pk, bytes_pk);
+    if (e != cudaSuccess) return bail(cuda_fail(e, "cudaMalloc(B packed)"));
+    const cudaMemcpyKind kind = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    if (layout == FC_LAYOUT_SQUARE) {
+        e = cudaMemcpyAsync(h->b_sq, b, bytes_sq, kind, st);
+        if (e != cudaSuccess) return bail(cuda_fail(e, "upload B"));
+        dim3 g((unsigned)n, (unsigned)naux);
+        pack_lower_kernel<<<g, 128, 0, st>>>(h->b_sq, n, pair, h->b_pk);
+        fc_status s = check_launch("pack_lower_kernel");
+        if (s != FC_OK) return bail(s);
+    } else {
+        e = cudaMemcpyAsync(h->b_pk, b, bytes_pk, kind, st);
+        if (e != cudaSuccess) return bail(cuda_fail(e, "upload B"));
+    }
+    if (precision != FC_PREC_F64) {
+        fc_status s = dfjk_prepare_mixed(h, st);
+        if (s != FC_OK) return bail(s);
+    }
+    e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return bail(cuda_fail(e, "fc_dfjk_create sync"));
+    ctx().handle_bytes += h->bytes;
+    *out = h;
+    return FC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+fc_status fc_dfjk_create(const double* b, int64_t naux, int64_t n, int32_t layout, int32_t precision,
+                         fc_dfjk** out) {
+    return create_common(b, naux, n, layout, precision, true, ctx().stream, out);
+}
+
+fc_status fc_dfjk_create_dev(const double* b, int64_t naux, int64_t n, int32_t layout, int32_t precision,
+                             void* stream, fc_dfjk** out) {
+    return create_common(b, naux, n, layout, precision, false, pick_stream(stream), out);
+}
+
+fc_status fc_dfj_set_metric_chol(fc_dfjk* h, const double* l) {
+    if (!h || !l) return fail(FC_ERR_INVALID, "fc_dfj_set_metric_chol: null argument");
+    FC_TRY(require_init());
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    const uint64_t bytes = (uint64_t)h->naux * h->naux * 8;
+    if (!h->l_chol) {
+        FC_TRY(pool_reserve(bytes));
+        FC_CUDA(cudaMalloc(&h->l_chol, bytes));
+        h->bytes += bytes;
+        ctx().handle_bytes += bytes;
+    }
+    FC_CUDA(cudaMemcpy(h->l_chol, l, bytes, cudaMemcpyHostToDevice));
+    return FC_OK;
+}
+
+fc_status fc_dfj_build_dev(fc_dfjk* h, const double* d, double* j, void* stream, fc_stats* stats) {
+    if (!h || !d || !j) return fail(FC_ERR_INVALID, "fc_dfj_build: null argument");
+    FC_TRY(require_init());
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (stats) *stats = fc_stats{};
+    cudaStream_t st = pick_stream(stream);
+    if (h->precision == FC_PREC_F64) return dfj_build_f64(h, d, j, st, stats);
+    return dfj_build_mixed(h, d, j, st, stats);
+}
+
+fc_status fc_dfj_build(fc_dfjk* h, const double* d, double* j, fc_stats* stats) {
+    if (!h || !d || !j) return fail(FC_ERR_INVALID, "fc_dfj_build: null argument");
+    FC_TRY(require_init());
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (stats) *stats = fc_stats{};
+    cudaStream_t st = ctx().stream;
+    const size_t nn = (size_t)h->n * h->n * 8;
+    void* buf;
+    FC_TRY(ws_get(WS_B, 2 * nn, &buf));
+    double* dd = (double*)buf;
+    double* dj = dd + h->n * h->n;
+    FC_CUDA(cudaMemcpyAsync(dd, d, nn, cudaMemcpyHostToDevice, st));
+    if (h->precision == FC_PREC_F64) FC_TRY(dfj_build_f64(h, dd, dj, st, stats));
+    else FC_TRY(dfj_build_mixed(h, dd, dj, st, stats));
+    FC_CUDA(cudaMemcpyAsync(j, dj, nn, cudaMemcpyDeviceToHost, st));
+    FC_CUDA(cudaStreamSynchronize(st));
+    if (stats) {
+        stats->h2d_bytes += nn;
+        stats->d2h_bytes += nn;
+    }
+    return FC_OK;
+}
+
+fc_status fc_dfk_build_occ_dev(fc_dfjk* h, const double* c_occ, int64_t nocc, double* k, void* stream,
+                               fc_stats* stats) {
+    if (!h || !k || (nocc > 0 && !c_occ)) return fail(FC_ERR_INVALID, "fc_dfk_build_occ: null argument");
+    if (nocc < 0) return fail(FC_ERR_LAYOUT, "fc_dfk_build_occ: nocc < 0");
+    if (!h->b_sq) return fail(FC_ERR_LAYOUT, "fc_dfk_build_occ: needs an FC_LAYOUT_SQUARE handle");
+    FC_TRY(require_init());
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (stats) *stats = fc_stats{};
+    cudaStream_t st = pick_stream(stream);
+    if (nocc == 0) {  // empty channel: K is identically zero (df_k.rs:1428-1436)
+        FC_CUDA(cudaMemsetAsync(k, 0, h->n * h->n * 8, st));
+        return FC_OK;
+    }
+    if (h->precision == FC_PREC_F64) return dfk_build_f64(h, c_occ, nocc, k, st, stats);
+    return dfk_build_mixed(h, c_occ, nocc, k, st, stats);
+}
+
+fc_status fc_dfk_build_occ(fc_dfjk* h, const double* c_occ, int64_t nocc, double* k, fc_stats* stats) {
+    if (!h || !k || (nocc > 0 && !c_occ)) return fail(FC_ERR_INVALID, "fc_dfk_build_occ: null argument");
+    if (nocc < 0) return fail(FC_ERR_LAYOUT, "fc_dfk_build_occ: nocc < 0");
+    if (!h->b_sq) return fail(FC_ERR_LAYOUT, "fc_dfk_build_occ: needs an FC_LAYOUT_SQUARE handle");
+    FC_TRY(require_init());
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (stats) *stats = fc_stats{};
+    cudaStream_t st = ctx().stream;
+    const size_t nn = (size_t)h->n * h->n * 8, nc = (size_t)h->n * nocc * 8;
+    if (nocc == 0) {
+        for (size_t q = 0; q < (size_t)h->n * h->n; ++q) k[q] = 0.0;
+        return FC_OK;
+    }
+    void* buf;
+    FC_TRY(ws_get(WS_B, nn + nc, &buf));
+    double* dk = (double*)buf;
+    double* dc = dk + h->n * h->n;
+    FC_CUDA(cudaMemcpyAsync(dc, c_occ, nc, cudaMemcpyHostToDevice, st));
+    if (h->precision == FC_PREC_F64) FC_TRY(dfk_build_f64(h, dc, nocc, dk, st, stats));
+    else FC_TRY(dfk_build_mixed(h, dc, nocc, dk, st, stats));
+    FC_CUDA(cudaMemcpyAsync(k, dk, nn, cudaMemcpyDeviceToHost, st));
+    FC_CUDA(cudaStreamSynchronize(st));
+    if (stats) {
+        stats->h2d_bytes += nc;
+        stats->d2h_bytes += nn;
+    }
+    return FC_OK;
+}
+
+fc_status fc_dfjk_destroy(fc_dfjk* h) {
+    if (!h) return FC_OK;
+    Context& c = ctx();
+    std::lock_guard<std::mutex> lk(c.mu);
+    if (c.device >= 0) cudaSetDevice(c.device);
+    cudaDeviceSynchronize();
+    if (h->b_sq) cudaFree(h->b_sq);
+    if (h->b_pk) cudaFree(h->b_pk);
+    if (h->l_chol) cudaFree(h->l_chol);
+    dfjk_free_mixed(h);
+    c.handle_bytes -= h->bytes < c.handle_bytes ? h->bytes : c.handle_bytes;
+    delete h;
+    return FC_OK;
+}
+
+}  // extern "C"

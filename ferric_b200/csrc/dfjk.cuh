@@ -1,0 +1,26 @@
+// Internal state of a DF-JK handle.
+#pragma once
+#include "fc_internal.cuh"
+
+struct fc_dfjk {
+    int64_t naux = 0, n = 0, pair = 0;
+    int layout = 0, precision = 0;
+    double* b_sq = nullptr;    // (naux, n, n) dressed tensor (square handles)
+    double* b_pk = nullptr;    // (naux, n(n+1)/2) packed lower rows
+    double* l_chol = nullptr;  // metric Cholesky factor (raw-Bp form)
+    // split-BF16 copies (mixed handles)
+    void* pk_split = nullptr;  // packed rows as (hi, lo) bf16 pairs
+    void* sq_split = nullptr;  // square tensor split for the tensor-core stages
+    uint64_t bytes = 0;        // device bytes owned by the handle
+};
+
+namespace fc {
+fc_status dfj_build_f64(fc_dfjk* h, const double* d, double* j, cudaStream_t st, fc_stats* stats);
+fc_status dfk_build_f64(fc_dfjk* h, const double* c_occ, int64_t nocc, double* k, cudaStream_t st,
+                        fc_stats* stats);
+fc_status dfjk_prepare_mixed(fc_dfjk* h, cudaStream_t st);
+void dfjk_free_mixed(fc_dfjk* h);
+fc_status dfj_build_mixed(fc_dfjk* h, const double* d, double* j, cudaStream_t st, fc_stats* stats);
+fc_status dfk_build_mixed(fc_dfjk* h, const double* c_occ, int64_t nocc, double* k, cudaStream_t st,
+                          fc_stats* stats);
+}  // namespace fc

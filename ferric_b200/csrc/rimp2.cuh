@@ -1,0 +1,30 @@
+// Internal interface of the RI-MP2 kernel sets (device pointers only).
+#pragma once
+#include "fc_internal.cuh"
+
+namespace fc {
+
+struct Rimp2Dev {
+    const double* b_ov;     // (naux, nocc*nvir) on the device
+    const double* eps_occ;  // [nocc] on the device
+    const double* eps_vir;  // [nvir] on the device
+    int64_t naux, nocc, nvir;
+    int has_kappa;
+    double kappa;
+    int64_t chunk_bytes;    // amplitude-chunk budget of the gradient
+};
+
+fc_status rimp2_energy_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, double* e_ss,
+                           fc_stats* stats);
+fc_status rimp2_grad_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, double* e_ss,
+                         double* gamma, double* de_docc, double* de_dvir, fc_stats* stats);
+
+// Split-BF16 (tcgen05) kernel set; `terms` = 2 (hi+lo, 3 products) or
+// 3 (hi+mid+lo, 6 products).
+fc_status rimp2_energy_mixed(const Rimp2Dev& d, int terms, cudaStream_t st, double* e_os,
+                             double* e_ss, fc_stats* stats);
+fc_status rimp2_grad_mixed(const Rimp2Dev& d, int terms, cudaStream_t st, double* e_os,
+                           double* e_ss, double* gamma, double* de_docc, double* de_dvir,
+                           fc_stats* stats);
+
+}  // namespace fc

@@ -1,0 +1,426 @@
+// All-FP64 RI-MP2 kernels (the drop-in "plain" set).
+//
+// Work item = (occupied pair, a-tile, b-tile) of 64 x 64 virtual indices.
+// For the pair (i, j) the item forms two tiles of the pair block on the DMMA
+// tensor path, both in (a, b) orientation:
+//     X[a, b] = (ia|jb) = sum_Q B[Q, i a] B[Q, j b]
+//     Y[a, b] = (ib|ja) = sum_Q B[Q, j a] B[Q, i b]
+// so the exchange partner of every element sits in the same thread and no
+// transpose is needed.  The orbital-energy denominator and the energy sums
+// are applied in the epilogue: (ia|jb) never reaches HBM.
+//
+// Energy mode (unordered pairs i <= j, weight 1/2 on i == j):
+//     E_OS += (X^2 + Y^2) / D,   E_SS += (X - Y)^2 / D
+// which is the reference's pair loop over the (i, j) and (j, i) orderings
+// (ferric-mp2/src/rimp2.rs:1399-1441, 1506-1544).
+//
+// Gradient mode (ordered pairs, i in the current chunk): the item writes
+// Tt_ij[a, b] = (2X - Y)/D into the chunk's amplitude rows and the partials
+// of c = t Tt for dE/d eps (ferric-mp2/src/oo_rimp2.rs:1170-1191); the second
+// contraction Gamma_i = 4 B Tt_i^T runs in dgemm_tn.
+#include "fc_internal.cuh"
+#include "dmma.cuh"
+#include "dgemm_tn.cuh"
+#include "rimp2.cuh"
+
+namespace fc {
+
+constexpr int PR_T = 64, PR_BK = 16, PR_LD = 68, PR_STAGES = 3;
+constexpr int PR_SMEM = PR_STAGES * 4 * PR_BK * PR_LD * 8;  // 104,448 B
+
+struct PairArgs {
+    const double* B;
+    int64_t ldb;
+    int naux, nvir;
+    const double* eo;
+    const double* ev;
+    const int2* pairs;
+    int ntile;
+    int has_kappa;
+    double kappa;
+    double* part;  // [item][2] energy partials
+    // gradient mode
+    double* T;
+    int64_t ldt;
+    int i0;
+    double* occ_part;  // [item]
+    double* vir_part;  // [item][64]
+};
+
+template <int GRAD>
+__global__ void __launch_bounds__(256, 2) pair_f64_kernel(PairArgs p) {
+    extern __shared__ __align__(16) double sm[];
+    __shared__ double red[32];
+    __shared__ double vsum[2][PR_T];
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int wr = warp & 3, wc = warp >> 2;
+    const int64_t item = blockIdx.x;
+    const int tb = (int)(item % p.ntile);
+    const int ta = (int)((item / p.ntile) % p.ntile);
+    const int64_t pidx = item / ((int64_t)p.ntile * p.ntile);
+    const int2 ij = p.pairs[pidx];
+    const int i = ij.x, j = ij.y;
+    const int A0 = ta * PR_T, B0 = tb * PR_T;
+    const int nvir = p.nvir, naux = p.naux;
+    const int64_t ldb = p.ldb;
+    const double* gAi = p.B + (int64_t)i * nvir + A0;
+    const double* gAj = p.B + (int64_t)j * nvir + A0;
+    const double* gBj = p.B + (int64_t)j * nvir + B0;
+    const double* gBi = p.B + (int64_t)i * nvir + B0;
+    const int nk = (naux + PR_BK - 1) / PR_BK;
+
+    auto load = [&](int stage, int kt) {
+        double* s = sm + stage * 4 * PR_BK * PR_LD;
+#pragma unroll
+        for (int e = 0; e < (PR_BK * PR_T) / 256; ++e) {
+            const int idx = tid + 256 * e, r = idx >> 6, c = idx & 63;
+            const int q = kt * PR_BK + r;
+            const bool okA = q < naux && A0 + c < nvir;
+            const bool okB = q < naux && B0 + c < nvir;
+            const int64_t off = (int64_t)q * ldb + c;
+            const int so = r * PR_LD + c;
+            cp_async8(s + 0 * PR_BK * PR_LD + so, okA ? gAi + off : p.B, okA);
+            cp_async8(s + 1 * PR_BK * PR_LD + so, okA ? gAj + off : p.B, okA);
+            cp_async8(s + 2 * PR_BK * PR_LD + so, okB ? gBj + off : p.B, okB);
+            cp_async8(s + 3 * PR_BK * PR_LD + so, okB ? gBi + off : p.B, okB);
+        }
+    };
+
+    double X[2][4][2], Y[2][4][2];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) X[a][b][0] = X[a][b][1] = Y[a][b][0] = Y[a][b][1] = 0.0;
+
+#pragma unroll
+    for (int s = 0; s < PR_STAGES - 1; ++s) {
+        if (s < nk) load(s, s);
+        cp_async_commit();
+    }
+    for (int kt = 0; kt < nk; ++kt) {
+        cp_async_wait<PR_STAGES - 2>();
+        __syncthreads();
+        const int pf = kt + PR_STAGES - 1;
+        if (pf < nk) load(pf % PR_STAGES, pf);
+        cp_async_commit();
+        const double* s = sm + (kt % PR_STAGES) * 4 * PR_BK * PR_LD;
+        const double* sAi = s;
+        const double* sAj = s + PR_BK * PR_LD;
+        const double* sBj = s + 2 * PR_BK * PR_LD;
+        const double* sBi = s + 3 * PR_BK * PR_LD;
+#pragma unroll
+        for (int ks = 0; ks < PR_BK / 4; ++ks) {
+            const int kr = (ks * 4 + t) * PR_LD;
+            double ax[2], ay[2], bx[4], by[4];
+#pragma unroll
+            for (int mt = 0; mt < 2; ++mt) {
+                ax[mt] = sAi[kr + wr * 16 + mt * 8 + g];
+                ay[mt] = sAj[kr + wr * 16 + mt * 8 + g];
+            }
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt) {
+                bx[nt] = sBj[kr + wc * 32 + nt * 8 + g];
+                by[nt] = sBi[kr + wc * 32 + nt * 8 + g];
+            }
+#pragma unroll
+            for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+                for (int nt = 0; nt < 4; ++nt) {
+                    dmma_8x8x4(X[mt][nt], ax[mt], bx[nt]);
+                    dmma_8x8x4(Y[mt][nt], ay[mt], by[nt]);
+                }
+        }
+    }
+    cp_async_wait<0>();
+
+    const double eij = p.eo[i] + p.eo[j];
+    KSum os, ss, oc;
+    double rowsum[2] = {0.0, 0.0};
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt) {
+        const int a = A0 + wr * 16 + mt * 8 + g;
+        const double ea = a < nvir ? p.ev[a] : 0.0;
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int b = B0 + wc * 32 + nt * 8 + 2 * t + h;
+                if (a < nvir && b < nvir) {
+                    const double D = eij - ea - p.ev[b];
+                    const double x = X[mt][nt][h], y = Y[mt][nt][h];
+                    double f = 1.0 / D;
+                    if (GRAD) {
+                        const double tt = (2.0 * x - y) * f;
+                        p.T[((int64_t)(i - p.i0) * nvir + a) * p.ldt + (int64_t)j * nvir + b] = tt;
+                        const double c = x * f * tt;
+                        os.add(x * x * f);
+                        ss.add(x * (x - y) * f);
+                        oc.add(c);
+                        rowsum[mt] += c;
+                    } else {
+                        if (p.has_kappa) {
+                            const double d1 = 1.0 - exp(p.kappa * D);
+                            f *= d1 * d1;
+                        }
+                        os.add((x * x + y * y) * f);
+                        ss.add((x - y) * (x - y) * f);
+                    }
+                }
+            }
+    }
+    const double w = (!GRAD && i == j) ? 0.5 : 1.0;
+    const double vos = block_sum(os.value(), red);
+    const double vss = block_sum(ss.value(), red);
+    if (tid == 0) {
+        p.part[item * 2 + 0] = w * vos;
+        p.part[item * 2 + 1] = w * vss;
+    }
+    if (GRAD) {
+        const double voc = block_sum(oc.value(), red);
+        if (tid == 0) p.occ_part[item] = voc;
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt) {
+            double r = rowsum[mt];
+            r += __shfl_xor_sync(0xffffffffu, r, 1);
+            r += __shfl_xor_sync(0xffffffffu, r, 2);
+            if (t == 0) vsum[wc][wr * 16 + mt * 8 + g] = r;
+        }
+        __syncthreads();
+        if (tid < PR_T) p.vir_part[item * PR_T + tid] = vsum[0][tid] + vsum[1][tid];
+    }
+}
+
+// Fixed-order compensated sum of n (os, ss) partials -> out[0..1].
+__global__ void __launch_bounds__(1024) reduce_pairs_kernel(const double* __restrict__ part,
+                                                            int64_t n, double* out) {
+    __shared__ double so[1024], sss[1024];
+    KSum a, b;
+    for (int64_t k = threadIdx.x; k < n; k += 1024) {
+        a.add(part[2 * k]);
+        b.add(part[2 * k + 1]);
+    }
+    so[threadIdx.x] = a.value();
+    sss[threadIdx.x] = b.value();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        KSum x, y;
+        for (int k = 0; k < 1024; ++k) {
+            x.add(so[k]);
+            y.add(sss[k]);
+        }
+        out[0] = x.value();
+        out[1] = y.value();
+    }
+}
+
+// de_docc[i0 + il] = -2 * sum of the occ partials of occupied il of the chunk.
+__global__ void __launch_bounds__(256) reduce_occ_kernel(const double* __restrict__ occ_part,
+                                                         int64_t items_per_i, int i0,
+                                                         double* de_docc) {
+    __shared__ double sh[256];
+    const int il = blockIdx.x;
+    const double* src = occ_part + (int64_t)il * items_per_i;
+    KSum a;
+    for (int64_t k = threadIdx.x; k < items_per_i; k += 256) a.add(src[k]);
+    sh[threadIdx.x] = a.value();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        KSum x;
+        for (int k = 0; k < 256; ++k) x.add(sh[k]);
+        de_docc[i0 + il] = -2.0 * x.value();
+    }
+}
+
+// acc_vir[a] += 2 * sum over the chunk's items with a in their a-tile.
+__global__ void __launch_bounds__(256) reduce_vir_kernel(const double* __restrict__ vir_part,
+                                                         int64_t npairs, int ntile, int nvir,
+                                                         double* acc_vir) {
+    const int a = blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (a >= nvir) return;
+    const int ta = a / PR_T, ar = a % PR_T;
+    const int64_t nterm = npairs * ntile;
+    KSum s;
+    for (int64_t k = lane; k < nterm; k += 32) {
+        const int64_t pidx = k / ntile, tb = k % ntile;
+        const int64_t item = (pidx * ntile + ta) * ntile + tb;
+        s.add(vir_part[item * PR_T + ar]);
+    }
+    double v = warp_sum(s.value());
+    if (lane == 0) acc_vir[a] += 2.0 * v;
+}
+
+static fc_status set_smem_once() {
+    static bool done = false;
+    if (done) return FC_OK;
+    FC_CUDA(cudaFuncSetAttribute(pair_f64_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, PR_SMEM));
+    FC_CUDA(cudaFuncSetAttribute(pair_f64_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, PR_SMEM));
+    FC_CUDA(cudaFuncSetAttribute(dgemm_tn_kernel<EpiStore>, cudaFuncAttributeMaxDynamicSharedMemorySize, DG_SMEM));
+    done = true;
+    return FC_OK;
+}
+
+fc_status rimp2_energy_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, double* e_ss,
+                           fc_stats* stats) {
+    FC_TRY(set_smem_once());
+    const int64_t nocc = d.nocc, nvir = d.nvir;
+    const int ntile = (int)((nvir + PR_T - 1) / PR_T);
+    const int64_t npairs = nocc * (nocc + 1) / 2;
+    const int64_t items = npairs * ntile * ntile;
+    if (items > INT32_MAX) return fail(FC_ERR_LAYOUT, "RI-MP2: too many pair tiles for one launch");
+
+    void *vpairs, *vpart, *vout;
+    FC_TRY(ws_get(WS_PAIRS, npairs * sizeof(int2), &vpairs));
+    FC_TRY(ws_get(WS_PART, items * 2 * sizeof(double), &vpart));
+    FC_TRY(ws_get(WS_OUT, 64 * sizeof(double), &vout));
+    std::vector<int2> hp((size_t)npairs);
+    {
+        size_t k = 0;
+        for (int i = 0; i < nocc; ++i)
+            for (int j = i; j < nocc; ++j) hp[k++] = make_int2(i, j);
+    }
+    FC_CUDA(cudaMemcpyAsync(vpairs, hp.data(), npairs * sizeof(int2), cudaMemcpyHostToDevice, st));
+
+    PairArgs a{};
+    a.B = d.b_ov;
+    a.ldb = nocc * nvir;
+    a.naux = (int)d.naux;
+    a.nvir = (int)nvir;
+    a.eo = d.eps_occ;
+    a.ev = d.eps_vir;
+    a.pairs = (const int2*)vpairs;
+    a.ntile = ntile;
+    a.has_kappa = d.has_kappa;
+    a.kappa = d.kappa;
+    a.part = (double*)vpart;
+
+    Context& c = ctx();
+    if (stats) FC_CUDA(cudaEventRecord(c.ev0, st));
+    pair_f64_kernel<0><<<(unsigned)items, 256, PR_SMEM, st>>>(a);
+    FC_TRY(check_launch("pair_f64_kernel<energy>"));
+    if (stats) FC_CUDA(cudaEventRecord(c.ev1, st));
+    reduce_pairs_kernel<<<1, 1024, 0, st>>>((const double*)vpart, items, (double*)vout);
+    FC_TRY(check_launch("reduce_pairs_kernel"));
+    double h[2];
+    FC_CUDA(cudaMemcpyAsync(h, vout, sizeof(h), cudaMemcpyDeviceToHost, st));
+    FC_CUDA(cudaStreamSynchronize(st));
+    *e_os = h[0];
+    *e_ss = h[1];
+    if (stats) {
+        float ms = 0.f;
+        FC_CUDA(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
+        stats->kernel_ms = ms;
+        stats->flops = 2.0 * (double)d.naux * (double)nvir * (double)nvir * (double)npairs;
+        stats->precision = FC_PREC_F64;
+        stats->launches += 2;
+        stats->tile_m = PR_T;
+        stats->tile_n = PR_T;
+        stats->k_panel = 0;
+        stats->d2h_bytes += sizeof(h);
+        stats->h2d_bytes += npairs * sizeof(int2);
+    }
+    return FC_OK;
+}
+
+fc_status rimp2_grad_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, double* e_ss,
+                         double* gamma, double* de_docc, double* de_dvir, fc_stats* stats) {
+    FC_TRY(set_smem_once());
+    const int64_t nocc = d.nocc, nvir = d.nvir, naux = d.naux, nov = nocc * nvir;
+    const int ntile = (int)((nvir + PR_T - 1) / PR_T);
+    // Amplitude chunk: ci occupied rows of Tt (ci*nvir x nov doubles), sized to
+    // a fixed budget so the call fits beside B and Gamma.
+    const int64_t per_i = nvir * nov * (int64_t)sizeof(double);
+    int64_t ci = d.chunk_bytes / (per_i > 0 ? per_i : 1);
+    if (ci < 1) ci = 1;
+    if (ci > nocc) ci = nocc;
+    const int64_t items_per_i = nocc * (int64_t)ntile * ntile;
+    const int64_t items = ci * items_per_i;
+    if (items > INT32_MAX) return fail(FC_ERR_LAYOUT, "RI-MP2 gradient: too many pair tiles per chunk");
+
+    void *vpairs, *vpart, *vT, *vocc, *vvir, *vout;
+    FC_TRY(ws_get(WS_PAIRS, nocc * nocc * sizeof(int2), &vpairs));
+    FC_TRY(ws_get(WS_T, ci * per_i, &vT));
+    FC_TRY(ws_get(WS_PART, items * (2 + 1 + PR_T) * sizeof(double), &vpart));
+    FC_TRY(ws_get(WS_OUT, ((nocc + 63) / 64 * 64 + 2) * 2 * sizeof(double) + 64, &vout));
+    vocc = (double*)vpart + items * 2;
+    vvir = (double*)vocc + items;
+    double* e_chunks = (double*)vout;  // [nchunks][2]
+    std::vector<int2> hp((size_t)(nocc * nocc));
+    for (int i = 0; i < nocc; ++i)
+        for (int j = 0; j < nocc; ++j) hp[(size_t)i * nocc + j] = make_int2(i, j);
+    FC_CUDA(cudaMemcpyAsync(vpairs, hp.data(), hp.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
+    FC_CUDA(cudaMemsetAsync(de_dvir, 0, nvir * sizeof(double), st));
+
+    Context& c = ctx();
+    const int64_t nchunks = (nocc + ci - 1) / ci;
+    if (stats) FC_CUDA(cudaEventRecord(c.ev0, st));
+    for (int64_t ch = 0; ch < nchunks; ++ch) {
+        const int64_t i0 = ch * ci;
+        const int64_t cn = (i0 + ci <= nocc) ? ci : nocc - i0;
+        PairArgs a{};
+        a.B = d.b_ov;
+        a.ldb = nov;
+        a.naux = (int)naux;
+        a.nvir = (int)nvir;
+        a.eo = d.eps_occ;
+        a.ev = d.eps_vir;
+        a.pairs = (const int2*)vpairs + i0 * nocc;
+        a.ntile = ntile;
+        a.part = (double*)vpart;
+        a.T = (double*)vT;
+        a.ldt = nov;
+        a.i0 = (int)i0;
+        a.occ_part = (double*)vocc;
+        a.vir_part = (double*)vvir;
+        const int64_t nit = cn * items_per_i;
+        pair_f64_kernel<1><<<(unsigned)nit, 256, PR_SMEM, st>>>(a);
+        FC_TRY(check_launch("pair_f64_kernel<grad>"));
+        reduce_pairs_kernel<<<1, 1024, 0, st>>>((const double*)vpart, nit, e_chunks + 2 * ch);
+        reduce_occ_kernel<<<(unsigned)cn, 256, 0, st>>>((const double*)vocc, items_per_i, (int)i0, de_docc);
+        reduce_vir_kernel<<<(unsigned)((nvir + 7) / 8), 256, 0, st>>>((const double*)vvir, cn * nocc, ntile,
+                                                                      (int)nvir, de_dvir);
+        FC_TRY(check_launch("rimp2 gradient reductions"));
+        // Gamma[:, i0*nvir : (i0+cn)*nvir] = 4 * B_ov . Tt_chunk^T
+        const int N = (int)(cn * nvir);
+        dim3 grid((N + DG_BN - 1) / DG_BN, (unsigned)((naux + DG_BM - 1) / DG_BM), 1);
+        EpiStore epi{gamma + i0 * nvir, nov, 4.0};
+        dgemm_tn_kernel<EpiStore><<<grid, 256, DG_SMEM, st>>>(d.b_ov, nov, (const double*)vT, nov,
+                                                               (int)naux, N, nov, nov, 0, epi);
+        FC_TRY(check_launch("dgemm_tn_kernel<gamma>"));
+    }
+    if (stats) FC_CUDA(cudaEventRecord(c.ev1, st));
+    std::vector<double> h((size_t)(2 * nchunks));
+    FC_CUDA(cudaMemcpyAsync(h.data(), e_chunks, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    FC_CUDA(cudaStreamSynchronize(st));
+    double eo = 0.0, co = 0.0, es = 0.0, cs = 0.0;
+    for (int64_t ch = 0; ch < nchunks; ++ch) {  // ascending-chunk compensated sum
+        double v = h[2 * ch], tt = eo + v;
+        co += (fabs(eo) >= fabs(v)) ? (eo - tt) + v : (v - tt) + eo;
+        eo = tt;
+        v = h[2 * ch + 1];
+        tt = es + v;
+        cs += (fabs(es) >= fabs(v)) ? (es - tt) + v : (v - tt) + es;
+        es = tt;
+    }
+    *e_os = eo + co;
+    *e_ss = es + cs;
+    if (stats) {
+        float ms = 0.f;
+        FC_CUDA(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
+        stats->kernel_ms = ms;
+        const double P = (double)nocc * (nocc + 1) / 2.0;
+        stats->flops = 2.0 * naux * (double)nvir * nvir * P + 2.0 * naux * (double)nov * nov;
+        stats->precision = FC_PREC_F64;
+        stats->launches += (int)(5 * nchunks);
+        stats->tile_m = PR_T;
+        stats->tile_n = PR_T;
+        stats->k_panel = 0;
+        stats->d2h_bytes += h.size() * sizeof(double);
+        stats->h2d_bytes += hp.size() * sizeof(int2);
+    }
+    return FC_OK;
+}
+
+}  // namespace fc

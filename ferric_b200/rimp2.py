@@ -1,0 +1,182 @@
+"""RI-MP2 on the B200, behind the reference's own entry points.
+
+Mirrors, with the same argument meaning:
+
+* ``spin_components_from_b_ov_kappa`` / ``try_spin_components_on_device``
+  (ferric-mp2/src/rimp2.rs:1330-1375, rimp2_gpu.rs:105-170):
+  ``b_ov`` (naux, nocc*nvir) with column ``i*nvir + a``, the full MO-energy
+  vector ``eps`` indexed ``first_occ + i`` / ``nocc_total + a``, optional
+  ``kappa``.  ``try_*`` returns ``None`` when the device declines (the
+  reference's "run the CPU path"), with the reason counted in ``STATS``;
+  the plain form raises :class:`FcError`.
+* ``Mp2Intermediates::from_ri_densities`` inputs (rimp2.rs:1841-1883):
+  :func:`rimp2_energy_grad` returns ``Gamma = dE/dB = 4 x_ov`` and
+  ``dE/d eps`` (``2 diag(P_oo)``, ``2 diag(P_vv)``) without storing amplitudes.
+
+Inputs may be NumPy arrays (host API: the library copies) or CUDA torch
+tensors (device API on torch's current stream).
+"""
+from __future__ import annotations
+
+import collections
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import FcError, FcStats, PRECISIONS, check, ptr
+
+STATS = collections.Counter()
+
+
+@dataclass
+class SpinComponents:
+    """``SpinComponents`` (ferric-mp2/src/rimp2.rs:134-141)."""
+    e_os: float
+    e_ss: float
+    e_total: float
+
+
+def _precision(p):
+    if isinstance(p, int):
+        return p
+    try:
+        return PRECISIONS[p]
+    except KeyError as exc:
+        raise ValueError(f"unknown precision {p!r}; expected one of {sorted(PRECISIONS)}") from exc
+
+
+def _is_torch_cuda(x):
+    return hasattr(x, "is_cuda") and x.is_cuda
+
+
+def _stream_of(x):
+    import torch
+    return ctypes.c_void_p(torch.cuda.current_stream(x.device).cuda_stream)
+
+
+def _split_eps(eps, nocc, nvir, first_occ, nocc_total):
+    if nocc_total is None:
+        nocc_total = first_occ + nocc
+    return eps[first_occ:first_occ + nocc], eps[nocc_total:nocc_total + nvir]
+
+
+def rimp2_energy(b_ov, eps_occ, eps_vir, kappa=None, precision="f64", stats=None):
+    """``(e_os, e_ss)`` for ``b_ov`` and the active orbital energies.
+
+    NumPy inputs use the host API; CUDA tensors (float64, contiguous) use
+    the device API on the current stream.
+    """
+    _lib.ensure_init()
+    nocc, nvir = int(eps_occ.shape[0]), int(eps_vir.shape[0])
+    naux = int(b_ov.shape[0])
+    if b_ov.shape[1] != nocc * nvir:
+        raise ValueError(f"b_ov has {b_ov.shape[1]} columns, expected nocc*nvir = {nocc * nvir}")
+    eo, es = ctypes.c_double(), ctypes.c_double()
+    st = FcStats()
+    prec = _precision(precision)
+    hk, kv = (0, 0.0) if kappa is None else (1, float(kappa))
+    if _is_torch_cuda(b_ov):
+        b, o, v = (t.contiguous() for t in (b_ov, eps_occ, eps_vir))
+        for t in (b, o, v):
+            if t.dtype != __import__("torch").float64:
+                raise TypeError("device inputs must be float64")
+        check(_lib.lib.fc_rimp2_energy_dev(ptr(b), naux, nocc, nvir, ptr(o), ptr(v), hk, kv, prec,
+                                           ctypes.byref(eo), ctypes.byref(es), _stream_of(b),
+                                           ctypes.byref(st)))
+    else:
+        b = np.ascontiguousarray(b_ov, dtype=np.float64)
+        o = np.ascontiguousarray(eps_occ, dtype=np.float64)
+        v = np.ascontiguousarray(eps_vir, dtype=np.float64)
+        check(_lib.lib.fc_rimp2_energy(ptr(b), naux, nocc, nvir, ptr(o), ptr(v), hk, kv, prec,
+                                       ctypes.byref(eo), ctypes.byref(es), ctypes.byref(st)))
+    if stats is not None:
+        stats.update(st.as_dict())
+    return eo.value, es.value
+
+
+def spin_components_on_device(b_ov, eps, nocc, nvir, first_occ=0, nocc_total=None, kappa=None,
+                              precision="f64", stats=None):
+    """Device spin components; raises :class:`FcError` when the device cannot run
+    (``spin_components_on_device``, ferric-mp2/src/rimp2_gpu.rs:198)."""
+    if len(eps) < (first_occ + nocc if nocc_total is None else nocc_total) + nvir:
+        raise ValueError("eps is shorter than nocc_total + nvir")
+    eo, ev = _split_eps(eps, nocc, nvir, first_occ, nocc_total)
+    e_os, e_ss = rimp2_energy(b_ov, eo, ev, kappa=kappa, precision=precision, stats=stats)
+    return SpinComponents(e_os, e_ss, e_os + e_ss)
+
+
+def try_spin_components_on_device(b_ov, eps, nocc, nvir, first_occ=0, nocc_total=None, kappa=None,
+                                  mixed_ok=False, stats=None):
+    """Dispatcher: ``None`` means "run the CPU path", with the reason counted.
+
+    Same contract as ``try_spin_components_on_device``
+    (ferric-mp2/src/rimp2_gpu.rs:105-170): mixed runs only when ``mixed_ok``
+    and no kappa; a mixed kernel failure (``FC_ERR_KERNEL``/``FC_ERR_RANGE``)
+    is retried in FP64 on the device, counted, never silent.
+    """
+    precision = "mixed" if (mixed_ok and kappa is None) else "f64"
+    try:
+        return spin_components_on_device(b_ov, eps, nocc, nvir, first_occ, nocc_total, kappa,
+                                         precision, stats)
+    except FcError as e:
+        if precision != "f64" and e.name in ("FC_ERR_KERNEL", "FC_ERR_RANGE"):
+            STATS[f"mixed_fallback:{e.name}"] += 1
+            try:
+                return spin_components_on_device(b_ov, eps, nocc, nvir, first_occ, nocc_total,
+                                                 kappa, "f64", stats)
+            except FcError as e2:
+                STATS[f"cpu:{e2.name}"] += 1
+                return None
+        STATS[f"cpu:{e.name}"] += 1
+        return None
+
+
+def rimp2_energy_grad(b_ov, eps_occ, eps_vir, precision="f64", stats=None, out=None):
+    """``(SpinComponents, gamma, de_docc, de_dvir)``.
+
+    ``gamma[P, ia] = dE/dB[P, ia]`` (= 4 x_ov, ferric-mp2/src/rimp2.rs:1832-1836),
+    ``de_docc[i] = dE/d eps_occ[i]``, ``de_dvir[a] = dE/d eps_vir[a]``.
+    """
+    _lib.ensure_init()
+    nocc, nvir = int(eps_occ.shape[0]), int(eps_vir.shape[0])
+    naux = int(b_ov.shape[0])
+    if b_ov.shape[1] != nocc * nvir:
+        raise ValueError(f"b_ov has {b_ov.shape[1]} columns, expected nocc*nvir = {nocc * nvir}")
+    eo, es = ctypes.c_double(), ctypes.c_double()
+    st = FcStats()
+    prec = _precision(precision)
+    if _is_torch_cuda(b_ov):
+        import torch
+        b, o, v = (t.contiguous() for t in (b_ov, eps_occ, eps_vir))
+        if out is None:
+            gamma = torch.empty_like(b)
+            d_o = torch.empty_like(o)
+            d_v = torch.empty_like(v)
+        else:
+            gamma, d_o, d_v = out
+        check(_lib.lib.fc_rimp2_energy_grad_dev(
+            ptr(b), naux, nocc, nvir, ptr(o), ptr(v), prec, ctypes.byref(eo), ctypes.byref(es),
+            ptr(gamma), ptr(d_o), ptr(d_v), _stream_of(b), ctypes.byref(st)))
+    else:
+        b = np.ascontiguousarray(b_ov, dtype=np.float64)
+        o = np.ascontiguousarray(eps_occ, dtype=np.float64)
+        v = np.ascontiguousarray(eps_vir, dtype=np.float64)
+        gamma = np.empty_like(b)
+        d_o = np.empty(nocc)
+        d_v = np.empty(nvir)
+        check(_lib.lib.fc_rimp2_energy_grad(
+            ptr(b), naux, nocc, nvir, ptr(o), ptr(v), prec, ctypes.byref(eo), ctypes.byref(es),
+            ptr(gamma), ptr(d_o), ptr(d_v), ctypes.byref(st)))
+    if stats is not None:
+        stats.update(st.as_dict())
+    return SpinComponents(eo.value, es.value, eo.value + es.value), gamma, d_o, d_v
+
+
+def ri_densities(b_ov, eps_occ, eps_vir, precision="f64"):
+    """``(x_ov, de_docc, de_dvir, e_corr)``: the inputs
+    ``Mp2Intermediates::from_ri_densities`` takes (rimp2.rs:1841-1883), with
+    ``x_ov = Gamma / 4``; the P diagonals enter as ``dE/deps / 2``."""
+    sc, gamma, d_o, d_v = rimp2_energy_grad(b_ov, eps_occ, eps_vir, precision)
+    return gamma / 4.0, d_o, d_v, sc.e_total

@@ -1,0 +1,149 @@
+/*
+ * ferric_cuda.h -- C ABI of libferric_cuda, the B200 (sm_100a) density-fitting
+ * contraction library that sits behind ferric's device hooks.
+ *
+ * Plain pointers, sizes and status codes only.  Every array is row-major
+ * (C order, as ndarray stores it) and contiguous.  Functions without a `_dev`
+ * suffix take HOST arrays and do their own host<->device copies (the
+ * reference hooks are host-array APIs); `_dev` variants take device pointers
+ * and a `cudaStream_t` passed as `void*` (NULL = the library's own stream) and
+ * return once the work is enqueued.
+ *
+ * No function falls back to the CPU.  A non-zero status means "not done":
+ * the caller keeps the reference's decline-to-CPU behaviour
+ * (ferric-mp2/src/rimp2_gpu.rs:105-179, ferric-scf/src/df_j_gpu.rs:622-676).
+ * fc_last_error() gives the message of the calling thread's last failure.
+ */
+#ifndef FERRIC_CUDA_H
+#define FERRIC_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  1..8 mirror GpuError (ferric-core/src/gpu/device.rs:16-36). */
+typedef int32_t fc_status;
+#define FC_OK             0
+#define FC_ERR_DRIVER     1  /* GpuError::DriverLibrary: CUDA driver unusable      */
+#define FC_ERR_BLAS       2  /* GpuError::BlasLibrary (reserved; no BLAS is used) */
+#define FC_ERR_DEVICE     3  /* GpuError::Device: no such device / not sm_100      */
+#define FC_ERR_POOL_FULL  4  /* GpuError::PoolFull: request exceeds the pool cap   */
+#define FC_ERR_LAYOUT     5  /* GpuError::Layout: bad shape, size or overflow      */
+#define FC_ERR_CUDA       6  /* GpuError::Cuda: a CUDA call failed                 */
+#define FC_ERR_KERNEL     7  /* GpuError::Kernel: kernel image or launch refused   */
+#define FC_ERR_RANGE      8  /* GpuError::F32Range: operand outside split-BF16 range*/
+#define FC_ERR_TIMEOUT    9  /* a bounded device wait ran out                      */
+#define FC_ERR_INVALID   10  /* null pointer, bad enum, library not initialised   */
+
+/* Arithmetic of the contraction kernels. */
+#define FC_PREC_F64       0  /* all-FP64 "plain" kernels: the drop-in              */
+#define FC_PREC_MIXED     1  /* split-BF16: hi+lo operands, 3 tensor-core products */
+#define FC_PREC_MIXED_X6  2  /* split-BF16: hi+mid+lo operands, 6 products        */
+
+/* Storage layout of the 3-index tensor handed to fc_dfjk_create. */
+#define FC_LAYOUT_SQUARE        0  /* (naux, n, n), symmetric in (mu, nu)          */
+#define FC_LAYOUT_PACKED_LOWER  1  /* (naux, n(n+1)/2), rows (mu, nu <= mu)        */
+
+/* Per-call record (the reference's gpu::stats counters, per call). */
+typedef struct fc_stats {
+    double   kernel_ms;    /* device time of the contraction kernels (CUDA events) */
+    double   flops;        /* algorithmic flops of the call                       */
+    uint64_t h2d_bytes;    /* host->device bytes copied by the call               */
+    uint64_t d2h_bytes;    /* device->host bytes copied by the call               */
+    int32_t  precision;    /* FC_PREC_* that ran                                  */
+    int32_t  launches;     /* kernels launched by the call                        */
+    int32_t  tile_m;       /* tile of the dominant kernel                         */
+    int32_t  tile_n;
+    int32_t  k_panel;      /* FP64 flush interval of mixed kernels (0 = none)     */
+    int32_t  reserved;
+} fc_stats;
+
+/* ---- library ------------------------------------------------------------ */
+
+/* Select `device` (ordinal) and cap the library's device allocations at
+ * `pool_bytes` (0 = no cap).  Replaces gpu::install/decide + DevicePool
+ * (ferric-core/src/gpu/mod.rs:110-373, ferric-core/src/gpu/pool.rs:1-30).
+ * Idempotent for the same device. */
+fc_status   fc_init(int32_t device, uint64_t pool_bytes);
+/* Free every cached workspace of the library.  Handles stay valid. */
+fc_status   fc_release_workspace(void);
+/* Bytes currently held by the library on the device (workspaces + handles). */
+uint64_t    fc_pool_used(void);
+/* Copy the calling thread's last error message into buf (NUL-terminated);
+ * returns the full message length. */
+size_t      fc_last_error(char* buf, size_t len);
+const char* fc_version(void);
+
+/* ---- RI-MP2 ---------------------------------------------------------------
+ * b_ov: (naux, nocc*nvir), column i*nvir + a, dressed B_Q,ia.
+ * eps_occ[nocc], eps_vir[nvir]: active occupied / virtual orbital energies
+ * (the reference's eps[first_occ + i], eps[nocc_total + a]).
+ *
+ * Replaces try_spin_components_on_device (ferric-mp2/src/rimp2_gpu.rs:105-170)
+ * and the CPU pair loop (ferric-mp2/src/rimp2.rs:1399-1544).
+ * has_kappa != 0 applies the kappa damping (1 - exp(kappa*D))^2
+ * (rimp2.rs:1425-1437); it is FP64 only, as mixed_energy_operator allows mixed
+ * only without kappa (rimp2.rs:1293-1300).  e_os/e_ss are host scalars. */
+fc_status fc_rimp2_energy(const double* b_ov, int64_t naux, int64_t nocc, int64_t nvir,
+                          const double* eps_occ, const double* eps_vir,
+                          int32_t has_kappa, double kappa, int32_t precision,
+                          double* e_os, double* e_ss, fc_stats* stats);
+fc_status fc_rimp2_energy_dev(const double* b_ov, int64_t naux, int64_t nocc, int64_t nvir,
+                              const double* eps_occ, const double* eps_vir,
+                              int32_t has_kappa, double kappa, int32_t precision,
+                              double* e_os, double* e_ss, void* stream, fc_stats* stats);
+
+/* Energy plus its adjoint: gamma[P, ia] = dE/dB[P, ia] (naux x nocc*nvir,
+ * = 4 x_ov of ferric-mp2/src/zvector.rs:651-703, rimp2.rs:1832-1836),
+ * de_docc[i] = dE/d eps_occ[i] and de_dvir[a] = dE/d eps_vir[a]
+ * (= 2 diag(P_oo), 2 diag(P_vv) of ferric-mp2/src/oo_rimp2.rs:1170-1300).
+ * E = E_os + E_ss.  No amplitudes are stored: occupied-pair blocks are
+ * recomputed.  In the _dev form e_os/e_ss are host scalars and the call
+ * synchronises its stream before returning. */
+fc_status fc_rimp2_energy_grad(const double* b_ov, int64_t naux, int64_t nocc, int64_t nvir,
+                               const double* eps_occ, const double* eps_vir, int32_t precision,
+                               double* e_os, double* e_ss, double* gamma,
+                               double* de_docc, double* de_dvir, fc_stats* stats);
+fc_status fc_rimp2_energy_grad_dev(const double* b_ov, int64_t naux, int64_t nocc, int64_t nvir,
+                                   const double* eps_occ, const double* eps_vir, int32_t precision,
+                                   double* e_os, double* e_ss, double* gamma,
+                                   double* de_docc, double* de_dvir, void* stream,
+                                   fc_stats* stats);
+
+/* ---- DF-JK ----------------------------------------------------------------
+ * A handle owns the device copy of the 3-index tensor for the lifetime of a
+ * builder (the reference's per-builder DeviceSlot, ferric-scf/src/df_j_gpu.rs:1-5,
+ * df_k_gpu.rs:1-4).  Without a metric the tensor is taken as dressed,
+ * B = L^-1 (P|mn), and J = B^T (B . D).  A handle is used by one thread at a
+ * time. */
+typedef struct fc_dfjk fc_dfjk;
+
+fc_status fc_dfjk_create(const double* b, int64_t naux, int64_t n, int32_t layout,
+                         int32_t precision, fc_dfjk** out);
+fc_status fc_dfjk_create_dev(const double* b, int64_t naux, int64_t n, int32_t layout,
+                             int32_t precision, void* stream, fc_dfjk** out);
+/* Raw (P|mn) form: l = lower Cholesky factor of the metric V = L L^T
+ * (naux x naux, row-major); each J build then solves V c = d on the device
+ * (DfJ::solve_metric, ferric-scf/src/df_j.rs:931). */
+fc_status fc_dfj_set_metric_chol(fc_dfjk* h, const double* l);
+/* J = sum_P B_P c_P, c = V^-1 d, d_P = <B_P, D>  (JBuilder::build,
+ * ferric-scf/src/fock.rs:10-19; df_j.rs:1459-1572).  d, j: n x n. */
+fc_status fc_dfj_build(fc_dfjk* h, const double* d, double* j, fc_stats* stats);
+fc_status fc_dfj_build_dev(fc_dfjk* h, const double* d, double* j, void* stream,
+                           fc_stats* stats);
+/* K = sum_Q (B_Q C)(B_Q C)^T for c_occ (n x nocc); no occupation factor
+ * (KBuilder::build_from_occ, ferric-scf/src/fock.rs:22-52;
+ * df_k.rs:1409-1520).  FC_LAYOUT_SQUARE handles only. */
+fc_status fc_dfk_build_occ(fc_dfjk* h, const double* c_occ, int64_t nocc, double* k,
+                           fc_stats* stats);
+fc_status fc_dfk_build_occ_dev(fc_dfjk* h, const double* c_occ, int64_t nocc, double* k,
+                               void* stream, fc_stats* stats);
+fc_status fc_dfjk_destroy(fc_dfjk* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FERRIC_CUDA_H */

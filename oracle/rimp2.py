@@ -1,0 +1,191 @@
+"""FP64 restatement of the reference's closed-shell RI-MP2 path (oracle only).
+
+Layout conventions follow the reference exactly:
+
+* ``b_ov`` is row-major ``(naux, nocc*nvir)`` with column ``i*nvir + a``
+  (ferric-mp2/src/rimp2.rs:1445-1499);
+* ``eps`` is the full MO-energy vector, indexed ``first_occ + i`` for an
+  active occupied orbital and ``nocc_total + a`` for a virtual
+  (ferric-mp2/src/rimp2.rs:1399-1441).
+
+Energies
+    ``E_OS = sum_ij sum_ab g_ab^2 / D``,
+    ``E_SS = sum_ij sum_ab g_ab (g_ab - g_ba) / D``, ``g_ab = (ia|jb)``,
+    ``D = e_i + e_j - e_a - e_b``, over unique pairs ``j >= i`` with weight 1
+    on the diagonal and 2 off it; per-i partials summed serially in ascending
+    i (rimp2.rs:1506-1544).  Optional kappa damping ``(1 - exp(kappa*D))^2``
+    on both components (rimp2.rs:1425-1437).
+
+Adjoint
+    ``Gamma[P, ia] = dE/dB[P, ia] = 4 x_ov[P, ia]`` (rimp2.rs:1832-1836) with
+    ``x_ov[P, ia] = sum_jb Tt_ij^ab B[P, jb]`` and ``Tt = 2t - tbar``
+    (zvector.rs:651-703); ``dE/d eps_p = 2 P_pp`` (rimp2.rs:1835-1836) with
+    the unrelaxed densities of oo_rimp2.rs:1170-1300.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def _pair_terms(g, e_ij, eps_vir, kappa):
+    """(e_os_ij, e_ss_ij) of one pair block ``g[a, b] = (ia|jb)``.
+
+    Restates ``pair_energy`` (ferric-mp2/src/rimp2.rs:1399-1441).
+    """
+    denom = e_ij - eps_vir[:, None] - eps_vir[None, :]
+    if kappa is None:
+        w = 1.0 / denom
+    else:
+        d1 = 1.0 - np.exp(kappa * denom)
+        w = d1 * d1 / denom
+    e_os = float(np.sum(g * g * w))
+    e_ss = float(np.sum(g * (g - g.T) * w))
+    return e_os, e_ss
+
+
+def spin_components(b_ov, eps, nocc, nvir, first_occ=0, nocc_total=None, kappa=None):
+    """Closed-shell RI-MP2 ``(e_os, e_ss, e_total)``.
+
+    Restates ``spin_components_from_b_ov_kappa_cpu`` and
+    ``spin_components_from_blocks`` (ferric-mp2/src/rimp2.rs:1445-1544):
+    one wide product ``G_i = B_i^T B_{j>=i}`` per occupied ``i``, the pair
+    loop over ``j >= i`` with weight 1 (i == j) or 2, and an ascending-i
+    serial sum of the per-i partials.
+    """
+    b_ov = np.ascontiguousarray(b_ov, dtype=np.float64)
+    eps = np.asarray(eps, dtype=np.float64)
+    if nocc_total is None:
+        nocc_total = first_occ + nocc
+    eps_vir = eps[nocc_total:nocc_total + nvir]
+    partials = []
+    for i in range(nocc):
+        b_i = b_ov[:, i * nvir:(i + 1) * nvir]
+        g_i = b_i.T @ b_ov[:, i * nvir:]
+        e_os_i = e_ss_i = 0.0
+        for j in range(i, nocc):
+            fac = 1.0 if i == j else 2.0
+            jcol = (j - i) * nvir
+            g = g_i[:, jcol:jcol + nvir]
+            e_ij = eps[first_occ + i] + eps[first_occ + j]
+            eo, es = _pair_terms(g, e_ij, eps_vir, kappa)
+            e_os_i += fac * eo
+            e_ss_i += fac * es
+        partials.append((e_os_i, e_ss_i))
+    e_os = 0.0
+    e_ss = 0.0
+    for eo, es in partials:
+        e_os += eo
+        e_ss += es
+    return e_os, e_ss, e_os + e_ss
+
+
+def spin_components_full_loop(b_ov, eps_occ, eps_vir, kappa=None):
+    """Every ordered pair (i, j), no symmetry weights: the naive cross-check
+    the reference keeps beside the fast loop
+    (ferric-mp2/src/rimp2.rs:984-1018 and the test at rimp2.rs:3107)."""
+    nocc, nvir = len(eps_occ), len(eps_vir)
+    e_os = e_ss = 0.0
+    for i in range(nocc):
+        for j in range(nocc):
+            g = b_ov[:, i * nvir:(i + 1) * nvir].T @ b_ov[:, j * nvir:(j + 1) * nvir]
+            eo, es = _pair_terms(g, eps_occ[i] + eps_occ[j], eps_vir, kappa)
+            e_os += eo
+            e_ss += es
+    return e_os, e_ss, e_os + e_ss
+
+
+def t2_and_integrals(b_ov, eps_occ, eps_vir):
+    """``(t2, eri_ov)`` flat ``nov x nov``: ``eri = B^T B`` and ``t2 = eri / D``.
+
+    Restates ``compute_t2_and_integrals`` (ferric-mp2/src/oo_rimp2.rs:1079-1123).
+    Small cases only (it stores ``nov^2`` doubles twice).
+    """
+    nocc, nvir = len(eps_occ), len(eps_vir)
+    eri = b_ov.T @ b_ov
+    e_ov = (eps_occ[:, None] - eps_vir[None, :]).reshape(-1)   # e_i - e_a at ia
+    denom = e_ov[:, None] + e_ov[None, :]
+    return eri / denom, eri
+
+
+def mp2_density(t2, nocc, nvir):
+    """Unrelaxed ``(P_oo, P_vv)`` from flat amplitudes ``t2[ia, jb]``.
+
+    Restates ``build_mp2_density`` (ferric-mp2/src/oo_rimp2.rs:1170-1300):
+    ``P_ij = -sum_kab t_ik^ab (2 t_jk^ab - t_jk^ba)``,
+    ``P_ab =  sum_ijc t_ij^ac (2 t_ij^bc - t_ij^cb)``.
+    """
+    t = np.asarray(t2).reshape(nocc, nvir, nocc, nvir)          # t[i,a,j,b]
+    tt = 2.0 * t - t.transpose(0, 3, 2, 1)                       # 2t - tbar
+    p_oo = -np.einsum("iakb,jakb->ij", t, tt, optimize=True)
+    p_vv = np.einsum("iajc,ibjc->ab", t, tt, optimize=True)
+    return p_oo, p_vv
+
+
+def x_ov_from_t2(t2, b_ov, nocc, nvir):
+    """``x_ov[P, ia] = sum_jb (2t - tbar)_ij^ab B[P, jb]``.
+
+    Restates ``build_x_ov_weighted`` / ``tt_block`` at MP2 weights (d, e) =
+    (2, 1) (ferric-mp2/src/zvector.rs:651-703).
+    """
+    nov = nocc * nvir
+    t = np.asarray(t2).reshape(nocc, nvir, nocc, nvir)
+    tt = (2.0 * t - t.transpose(0, 3, 2, 1)).reshape(nov, nov)
+    return b_ov @ tt.T
+
+
+def energy_gamma_deps_small(b_ov, eps_occ, eps_vir):
+    """E, Gamma and dE/deps through the stored-amplitude route the reference
+    takes (t2 -> P, x_ov).  Small cases only.
+
+    Returns ``(e_os, e_ss, gamma, de_docc, de_dvir)``.
+    """
+    nocc, nvir = len(eps_occ), len(eps_vir)
+    t2, eri = t2_and_integrals(b_ov, eps_occ, eps_vir)
+    tt = (2.0 * t2.reshape(nocc, nvir, nocc, nvir)
+          - t2.reshape(nocc, nvir, nocc, nvir).transpose(0, 3, 2, 1)).reshape(t2.shape)
+    e_os = float(np.sum(eri * t2))
+    e_ss = float(np.sum(eri * (t2 - t2.reshape(nocc, nvir, nocc, nvir)
+                                  .transpose(0, 3, 2, 1).reshape(t2.shape))))
+    gamma = 4.0 * x_ov_from_t2(t2, b_ov, nocc, nvir)
+    p_oo, p_vv = mp2_density(t2, nocc, nvir)
+    del tt
+    return e_os, e_ss, gamma, 2.0 * np.diag(p_oo).copy(), 2.0 * np.diag(p_vv).copy()
+
+
+def energy_gamma_deps(b_ov, eps_occ, eps_vir, i_block=None):
+    """E, Gamma = dE/dB and dE/deps without storing ``t2``.
+
+    The amplitudes of one occupied ``i`` are recomputed from
+    ``G_i = B_i^T B`` (``nvir x nov``), turned into ``Tt_i = (2 G_i - G_i^swap)/D``
+    and contracted at once: ``x_i = B Tt_i^T`` -- the per-i GEMM of
+    ``build_x_ov_weighted`` (zvector.rs:651-703) with ``tt_block`` built from
+    the recomputed block instead of the stored ``t2``.  The densities'
+    diagonals follow ``P_ii = -sum_jab t_ij^ab Tt_ij^ab`` and
+    ``P_aa = sum_ijb t_ij^ab Tt_ij^ab`` (oo_rimp2.rs:1170-1191).
+
+    Returns ``(e_os, e_ss, gamma, de_docc, de_dvir)``.
+    """
+    b_ov = np.ascontiguousarray(b_ov, dtype=np.float64)
+    eps_occ = np.asarray(eps_occ, dtype=np.float64)
+    eps_vir = np.asarray(eps_vir, dtype=np.float64)
+    naux = b_ov.shape[0]
+    nocc, nvir = len(eps_occ), len(eps_vir)
+    nov = nocc * nvir
+    gamma = np.empty((naux, nov))
+    de_docc = np.zeros(nocc)
+    de_dvir = np.zeros(nvir)
+    e_os = e_ss = 0.0
+    for i in range(nocc):
+        g = (b_ov[:, i * nvir:(i + 1) * nvir].T @ b_ov).reshape(nvir, nocc, nvir)  # g[a,j,b]
+        gs = g.transpose(2, 1, 0)                                                # g[b,j,a] at [a,j,b]
+        denom = (eps_occ[i] + eps_occ[None, :, None]
+                 - eps_vir[:, None, None] - eps_vir[None, None, :])
+        t = g / denom
+        tt = (2.0 * g - gs) / denom
+        e_os += float(np.sum(g * t))
+        e_ss += float(np.sum(g * (g - gs) / denom))
+        c = t * tt                                 # t_ij^ab Tt_ij^ab
+        de_docc[i] += -2.0 * float(np.sum(c))
+        de_dvir += 2.0 * np.sum(c, axis=(1, 2))
+        gamma[:, i * nvir:(i + 1) * nvir] = 4.0 * (b_ov @ tt.reshape(nvir, nov).T)
+    return e_os, e_ss, gamma, de_docc, de_dvir
