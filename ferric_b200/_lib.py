@@ -55,11 +55,13 @@ class FcStats(ctypes.Structure):
         ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64),
         ("precision", ctypes.c_int32), ("launches", ctypes.c_int32),
         ("tile_m", ctypes.c_int32), ("tile_n", ctypes.c_int32),
-        ("k_panel", ctypes.c_int32), ("reserved", ctypes.c_int32),
+        ("k_panel", ctypes.c_int32), ("main_launches", ctypes.c_int32),
+        ("main_ms", ctypes.c_double), ("main_flops", ctypes.c_double),
+        ("main_bytes", ctypes.c_double),
     ]
 
     def as_dict(self):
-        return {f: getattr(self, f) for f, _ in self._fields_ if f != "reserved"}
+        return {f: getattr(self, f) for f, _ in self._fields_}
 
 
 class FcError(RuntimeError):

@@ -210,6 +210,10 @@ fc_status dfj_build_f64(fc_dfjk* h, const double* d, double* j, cudaStream_t st,
         stats->flops = 4.0 * (double)naux * (double)pair;
         stats->precision = FC_PREC_F64;
         stats->launches += 4 + (h->l_chol ? 1 : 0);
+        stats->main_launches = 2;
+        stats->main_ms = ms;
+        stats->main_flops = stats->flops;
+        stats->main_bytes = 2.0 * 8.0 * (double)naux * (double)pair;
     }
     return FC_OK;
 }
@@ -263,6 +267,10 @@ fc_status dfk_build_f64(fc_dfjk* h, const double* c_occ, int64_t nocc, double* k
         stats->flops = 4.0 * (double)naux * (double)n * (double)n * (double)nocc;
         stats->precision = FC_PREC_F64;
         stats->launches += 4;
+        stats->main_launches = 2;
+        stats->main_ms = ms;
+        stats->main_flops = stats->flops;
+        stats->main_bytes = 8.0 * (double)naux * (double)n * (double)n;
         stats->tile_m = DG_BM;
         stats->tile_n = DG_BN;
     }

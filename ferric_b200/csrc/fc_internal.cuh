@@ -68,6 +68,7 @@ struct Context {
     std::mutex mu;
     Workspace ws[WS_COUNT];
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<cudaEvent_t> evs;  // per-launch timing pairs of the dominant kernel
 };
 
 Context& ctx();
@@ -78,6 +79,10 @@ uint64_t ws_bytes();
 fc_status ws_get(int slot, size_t bytes, void** out);
 fc_status pool_reserve(uint64_t bytes);  // handle allocation check
 cudaStream_t pick_stream(void* s);
+// At least 2*n timing events (created on first use, kept by the context).
+fc_status timing_events(int n, cudaEvent_t** out);
+// Sum of elapsed times of the n event pairs (waits for the last one).
+fc_status timing_sum(int n, double* ms);
 
 // Overflow-checked size products.
 bool mul_ok(int64_t a, int64_t b, int64_t* out);

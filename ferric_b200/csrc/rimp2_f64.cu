@@ -320,6 +320,10 @@ fc_status rimp2_energy_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, dou
         stats->k_panel = 0;
         stats->d2h_bytes += sizeof(h);
         stats->h2d_bytes += npairs * sizeof(int2);
+        stats->main_launches = 1;
+        stats->main_ms = ms;
+        stats->main_flops = stats->flops;
+        stats->main_bytes = 8.0 * (double)d.naux * (double)(nocc * nvir);
     }
     return FC_OK;
 }
@@ -355,6 +359,8 @@ fc_status rimp2_grad_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, doubl
 
     Context& c = ctx();
     const int64_t nchunks = (nocc + ci - 1) / ci;
+    cudaEvent_t* ev = nullptr;
+    if (stats) FC_TRY(timing_events((int)nchunks, &ev));
     if (stats) FC_CUDA(cudaEventRecord(c.ev0, st));
     for (int64_t ch = 0; ch < nchunks; ++ch) {
         const int64_t i0 = ch * ci;
@@ -375,8 +381,10 @@ fc_status rimp2_grad_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, doubl
         a.occ_part = (double*)vocc;
         a.vir_part = (double*)vvir;
         const int64_t nit = cn * items_per_i;
+        if (stats) FC_CUDA(cudaEventRecord(ev[2 * ch], st));
         pair_f64_kernel<1><<<(unsigned)nit, 256, PR_SMEM, st>>>(a);
         FC_TRY(check_launch("pair_f64_kernel<grad>"));
+        if (stats) FC_CUDA(cudaEventRecord(ev[2 * ch + 1], st));
         reduce_pairs_kernel<<<1, 1024, 0, st>>>((const double*)vpart, nit, e_chunks + 2 * ch);
         reduce_occ_kernel<<<(unsigned)cn, 256, 0, st>>>((const double*)vocc, items_per_i, (int)i0, de_docc);
         reduce_vir_kernel<<<(unsigned)((nvir + 7) / 8), 256, 0, st>>>((const double*)vvir, cn * nocc, ntile,
@@ -419,6 +427,12 @@ fc_status rimp2_grad_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, doubl
         stats->k_panel = 0;
         stats->d2h_bytes += h.size() * sizeof(double);
         stats->h2d_bytes += hp.size() * sizeof(int2);
+        // dominant kernel: the fused pair kernel, one launch per chunk, forming
+        // the G_ij blocks of every ordered pair (i in chunk, all j)
+        stats->main_launches = (int)nchunks;
+        FC_TRY(timing_sum((int)nchunks, &stats->main_ms));
+        stats->main_flops = 2.0 * naux * (double)nov * nov;
+        stats->main_bytes = 8.0 * naux * (double)nov * (double)nchunks + 8.0 * (double)nov * nov;
     }
     return FC_OK;
 }

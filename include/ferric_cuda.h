@@ -58,7 +58,10 @@ typedef struct fc_stats {
     int32_t  tile_m;       /* tile of the dominant kernel                         */
     int32_t  tile_n;
     int32_t  k_panel;      /* FP64 flush interval of mixed kernels (0 = none)     */
-    int32_t  reserved;
+    int32_t  main_launches;/* launches of the dominant kernel                      */
+    double   main_ms;      /* device time of the dominant kernel, all its launches */
+    double   main_flops;   /* algorithmic flops done by the dominant kernel        */
+    double   main_bytes;   /* algorithmic bytes moved by the dominant kernel       */
 } fc_stats;
 
 /* ---- library ------------------------------------------------------------ */

@@ -152,7 +152,7 @@ def energy_gamma_deps_small(b_ov, eps_occ, eps_vir):
     return e_os, e_ss, gamma, 2.0 * np.diag(p_oo).copy(), 2.0 * np.diag(p_vv).copy()
 
 
-def energy_gamma_deps(b_ov, eps_occ, eps_vir, i_block=None):
+def energy_gamma_deps(b_ov, eps_occ, eps_vir, occ=None):
     """E, Gamma = dE/dB and dE/deps without storing ``t2``.
 
     The amplitudes of one occupied ``i`` are recomputed from
@@ -163,6 +163,10 @@ def energy_gamma_deps(b_ov, eps_occ, eps_vir, i_block=None):
     diagonals follow ``P_ii = -sum_jab t_ij^ab Tt_ij^ab`` and
     ``P_aa = sum_ijb t_ij^ab Tt_ij^ab`` (oo_rimp2.rs:1170-1191).
 
+    ``occ`` restricts the loop to a subset of occupied ``i`` (a bounded
+    sample: the energies, Gamma columns and dE/deps then hold only those
+    rows' contributions).
+
     Returns ``(e_os, e_ss, gamma, de_docc, de_dvir)``.
     """
     b_ov = np.ascontiguousarray(b_ov, dtype=np.float64)
@@ -171,11 +175,11 @@ def energy_gamma_deps(b_ov, eps_occ, eps_vir, i_block=None):
     naux = b_ov.shape[0]
     nocc, nvir = len(eps_occ), len(eps_vir)
     nov = nocc * nvir
-    gamma = np.empty((naux, nov))
+    gamma = np.zeros((naux, nov))
     de_docc = np.zeros(nocc)
     de_dvir = np.zeros(nvir)
     e_os = e_ss = 0.0
-    for i in range(nocc):
+    for i in (range(nocc) if occ is None else occ):
         g = (b_ov[:, i * nvir:(i + 1) * nvir].T @ b_ov).reshape(nvir, nocc, nvir)  # g[a,j,b]
         gs = g.transpose(2, 1, 0)                                                # g[b,j,a] at [a,j,b]
         denom = (eps_occ[i] + eps_occ[None, :, None]
