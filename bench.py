@@ -35,8 +35,8 @@ if ROOT not in sys.path:
 
 RIMP2 = dict(naux=4800, nocc=120, nvir=1100)
 DFJK = dict(n=600, naux=2400, nocc=60)
-PREC_NAMES = {"f64": 0, "mixed": 1, "mixed_x6": 2}
-EXECUTED_PRODUCTS = {"f64": 1, "mixed": 3, "mixed_x6": 6}
+PREC_NAMES = {"f64": 0, "mixed": 1, "mixed_fast": 2}
+EXECUTED_PRODUCTS = {"f64": 1, "mixed": 6, "mixed_fast": 3}
 
 
 def step_flops():
@@ -248,7 +248,8 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--precision", choices=["auto", "f64", "mixed", "mixed_x6"], default="auto")
+    ap.add_argument("--precision", choices=["auto", "f64", "mixed"], default="auto")
+    ap.add_argument("--no-plain", action="store_true", help="skip the one FP64-plain reference step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--size", choices=["full", "small"], default="full",
@@ -308,7 +309,7 @@ def main():
     _lib.init(local)
     prec = args.precision
     if prec == "auto":
-        prec = os.environ.get("FERRIC_BENCH_PRECISION", "mixed_x6")
+        prec = os.environ.get("FERRIC_BENCH_PRECISION", "mixed")
         try:  # the split-BF16 kernels; FP64 plain when this build has none
             tb = torch.zeros((64, 2), dtype=torch.float64, device=dev)
             rimp2.rimp2_energy(tb, torch.zeros(1, dtype=torch.float64, device=dev) - 1,
@@ -321,7 +322,12 @@ def main():
     gamma = torch.empty_like(inp["b_ov"])
     d_o = torch.empty_like(inp["eo"])
     d_v = torch.empty_like(inp["ev"])
-    jk = DfJK(inp["bjk"], layout="square", precision=prec)
+    dfjk_prec = prec
+    try:
+        jk = DfJK(inp["bjk"], layout="square", precision=prec)
+    except _lib.FcError:
+        dfjk_prec = "f64"  # this build has no split-BF16 DF-JK kernels: FP64 on the device, reported
+        jk = DfJK(inp["bjk"], layout="square", precision="f64")
     jbuf = torch.empty_like(inp["d"])
     kbuf = torch.empty_like(inp["d"])
     stream = torch.cuda.current_stream(dev)
@@ -393,6 +399,32 @@ def main():
                 "peak": peaks["hbm_gbs"], "unit": "GB/s"}
     roof_dfj["frac"] = roof_dfj["achieved"] / roof_dfj["peak"]
 
+    # ---- one FP64-plain step on the same inputs (the "mixed vs FP64 plain" ratio)
+    plain = None
+    if prec != "f64" and not args.no_plain:
+        sp_r, sp_j, sp_k = {}, {}, {}
+        jk64 = DfJK(inp["bjk"], layout="square", precision="f64")
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        sc64, g64, _, _ = rimp2.rimp2_energy_grad(inp["b_ov"], inp["eo"], inp["ev"], precision="f64", stats=sp_r)
+        j64 = jk64.j(inp["d"], stats=sp_j)
+        k64 = jk64.k_from_occ(inp["c"], stats=sp_k)
+        p1.record(stream)
+        torch.cuda.synchronize()
+        pms = p0.elapsed_time(p1)
+        plain = {"ms_per_step": pms, "value": flops["total"] / (pms * 1e-3) / 1e12, "unit": "TFLOP/s",
+                 "speedup_mixed_vs_plain": pms / ms_step,
+                 "components_ms": {"rimp2_e_grad": sp_r["kernel_ms"], "dfj": sp_j["kernel_ms"],
+                                   "dfk": sp_k["kernel_ms"]},
+                 "mixed_error": {"e_total_abs": (sc.e_os + sc.e_ss) - sc64.e_total,
+                                 "e_total_rel": ((sc.e_os + sc.e_ss) - sc64.e_total) / abs(sc64.e_total),
+                                 "gamma_max_rel": float((gamma - g64).abs().max() / g64.abs().max()),
+                                 "j_max_abs": float((jbuf - j64).abs().max()),
+                                 "k_max_abs": float((kbuf - k64).abs().max())}}
+        del g64, j64, k64
+        jk64.close()
+
     # ---- e2e through the host-array C ABI, pinned host buffers
     e2e = None
     if not args.no_e2e:
@@ -451,13 +483,15 @@ def main():
             "metric": "RI-MP2 E+grad & DF-JK step throughput (algorithmic TFLOP/s)",
             "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": {"f64": "f64", "mixed": "bf16x3 split (f32 acc, f64 epilogue)",
-                      "mixed_x6": "bf16x6 split (f32 acc, f64 epilogue)"}[prec],
-            "precision": prec, "data": "synthetic (seeded, generated on device)", "config": config,
+            "dtype": {"f64": "f64",
+                      "mixed": "bf16 x3 integer slices, 6 products, exact f32 accumulation, f64 epilogue"}[prec],
+            "precision": prec, "dfjk_precision": dfjk_prec,
+            "data": "synthetic (seeded, generated on device)", "config": config,
             "components_ms": {"rimp2_e_grad": last["rimp2"]["kernel_ms"], "dfj": last["dfj"]["kernel_ms"],
                               "dfk": last["dfk"]["kernel_ms"]},
             "flops": flops, "energy": {"e_os": sc.e_os, "e_ss": sc.e_ss},
             "roofline": roofline, "roofline_dfj": roof_dfj,
+            "plain_f64": plain,
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
         }
         print(json.dumps(out))

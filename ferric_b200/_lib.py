@@ -18,7 +18,7 @@ STATUS_NAMES = {
     5: "FC_ERR_LAYOUT", 6: "FC_ERR_CUDA", 7: "FC_ERR_KERNEL", 8: "FC_ERR_RANGE", 9: "FC_ERR_TIMEOUT",
     10: "FC_ERR_INVALID",
 }
-PRECISIONS = {"f64": 0, "mixed": 1, "mixed_x6": 2}
+PRECISIONS = {"f64": 0, "mixed": 1, "mixed_fast": 2}
 LAYOUTS = {"square": 0, "packed_lower": 1}
 
 # Every symbol include/ferric_cuda.h declares, with its ctypes signature.

@@ -23,7 +23,7 @@ fc_status check_shapes(const void* b_ov, int64_t naux, int64_t nocc, int64_t nvi
         return fail(FC_ERR_LAYOUT, "RI-MP2: naux*nocc*nvir overflows");
     if (nocc > 1 << 20 || nvir > 1 << 24) return fail(FC_ERR_LAYOUT, "RI-MP2: nocc/nvir out of range");
     if (nov && naux && (!b_ov || !eo || !ev)) return fail(FC_ERR_INVALID, "RI-MP2: null input pointer");
-    if (precision < FC_PREC_F64 || precision > FC_PREC_MIXED_X6)
+    if (precision < FC_PREC_F64 || precision > FC_PREC_MIXED_FAST)
         return fail(FC_ERR_INVALID, "RI-MP2: unknown precision " + std::to_string(precision));
     if (has_kappa && precision != FC_PREC_F64)
         return fail(FC_ERR_INVALID,
@@ -50,7 +50,8 @@ int64_t chunk_budget() {
 fc_status energy_dispatch(const Rimp2Dev& d, int32_t precision, cudaStream_t st, double* e_os,
                           double* e_ss, fc_stats* stats) {
     if (precision == FC_PREC_F64) return rimp2_energy_f64(d, st, e_os, e_ss, stats);
-    return rimp2_energy_mixed(d, precision == FC_PREC_MIXED ? 2 : 3, st, e_os, e_ss, stats);
+    if (precision == FC_PREC_MIXED) return rimp2_energy_fx(d, st, e_os, e_ss, stats);
+    return rimp2_energy_mixed(d, 2, st, e_os, e_ss, stats);
 }
 
 fc_status grad_dispatch(const Rimp2Dev& d, int32_t precision, cudaStream_t st, double* e_os,
@@ -58,8 +59,8 @@ fc_status grad_dispatch(const Rimp2Dev& d, int32_t precision, cudaStream_t st, d
                         fc_stats* stats) {
     if (precision == FC_PREC_F64)
         return rimp2_grad_f64(d, st, e_os, e_ss, gamma, de_docc, de_dvir, stats);
-    return rimp2_grad_mixed(d, precision == FC_PREC_MIXED ? 2 : 3, st, e_os, e_ss, gamma, de_docc,
-                            de_dvir, stats);
+    if (precision == FC_PREC_MIXED) return rimp2_grad_fx(d, st, e_os, e_ss, gamma, de_docc, de_dvir, stats);
+    return fail(FC_ERR_KERNEL, "FC_PREC_MIXED_FAST has no adjoint kernel; use FC_PREC_MIXED");
 }
 
 }  // namespace
@@ -159,7 +160,7 @@ fc_status fc_rimp2_energy_grad(const double* b_ov, int64_t naux, int64_t nocc, i
     FC_TRY(ws_get(WS_B, nel * 8, &db));
     FC_TRY(ws_get(WS_EPS, (nocc + nvir) * 8, &de));
     FC_TRY(ws_get(WS_GAMMA, nel * 8, &dg));
-    FC_TRY(ws_get(WS_MISC, (nocc + nvir) * 8, &dd));
+    FC_TRY(ws_get(WS_HOSTOUT, (nocc + nvir) * 8, &dd));
     FC_CUDA(cudaMemcpyAsync(db, b_ov, nel * 8, cudaMemcpyHostToDevice, st));
     FC_CUDA(cudaMemcpyAsync(de, eps_occ, nocc * 8, cudaMemcpyHostToDevice, st));
     FC_CUDA(cudaMemcpyAsync((double*)de + nocc, eps_vir, nvir * 8, cudaMemcpyHostToDevice, st));

@@ -291,7 +291,7 @@ fc_status create_common(const double* b, int64_t naux, int64_t n, int32_t layout
     if (!b) return fail(FC_ERR_INVALID, "fc_dfjk_create: null tensor");
     if (layout != FC_LAYOUT_SQUARE && layout != FC_LAYOUT_PACKED_LOWER)
         return fail(FC_ERR_INVALID, "fc_dfjk_create: unknown layout");
-    if (precision < FC_PREC_F64 || precision > FC_PREC_MIXED_X6)
+    if (precision < FC_PREC_F64 || precision > FC_PREC_MIXED_FAST)
         return fail(FC_ERR_INVALID, "fc_dfjk_create: unknown precision");
     int64_t nn, pair = n * (n + 1) / 2, bytes_sq = 0, bytes_pk;
     if (!mul_ok(n, n, &nn) || !mul_ok(nn, naux, &bytes_sq) || !mul_ok(bytes_sq, 8, &bytes_sq))

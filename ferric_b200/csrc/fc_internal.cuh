@@ -45,17 +45,22 @@ struct Workspace {
     size_t bytes = 0;
 };
 
+// Each slot has one owner per call path, so no call frees memory another
+// part of the same call still uses.
 enum WsSlot {
-    WS_B = 0,      // uploaded B_ov / operand
-    WS_EPS,        // orbital energies
-    WS_PAIRS,      // pair table
+    WS_B = 0,      // host API: uploaded B_ov, or D/J, C/K staging
+    WS_EPS,        // host API: orbital energies
+    WS_GAMMA,      // host API: gamma
+    WS_HOSTOUT,    // host API: dE/deps outputs
+    WS_PAIRS,      // pair tables (+ Q-row scales of the adjoint split)
     WS_PART,       // per-tile partials
-    WS_OUT,        // small outputs
-    WS_GAMMA,      // gamma (host API)
-    WS_T,          // amplitude chunk (Tt rows)
-    WS_SPLIT,      // split-BF16 operand copies
-    WS_SPLIT2,
-    WS_MISC,
+    WS_OUT,        // small results and error flags
+    WS_T,          // amplitude chunk (FP64 or FP32) + row scales
+    WS_TS,         // amplitude chunk slices
+    WS_SPLIT,      // split-BF16 pair operands
+    WS_SPLIT2,     // split-BF16 adjoint operand (Q rows)
+    WS_SCALE,      // column maxima + operand-row scales
+    WS_MISC,       // DF-J weights / d_P, DF-K C^T
     WS_COUNT
 };
 

@@ -5,13 +5,6 @@
 #include "dfjk.cuh"
 
 namespace fc {
-fc_status rimp2_energy_mixed(const Rimp2Dev&, int, cudaStream_t, double*, double*, fc_stats*) {
-    return fail(FC_ERR_KERNEL, "split-BF16 RI-MP2 energy kernel not available in this build");
-}
-fc_status rimp2_grad_mixed(const Rimp2Dev&, int, cudaStream_t, double*, double*, double*, double*,
-                           double*, fc_stats*) {
-    return fail(FC_ERR_KERNEL, "split-BF16 RI-MP2 gradient kernel not available in this build");
-}
 fc_status dfjk_prepare_mixed(fc_dfjk*, cudaStream_t) {
     return fail(FC_ERR_KERNEL, "split-BF16 DF-JK kernels not available in this build");
 }

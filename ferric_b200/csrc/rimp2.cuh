@@ -19,12 +19,14 @@ fc_status rimp2_energy_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, dou
 fc_status rimp2_grad_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, double* e_ss,
                          double* gamma, double* de_docc, double* de_dvir, fc_stats* stats);
 
-// Split-BF16 (tcgen05) kernel set; `terms` = 2 (hi+lo, 3 products) or
-// 3 (hi+mid+lo, 6 products).
+// Split-BF16 (tcgen05) kernel sets.  _fx: integer-valued slices with exact
+// FP32 accumulation (FC_PREC_MIXED).  _mixed: floating hi+lo split, 3
+// products, FP32 accumulation (FC_PREC_MIXED_FAST; energy only).
 fc_status rimp2_energy_mixed(const Rimp2Dev& d, int terms, cudaStream_t st, double* e_os,
                              double* e_ss, fc_stats* stats);
-fc_status rimp2_grad_mixed(const Rimp2Dev& d, int terms, cudaStream_t st, double* e_os,
-                           double* e_ss, double* gamma, double* de_docc, double* de_dvir,
-                           fc_stats* stats);
+fc_status rimp2_energy_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double* e_ss,
+                          fc_stats* stats);
+fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double* e_ss, double* gamma,
+                        double* de_docc, double* de_dvir, fc_stats* stats);
 
 }  // namespace fc

@@ -1,0 +1,35 @@
+// TMA tensor-map encoding through the driver entry point (no link-time
+// dependency on libcuda).
+#include <cudaTypedefs.h>
+
+#include "fc_internal.cuh"
+#include "tmap.cuh"
+
+namespace fc {
+
+fc_status make_tmap_bf16_2d(CUtensorMap* map, const void* base, uint64_t inner, uint64_t outer,
+                            uint64_t row_bytes, uint32_t box_inner, uint32_t box_outer) {
+    static PFN_cuTensorMapEncodeTiled_v12000 enc = nullptr;
+    if (!enc) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn)
+            return fail(FC_ERR_DRIVER, "cuTensorMapEncodeTiled is not available from the driver");
+        enc = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    if ((reinterpret_cast<uintptr_t>(base) & 15) || (row_bytes & 15))
+        return fail(FC_ERR_LAYOUT, "TMA operand base/stride not 16-byte aligned");
+    cuuint64_t dims[2] = {inner, outer};
+    cuuint64_t strides[1] = {row_bytes};
+    cuuint32_t box[2] = {box_inner, box_outer};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+        return fail(FC_ERR_LAYOUT, "cuTensorMapEncodeTiled failed with CUresult " + std::to_string((int)r));
+    return FC_OK;
+}
+
+}  // namespace fc

@@ -39,9 +39,13 @@ typedef int32_t fc_status;
 #define FC_ERR_INVALID   10  /* null pointer, bad enum, library not initialised   */
 
 /* Arithmetic of the contraction kernels. */
-#define FC_PREC_F64       0  /* all-FP64 "plain" kernels: the drop-in              */
-#define FC_PREC_MIXED     1  /* split-BF16: hi+lo operands, 3 tensor-core products */
-#define FC_PREC_MIXED_X6  2  /* split-BF16: hi+mid+lo operands, 6 products        */
+#define FC_PREC_F64        0  /* all-FP64 "plain" kernels: the drop-in             */
+#define FC_PREC_MIXED      1  /* split-BF16, exact accumulation: each operand row   */
+                              /* scaled by a power of two and split into 3 bf16    */
+                              /* slices holding integers; 6 tensor-core products   */
+                              /* into 3 FP32 accumulators that never round         */
+#define FC_PREC_MIXED_FAST 2  /* split-BF16 hi+lo, 3 products, FP32 accumulation   */
+                              /* (energy only; ~1e-5 relative, accumulation-bound) */
 
 /* Storage layout of the 3-index tensor handed to fc_dfjk_create. */
 #define FC_LAYOUT_SQUARE        0  /* (naux, n, n), symmetric in (mu, nu)          */

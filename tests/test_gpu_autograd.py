@@ -50,3 +50,27 @@ def test_no_grad_forward_is_energy_only(fc):
                               torch.from_numpy(ev).cuda(), "f64")
     ref = orc.spin_components(b, np.concatenate([eo, ev]), 5, 23)[2]
     assert abs(e.item() - ref) < 1e-10
+
+
+def test_autograd_mixed_matches_fd_of_fp64_oracle(fc):
+    import torch
+    from ferric_b200.torch_ops import RiMp2Energy
+    naux, nocc, nvir = 150, 6, 45
+    b, eo, ev = synthetic.rimp2_inputs(naux, nocc, nvir)
+    tb = torch.from_numpy(b).cuda().requires_grad_(True)
+    to = torch.from_numpy(eo).cuda().requires_grad_(True)
+    tv = torch.from_numpy(ev).cuda().requires_grad_(True)
+    e = RiMp2Energy.apply(tb, to, tv, "mixed")
+    e.backward()
+    gb = tb.grad.cpu().numpy()
+    eps = np.concatenate([eo, ev])
+    ref = orc.spin_components(b, eps, nocc, nvir)[2]
+    assert abs(e.item() - ref) <= 5e-8 * abs(ref)
+    h = 1e-5
+    rows, cols = synthetic.fd_entries(naux, nocc * nvir, count=16)
+    scale = np.abs(gb).max()
+    for p, ia in zip(rows, cols):
+        bp = b.copy(); bp[p, ia] += h
+        bm = b.copy(); bm[p, ia] -= h
+        fd = (orc.spin_components(bp, eps, nocc, nvir)[2] - orc.spin_components(bm, eps, nocc, nvir)[2]) / (2 * h)
+        assert abs(fd - gb[p, ia]) <= 1e-5 * scale

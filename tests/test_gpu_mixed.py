@@ -1,0 +1,138 @@
+"""Split-BF16 RI-MP2 kernels (tcgen05) against the FP64 oracle and against an
+exact NumPy emulation of the split algorithm.
+
+FC_PREC_MIXED slices every operand row into three bf16 integers at a power-of-
+two scale; the tensor-core sums of integer products stay below 2^24 and are
+exact in FP32, so the device energy must equal the emulation (slices in
+NumPy, integer products summed exactly in FP64) to FP64 rounding, and the FP64
+oracle to the slice truncation error (~1e-9 relative measured on B200).
+"""
+import numpy as np
+import pytest
+
+from oracle import rimp2 as orc
+from oracle import synthetic
+
+pytestmark = pytest.mark.gpu
+
+# error bounds of the split (measured max x 5): energy, Gamma (max-normalised), dE/deps
+MIXED_E_REL = 5e-8
+MIXED_G_REL = 1e-5
+MIXED_D_REL = 1e-6
+FAST_E_REL = 2e-4     # hi+lo, FP32 accumulation (accumulation-bound)
+
+
+def emulate_fixed_slices(b):
+    """The FC_PREC_MIXED split of every column of b (power-of-two scale with
+    max|x|/s in [64, 128), three integer slices) and the exact level sums."""
+    mx = np.abs(b).max(axis=0)
+    k = np.frexp(np.where(mx > 0, mx, 1.0))[1]
+    s = np.ldexp(1.0, k - 7)
+    s = np.where(mx > 0, s, 1.0)
+    y = b / s[None, :]
+    c1 = np.rint(y)
+    y2 = (y - c1) * 256.0
+    c2 = np.rint(y2)
+    c3 = np.rint((y2 - c2) * 256.0)
+    assert np.abs(c1).max() <= 128 and np.abs(c2).max() <= 128 and np.abs(c3).max() <= 128
+    l0 = c1.T @ c1
+    l1 = c1.T @ c2 + c2.T @ c1
+    l2 = c1.T @ c3 + c2.T @ c2 + c3.T @ c1
+    return np.outer(s, s) * (l0 + l1 / 256.0 + l2 / 65536.0)
+
+
+def energy_from_g(g, eo, ev):
+    nocc, nvir = len(eo), len(ev)
+    e_os = e_ss = 0.0
+    for i in range(nocc):
+        for j in range(nocc):
+            blk = g[i * nvir:(i + 1) * nvir, j * nvir:(j + 1) * nvir]
+            d = eo[i] + eo[j] - ev[:, None] - ev[None, :]
+            e_os += np.sum(blk * blk / d)
+            e_ss += np.sum(blk * (blk - blk.T) / d)
+    return e_os, e_ss
+
+
+SHAPES = [(96, 5, 23), (84, 5, 19), (200, 7, 65), (300, 4, 130), (130, 3, 128), (480, 12, 110)]
+
+
+@pytest.mark.parametrize("naux,nocc,nvir", SHAPES)
+def test_mixed_energy_matches_oracle_and_emulation(fc, naux, nocc, nvir):
+    from ferric_b200 import rimp2
+    b, eo, ev = synthetic.rimp2_inputs(naux, nocc, nvir)
+    ref = orc.spin_components(b, np.concatenate([eo, ev]), nocc, nvir)
+    st = {}
+    e_os, e_ss = rimp2.rimp2_energy(b, eo, ev, precision="mixed", stats=st)
+    assert st["precision"] == 1 and st["launches"] > 0
+    assert abs(e_os + e_ss - ref[2]) <= MIXED_E_REL * abs(ref[2]) + 1e-12
+    em = energy_from_g(emulate_fixed_slices(b), eo, ev)
+    # exact accumulation: device == emulation to FP64 summation rounding
+    assert abs(e_os - em[0]) <= 1e-12 * abs(em[0]) + 1e-15
+    assert abs(e_ss - em[1]) <= 1e-12 * abs(em[0]) + 1e-15
+
+
+@pytest.mark.parametrize("naux,nocc,nvir", [(96, 5, 23), (200, 7, 65), (300, 4, 130)])
+def test_mixed_gradient_matches_oracle(fc, naux, nocc, nvir):
+    from ferric_b200 import rimp2
+    b, eo, ev = synthetic.rimp2_inputs(naux, nocc, nvir)
+    e_os, e_ss, gamma, d_o, d_v = orc.energy_gamma_deps(b, eo, ev)
+    sc, g, go, gv = rimp2.rimp2_energy_grad(b, eo, ev, precision="mixed")
+    assert abs(sc.e_total - (e_os + e_ss)) <= MIXED_E_REL * abs(e_os + e_ss) + 1e-12
+    assert np.abs(g - gamma).max() <= MIXED_G_REL * np.abs(gamma).max()
+    assert np.abs(go - d_o).max() <= MIXED_D_REL * np.abs(d_o).max()
+    assert np.abs(gv - d_v).max() <= MIXED_D_REL * np.abs(d_v).max()
+    # the gradient call's energy is the energy call's energy
+    e2 = rimp2.rimp2_energy(b, eo, ev, precision="mixed")
+    assert abs(sum(e2) - sc.e_total) <= 1e-13 * abs(sc.e_total)
+
+
+def test_mixed_gradient_chunked(fc, monkeypatch):
+    from ferric_b200 import rimp2
+    b, eo, ev = synthetic.rimp2_inputs(160, 9, 40)
+    one = rimp2.rimp2_energy_grad(b, eo, ev, precision="mixed")
+    monkeypatch.setenv("FERRIC_CUDA_CHUNK_BYTES", str(2 * 128 * 9 * 128 * 10))
+    many = rimp2.rimp2_energy_grad(b, eo, ev, precision="mixed")
+    assert abs(one[0].e_total - many[0].e_total) <= 1e-14 * abs(one[0].e_total)
+    assert np.array_equal(one[1], many[1])
+    assert np.array_equal(one[2], many[2])
+
+
+def test_mixed_deterministic(fc):
+    from ferric_b200 import rimp2
+    b, eo, ev = synthetic.rimp2_inputs(200, 7, 65)
+    r = [rimp2.rimp2_energy(b, eo, ev, precision="mixed") for _ in range(3)]
+    assert r[0] == r[1] == r[2]
+    g1 = rimp2.rimp2_energy_grad(b, eo, ev, precision="mixed")
+    g2 = rimp2.rimp2_energy_grad(b, eo, ev, precision="mixed")
+    assert np.array_equal(g1[1], g2[1])
+
+
+@pytest.mark.parametrize("naux,nocc,nvir", [(96, 5, 23), (200, 7, 65), (480, 12, 110)])
+def test_mixed_fast_energy(fc, naux, nocc, nvir):
+    from ferric_b200 import rimp2
+    b, eo, ev = synthetic.rimp2_inputs(naux, nocc, nvir)
+    ref = orc.spin_components(b, np.concatenate([eo, ev]), nocc, nvir)
+    e = rimp2.rimp2_energy(b, eo, ev, precision="mixed_fast")
+    assert abs(sum(e) - ref[2]) <= FAST_E_REL * abs(ref[2])
+
+
+def test_mixed_refuses_nonfinite(fc):
+    import ferric_b200._lib as L
+    from ferric_b200 import rimp2
+    b, eo, ev = synthetic.rimp2_inputs(96, 5, 23)
+    b[3, 7] = np.inf
+    with pytest.raises(L.FcError) as ei:
+        rimp2.rimp2_energy(b, eo, ev, precision="mixed")
+    assert ei.value.name == "FC_ERR_RANGE"
+    # the dispatcher retries in FP64 on the device; FP64 then sees the inf too
+    sc = rimp2.try_spin_components_on_device(b, np.concatenate([eo, ev]), 5, 23, mixed_ok=True)
+    assert sc is None or not np.isfinite(sc.e_total)
+
+
+def test_mixed_fast_has_no_adjoint(fc):
+    import ferric_b200._lib as L
+    from ferric_b200 import rimp2
+    b, eo, ev = synthetic.rimp2_inputs(96, 5, 23)
+    with pytest.raises(L.FcError) as ei:
+        rimp2.rimp2_energy_grad(b, eo, ev, precision="mixed_fast")
+    assert ei.value.name == "FC_ERR_KERNEL"
