@@ -10,8 +10,15 @@ mirror of ferric's entry points for that path:
 * :mod:`ferric_b200.dfjk`      -- ``DfJ`` / ``DfK`` builders (``JBuilder`` / ``KBuilder``);
 * :mod:`ferric_b200.torch_ops` -- ``RiMp2Energy`` autograd function.
 
-Importing the package loads the library; a missing library is an ImportError.
+Importing any of those modules loads the library; a missing library is an
+ImportError.  The package itself imports nothing, so ``ferric_b200.build`` can
+(re)build the library in a process that has not loaded it.
 """
-from ._lib import FcError, FcStats, init, last_error  # noqa: F401
-
 __version__ = "0.1.0"
+
+
+def __getattr__(name):
+    if name in ("FcError", "FcStats", "init", "last_error"):
+        from . import _lib
+        return getattr(_lib, name)
+    raise AttributeError(name)
