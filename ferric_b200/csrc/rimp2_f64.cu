@@ -437,4 +437,108 @@ fc_status rimp2_grad_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, doubl
     return FC_OK;
 }
 
+// ------------------------------------------------ allocation-free energy --
+//
+// fc_rimp2_energy_noalloc: the FP64 RI-MP2 energy with all of its scratch
+// (pair table, per-tile partials, the two reduced sums) in one fixed
+// device array that lives in this library's module, so the call allocates
+// no device memory.  It exists for callers that cannot call cudaMalloc: code
+// whose device memory is owned by another allocator (ferric's device-pool
+// ledger charges every byte to a reservation and refuses beyond it; a
+// framework's caching allocator may hold nearly all of the device), and
+// inner-loop code that must not pay cudaMalloc/cudaFree's implicit device
+// synchronisation.  Limits and sharing rules are in include/ferric_cuda.h.
+
+namespace {
+
+constexpr size_t kNoallocScratchBytes = size_t(4) << 20;  // 4 MiB, held by every device that loads the library
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratchBytes];
+
+constexpr int kNoallocMaxDevices = 64;
+void* g_noalloc_ptr[kNoallocMaxDevices] = {};  // device address of g_noalloc_scratch, per ordinal
+std::mutex g_noalloc_mu;
+
+// Unordered pairs (i <= j) in row-major order, one thread per i.
+__global__ void noalloc_pairs_kernel(int nocc, int2* pairs) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nocc) return;
+    const int64_t off = (int64_t)i * nocc - (int64_t)i * (i - 1) / 2;
+    for (int j = i; j < nocc; ++j) pairs[off + (j - i)] = make_int2(i, j);
+}
+
+}  // namespace
+
 }  // namespace fc
+
+extern "C" fc_status fc_rimp2_energy_noalloc(const double* b_ov, int64_t naux, int64_t nocc, int64_t nvir,
+                                             const double* eps_occ, const double* eps_vir, int32_t has_kappa,
+                                             double kappa, double* e_os, double* e_ss, void* stream) {
+    using namespace fc;
+    if (!e_os || !e_ss) return fail(FC_ERR_INVALID, "fc_rimp2_energy_noalloc: null output pointer");
+    if (naux < 0 || nocc < 0 || nvir < 0) return fail(FC_ERR_LAYOUT, "fc_rimp2_energy_noalloc: negative dimension");
+    if (has_kappa && !(kappa > 0.0 && kappa < 1e300))
+        return fail(FC_ERR_INVALID, "fc_rimp2_energy_noalloc: kappa must be finite and > 0");
+    if (naux == 0 || nocc == 0 || nvir == 0) {
+        *e_os = 0.0;
+        *e_ss = 0.0;
+        return FC_OK;
+    }
+    if (!b_ov || !eps_occ || !eps_vir) return fail(FC_ERR_INVALID, "fc_rimp2_energy_noalloc: null input pointer");
+    if (nocc > (1 << 20) || nvir > (1 << 24) || naux > INT32_MAX)
+        return fail(FC_ERR_LAYOUT, "fc_rimp2_energy_noalloc: dimension out of range");
+    const int64_t npairs = nocc * (nocc + 1) / 2;
+    const int64_t ntile = (nvir + PR_T - 1) / PR_T;
+    const int64_t items = npairs * ntile * ntile;
+    const size_t pair_bytes = ((size_t)npairs * sizeof(int2) + 255) / 256 * 256;
+    const size_t part_bytes = ((size_t)items * 2 * sizeof(double) + 255) / 256 * 256;
+    const size_t need = pair_bytes + part_bytes + 256;
+    if (items > INT32_MAX || need > kNoallocScratchBytes)
+        return fail(FC_ERR_LAYOUT,
+                    "fc_rimp2_energy_noalloc: needs " + std::to_string(need) + " B of scratch for " +
+                        std::to_string(items) + " pair tiles; the fixed scratch holds " +
+                        std::to_string(kNoallocScratchBytes) + " B (about " +
+                        std::to_string((kNoallocScratchBytes - 512) / 16) +
+                        " tiles of 64 x 64 virtuals); use fc_rimp2_energy_dev");
+
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    int dev = -1;
+    FC_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoallocMaxDevices) return fail(FC_ERR_DEVICE, "fc_rimp2_energy_noalloc: device ordinal out of range");
+    if (!g_noalloc_ptr[dev]) {
+        // once per device, with that device current
+        void* p = nullptr;
+        FC_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        FC_CUDA(cudaFuncSetAttribute(pair_f64_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, PR_SMEM));
+        g_noalloc_ptr[dev] = p;
+    }
+    char* base = static_cast<char*>(g_noalloc_ptr[dev]);
+    int2* pairs = reinterpret_cast<int2*>(base);
+    double* part = reinterpret_cast<double*>(base + pair_bytes);
+    double* out = reinterpret_cast<double*>(base + pair_bytes + part_bytes);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+
+    // Every byte read below is written earlier in this call (pairs, then all
+    // partials, then the sums), so contents left by a previous call are never read.
+    noalloc_pairs_kernel<<<(unsigned)((nocc + 127) / 128), 128, 0, st>>>((int)nocc, pairs);
+    PairArgs a{};
+    a.B = b_ov;
+    a.ldb = nocc * nvir;
+    a.naux = (int)naux;
+    a.nvir = (int)nvir;
+    a.eo = eps_occ;
+    a.ev = eps_vir;
+    a.pairs = pairs;
+    a.ntile = (int)ntile;
+    a.has_kappa = has_kappa;
+    a.kappa = kappa;
+    a.part = part;
+    pair_f64_kernel<0><<<(unsigned)items, 256, PR_SMEM, st>>>(a);
+    reduce_pairs_kernel<<<1, 1024, 0, st>>>(part, items, out);
+    FC_TRY(check_launch("fc_rimp2_energy_noalloc kernels"));
+    double h[2];
+    FC_CUDA(cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, st));
+    FC_CUDA(cudaStreamSynchronize(st));
+    *e_os = h[0];
+    *e_ss = h[1];
+    return FC_OK;
+}

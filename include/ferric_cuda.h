@@ -120,6 +120,30 @@ fc_status fc_rimp2_energy_grad_dev(const double* b_ov, int64_t naux, int64_t noc
                                    double* de_docc, double* de_dvir, void* stream,
                                    fc_stats* stats);
 
+/* FP64 RI-MP2 energy that allocates no device memory.  No counterpart in the
+ * reference: it is for callers that cannot call cudaMalloc -- callers whose
+ * device memory belongs to another allocator (ferric's device-pool ledger
+ * charges every byte to a reservation and refuses past it; a framework's
+ * caching allocator may hold nearly all of the device) and inner loops that
+ * must not take cudaMalloc/cudaFree's implicit device synchronisation.
+ * Arguments are device pointers as in fc_rimp2_energy_dev; e_os/e_ss are host
+ * scalars; the call synchronises `stream` (NULL = the legacy default stream)
+ * and does not need fc_init.  Its scratch is a fixed 4 MiB array inside the
+ * library, held by every device that loads the library until the process
+ * exits; problems needing more (about 262,000 tiles of 64 x 64 virtual
+ * indices, i.e. nocc(nocc+1)/2 * ceil(nvir/64)^2) are refused with
+ * FC_ERR_LAYOUT.  The first call on a device looks up the array's device
+ * address and sets the kernel's shared-memory limit; make that first call
+ * before any stream capture.  All calls on a device share the one array
+ * (each call writes every byte it later reads, so earlier contents do not
+ * matter): calls that overlap on the GPU, e.g. from two streams or two
+ * threads' streams, race.  Calls within one process are serialised on the
+ * host. */
+fc_status fc_rimp2_energy_noalloc(const double* b_ov, int64_t naux, int64_t nocc, int64_t nvir,
+                                  const double* eps_occ, const double* eps_vir,
+                                  int32_t has_kappa, double kappa,
+                                  double* e_os, double* e_ss, void* stream);
+
 /* ---- DF-JK ----------------------------------------------------------------
  * A handle owns the device copy of the 3-index tensor for the lifetime of a
  * builder (the reference's per-builder DeviceSlot, ferric-scf/src/df_j_gpu.rs:1-5,
