@@ -1,0 +1,79 @@
+"""Generate the golden fixtures of the RI-MP2 / DF-JK parity tests.
+
+Runs the oracle's own integral engine and RHF (oracle/integrals.py, oracle/scf.py)
+on the reference's validation molecules and writes, per system, the RI-MP2
+inputs (dressed B_ov, orbital energies) and the reference's golden energies
+(PySCF 2.13.1 numbers from the reference's testdata/reference/validation JSONs)
+into ``<name>.npz``.  The device tests read only these fixtures.
+
+    python tests/golden/make_golden.py [name ...]
+
+Needs the reference mount for the basis JSONs and golden JSONs.
+"""
+from __future__ import annotations
+
+import json
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import basis, integrals, scf  # noqa: E402
+from oracle import rimp2 as orc  # noqa: E402
+
+REF = "/root/reference/testdata/reference/validation"
+SYSTEMS = {
+    # name: (golden json, basis, aux basis, kappa json or None, JK-fit basis for the DF-JK SCF or None)
+    "h2o_ccpvdz": ("sos_mp2/h2o_cc-pvdz.json", "cc-pvdz", "cc-pvdz-ri", "kappa_mp2/h2o_cc-pvdz.json", "cc-pvtz-jkfit"),
+    "ch4_ccpvdz": ("sos_mp2/ch4_cc-pvdz.json", "cc-pvdz", "cc-pvdz-ri", "kappa_mp2/ch4_cc-pvdz.json", None),
+    "h2o_augccpvdz": ("sos_mp2/h2o_aug_aug-cc-pvdz.json", "aug-cc-pvdz", "aug-cc-pvdz-rifit", None, None),
+}
+
+
+def build(name):
+    gfile, bas, aux, kfile, jkfit = SYSTEMS[name]
+    g = json.load(open(os.path.join(REF, gfile)))
+    atoms = [(s, (x, y, z)) for s, x, y, z in g["provenance"]["geometry_bohr"]]
+    zs = [basis.SYMBOLS[s] for s, _ in atoms]
+    rs = [c for _, c in atoms]
+    t0 = time.time()
+    sh = basis.shells_for(atoms, bas)
+    S, T = integrals.overlap_kinetic(sh)
+    V = integrals.nuclear(sh, zs, rs)
+    eri = integrals.eri4(sh)
+    enuc = scf.nuclear_repulsion(zs, rs)
+    nocc = int(g["nocc"])
+    e_rhf, eps, C = scf.rhf(S, T + V, nocc, enuc, scf.exact_jk(eri))
+    b, _, _ = scf.dressed(basis.shells_for(atoms, aux), sh)
+    bov = scf.b_ov(b, C, nocc)
+    nvir = C.shape[1] - nocc
+    e_os, e_ss, _ = orc.spin_components(bov, eps, nocc, nvir)
+    out = dict(b_ov=bov, eps=eps, nocc=nocc, nvir=nvir,
+               golden_e_rhf=g["e_rhf"], golden_e_os=g["dfmp2"]["e_os"], golden_e_ss=g["dfmp2"]["e_ss"],
+               oracle_e_rhf=e_rhf, oracle_e_os=e_os, oracle_e_ss=e_ss)
+    if kfile:
+        k = json.load(open(os.path.join(REF, kfile)))
+        out["kappa"] = np.array([r["kappa"] for r in k["kappa"]])
+        out["golden_kappa_e_os"] = np.array([r["e_os"] for r in k["kappa"]])
+        out["golden_kappa_e_ss"] = np.array([r["e_ss"] for r in k["kappa"]])
+    if jkfit:
+        # config 1: RHF with DF-JK (JK-fit basis), then RI-MP2 on its orbitals
+        bjk, _, _ = scf.dressed(basis.shells_for(atoms, jkfit), sh)
+        e_df, eps_df, c_df = scf.rhf(S, T + V, nocc, enuc, scf.df_jk(bjk))
+        bov_df = scf.b_ov(b, c_df, nocc)
+        d_os, d_ss, _ = orc.spin_components(bov_df, eps_df, nocc, nvir)
+        out.update(b_jk=bjk, b_ri=b, h_core=T + V, s=S, e_nuc=enuc, oracle_e_dfrhf=e_df,
+                   oracle_dfrhf_e_os=d_os, oracle_dfrhf_e_ss=d_ss)
+    print(f"{name}: n {C.shape[0]} naux {bov.shape[0]} E_rhf {e_rhf:.12f} (golden {g['e_rhf']:.12f}) "
+          f"E_os {e_os:.14f} (golden {g['dfmp2']['e_os']:.14f}) {time.time() - t0:.1f} s", flush=True)
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+
+
+if __name__ == "__main__":
+    for n in (sys.argv[1:] or SYSTEMS):
+        build(n)
