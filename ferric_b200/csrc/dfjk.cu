@@ -41,25 +41,27 @@ __global__ void density_weights_kernel(const double* __restrict__ d, int64_t n,
 
 // ---------------------------------------------------------- DF-J passes --
 
-__global__ void __launch_bounds__(256) dfj_pass1_kernel(const double* __restrict__ bp, int64_t pair,
+template <typename TB>
+__global__ void __launch_bounds__(256) dfj_pass1_kernel(const TB* __restrict__ bp, int64_t pair,
                                                         const double* __restrict__ w,
                                                         double* __restrict__ dp) {
     __shared__ double red[32];
-    const double* row = bp + (int64_t)blockIdx.x * pair;
+    const TB* row = bp + (int64_t)blockIdx.x * pair;
     double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
     int64_t k = threadIdx.x;
     for (; k + 768 < pair; k += 1024) {
-        s0 += row[k] * w[k];
-        s1 += row[k + 256] * w[k + 256];
-        s2 += row[k + 512] * w[k + 512];
-        s3 += row[k + 768] * w[k + 768];
+        s0 += (double)row[k] * w[k];
+        s1 += (double)row[k + 256] * w[k + 256];
+        s2 += (double)row[k + 512] * w[k + 512];
+        s3 += (double)row[k + 768] * w[k + 768];
     }
-    for (; k < pair; k += 256) s0 += row[k] * w[k];
+    for (; k < pair; k += 256) s0 += (double)row[k] * w[k];
     const double v = block_sum((s0 + s1) + (s2 + s3), red);
     if (threadIdx.x == 0) dp[blockIdx.x] = v;
 }
 
-__global__ void __launch_bounds__(256) dfj_pass2_kernel(const double* __restrict__ bp, int64_t naux,
+template <typename TB>
+__global__ void __launch_bounds__(256) dfj_pass2_kernel(const TB* __restrict__ bp, int64_t naux,
                                                         int64_t pair, const double* __restrict__ c,
                                                         int64_t rows_per_split,
                                                         double* __restrict__ part) {
@@ -70,11 +72,22 @@ __global__ void __launch_bounds__(256) dfj_pass2_kernel(const double* __restrict
     double s0 = 0.0, s1 = 0.0;
     int64_t p = p0;
     for (; p + 1 < p1; p += 2) {
-        s0 += bp[p * pair + k] * c[p];
-        s1 += bp[(p + 1) * pair + k] * c[p + 1];
+        s0 += (double)bp[p * pair + k] * c[p];
+        s1 += (double)bp[(p + 1) * pair + k] * c[p + 1];
     }
-    if (p < p1) s0 += bp[p * pair + k] * c[p];
+    if (p < p1) s0 += (double)bp[p * pair + k] * c[p];
     part[(int64_t)blockIdx.y * pair + k] = s0 + s1;
+}
+
+// FP64 -> FP32 (round to nearest) copy of the packed rows; flags values
+// outside the FP32 range (the reference's F32Range check,
+// ferric-core/src/gpu/kernels/round_f64_to_f32.cu semantics).
+__global__ void round_f32_kernel(const double* __restrict__ x, int64_t n, float* __restrict__ y, int* bad) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const double v = x[k];
+    if (!(fabs(v) <= 3.4028234663852886e38)) atomicOr(bad, 1);
+    y[k] = __double2float_rn(v);
 }
 
 __global__ void dfj_unpack_kernel(const double* __restrict__ part, int nsplit, int64_t pair, int64_t n,
@@ -183,22 +196,24 @@ static fc_status dfjk_smem_once() {
     return FC_OK;
 }
 
-fc_status dfj_build_f64(fc_dfjk* h, const double* d, double* j, cudaStream_t st, fc_stats* stats) {
+template <typename TB>
+static fc_status dfj_build_t(fc_dfjk* h, const TB* bp, int prec, const double* d, double* j, cudaStream_t st,
+                             fc_stats* stats) {
     const int64_t naux = h->naux, n = h->n, pair = h->pair;
-    void *vw, *vdp, *vpart;
+    void *vw, *vpart;
     const int nsplit = 4;
     FC_TRY(ws_get(WS_MISC, (pair + naux + 64) * 8, &vw));
     FC_TRY(ws_get(WS_PART, (int64_t)nsplit * pair * 8, &vpart));
     double* w = (double*)vw;
-    vdp = w + pair;
+    double* dp = w + pair;
     Context& c = ctx();
     if (stats) FC_CUDA(cudaEventRecord(c.ev0, st));
     density_weights_kernel<<<(unsigned)n, 128, 0, st>>>(d, n, w);
-    dfj_pass1_kernel<<<(unsigned)naux, 256, 0, st>>>(h->b_pk, pair, w, (double*)vdp);
-    if (h->l_chol) chol_solve_kernel<<<1, 1024, 0, st>>>(h->l_chol, naux, (double*)vdp);
+    dfj_pass1_kernel<TB><<<(unsigned)naux, 256, 0, st>>>(bp, pair, w, dp);
+    if (h->l_chol) chol_solve_kernel<<<1, 1024, 0, st>>>(h->l_chol, naux, dp);
     const int64_t rps = (naux + nsplit - 1) / nsplit;
     dim3 g2((unsigned)((pair + 255) / 256), nsplit);
-    dfj_pass2_kernel<<<g2, 256, 0, st>>>(h->b_pk, naux, pair, (const double*)vdp, rps, (double*)vpart);
+    dfj_pass2_kernel<TB><<<g2, 256, 0, st>>>(bp, naux, pair, dp, rps, (double*)vpart);
     dfj_unpack_kernel<<<(unsigned)((n * n + 255) / 256), 256, 0, st>>>((const double*)vpart, nsplit, pair, n, j);
     FC_TRY(check_launch("DF-J kernels"));
     if (stats) {
@@ -208,14 +223,45 @@ fc_status dfj_build_f64(fc_dfjk* h, const double* d, double* j, cudaStream_t st,
         FC_CUDA(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
         stats->kernel_ms = ms;
         stats->flops = 4.0 * (double)naux * (double)pair;
-        stats->precision = FC_PREC_F64;
+        stats->precision = prec;
         stats->launches += 4 + (h->l_chol ? 1 : 0);
         stats->main_launches = 2;
         stats->main_ms = ms;
         stats->main_flops = stats->flops;
-        stats->main_bytes = 2.0 * 8.0 * (double)naux * (double)pair;
+        stats->main_bytes = 2.0 * sizeof(TB) * (double)naux * (double)pair;
     }
     return FC_OK;
+}
+
+fc_status dfj_build_f64(fc_dfjk* h, const double* d, double* j, cudaStream_t st, fc_stats* stats) {
+    return dfj_build_t<double>(h, h->b_pk, FC_PREC_F64, d, j, st, stats);
+}
+
+fc_status dfj_build_mixed(fc_dfjk* h, const double* d, double* j, cudaStream_t st, fc_stats* stats) {
+    if (!h->pk32) return fail(FC_ERR_KERNEL, "DF-J: handle has no FP32 copy (created with FC_PREC_F64)");
+    return dfj_build_t<float>(h, h->pk32, FC_PREC_MIXED, d, j, st, stats);
+}
+
+fc_status dfjk_prepare_mixed(fc_dfjk* h, cudaStream_t st) {
+    const int64_t npk = h->naux * h->pair;
+    FC_TRY(pool_reserve((uint64_t)npk * 4));
+    FC_CUDA(cudaMalloc(&h->pk32, (size_t)npk * 4));
+    h->bytes += (uint64_t)npk * 4;
+    void* vf;
+    FC_TRY(ws_get(WS_OUT, 256, &vf));
+    FC_CUDA(cudaMemsetAsync(vf, 0, 256, st));
+    round_f32_kernel<<<(unsigned)((npk + 255) / 256), 256, 0, st>>>(h->b_pk, npk, h->pk32, (int*)vf);
+    FC_TRY(check_launch("round_f32_kernel"));
+    int bad = 0;
+    FC_CUDA(cudaMemcpyAsync(&bad, vf, sizeof(int), cudaMemcpyDeviceToHost, st));
+    FC_CUDA(cudaStreamSynchronize(st));
+    if (bad) return fail(FC_ERR_RANGE, "DF-JK: tensor element outside the FP32 range (mixed storage refused)");
+    return FC_OK;
+}
+
+void dfjk_free_mixed(fc_dfjk* h) {
+    if (h->pk32) cudaFree(h->pk32);
+    h->pk32 = nullptr;
 }
 
 fc_status dfk_build_f64(fc_dfjk* h, const double* c_occ, int64_t nocc, double* k, cudaStream_t st,
@@ -309,10 +355,12 @@ fc_status create_common(const double* b, int64_t naux, int64_t n, int32_t layout
     h->pair = pair;
     h->layout = layout;
     h->precision = precision;
+    h->active = precision;
     h->bytes = need;
     auto bail = [&](fc_status s) {
         if (h->b_sq) cudaFree(h->b_sq);
         if (h->b_pk) cudaFree(h->b_pk);
+        dfjk_free_mixed(h);
         delete h;
         return s;
     };
@@ -381,7 +429,7 @@ fc_status fc_dfj_build_dev(fc_dfjk* h, const double* d, double* j, void* stream,
     std::lock_guard<std::mutex> lk(ctx().mu);
     if (stats) *stats = fc_stats{};
     cudaStream_t st = pick_stream(stream);
-    if (h->precision == FC_PREC_F64) return dfj_build_f64(h, d, j, st, stats);
+    if (h->active == FC_PREC_F64) return dfj_build_f64(h, d, j, st, stats);
     return dfj_build_mixed(h, d, j, st, stats);
 }
 
@@ -397,7 +445,7 @@ fc_status fc_dfj_build(fc_dfjk* h, const double* d, double* j, fc_stats* stats) 
     double* dd = (double*)buf;
     double* dj = dd + h->n * h->n;
     FC_CUDA(cudaMemcpyAsync(dd, d, nn, cudaMemcpyHostToDevice, st));
-    if (h->precision == FC_PREC_F64) FC_TRY(dfj_build_f64(h, dd, dj, st, stats));
+    if (h->active == FC_PREC_F64) FC_TRY(dfj_build_f64(h, dd, dj, st, stats));
     else FC_TRY(dfj_build_mixed(h, dd, dj, st, stats));
     FC_CUDA(cudaMemcpyAsync(j, dj, nn, cudaMemcpyDeviceToHost, st));
     FC_CUDA(cudaStreamSynchronize(st));
@@ -421,7 +469,7 @@ fc_status fc_dfk_build_occ_dev(fc_dfjk* h, const double* c_occ, int64_t nocc, do
         FC_CUDA(cudaMemsetAsync(k, 0, h->n * h->n * 8, st));
         return FC_OK;
     }
-    if (h->precision == FC_PREC_F64) return dfk_build_f64(h, c_occ, nocc, k, st, stats);
+    if (h->active == FC_PREC_F64) return dfk_build_f64(h, c_occ, nocc, k, st, stats);
     return dfk_build_mixed(h, c_occ, nocc, k, st, stats);
 }
 
@@ -443,7 +491,7 @@ fc_status fc_dfk_build_occ(fc_dfjk* h, const double* c_occ, int64_t nocc, double
     double* dk = (double*)buf;
     double* dc = dk + h->n * h->n;
     FC_CUDA(cudaMemcpyAsync(dc, c_occ, nc, cudaMemcpyHostToDevice, st));
-    if (h->precision == FC_PREC_F64) FC_TRY(dfk_build_f64(h, dc, nocc, dk, st, stats));
+    if (h->active == FC_PREC_F64) FC_TRY(dfk_build_f64(h, dc, nocc, dk, st, stats));
     else FC_TRY(dfk_build_mixed(h, dc, nocc, dk, st, stats));
     FC_CUDA(cudaMemcpyAsync(k, dk, nn, cudaMemcpyDeviceToHost, st));
     FC_CUDA(cudaStreamSynchronize(st));
@@ -451,6 +499,18 @@ fc_status fc_dfk_build_occ(fc_dfjk* h, const double* c_occ, int64_t nocc, double
         stats->h2d_bytes += nc;
         stats->d2h_bytes += nn;
     }
+    return FC_OK;
+}
+
+fc_status fc_dfjk_set_precision(fc_dfjk* h, int32_t precision) {
+    if (!h) return fail(FC_ERR_INVALID, "fc_dfjk_set_precision: null handle");
+    if (precision == FC_PREC_F64) {
+        h->active = FC_PREC_F64;
+        return FC_OK;
+    }
+    if (precision != h->precision || h->precision == FC_PREC_F64)
+        return fail(FC_ERR_INVALID, "fc_dfjk_set_precision: the handle holds no copy for that precision");
+    h->active = precision;
     return FC_OK;
 }
 

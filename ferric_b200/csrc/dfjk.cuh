@@ -5,11 +5,12 @@
 struct fc_dfjk {
     int64_t naux = 0, n = 0, pair = 0;
     int layout = 0, precision = 0;
+    int active = 0;            // precision of the next build (FC_PREC_F64 or `precision`)
     double* b_sq = nullptr;    // (naux, n, n) dressed tensor (square handles)
     double* b_pk = nullptr;    // (naux, n(n+1)/2) packed lower rows
     double* l_chol = nullptr;  // metric Cholesky factor (raw-Bp form)
-    // split-BF16 copies (mixed handles)
-    void* pk_split = nullptr;  // packed rows as (hi, lo) bf16 pairs
+    // mixed handles
+    float* pk32 = nullptr;     // packed rows, FP32 (DF-J reads 4 B per element)
     void* sq_split = nullptr;  // square tensor split for the tensor-core stages
     uint64_t bytes = 0;        // device bytes owned by the handle
 };

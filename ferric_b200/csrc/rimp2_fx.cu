@@ -17,10 +17,13 @@
 // (6 bf16 tensor-core products), combined in FP64 in the epilogue:
 //     g = s_r s_r' (L0 + L1 / 256 + L2 / 65536).
 //
-// Pair kernel (this file): item = (pair, a-tile 128, b-tile 64); the X phase
-// accumulates (ia|jb) and the Y phase (ib|ja) = G_ji[a, b] into separate
-// level sets (6 x 64 TMEM columns), so each thread holds an element and its
-// exchange partner.  Energy mode: unordered pairs, E_OS += (X^2 + Y^2)/D,
+// Pair kernel (this file): item = (pair, a-tile 128, b-tile 128); the X phase
+// accumulates (ia|jb) into the three level accumulators (3 x 128 TMEM
+// columns), the epilogue parks it in registers (FP32, round to nearest), and
+// the Y phase accumulates (ib|ja) = G_ji[a, b] into the same columns, so each
+// thread holds an element and its exchange partner.  128 x 128 UMMAs keep the
+// shared-memory operand reads at 128 B/clk (128 x 64 ones need 192 B/clk, more
+// than an SM delivers).  Energy mode: unordered pairs, E_OS += (X^2 + Y^2)/D,
 // E_SS += (X - Y)^2/D (i == j: X phase only, E_SS = 0), the reference pair
 // loop of ferric-mp2/src/rimp2.rs:1399-1544 over both orderings.  Gradient
 // mode: ordered pairs of an occupied chunk; writes Tt_ij = (2X - Y)/D (FP32)
@@ -35,14 +38,14 @@ namespace fc {
 
 namespace fx {
 
-constexpr int BM = 128, BN = 64, KT = 64;
+constexpr int BM = 128, BN = 128, KT = 64;
 constexpr int A_BYTES = BM * KT * 2;  // 16 KiB
-constexpr int B_BYTES = BN * KT * 2;  // 8 KiB
+constexpr int B_BYTES = BN * KT * 2;  // 16 KiB
 constexpr int NSL = 3;
-constexpr int STAGE_BYTES = NSL * (A_BYTES + B_BYTES);  // 72 KiB
-constexpr int STAGES = 3;
-constexpr int SMEM = STAGES * STAGE_BYTES + 1024 + 1024;
-constexpr uint32_t IDESC = tc::idesc_bf16_f32(128, 64);
+constexpr int STAGE_BYTES = NSL * (A_BYTES + B_BYTES);  // 96 KiB
+constexpr int STAGES = 2;
+constexpr int SMEM = STAGES * STAGE_BYTES + 1024 + 7168;
+constexpr uint32_t IDESC = tc::idesc_bf16_f32(128, 128);
 constexpr double L1W = 1.0 / 256.0, L2W = 1.0 / 65536.0;
 
 // products: (A slice, B slice, level)
@@ -239,6 +242,8 @@ struct PairFxArgs {
     const double* ev;
     const double* scl;  // [nocc * a_pad] operand-row scales
     const int2* pairs;  // pairs of the launch
+    const int2* tiles;  // (a-tile, b-tile) of each item of a pair
+    int ntiles;         // tiles per pair
     int npairs;
     int nocc, nvir, a_pad, nTa, nTb, nk;
     int64_t items;
@@ -253,7 +258,7 @@ struct PairFxArgs {
 };
 
 template <int GRAD>
-__global__ void __launch_bounds__(192, 1)
+__global__ void __launch_bounds__(320, 1)
     pair_fx_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                    const PairFxArgs p) {
     using namespace fx;
@@ -265,12 +270,14 @@ __global__ void __launch_bounds__(192, 1)
     uint64_t* bars = reinterpret_cast<uint64_t*>(base + S * STAGE_BYTES);
     uint64_t* full = bars;                // [S]
     uint64_t* empty = bars + S;           // [S]
-    uint64_t* tfull = bars + 2 * S;       // [1]
-    uint64_t* tempty = bars + 2 * S + 1;  // [1]
+    uint64_t* tfull = bars + 2 * S;       // [1] a phase's levels are complete in TMEM
+    uint64_t* tempty = bars + 2 * S + 1;  // [1] the epilogue has read them out
     uint64_t* drain = bars + 2 * S + 2;   // [1]
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * S + 3);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
-    double* red = reinterpret_cast<double*>(bars + 2 * S + 4);  // [2][4][3]
+    double* red = reinterpret_cast<double*>(bars + 2 * S + 4);  // [2][8][3]
+    double* rowsh = red + 48;                                    // [128] row sums of the upper column half
+    double* colsh = rowsh + 128;                                 // [4 quadrants][2 halves][64] column sums
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (tid == 0) {
@@ -279,7 +286,7 @@ __global__ void __launch_bounds__(192, 1)
             tc::mbar_init(&empty[s], 1);
         }
         tc::mbar_init(tfull, 1);
-        tc::mbar_init(tempty, 128);
+        tc::mbar_init(tempty, 256);
         tc::mbar_init(drain, 1);
         *abort_flag = 0;
         tc::fence_barrier_init();
@@ -296,18 +303,20 @@ __global__ void __launch_bounds__(192, 1)
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem_base = *tmem_slot;
-    const int64_t tpp = (int64_t)p.nTa * p.nTb;  // tiles per pair
+    const int64_t tpp = p.ntiles;  // tiles per pair
 
     auto sa = [&](int s, int sl) { return base_u32 + s * STAGE_BYTES + sl * A_BYTES; };
     auto sb = [&](int s, int sl) { return base_u32 + s * STAGE_BYTES + NSL * A_BYTES + sl * B_BYTES; };
     auto row_of = [&](int sl, int i, int r0) { return (sl * p.nocc + i) * p.a_pad + r0; };
 
     if (warp == 0) {
+        // ------------------------------------------------------ TMA producer
         if (lane == 0) {
             uint32_t g = 0;
             for (int64_t k = blockIdx.x; k < p.items && !*abort_flag; k += gridDim.x) {
                 const int2 ij = p.pairs[k / tpp];
-                const int ta = (int)((k % tpp) / p.nTb), tb = (int)(k % p.nTb);
+                const int2 tt = p.tiles[k % tpp];
+                const int ta = tt.x, tb = tt.y;
                 const int nph = ij.x == ij.y ? 1 : 2;
                 for (int ph = 0; ph < nph; ++ph) {
                     const int ia = ph == 0 ? ij.x : ij.y, ib = ph == 0 ? ij.y : ij.x;
@@ -334,15 +343,15 @@ __global__ void __launch_bounds__(192, 1)
             }
         }
     } else if (warp == 1) {
+        // ------------------------------------------------------ UMMA issuer
         if (lane == 0) {
-            uint32_t g = 0, li = 0;
-            for (int64_t k = blockIdx.x; k < p.items && !*abort_flag; k += gridDim.x, ++li) {
+            uint32_t g = 0, pc = 0;  // pc: phases issued (TMEM hand-overs)
+            for (int64_t k = blockIdx.x; k < p.items && !*abort_flag; k += gridDim.x) {
                 const int2 ij = p.pairs[k / tpp];
-                if (!tc::mbar_wait(tempty, (li & 1) ^ 1, abort_flag, p.err)) break;
-                tc::fence_after_sync();
                 const int nph = ij.x == ij.y ? 1 : 2;
-                for (int ph = 0; ph < nph; ++ph) {
-                    const uint32_t d0 = tmem_base + ph * 192;
+                for (int ph = 0; ph < nph; ++ph, ++pc) {
+                    if (!tc::mbar_wait(tempty, (pc & 1) ^ 1, abort_flag, p.err)) goto mma_done;
+                    tc::fence_after_sync();
                     for (int kt = 0; kt < p.nk; ++kt, ++g) {
                         const int s = g % S;
                         const uint32_t u = g / S;
@@ -351,7 +360,7 @@ __global__ void __launch_bounds__(192, 1)
 #pragma unroll
                         for (int pr = 0; pr < 6; ++pr) {
                             const uint32_t a0 = sa(s, kPA[pr]), b0 = sb(s, kPB[pr]);
-                            const uint32_t dcol = d0 + kPL[pr] * 64;
+                            const uint32_t dcol = tmem_base + kPL[pr] * BN;
 #pragma unroll
                             for (int kk = 0; kk < KT / 16; ++kk)
                                 tc::umma_bf16(dcol, tc::sdesc_k128(a0 + kk * 32), tc::sdesc_k128(b0 + kk * 32),
@@ -359,8 +368,8 @@ __global__ void __launch_bounds__(192, 1)
                         }
                         tc::umma_commit(&empty[s]);
                     }
+                    tc::umma_commit(tfull);
                 }
-                tc::umma_commit(tfull);
             }
         mma_done:
             tc::umma_commit(drain);
@@ -370,100 +379,175 @@ __global__ void __launch_bounds__(192, 1)
         __syncwarp();
     } else {
         // ---------------------------------------------------------- epilogue
+        // 8 warps: lane quadrant q = warp % 4 (TMEM lanes 32q..32q+31), column
+        // half h = (warp - 2) / 4; each thread owns row `row`, columns [64h, 64h + 64).
+        constexpr int HC = BN / 2;
         const int q = warp & 3;
+        const int h = (warp - 2) >> 2;
         const int row = q * 32 + lane;  // a within the tile
-        const int et = tid - 64;
-        uint32_t li = 0;
+        const int et = tid - 64;        // 0..255
+        const uint32_t tl = tmem_base + ((uint32_t)(q * 32) << 16) + h * HC;
+        uint32_t li = 0, pc = 0;
         for (int64_t k = blockIdx.x; k < p.items; k += gridDim.x, ++li) {
             const int2 ij = p.pairs[k / tpp];
             const int i = ij.x, j = ij.y;
             const bool diag = i == j;
-            const int ta = (int)((k % tpp) / p.nTb), tb = (int)(k % p.nTb);
-            if (!tc::mbar_wait(tfull, li & 1, abort_flag, p.err)) break;
-            tc::fence_after_sync();
+            const int2 tt2 = p.tiles[k % tpp];
+            const int ta = tt2.x, tb = tt2.y;
+            // tiles ta <= tb only: X_ba = Y_ab, so the mirrored tile (tb, ta) is this
+            // tile transposed.  Energy mode weights it 2; gradient mode also
+            // writes its amplitudes (transposed) and its derivative terms.
+            const double wt = (!GRAD && ta < tb) ? 2.0 : 1.0;
+            const bool mir = GRAD && ta < tb;
             const int a = ta * BM + row;
             const bool va = a < p.nvir;
             const double dA = p.eo[i] + p.eo[j] - (va ? p.ev[a] : 0.0);
             const double sxa = p.scl[(int64_t)i * p.a_pad + a];
             const double sya = p.scl[(int64_t)j * p.a_pad + a];
-            const double* sxb = p.scl + (int64_t)j * p.a_pad + tb * BN;
-            const double* syb = p.scl + (int64_t)i * p.a_pad + tb * BN;
-            KSum os, ss, oc;
-            double rowc = 0.0;
-            const uint32_t tl = tmem_base + ((uint32_t)(q * 32) << 16);
-#pragma unroll 1
-            for (int c0 = 0; c0 < BN; c0 += 16) {
-                float x0[16], x1[16], x2[16], y0[16], y1[16], y2[16];
-                tc::tmem_ld16(tl + c0, x0);
-                tc::tmem_ld16(tl + 64 + c0, x1);
-                tc::tmem_ld16(tl + 128 + c0, x2);
-                if (!diag) {
-                    tc::tmem_ld16(tl + 192 + c0, y0);
-                    tc::tmem_ld16(tl + 256 + c0, y1);
-                    tc::tmem_ld16(tl + 320 + c0, y2);
-                }
+            const int b0 = tb * BN + h * HC;  // first column of this thread
+            const double* sxb = p.scl + (int64_t)j * p.a_pad + b0;
+            const double* syb = p.scl + (int64_t)i * p.a_pad + b0;
+            const double* evb = p.ev + b0;
+            const int bmax = p.nvir - b0;    // columns c < bmax are real virtuals
+
+            // X phase: park (ia|jb) of this half row in registers (FP32, round to nearest)
+            if (!tc::mbar_wait(tfull, pc & 1, abort_flag, p.err)) break;
+            tc::fence_after_sync();
+            float xr[HC];
+#pragma unroll
+            for (int c0 = 0; c0 < HC; c0 += 16) {
+                float l0[16], l1[16], l2[16];
+                tc::tmem_ld16(tl + c0, l0);
+                tc::tmem_ld16(tl + BN + c0, l1);
+                tc::tmem_ld16(tl + 2 * BN + c0, l2);
                 tc::tmem_wait_ld();
-                float tt4[16];
 #pragma unroll
-                for (int cc = 0; cc < 16; ++cc) {
-                    const int b = tb * BN + c0 + cc;
-                    const double x = sxa * sxb[c0 + cc] * ((double)x0[cc] + (double)x1[cc] * L1W + (double)x2[cc] * L2W);
-                    const double y = diag ? x
-                                          : sya * syb[c0 + cc] *
-                                                ((double)y0[cc] + (double)y1[cc] * L1W + (double)y2[cc] * L2W);
-                    float tval = 0.f;
-                    if (va && b < p.nvir) {
-                        const double D = dA - p.ev[b];
-                        const double r = 1.0 / D;
-                        if (GRAD) {
-                            const double tt = (2.0 * x - y) * r;
-                            tval = (float)tt;
-                            const double c = x * r * tt;
-                            os.add(x * x * r);
-                            ss.add(x * (x - y) * r);
-                            oc.add(c);
-                            rowc += c;
-                        } else if (diag) {
-                            os.add(x * x * r);
-                        } else {
-                            os.add((x * x + y * y) * r);
-                            ss.add((x - y) * (x - y) * r);
-                        }
-                    }
-                    tt4[cc] = tval;
-                }
-                if (GRAD) {
-                    float4* dst = reinterpret_cast<float4*>(
-                        p.T + ((int64_t)(i - p.i0) * p.a_pad + a) * p.ldt + (int64_t)j * p.a_pad + tb * BN + c0);
-#pragma unroll
-                    for (int v = 0; v < 4; ++v)
-                        dst[v] = make_float4(tt4[4 * v], tt4[4 * v + 1], tt4[4 * v + 2], tt4[4 * v + 3]);
-                }
+                for (int cc = 0; cc < 16; ++cc)
+                    xr[c0 + cc] = (float)(sxa * sxb[c0 + cc] *
+                                          ((double)l0[cc] + (double)l1[cc] * L1W + (double)l2[cc] * L2W));
             }
             tc::fence_before_sync();
             tc::mbar_arrive(tempty);
-            if (GRAD) p.vir_part[k * BM + row] = rowc;
-            const double vo = warp_sum(os.value()), vs = warp_sum(ss.value());
-            const double vc = GRAD ? warp_sum(oc.value()) : 0.0;
-            double* rb = red + (li & 1) * 12;
+            ++pc;
+            if (!diag) {
+                if (!tc::mbar_wait(tfull, pc & 1, abort_flag, p.err)) break;
+                tc::fence_after_sync();
+            }
+            // plain FP64 sums over this thread's 64 terms (relative error <= 64 u);
+            // the tile partials are summed compensated
+            double os = 0.0, ss = 0.0, oc = 0.0, rowc = 0.0;
+#pragma unroll
+            for (int c0 = 0; c0 < HC; c0 += 8) {
+                float y0[8], y1[8], y2[8];
+                if (!diag) {
+                    tc::tmem_ld8(tl + c0, y0);
+                    tc::tmem_ld8(tl + BN + c0, y1);
+                    tc::tmem_ld8(tl + 2 * BN + c0, y2);
+                    tc::tmem_wait_ld();
+                    if (c0 + 8 == HC) {  // every level of this phase is read: release TMEM
+                        tc::fence_before_sync();
+                        tc::mbar_arrive(tempty);
+                    }
+                }
+                float tt8[8], mv8[8];
+#pragma unroll
+                for (int cc = 0; cc < 8; ++cc) {
+                    const double x = (double)xr[c0 + cc];
+                    const double y = diag ? x
+                                          : sya * syb[c0 + cc] *
+                                                ((double)y0[cc] + (double)y1[cc] * L1W + (double)y2[cc] * L2W);
+                    float tval = 0.f, mval = 0.f, colv = 0.f;
+                    if (va && c0 + cc < bmax) {
+                        const double r = 1.0 / (dA - evb[c0 + cc]);
+                        if (GRAD) {
+                            const double tt = (2.0 * x - y) * r;   // Tt_ij[a, b]
+                            const double cd = x * r * tt;          // t Tt at (a, b)
+                            tval = (float)tt;
+                            os += x * x * r;
+                            ss += x * (x - y) * r;
+                            oc += cd;
+                            rowc += cd;
+                            if (mir) {
+                                const double tm = (2.0 * y - x) * r;  // Tt_ij[b, a]
+                                const double cm = y * r * tm;         // t Tt at (b, a)
+                                mval = (float)tm;
+                                colv = (float)cm;
+                                os += y * y * r;
+                                ss += y * (y - x) * r;
+                                oc += cm;
+                            }
+                        } else if (diag) {
+                            os += x * x * r;
+                        } else {
+                            os += (x * x + y * y) * r;
+                            ss += (x - y) * (x - y) * r;
+                        }
+                    }
+                    tt8[cc] = tval;
+                    mv8[cc] = mval;
+                    if (GRAD) xr[c0 + cc] = colv;  // x of this column is consumed: keep cm there
+                }
+                if (GRAD) {
+                    float* trow = p.T + ((int64_t)(i - p.i0) * p.a_pad) * p.ldt + (int64_t)j * p.a_pad;
+                    float4* dst = reinterpret_cast<float4*>(trow + (int64_t)a * p.ldt + b0 + c0);
+                    dst[0] = make_float4(tt8[0], tt8[1], tt8[2], tt8[3]);
+                    dst[1] = make_float4(tt8[4], tt8[5], tt8[6], tt8[7]);
+                    if (mir) {
+#pragma unroll
+                        for (int cc = 0; cc < 8; ++cc)  // lanes hold consecutive a: coalesced
+                            trow[(int64_t)(b0 + c0 + cc) * p.ldt + a] = mv8[cc];
+                    }
+                }
+            }
+            if (!diag) ++pc;
+            const double vo = warp_sum(os), vs = warp_sum(ss);
+            const double vc = GRAD ? warp_sum(oc) : 0.0;
+            double* rb = red + (li & 1) * 24;
             if (lane == 0) {
                 rb[(warp - 2) * 3 + 0] = vo;
                 rb[(warp - 2) * 3 + 1] = vs;
                 rb[(warp - 2) * 3 + 2] = vc;
             }
-            asm volatile("bar.sync 1, 128;" ::: "memory");
-            if (et == 0) {
-                double so = 0.0, sn = 0.0, sc = 0.0;
+            if (GRAD && h == 1) rowsh[row] = rowc;
+            if (mir) {
+                // column sums of the mirrored terms over this warp's 32 rows: a
+                // reduce-scatter butterfly leaves columns 2*lane, 2*lane+1 in xr[0..1]
 #pragma unroll
-                for (int w = 0; w < 4; ++w) {
-                    so += rb[w * 3];
-                    sn += rb[w * 3 + 1];
-                    sc += rb[w * 3 + 2];
+                for (int half = HC / 2, off = 16; off > 0; half >>= 1, off >>= 1) {
+                    const bool up = (lane & off) != 0;
+#pragma unroll
+                    for (int c = 0; c < half; ++c) {
+                        const float send = up ? xr[c] : xr[c + half];
+                        const float recv = __shfl_xor_sync(0xffffffffu, send, off);
+                        xr[c] = (up ? xr[c + half] : xr[c]) + recv;
+                    }
                 }
-                p.part[2 * k] = so;
-                p.part[2 * k + 1] = sn;
-                if (GRAD) p.occ_part[k] = sc;
+                colsh[(q * 2 + h) * 64 + 2 * lane] = (double)xr[0];
+                colsh[(q * 2 + h) * 64 + 2 * lane + 1] = (double)xr[1];
             }
+            asm volatile("bar.sync 1, 256;" ::: "memory");
+            if (GRAD && h == 0) p.vir_part[k * 2 * BM + row] = rowc + rowsh[row];
+            if (mir && et < BM) {
+                const int hh = et >> 6, c = et & 63;
+                double v = 0.0;
+#pragma unroll
+                for (int qq = 0; qq < 4; ++qq) v += colsh[(qq * 2 + hh) * 64 + c];
+                p.vir_part[k * 2 * BM + BM + et] = v;
+            }
+            if (et == 0) {
+                KSum so, sn, sc;
+#pragma unroll
+                for (int w = 0; w < 8; ++w) {
+                    so.add(rb[w * 3]);
+                    sn.add(rb[w * 3 + 1]);
+                    sc.add(rb[w * 3 + 2]);
+                }
+                p.part[2 * k] = wt * so.value();
+                p.part[2 * k + 1] = wt * sn.value();
+                if (GRAD) p.occ_part[k] = sc.value();
+            }
+            // rowsh is rewritten next item only after every thread passed the next barrier
+            asm volatile("bar.sync 1, 256;" ::: "memory");
         }
     }
 
@@ -680,22 +764,25 @@ __global__ void __launch_bounds__(256) fx_reduce_occ_kernel(const double* __rest
     }
 }
 
-// acc_vir[a] += 2 * sum of the chunk's row partials of virtual a.
-__global__ void __launch_bounds__(256) fx_reduce_vir_kernel(const double* __restrict__ vir_part, int64_t npairs,
-                                                            int nTa, int nTb, int nvir, double* acc_vir) {
-    const int a = blockIdx.x * 8 + (threadIdx.x >> 5);
+// acc_vir[v] += 2 * (sum over the chunk's items of the row partials of v, from
+// direct tiles (ta, tb) with v in ta, and of the column partials, from the
+// mirrored tiles (tb, ta) with v in tb).  Fixed order: deterministic.
+__global__ void __launch_bounds__(256) fx_reduce_vir_kernel(const double* __restrict__ vir_part,
+                                                            const int2* __restrict__ tiles, int64_t npairs,
+                                                            int ntiles, int nvir, double* acc_vir) {
+    const int v = blockIdx.x * 8 + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
-    if (a >= nvir) return;
-    const int ta = a / fx::BM, ar = a % fx::BM;
-    const int64_t nterm = npairs * nTb;
+    if (v >= nvir) return;
+    const int tv = v / fx::BM, rv = v % fx::BM;
+    const int64_t nterm = npairs * ntiles;
     KSum s;
     for (int64_t k = lane; k < nterm; k += 32) {
-        const int64_t pidx = k / nTb, tb = k % nTb;
-        const int64_t item = (pidx * nTa + ta) * nTb + tb;
-        s.add(vir_part[item * fx::BM + ar]);
+        const int2 t = tiles[k % ntiles];
+        if (t.x == tv) s.add(vir_part[k * 2 * fx::BM + rv]);
+        if (t.y == tv && t.x < t.y) s.add(vir_part[k * 2 * fx::BM + fx::BM + rv]);
     }
-    const double v = warp_sum(s.value());
-    if (lane == 0) acc_vir[a] += 2.0 * v;
+    const double r = warp_sum(s.value());
+    if (lane == 0) acc_vir[v] += 2.0 * r;
 }
 
 // ------------------------------------------------------------------ host --
@@ -769,9 +856,13 @@ fc_status rimp2_energy_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, doub
     FxSplit sp;
     FC_TRY(fx_split_pairs(d, st, flags, &sp));
     const int nocc = (int)d.nocc;
+    const int nT = (int)(sp.a_pad / fx::BM);
     std::vector<int2> pairs;
     for (int i = 0; i < nocc; ++i)
         for (int j = i; j < nocc; ++j) pairs.push_back(make_int2(i, j));
+    const size_t npairs = pairs.size();
+    for (int ta = 0; ta < nT; ++ta)
+        for (int tb = ta; tb < nT; ++tb) pairs.push_back(make_int2(ta, tb));
     void* vtab;
     FC_TRY(ws_get(WS_PAIRS, pairs.size() * sizeof(int2), &vtab));
     FC_CUDA(cudaMemcpyAsync(vtab, pairs.data(), pairs.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
@@ -780,14 +871,16 @@ fc_status rimp2_energy_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, doub
     a.ev = d.eps_vir;
     a.scl = sp.scl;
     a.pairs = (const int2*)vtab;
-    a.npairs = (int)pairs.size();
+    a.tiles = (const int2*)vtab + npairs;
+    a.ntiles = nT * (nT + 1) / 2;
+    a.npairs = (int)npairs;
     a.nocc = nocc;
     a.nvir = (int)d.nvir;
     a.a_pad = (int)sp.a_pad;
     a.nTa = (int)(sp.a_pad / fx::BM);
     a.nTb = (int)(sp.a_pad / fx::BN);
     a.nk = (int)(sp.q_pad / fx::KT);
-    a.items = (int64_t)a.npairs * a.nTa * a.nTb;
+    a.items = (int64_t)a.npairs * a.ntiles;
     void* vpart;
     FC_TRY(ws_get(WS_PART, a.items * 2 * sizeof(double), &vpart));
     a.part = (double*)vpart;
@@ -798,7 +891,7 @@ fc_status rimp2_energy_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, doub
         FC_TRY(timing_events(1, &ev));
         FC_CUDA(cudaEventRecord(ev[0], st));
     }
-    pair_fx_kernel<0><<<grid, 192, fx::SMEM, st>>>(sp.tmA, sp.tmB, a);
+    pair_fx_kernel<0><<<grid, 320, fx::SMEM, st>>>(sp.tmA, sp.tmB, a);
     FC_TRY(check_launch("pair_fx_kernel<energy>"));
     if (stats) FC_CUDA(cudaEventRecord(ev[1], st));
     fx_reduce_pairs_kernel<<<1, 1024, 0, st>>>((const double*)vpart, a.items, out);
@@ -853,7 +946,8 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
     const int64_t q_rows = (naux + 127) / 128 * 128;
     // per-Q-row split of B_ov for the adjoint contraction
     const int64_t npairs_all = nocc * nocc;
-    const size_t tab_bytes = ((npairs_all * sizeof(int2) + 255) / 256) * 256;
+    const int64_t ntile_all = (a_pad / fx::BM) * (a_pad / fx::BM + 1) / 2;
+    const size_t tab_bytes = (((npairs_all + ntile_all) * sizeof(int2) + 255) / 256) * 256;
     void *vbq, *vtab;
     FC_TRY(ws_get(WS_SPLIT2, (size_t)3 * q_rows * K2 * 2, &vbq));
     FC_TRY(ws_get(WS_PAIRS, tab_bytes + q_rows * 8, &vtab));
@@ -873,21 +967,24 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
     if (ci < 1) ci = 1;
     if (ci > nocc) ci = nocc;
     const int nTa = (int)(a_pad / fx::BM), nTb = (int)(a_pad / fx::BN);
-    const int64_t items_per_i = nocc * (int64_t)nTa * nTb;
+    const int ntiles = nTa * (nTa + 1) / 2;  // tiles ta <= tb (nTa == nTb)
+    const int64_t items_per_i = nocc * (int64_t)ntiles;
     const size_t t_bytes = (size_t)ci * a_pad * K2 * 4;
     void *vT, *vTs, *vpart;
     FC_TRY(ws_get(WS_T, t_bytes + (size_t)ci * a_pad * 8, &vT));
     FC_TRY(ws_get(WS_TS, (size_t)3 * ci * a_pad * K2 * 2, &vTs));
-    FC_TRY(ws_get(WS_PART, (size_t)ci * items_per_i * (2 + 1 + fx::BM) * 8, &vpart));
+    FC_TRY(ws_get(WS_PART, (size_t)ci * items_per_i * (2 + 1 + 2 * fx::BM) * 8, &vpart));
     float* T = (float*)vT;
     double* ts = (double*)((char*)vT + t_bytes);
     void* ts_slices = vTs;
     double* occ_part = (double*)vpart + ci * items_per_i * 2;
     double* vir_part = occ_part + ci * items_per_i;
-    // pair table: ordered pairs, row-major by i
+    // pair table: ordered pairs, row-major by i; then every (a-tile, b-tile)
     std::vector<int2> pairs((size_t)npairs_all);
     for (int i = 0; i < nocc; ++i)
         for (int j = 0; j < nocc; ++j) pairs[(size_t)i * nocc + j] = make_int2(i, j);
+    for (int ta = 0; ta < nTa; ++ta)
+        for (int tb = ta; tb < nTb; ++tb) pairs.push_back(make_int2(ta, tb));
     FC_CUDA(cudaMemcpyAsync(vtab, pairs.data(), pairs.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
     FC_CUDA(cudaMemsetAsync(de_dvir, 0, nvir * 8, st));
 
@@ -904,6 +1001,8 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
         a.ev = d.eps_vir;
         a.scl = sp.scl;
         a.pairs = (const int2*)vtab + i0 * nocc;
+        a.tiles = (const int2*)vtab + npairs_all;
+        a.ntiles = ntiles;
         a.npairs = (int)(cn * nocc);
         a.nocc = (int)nocc;
         a.nvir = (int)nvir;
@@ -921,13 +1020,13 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
         a.vir_part = vir_part;
         const int grid = (int)(a.items < c.sm_count ? a.items : c.sm_count);
         if (stats) FC_CUDA(cudaEventRecord(ev[2 * ch], st));
-        pair_fx_kernel<1><<<grid, 192, fx::SMEM, st>>>(sp.tmA, sp.tmB, a);
+        pair_fx_kernel<1><<<grid, 320, fx::SMEM, st>>>(sp.tmA, sp.tmB, a);
         FC_TRY(check_launch("pair_fx_kernel<grad>"));
         if (stats) FC_CUDA(cudaEventRecord(ev[2 * ch + 1], st));
         fx_reduce_pairs_kernel<<<1, 1024, 0, st>>>((const double*)vpart, a.items, e_chunks + 2 * ch);
         fx_reduce_occ_kernel<<<(unsigned)cn, 256, 0, st>>>(occ_part, items_per_i, (int)i0, de_docc);
-        fx_reduce_vir_kernel<<<(unsigned)((nvir + 7) / 8), 256, 0, st>>>(vir_part, cn * nocc, nTa, nTb,
-                                                                          (int)nvir, de_dvir);
+        fx_reduce_vir_kernel<<<(unsigned)((nvir + 7) / 8), 256, 0, st>>>(
+            vir_part, (const int2*)vtab + npairs_all, cn * nocc, ntiles, (int)nvir, de_dvir);
         split_fx_rows_f32_kernel<<<(unsigned)(cn * a_pad), 256, 0, st>>>(T, K2, ci * a_pad, ts,
                                                                           (__nv_bfloat16*)ts_slices);
         FC_TRY(check_launch("gradient chunk reductions / split"));

@@ -57,9 +57,16 @@ class DfJK:
             check(_lib.lib.fc_dfjk_create(ptr(bb), self.naux, self.n, LAYOUTS[layout], _prec(precision),
                                           ctypes.byref(h)))
         self._h = h
+        self.active = precision
         if metric_chol is not None:
             lc = np.ascontiguousarray(metric_chol, dtype=np.float64)
             check(_lib.lib.fc_dfj_set_metric_chol(self._h, ptr(lc)))
+
+    def set_precision(self, precision):
+        """Precision of the next builds: "f64" always, or the handle's own
+        mixed precision (``fc_dfjk_set_precision``)."""
+        check(_lib.lib.fc_dfjk_set_precision(self._h, _prec(precision)))
+        self.active = precision
 
     def close(self):
         if getattr(self, "_h", None) and self._h.value:

@@ -51,6 +51,10 @@ typedef int32_t fc_status;
 #define FC_LAYOUT_SQUARE        0  /* (naux, n, n), symmetric in (mu, nu)          */
 #define FC_LAYOUT_PACKED_LOWER  1  /* (naux, n(n+1)/2), rows (mu, nu <= mu)        */
 
+/* Mixed DF-J keeps B as FP32 (the reference's f32 RI-J tier,
+ * ferric-scf/src/df_j.rs:33-91) with FP64 accumulation: half the bytes of the
+ * bandwidth-bound passes. */
+
 /* Per-call record (the reference's gpu::stats counters, per call). */
 typedef struct fc_stats {
     double   kernel_ms;    /* device time of the contraction kernels (CUDA events) */
@@ -172,6 +176,11 @@ fc_status fc_dfk_build_occ(fc_dfjk* h, const double* c_occ, int64_t nocc, double
                            fc_stats* stats);
 fc_status fc_dfk_build_occ_dev(fc_dfjk* h, const double* c_occ, int64_t nocc, double* k,
                                void* stream, fc_stats* stats);
+/* Precision of the handle's next builds: FC_PREC_F64 always works (the FP64
+ * tensor stays resident beside the mixed copy); the handle's creation
+ * precision switches back.  This is how the SCF precision ladder
+ * (ferric-scf/src/jk_ladder.rs:312-430) publishes its per-build decision. */
+fc_status fc_dfjk_set_precision(fc_dfjk* h, int32_t precision);
 fc_status fc_dfjk_destroy(fc_dfjk* h);
 
 #ifdef __cplusplus

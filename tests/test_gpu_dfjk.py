@@ -73,3 +73,35 @@ def test_device_api(fc):
     k = jk.k_from_occ(torch.from_numpy(c).cuda()).cpu().numpy()
     assert np.abs(j - orc.df_j_square(b, d)).max() < F_TOL
     assert np.abs(k - orc.df_k_occ(b, c)).max() < F_TOL
+
+
+def test_mixed_dfj_fp32_storage(fc):
+    """Mixed DF-J keeps B in FP32 (the reference's f32 RI-J tier) with FP64
+    accumulation: max|dJ| within FP32 rounding of the terms."""
+    from ferric_b200.dfjk import DfJK
+    b, c, d = synthetic.dfjk_inputs(130, 260, 17)
+    ref = orc.df_j_square(b, d)
+    jk = DfJK(b, precision="mixed")
+    st = {}
+    j = jk.j(d, stats=st)
+    assert st["precision"] == 1
+    # |dJ_k| <= 2 u32 sum_P |B_Pk| |c_P| (two passes through the rounded B)
+    bound = 2 * 2.0 ** -24 * np.abs(b).reshape(260, -1).T @ np.abs(np.einsum("qmn,mn->q", b, d))
+    assert np.all(np.abs(j - ref).reshape(-1) <= bound + 1e-300)
+    assert np.abs(j - ref).max() > 0      # it really ran on the FP32 copy
+    jk.set_precision("f64")
+    j64 = jk.j(d)
+    assert np.abs(j64 - ref).max() < F_TOL
+    k64 = jk.k_from_occ(c)
+    assert np.abs(k64 - orc.df_k_occ(b, c)).max() < F_TOL
+    jk.set_precision("mixed")
+    assert np.array_equal(jk.j(d), j)
+
+
+def test_set_precision_refuses_missing_copy(fc):
+    import ferric_b200._lib as L
+    from ferric_b200.dfjk import DfJK
+    b, c, d = synthetic.dfjk_inputs(20, 30, 3)
+    jk = DfJK(b, precision="f64")
+    with pytest.raises(L.FcError):
+        jk.set_precision("mixed")

@@ -41,15 +41,32 @@ def emulate_fixed_slices(b):
     return np.outer(s, s) * (l0 + l1 / 256.0 + l2 / 65536.0)
 
 
-def energy_from_g(g, eo, ev):
+def energy_from_g(g, eo, ev, tile=128):
+    """The device's energy from the exact level sums.  Per pair i <= j the
+    device visits 128 x 128 tiles (ta, tb) with ta <= tb (weight 2 off the tile
+    diagonal: the summands are symmetric under a <-> b); in each the X element
+    (ia|jb) is parked in FP32 (round to nearest) between the two tensor-core
+    phases and the Y element (ib|ja) stays FP64; i == j uses X only."""
     nocc, nvir = len(eo), len(ev)
+    nt = (nvir + tile - 1) // tile
     e_os = e_ss = 0.0
     for i in range(nocc):
-        for j in range(nocc):
-            blk = g[i * nvir:(i + 1) * nvir, j * nvir:(j + 1) * nvir]
-            d = eo[i] + eo[j] - ev[:, None] - ev[None, :]
-            e_os += np.sum(blk * blk / d)
-            e_ss += np.sum(blk * (blk - blk.T) / d)
+        for j in range(i, nocc):
+            gx = g[i * nvir:(i + 1) * nvir, j * nvir:(j + 1) * nvir]
+            gy = g[j * nvir:(j + 1) * nvir, i * nvir:(i + 1) * nvir]   # G_ji[a, b] = (ib|ja)
+            for ta in range(nt):
+                for tb in range(ta, nt):
+                    sa = slice(ta * tile, min(nvir, (ta + 1) * tile))
+                    sb = slice(tb * tile, min(nvir, (tb + 1) * tile))
+                    w = 2.0 if ta < tb else 1.0
+                    x = gx[sa, sb].astype(np.float32).astype(np.float64)
+                    d = eo[i] + eo[j] - ev[sa, None] - ev[None, sb]
+                    if i == j:
+                        e_os += w * np.sum(x * x / d)
+                    else:
+                        y = gy[sa, sb]
+                        e_os += w * np.sum((x * x + y * y) / d)
+                        e_ss += w * np.sum((x - y) ** 2 / d)
     return e_os, e_ss
 
 
@@ -66,7 +83,7 @@ def test_mixed_energy_matches_oracle_and_emulation(fc, naux, nocc, nvir):
     assert st["precision"] == 1 and st["launches"] > 0
     assert abs(e_os + e_ss - ref[2]) <= MIXED_E_REL * abs(ref[2]) + 1e-12
     em = energy_from_g(emulate_fixed_slices(b), eo, ev)
-    # exact accumulation: device == emulation to FP64 summation rounding
+    # exact accumulation: device == emulation (incl. the FP32 parking of X) to summation rounding
     assert abs(e_os - em[0]) <= 1e-12 * abs(em[0]) + 1e-15
     assert abs(e_ss - em[1]) <= 1e-12 * abs(em[0]) + 1e-15
 
@@ -81,9 +98,10 @@ def test_mixed_gradient_matches_oracle(fc, naux, nocc, nvir):
     assert np.abs(g - gamma).max() <= MIXED_G_REL * np.abs(gamma).max()
     assert np.abs(go - d_o).max() <= MIXED_D_REL * np.abs(d_o).max()
     assert np.abs(gv - d_v).max() <= MIXED_D_REL * np.abs(d_v).max()
-    # the gradient call's energy is the energy call's energy
+    # the gradient call's energy is the energy call's energy, up to which
+    # element of each pair was parked in FP32 (2^-24 relative, random)
     e2 = rimp2.rimp2_energy(b, eo, ev, precision="mixed")
-    assert abs(sum(e2) - sc.e_total) <= 1e-13 * abs(sc.e_total)
+    assert abs(sum(e2) - sc.e_total) <= 1e-9 * abs(sc.e_total)
 
 
 def test_mixed_gradient_chunked(fc, monkeypatch):
