@@ -322,12 +322,17 @@ def main():
     gamma = torch.empty_like(inp["b_ov"])
     d_o = torch.empty_like(inp["eo"])
     d_v = torch.empty_like(inp["ev"])
-    dfjk_prec = prec
+    dfj_prec = dfk_prec = prec
     try:
         jk = DfJK(inp["bjk"], layout="square", precision=prec)
     except _lib.FcError:
-        dfjk_prec = "f64"  # this build has no split-BF16 DF-JK kernels: FP64 on the device, reported
+        dfj_prec = dfk_prec = "f64"
         jk = DfJK(inp["bjk"], layout="square", precision="f64")
+    if dfk_prec != "f64":
+        try:  # K on the handle's mixed path when this build has one, FP64 on the device otherwise
+            jk.k_from_occ(inp["c"][:, :1])
+        except _lib.FcError:
+            dfk_prec = "f64"
     jbuf = torch.empty_like(inp["d"])
     kbuf = torch.empty_like(inp["d"])
     stream = torch.cuda.current_stream(dev)
@@ -342,7 +347,9 @@ def main():
         st_r, st_j, st_k = {}, {}, {}
         sc, *_ = rimp2.rimp2_energy_grad(inp["b_ov"], inp["eo"], inp["ev"], precision=prec, stats=st_r,
                                          out=(gamma, d_o, d_v))
+        jk.set_precision(dfj_prec)
         jk.j(inp["d"], out=jbuf, stats=st_j)
+        jk.set_precision(dfk_prec)
         jk.k_from_occ(inp["c"], out=kbuf, stats=st_k)
         last.update(rimp2=st_r, dfj=st_j, dfk=st_k, energy=sc)
 
@@ -450,7 +457,9 @@ def main():
                                                 ctypes.byref(eo_), ctypes.byref(es_), ptr(hg), ptr(ddo),
                                                 ptr(ddv), ctypes.byref(s)))
             s2, s3 = FcStats(), FcStats()
+            jk.set_precision(dfj_prec)
             check(_lib.lib.fc_dfj_build(jk._h, ptr(hd), ptr(hj), ctypes.byref(s2)))
+            jk.set_precision(dfk_prec)
             check(_lib.lib.fc_dfk_build_occ(jk._h, ptr(hc), DFJK["nocc"], ptr(hk), ctypes.byref(s3)))
             return s.h2d_bytes + s2.h2d_bytes + s3.h2d_bytes, s.d2h_bytes + s2.d2h_bytes + s3.d2h_bytes
 
@@ -485,7 +494,7 @@ def main():
             "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": {"f64": "f64",
                       "mixed": "bf16 x3 integer slices, 6 products, exact f32 accumulation, f64 epilogue"}[prec],
-            "precision": prec, "dfjk_precision": dfjk_prec,
+            "precision": prec, "dfj_precision": dfj_prec, "dfk_precision": dfk_prec,
             "data": "synthetic (seeded, generated on device)", "config": config,
             "components_ms": {"rimp2_e_grad": last["rimp2"]["kernel_ms"], "dfj": last["dfj"]["kernel_ms"],
                               "dfk": last["dfk"]["kernel_ms"]},

@@ -35,7 +35,8 @@ struct PairArgs {
     const double* eo;
     const double* ev;
     const int2* pairs;
-    int ntile;
+    const int2* tiles;  // (a-tile, b-tile) of each item of a pair
+    int ntiles;         // items per pair
     int has_kappa;
     double kappa;
     double* part;  // [item][2] energy partials
@@ -57,9 +58,9 @@ __global__ void __launch_bounds__(256, 2) pair_f64_kernel(PairArgs p) {
     const int g = lane >> 2, t = lane & 3;
     const int wr = warp & 3, wc = warp >> 2;
     const int64_t item = blockIdx.x;
-    const int tb = (int)(item % p.ntile);
-    const int ta = (int)((item / p.ntile) % p.ntile);
-    const int64_t pidx = item / ((int64_t)p.ntile * p.ntile);
+    const int64_t pidx = item / p.ntiles;
+    const int2 tt = p.tiles[item % p.ntiles];
+    const int ta = tt.x, tb = tt.y;
     const int2 ij = p.pairs[pidx];
     const int i = ij.x, j = ij.y;
     const int A0 = ta * PR_T, B0 = tb * PR_T;
@@ -170,7 +171,9 @@ __global__ void __launch_bounds__(256, 2) pair_f64_kernel(PairArgs p) {
                 }
             }
     }
-    const double w = (!GRAD && i == j) ? 0.5 : 1.0;
+    // energy mode visits tiles ta <= tb only: the summands are symmetric under
+    // a <-> b (X_ba = Y_ab), so an off-diagonal tile counts twice
+    const double w = GRAD ? 1.0 : (i == j ? 0.5 : 1.0) * (ta < tb ? 2.0 : 1.0);
     const double vos = block_sum(os.value(), red);
     const double vss = block_sum(ss.value(), red);
     if (tid == 0) {
@@ -267,21 +270,21 @@ fc_status rimp2_energy_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, dou
     FC_TRY(set_smem_once());
     const int64_t nocc = d.nocc, nvir = d.nvir;
     const int ntile = (int)((nvir + PR_T - 1) / PR_T);
+    const int ntiles = ntile * (ntile + 1) / 2;  // tiles ta <= tb
     const int64_t npairs = nocc * (nocc + 1) / 2;
-    const int64_t items = npairs * ntile * ntile;
+    const int64_t items = npairs * ntiles;
     if (items > INT32_MAX) return fail(FC_ERR_LAYOUT, "RI-MP2: too many pair tiles for one launch");
 
     void *vpairs, *vpart, *vout;
-    FC_TRY(ws_get(WS_PAIRS, npairs * sizeof(int2), &vpairs));
+    FC_TRY(ws_get(WS_PAIRS, (npairs + ntiles) * sizeof(int2), &vpairs));
     FC_TRY(ws_get(WS_PART, items * 2 * sizeof(double), &vpart));
     FC_TRY(ws_get(WS_OUT, 64 * sizeof(double), &vout));
-    std::vector<int2> hp((size_t)npairs);
-    {
-        size_t k = 0;
-        for (int i = 0; i < nocc; ++i)
-            for (int j = i; j < nocc; ++j) hp[k++] = make_int2(i, j);
-    }
-    FC_CUDA(cudaMemcpyAsync(vpairs, hp.data(), npairs * sizeof(int2), cudaMemcpyHostToDevice, st));
+    std::vector<int2> hp;
+    for (int i = 0; i < nocc; ++i)
+        for (int j = i; j < nocc; ++j) hp.push_back(make_int2(i, j));
+    for (int ta = 0; ta < ntile; ++ta)
+        for (int tb = ta; tb < ntile; ++tb) hp.push_back(make_int2(ta, tb));
+    FC_CUDA(cudaMemcpyAsync(vpairs, hp.data(), hp.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
 
     PairArgs a{};
     a.B = d.b_ov;
@@ -291,7 +294,8 @@ fc_status rimp2_energy_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, dou
     a.eo = d.eps_occ;
     a.ev = d.eps_vir;
     a.pairs = (const int2*)vpairs;
-    a.ntile = ntile;
+    a.tiles = (const int2*)vpairs + npairs;
+    a.ntiles = ntiles;
     a.has_kappa = d.has_kappa;
     a.kappa = d.kappa;
     a.part = (double*)vpart;
@@ -319,7 +323,7 @@ fc_status rimp2_energy_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, dou
         stats->tile_n = PR_T;
         stats->k_panel = 0;
         stats->d2h_bytes += sizeof(h);
-        stats->h2d_bytes += npairs * sizeof(int2);
+        stats->h2d_bytes += hp.size() * sizeof(int2);
         stats->main_launches = 1;
         stats->main_ms = ms;
         stats->main_flops = stats->flops;
@@ -344,7 +348,7 @@ fc_status rimp2_grad_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, doubl
     if (items > INT32_MAX) return fail(FC_ERR_LAYOUT, "RI-MP2 gradient: too many pair tiles per chunk");
 
     void *vpairs, *vpart, *vT, *vocc, *vvir, *vout;
-    FC_TRY(ws_get(WS_PAIRS, nocc * nocc * sizeof(int2), &vpairs));
+    FC_TRY(ws_get(WS_PAIRS, (nocc * nocc + (int64_t)ntile * ntile) * sizeof(int2), &vpairs));
     FC_TRY(ws_get(WS_T, ci * per_i, &vT));
     FC_TRY(ws_get(WS_PART, items * (2 + 1 + PR_T) * sizeof(double), &vpart));
     FC_TRY(ws_get(WS_OUT, ((nocc + 63) / 64 * 64 + 2) * 2 * sizeof(double) + 64, &vout));
@@ -354,6 +358,8 @@ fc_status rimp2_grad_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, doubl
     std::vector<int2> hp((size_t)(nocc * nocc));
     for (int i = 0; i < nocc; ++i)
         for (int j = 0; j < nocc; ++j) hp[(size_t)i * nocc + j] = make_int2(i, j);
+    for (int ta = 0; ta < ntile; ++ta)
+        for (int tb = 0; tb < ntile; ++tb) hp.push_back(make_int2(ta, tb));  // every tile: ta-major
     FC_CUDA(cudaMemcpyAsync(vpairs, hp.data(), hp.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
     FC_CUDA(cudaMemsetAsync(de_dvir, 0, nvir * sizeof(double), st));
 
@@ -373,7 +379,8 @@ fc_status rimp2_grad_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, doubl
         a.eo = d.eps_occ;
         a.ev = d.eps_vir;
         a.pairs = (const int2*)vpairs + i0 * nocc;
-        a.ntile = ntile;
+        a.tiles = (const int2*)vpairs + nocc * nocc;
+        a.ntiles = ntile * ntile;
         a.part = (double*)vpart;
         a.T = (double*)vT;
         a.ldt = nov;
@@ -458,12 +465,18 @@ constexpr int kNoallocMaxDevices = 64;
 void* g_noalloc_ptr[kNoallocMaxDevices] = {};  // device address of g_noalloc_scratch, per ordinal
 std::mutex g_noalloc_mu;
 
-// Unordered pairs (i <= j) in row-major order, one thread per i.
-__global__ void noalloc_pairs_kernel(int nocc, int2* pairs) {
+// Unordered pairs (i <= j) in row-major order, one thread per i; then the
+// tiles (ta <= tb) of a pair.
+__global__ void noalloc_pairs_kernel(int nocc, int ntile, int2* pairs, int2* tiles) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nocc) return;
-    const int64_t off = (int64_t)i * nocc - (int64_t)i * (i - 1) / 2;
-    for (int j = i; j < nocc; ++j) pairs[off + (j - i)] = make_int2(i, j);
+    if (i < nocc) {
+        const int64_t off = (int64_t)i * nocc - (int64_t)i * (i - 1) / 2;
+        for (int j = i; j < nocc; ++j) pairs[off + (j - i)] = make_int2(i, j);
+    }
+    if (i < ntile) {
+        const int off = i * ntile - i * (i - 1) / 2;
+        for (int tb = i; tb < ntile; ++tb) tiles[off + (tb - i)] = make_int2(i, tb);
+    }
 }
 
 }  // namespace
@@ -488,8 +501,9 @@ extern "C" fc_status fc_rimp2_energy_noalloc(const double* b_ov, int64_t naux, i
         return fail(FC_ERR_LAYOUT, "fc_rimp2_energy_noalloc: dimension out of range");
     const int64_t npairs = nocc * (nocc + 1) / 2;
     const int64_t ntile = (nvir + PR_T - 1) / PR_T;
-    const int64_t items = npairs * ntile * ntile;
-    const size_t pair_bytes = ((size_t)npairs * sizeof(int2) + 255) / 256 * 256;
+    const int64_t ntiles = ntile * (ntile + 1) / 2;
+    const int64_t items = npairs * ntiles;
+    const size_t pair_bytes = ((size_t)(npairs + ntiles) * sizeof(int2) + 255) / 256 * 256;
     const size_t part_bytes = ((size_t)items * 2 * sizeof(double) + 255) / 256 * 256;
     const size_t need = pair_bytes + part_bytes + 256;
     if (items > INT32_MAX || need > kNoallocScratchBytes)
@@ -519,7 +533,9 @@ extern "C" fc_status fc_rimp2_energy_noalloc(const double* b_ov, int64_t naux, i
 
     // Every byte read below is written earlier in this call (pairs, then all
     // partials, then the sums), so contents left by a previous call are never read.
-    noalloc_pairs_kernel<<<(unsigned)((nocc + 127) / 128), 128, 0, st>>>((int)nocc, pairs);
+    const int64_t nthr = nocc > ntile ? nocc : ntile;
+    noalloc_pairs_kernel<<<(unsigned)((nthr + 127) / 128), 128, 0, st>>>((int)nocc, (int)ntile, pairs,
+                                                                         pairs + npairs);
     PairArgs a{};
     a.B = b_ov;
     a.ldb = nocc * nvir;
@@ -528,7 +544,8 @@ extern "C" fc_status fc_rimp2_energy_noalloc(const double* b_ov, int64_t naux, i
     a.eo = eps_occ;
     a.ev = eps_vir;
     a.pairs = pairs;
-    a.ntile = (int)ntile;
+    a.tiles = pairs + npairs;
+    a.ntiles = (int)ntiles;
     a.has_kappa = has_kappa;
     a.kappa = kappa;
     a.part = part;

@@ -135,7 +135,7 @@ fc_status fc_rimp2_energy_grad_dev(const double* b_ov, int64_t naux, int64_t noc
  * and does not need fc_init.  Its scratch is a fixed 4 MiB array inside the
  * library, held by every device that loads the library until the process
  * exits; problems needing more (about 262,000 tiles of 64 x 64 virtual
- * indices, i.e. nocc(nocc+1)/2 * ceil(nvir/64)^2) are refused with
+ * indices, i.e. nocc(nocc+1)/2 * T(T+1)/2 with T = ceil(nvir/64)) are refused with
  * FC_ERR_LAYOUT.  The first call on a device looks up the array's device
  * address and sets the kernel's shared-memory limit; make that first call
  * before any stream capture.  All calls on a device share the one array
