@@ -48,7 +48,36 @@ SIGNATURES = {
     "fc_dfjk_set_precision": (_I32, [_P, _I32]),
     "fc_dfjk_destroy": (_I32, [_P]),
     "fc_rimp2_energy_noalloc": (_I32, [_P, _I64, _I64, _I64, _P, _P, _I32, _D, _DP, _DP, _P]),
+    "fc_rimp2_batched_create": (_I32, [_P, _I64, _I32, _c.POINTER(_P)]),
+    "fc_rimp2_batched_replay": (_I32, [_P, _P]),
+    "fc_rimp2_batched_energies": (_I32, [_P, _DP, _DP]),
+    "fc_rimp2_batched_info": (_I32, [_P, _P]),
+    "fc_rimp2_batched_destroy": (_I32, [_P]),
+    "fc_rimp2_batched": (_I32, [_P, _I64, _I32, _DP, _DP]),
 }
+
+
+class FcMolDesc(ctypes.Structure):
+    """``fc_mol_desc``: one molecule of a batch (device pointers)."""
+    _fields_ = [
+        ("b_ov", ctypes.c_void_p), ("eps_occ", ctypes.c_void_p), ("eps_vir", ctypes.c_void_p),
+        ("naux", ctypes.c_int64), ("nocc", ctypes.c_int64), ("nvir", ctypes.c_int64),
+        ("gamma", ctypes.c_void_p), ("de_deps_occ", ctypes.c_void_p), ("de_deps_vir", ctypes.c_void_p),
+    ]
+
+
+class FcBatchInfo(ctypes.Structure):
+    """``fc_batch_info``."""
+    _fields_ = [
+        ("nmol", ctypes.c_int64), ("items", ctypes.c_int64), ("gemm_tiles", ctypes.c_int64),
+        ("launches", ctypes.c_int32), ("groups", ctypes.c_int32), ("pair_launches", ctypes.c_int32),
+        ("precision", ctypes.c_int32), ("grad", ctypes.c_int32),
+        ("tile_m", ctypes.c_int32), ("tile_n", ctypes.c_int32), ("k_panel", ctypes.c_int32),
+        ("flops", ctypes.c_double), ("last_ms", ctypes.c_double), ("bytes", ctypes.c_uint64),
+    ]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
 
 
 class FcStats(ctypes.Structure):

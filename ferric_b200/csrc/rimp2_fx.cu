@@ -29,6 +29,9 @@
 // mode: ordered pairs of an occupied chunk; writes Tt_ij = (2X - Y)/D (FP32)
 // and the dE/deps partials; the adjoint contraction Gamma = 4 B Tt^T runs in
 // gemm_fx_kernel with the same exact-level scheme.
+#include <algorithm>
+
+#include "batch.cuh"
 #include "fc_internal.cuh"
 #include "rimp2.cuh"
 #include "tc.cuh"
@@ -59,11 +62,12 @@ __constant__ int8_t kPFirst[6] = {1, 1, 0, 1, 0, 0};  // first product of its le
 // ---------------------------------------------------------- split kernels --
 
 // cmax[c] = max over rows of |B[r, c]| (as ordered uint64 bits of a double).
-__global__ void colmax_kernel(const double* __restrict__ B, int64_t rows, int64_t cols,
-                              int64_t rows_per_split, unsigned long long* cmax, int* bad) {
-    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void colmax_body(const double* __restrict__ B, int64_t rows, int64_t cols,
+                                            int64_t rows_per_split, unsigned long long* cmax, int* bad, int64_t bx,
+                                            int64_t by) {
+    const int64_t c = bx * 256 + threadIdx.x;
     if (c >= cols) return;
-    const int64_t r0 = (int64_t)blockIdx.y * rows_per_split;
+    const int64_t r0 = by * rows_per_split;
     const int64_t r1 = r0 + rows_per_split < rows ? r0 + rows_per_split : rows;
     double m = 0.0;
     bool nf = false;
@@ -74,6 +78,11 @@ __global__ void colmax_kernel(const double* __restrict__ B, int64_t rows, int64_
     }
     if (nf) atomicOr(bad, 1);
     atomicMax(cmax + c, (unsigned long long)__double_as_longlong(m));
+}
+
+__global__ void __launch_bounds__(256) colmax_kernel(const double* __restrict__ B, int64_t rows, int64_t cols,
+                                                     int64_t rows_per_split, unsigned long long* cmax, int* bad) {
+    colmax_body(B, rows, cols, rows_per_split, cmax, bad, blockIdx.x, blockIdx.y);
 }
 
 // Power-of-two scale with max / s in [64, 128).
@@ -106,13 +115,13 @@ __device__ __forceinline__ void fx_slices(double x, double inv_s, __nv_bfloat16&
 }
 
 // B[q, ia] -> Bt[s][i][a][q] (q < q_pad) integer slices at scale scl[i*a_pad+a].
-__global__ void __launch_bounds__(256) split_fx_transpose_kernel(const double* __restrict__ B, int64_t naux,
-                                                                 int64_t nocc, int64_t nvir, int64_t a_pad,
-                                                                 int64_t q_pad, const double* __restrict__ scl,
-                                                                 __nv_bfloat16* __restrict__ Bt) {
+__device__ __forceinline__ void split_fx_transpose_body(const double* __restrict__ B, int64_t naux, int64_t nocc,
+                                                        int64_t nvir, int64_t a_pad, int64_t q_pad,
+                                                        const double* __restrict__ scl,
+                                                        __nv_bfloat16* __restrict__ Bt, int64_t bx, int64_t by) {
     __shared__ double tile[64][65];
     const int64_t nov = nocc * nvir;
-    const int64_t q0 = (int64_t)blockIdx.y * 64, ia0 = (int64_t)blockIdx.x * 64;
+    const int64_t q0 = by * 64, ia0 = bx * 64;
     const int tid = threadIdx.x;
 #pragma unroll
     for (int e = 0; e < 16; ++e) {
@@ -139,6 +148,13 @@ __global__ void __launch_bounds__(256) split_fx_transpose_kernel(const double* _
     }
 }
 
+__global__ void __launch_bounds__(256) split_fx_transpose_kernel(const double* __restrict__ B, int64_t naux,
+                                                                 int64_t nocc, int64_t nvir, int64_t a_pad,
+                                                                 int64_t q_pad, const double* __restrict__ scl,
+                                                                 __nv_bfloat16* __restrict__ Bt) {
+    split_fx_transpose_body(B, naux, nocc, nvir, a_pad, q_pad, scl, Bt, blockIdx.x, blockIdx.y);
+}
+
 __global__ void fill_kernel(double* __restrict__ x, int64_t n, double v) {
     const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k < n) x[k] = v;
@@ -146,13 +162,13 @@ __global__ void fill_kernel(double* __restrict__ x, int64_t n, double v) {
 
 // Per-Q-row split of B_ov over (j, b) with b padded to a_pad:
 // Bq[s][q][j*a_pad + b] (q < q_rows), scale qs[q].  One CTA per Q row.
-__global__ void __launch_bounds__(256) split_fx_qrows_kernel(const double* __restrict__ B, int64_t naux,
-                                                             int64_t nocc, int64_t nvir, int64_t a_pad,
-                                                             int64_t q_rows, double* __restrict__ qs,
-                                                             __nv_bfloat16* __restrict__ Bq) {
+// Row q of B_ov -> Bq[s][q][j*tpad + b] (row pitch K) at the row's scale qs[q].
+__device__ __forceinline__ void split_fx_qrows_body(const double* __restrict__ B, int64_t nocc, int64_t nvir,
+                                                    int64_t tpad, int64_t K, int64_t q_rows,
+                                                    double* __restrict__ qs, __nv_bfloat16* __restrict__ Bq,
+                                                    int64_t q) {
     __shared__ double red[32];
-    const int64_t q = blockIdx.x;
-    const int64_t nov = nocc * nvir, K = nocc * a_pad;
+    const int64_t nov = nocc * nvir;
     const double* row = B + q * nov;
     double m = 0.0;
     for (int64_t k = threadIdx.x; k < nov; k += 256) m = fmax(m, fabs(row[k]));
@@ -175,22 +191,29 @@ __global__ void __launch_bounds__(256) split_fx_qrows_kernel(const double* __res
         const int64_t j = k / nvir, b = k % nvir;
         __nv_bfloat16 c1, c2, c3;
         fx_slices(row[k], inv, c1, c2, c3);
-        const int64_t d = j * a_pad + b;
+        const int64_t d = j * tpad + b;
         o0[d] = c1;
         o0[ss + d] = c2;
         o0[2 * ss + d] = c3;
     }
 }
 
-// Per-row split of the FP32 amplitude chunk T[rows][K] -> Ts[s][rows][K],
-// ts[row].  One CTA per row; the row is read twice (max, then slices).
-__global__ void __launch_bounds__(256) split_fx_rows_f32_kernel(const float* __restrict__ T, int64_t K,
-                                                                int64_t slice_rows, double* __restrict__ ts,
-                                                                __nv_bfloat16* __restrict__ Ts) {
+__global__ void __launch_bounds__(256) split_fx_qrows_kernel(const double* __restrict__ B, int64_t naux,
+                                                             int64_t nocc, int64_t nvir, int64_t a_pad,
+                                                             int64_t q_rows, double* __restrict__ qs,
+                                                             __nv_bfloat16* __restrict__ Bq) {
+    split_fx_qrows_body(B, nocc, nvir, a_pad, nocc * a_pad, q_rows, qs, Bq, blockIdx.x);
+}
+
+// Per-row split of the FP32 amplitude chunk T[rows][pitch] (first Kv columns)
+// -> Ts[s][rows][pitch], ts[row].  One CTA per row; the row is read twice
+// (max, then slices).  Kv and pitch are multiples of 4.
+__device__ __forceinline__ void split_fx_rows_f32_body(const float* __restrict__ T, int64_t Kv, int64_t K,
+                                                       int64_t slice_rows, double* __restrict__ ts,
+                                                       __nv_bfloat16* __restrict__ Ts, int64_t r) {
     __shared__ double red[32];
-    const int64_t r = blockIdx.x;
     const float4* row = reinterpret_cast<const float4*>(T + r * K);
-    const int64_t K4 = K / 4;
+    const int64_t K4 = Kv / 4;
     float m = 0.f;
     for (int64_t k = threadIdx.x; k < K4; k += 256) {
         const float4 v = row[k];
@@ -235,9 +258,30 @@ __global__ void __launch_bounds__(256) split_fx_rows_f32_kernel(const float* __r
     }
 }
 
+__global__ void __launch_bounds__(256) split_fx_rows_f32_kernel(const float* __restrict__ T, int64_t K,
+                                                                int64_t slice_rows, double* __restrict__ ts,
+                                                                __nv_bfloat16* __restrict__ Ts) {
+    split_fx_rows_f32_body(T, K, K, slice_rows, ts, Ts, blockIdx.x);
+}
+
 // ------------------------------------------------------------ pair kernel --
 
+// One molecule of a batch (operand rows row0 .. row0 + 3*nocc*a_pad of the
+// concatenated slice buffer, slice-major).
+struct BatchMol {
+    const double* eo;
+    const double* ev;
+    const double* scl;
+    int nocc, nvir, a_pad, nk;
+    int row0, tpad;  // tpad: virtual pitch of the amplitude rows/columns (gradient)
+    float* T;        // amplitudes [nocc*tpad][ldt] (gradient)
+    int64_t ldt;
+};
+
 struct PairFxArgs {
+    // batch mode: item k is bitems[k] = (molecule, i, j, ta | tb << 16)
+    const int4* bitems;
+    const BatchMol* bmols;
     const double* eo;
     const double* ev;
     const double* scl;  // [nocc * a_pad] operand-row scales
@@ -257,7 +301,62 @@ struct PairFxArgs {
     double* vir_part;  // [item][128]
 };
 
-template <int GRAD>
+// Everything the roles need about item k.
+struct ItemView {
+    int i, j, ta, tb, nk, a_pad, nvir, row0, slice_rows, tpad, i0;
+    const double* eo;
+    const double* ev;
+    const double* scl;
+    float* T;
+    int64_t ldt;
+};
+
+template <int BATCH>
+__device__ __forceinline__ ItemView item_view(const PairFxArgs& p, int64_t k) {
+    ItemView v;
+    if (BATCH) {
+        const int4 it = p.bitems[k];
+        const BatchMol& m = p.bmols[it.x];
+        v.i = it.y;
+        v.j = it.z;
+        v.ta = it.w & 0xFFFF;
+        v.tb = it.w >> 16;
+        v.nk = m.nk;
+        v.a_pad = m.a_pad;
+        v.nvir = m.nvir;
+        v.row0 = m.row0;
+        v.slice_rows = m.nocc * m.a_pad;
+        v.eo = m.eo;
+        v.ev = m.ev;
+        v.scl = m.scl;
+        v.tpad = m.tpad;
+        v.i0 = 0;
+        v.T = m.T;
+        v.ldt = m.ldt;
+    } else {
+        const int2 ij = p.pairs[k / p.ntiles];
+        const int2 tt = p.tiles[k % p.ntiles];
+        v.i = ij.x;
+        v.j = ij.y;
+        v.ta = tt.x;
+        v.tb = tt.y;
+        v.nk = p.nk;
+        v.a_pad = p.a_pad;
+        v.nvir = p.nvir;
+        v.row0 = 0;
+        v.slice_rows = p.nocc * p.a_pad;
+        v.eo = p.eo;
+        v.ev = p.ev;
+        v.scl = p.scl;
+        v.tpad = p.a_pad;
+        v.i0 = p.i0;
+        v.T = p.T;
+        v.ldt = p.ldt;
+    }
+    return v;
+}
+
+template <int GRAD, int BATCH = 0>
 __global__ void __launch_bounds__(320, 1)
     pair_fx_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                    const PairFxArgs p) {
@@ -303,24 +402,23 @@ __global__ void __launch_bounds__(320, 1)
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem_base = *tmem_slot;
-    const int64_t tpp = p.ntiles;  // tiles per pair
 
     auto sa = [&](int s, int sl) { return base_u32 + s * STAGE_BYTES + sl * A_BYTES; };
     auto sb = [&](int s, int sl) { return base_u32 + s * STAGE_BYTES + NSL * A_BYTES + sl * B_BYTES; };
-    auto row_of = [&](int sl, int i, int r0) { return (sl * p.nocc + i) * p.a_pad + r0; };
+    auto row_of = [&](const ItemView& v, int sl, int i, int r0) {
+        return v.row0 + sl * v.slice_rows + i * v.a_pad + r0;
+    };
 
     if (warp == 0) {
         // ------------------------------------------------------ TMA producer
         if (lane == 0) {
             uint32_t g = 0;
             for (int64_t k = blockIdx.x; k < p.items && !*abort_flag; k += gridDim.x) {
-                const int2 ij = p.pairs[k / tpp];
-                const int2 tt = p.tiles[k % tpp];
-                const int ta = tt.x, tb = tt.y;
-                const int nph = ij.x == ij.y ? 1 : 2;
+                const ItemView v = item_view<BATCH>(p, k);
+                const int nph = v.i == v.j ? 1 : 2;
                 for (int ph = 0; ph < nph; ++ph) {
-                    const int ia = ph == 0 ? ij.x : ij.y, ib = ph == 0 ? ij.y : ij.x;
-                    for (int kt = 0; kt < p.nk; ++kt, ++g) {
+                    const int ia = ph == 0 ? v.i : v.j, ib = ph == 0 ? v.j : v.i;
+                    for (int kt = 0; kt < v.nk; ++kt, ++g) {
                         const int s = g % S;
                         const uint32_t u = g / S;
                         if (!tc::mbar_wait(&empty[s], (u & 1) ^ 1, abort_flag, p.err)) goto prod_done;
@@ -328,9 +426,9 @@ __global__ void __launch_bounds__(320, 1)
 #pragma unroll
                         for (int sl = 0; sl < NSL; ++sl) {
                             tc::tma_load_2d(base + (sa(s, sl) - base_u32), &tmA, &full[s], kt * KT,
-                                            row_of(sl, ia, ta * BM));
+                                            row_of(v, sl, ia, v.ta * BM));
                             tc::tma_load_2d(base + (sb(s, sl) - base_u32), &tmB, &full[s], kt * KT,
-                                            row_of(sl, ib, tb * BN));
+                                            row_of(v, sl, ib, v.tb * BN));
                         }
                     }
                 }
@@ -347,12 +445,12 @@ __global__ void __launch_bounds__(320, 1)
         if (lane == 0) {
             uint32_t g = 0, pc = 0;  // pc: phases issued (TMEM hand-overs)
             for (int64_t k = blockIdx.x; k < p.items && !*abort_flag; k += gridDim.x) {
-                const int2 ij = p.pairs[k / tpp];
-                const int nph = ij.x == ij.y ? 1 : 2;
+                const ItemView v = item_view<BATCH>(p, k);
+                const int nph = v.i == v.j ? 1 : 2;
                 for (int ph = 0; ph < nph; ++ph, ++pc) {
                     if (!tc::mbar_wait(tempty, (pc & 1) ^ 1, abort_flag, p.err)) goto mma_done;
                     tc::fence_after_sync();
-                    for (int kt = 0; kt < p.nk; ++kt, ++g) {
+                    for (int kt = 0; kt < v.nk; ++kt, ++g) {
                         const int s = g % S;
                         const uint32_t u = g / S;
                         if (!tc::mbar_wait(&full[s], u & 1, abort_flag, p.err)) goto mma_done;
@@ -389,26 +487,25 @@ __global__ void __launch_bounds__(320, 1)
         const uint32_t tl = tmem_base + ((uint32_t)(q * 32) << 16) + h * HC;
         uint32_t li = 0, pc = 0;
         for (int64_t k = blockIdx.x; k < p.items; k += gridDim.x, ++li) {
-            const int2 ij = p.pairs[k / tpp];
-            const int i = ij.x, j = ij.y;
+            const ItemView v = item_view<BATCH>(p, k);
+            const int i = v.i, j = v.j;
             const bool diag = i == j;
-            const int2 tt2 = p.tiles[k % tpp];
-            const int ta = tt2.x, tb = tt2.y;
+            const int ta = v.ta, tb = v.tb;
             // tiles ta <= tb only: X_ba = Y_ab, so the mirrored tile (tb, ta) is this
             // tile transposed.  Energy mode weights it 2; gradient mode also
             // writes its amplitudes (transposed) and its derivative terms.
             const double wt = (!GRAD && ta < tb) ? 2.0 : 1.0;
             const bool mir = GRAD && ta < tb;
             const int a = ta * BM + row;
-            const bool va = a < p.nvir;
-            const double dA = p.eo[i] + p.eo[j] - (va ? p.ev[a] : 0.0);
-            const double sxa = p.scl[(int64_t)i * p.a_pad + a];
-            const double sya = p.scl[(int64_t)j * p.a_pad + a];
+            const bool va = a < v.nvir;
+            const double dA = v.eo[i] + v.eo[j] - (va ? v.ev[a] : 0.0);
+            const double sxa = v.scl[(int64_t)i * v.a_pad + a];
+            const double sya = v.scl[(int64_t)j * v.a_pad + a];
             const int b0 = tb * BN + h * HC;  // first column of this thread
-            const double* sxb = p.scl + (int64_t)j * p.a_pad + b0;
-            const double* syb = p.scl + (int64_t)i * p.a_pad + b0;
-            const double* evb = p.ev + b0;
-            const int bmax = p.nvir - b0;    // columns c < bmax are real virtuals
+            const double* sxb = v.scl + (int64_t)j * v.a_pad + b0;
+            const double* syb = v.scl + (int64_t)i * v.a_pad + b0;
+            const double* evb = v.ev + b0;
+            const int bmax = v.nvir - b0;    // columns c < bmax are real virtuals
 
             // X phase: park (ia|jb) of this half row in registers (FP32, round to nearest)
             if (!tc::mbar_wait(tfull, pc & 1, abort_flag, p.err)) break;
@@ -488,14 +585,26 @@ __global__ void __launch_bounds__(320, 1)
                     if (GRAD) xr[c0 + cc] = colv;  // x of this column is consumed: keep cm there
                 }
                 if (GRAD) {
-                    float* trow = p.T + ((int64_t)(i - p.i0) * p.a_pad) * p.ldt + (int64_t)j * p.a_pad;
-                    float4* dst = reinterpret_cast<float4*>(trow + (int64_t)a * p.ldt + b0 + c0);
-                    dst[0] = make_float4(tt8[0], tt8[1], tt8[2], tt8[3]);
-                    dst[1] = make_float4(tt8[4], tt8[5], tt8[6], tt8[7]);
-                    if (mir) {
+                    // amplitude rows (i, a) and columns (j, b) at pitch tpad (>= nvir);
+                    // elements with a or b >= tpad belong to no amplitude
+                    float* trow = v.T + ((int64_t)(i - v.i0) * v.tpad) * v.ldt + (int64_t)j * v.tpad;
+                    const int bw = v.tpad - (b0 + c0);  // columns of this group inside the pitch
+                    if (a < v.tpad) {
+                        float* d = trow + (int64_t)a * v.ldt + b0 + c0;
+                        if (bw >= 8) {
+                            float4* dst = reinterpret_cast<float4*>(d);
+                            dst[0] = make_float4(tt8[0], tt8[1], tt8[2], tt8[3]);
+                            dst[1] = make_float4(tt8[4], tt8[5], tt8[6], tt8[7]);
+                        } else {
+#pragma unroll
+                            for (int cc = 0; cc < 8; ++cc)
+                                if (cc < bw) d[cc] = tt8[cc];
+                        }
+                    }
+                    if (mir && a < v.tpad) {
 #pragma unroll
                         for (int cc = 0; cc < 8; ++cc)  // lanes hold consecutive a: coalesced
-                            trow[(int64_t)(b0 + c0 + cc) * p.ldt + a] = mv8[cc];
+                            if (cc < bw) trow[(int64_t)(b0 + c0 + cc) * v.ldt + a] = mv8[cc];
                     }
                 }
             }
@@ -529,10 +638,10 @@ __global__ void __launch_bounds__(320, 1)
             if (GRAD && h == 0) p.vir_part[k * 2 * BM + row] = rowc + rowsh[row];
             if (mir && et < BM) {
                 const int hh = et >> 6, c = et & 63;
-                double v = 0.0;
+                double cs = 0.0;
 #pragma unroll
-                for (int qq = 0; qq < 4; ++qq) v += colsh[(qq * 2 + hh) * 64 + c];
-                p.vir_part[k * 2 * BM + BM + et] = v;
+                for (int qq = 0; qq < 4; ++qq) cs += colsh[(qq * 2 + hh) * 64 + c];
+                p.vir_part[k * 2 * BM + BM + et] = cs;
             }
             if (et == 0) {
                 KSum so, sn, sc;
@@ -562,6 +671,18 @@ __global__ void __launch_bounds__(320, 1)
 
 // --------------------------------------------------- adjoint contraction --
 
+// One molecule of a batched adjoint contraction: its own tensor maps (in
+// global memory), scales, shape and output.
+struct GemmMol {
+    const CUtensorMap* tA;  // amplitude slices [3][M][K]
+    const CUtensorMap* tB;  // Q-row slices [3][N][K]
+    const double* rs;
+    const double* cs;
+    int M, N, nk, tpad, nvir, naux, rows, pad_;
+    int64_t nov;
+    double* out;
+};
+
 struct GemmFxArgs {
     const double* rs;  // [M] scales of the A rows (amplitude rows (i, a))
     const double* cs;  // [N] scales of the B rows (Q)
@@ -573,7 +694,64 @@ struct GemmFxArgs {
     double alpha;
     double* out;  // Gamma (naux, nov)
     int* err;
+    // batch mode: tile t is bitems[t] = (molecule, m-tile, n-tile, 0)
+    const int4* bitems;
+    const GemmMol* gmols;
 };
+
+struct GemmView {
+    const CUtensorMap* tA;
+    const CUtensorMap* tB;
+    const double* rs;
+    const double* cs;
+    double* out;
+    int64_t nov;
+    int tm, tn, M, N, nk, tpad, nvir, naux, rows, i0;
+};
+
+template <int BATCH>
+__device__ __forceinline__ GemmView gemm_view(const GemmFxArgs& p, const CUtensorMap* tmA, const CUtensorMap* tmB,
+                                              int64_t t) {
+    GemmView v;
+    if (BATCH) {
+        const int4 it = p.bitems[t];
+        const GemmMol& g = p.gmols[it.x];
+        v.tA = g.tA;
+        v.tB = g.tB;
+        v.rs = g.rs;
+        v.cs = g.cs;
+        v.out = g.out;
+        v.nov = g.nov;
+        v.tm = it.y;
+        v.tn = it.z;
+        v.M = g.M;
+        v.N = g.N;
+        v.nk = g.nk;
+        v.tpad = g.tpad;
+        v.nvir = g.nvir;
+        v.naux = g.naux;
+        v.rows = g.rows;
+        v.i0 = 0;
+    } else {
+        v.tA = tmA;
+        v.tB = tmB;
+        v.rs = p.rs;
+        v.cs = p.cs;
+        v.out = p.out;
+        v.nov = p.nov;
+        v.tm = (int)(t / p.nTn);
+        v.tn = (int)(t % p.nTn);
+        v.M = p.M;
+        v.N = p.N;
+        v.nk = p.nk;
+        v.tpad = p.a_pad;
+        v.nvir = p.nvir;
+        v.naux = p.naux;
+        v.rows = p.nTm * 128;
+        v.i0 = p.i0;
+    }
+    return v;
+}
 
 constexpr int GF_STAGE = 3 * (16384 + 16384);  // 96 KiB
 constexpr int GF_STAGES = 2;
@@ -581,6 +759,7 @@ constexpr int GF_SMEM = GF_STAGES * GF_STAGE + 1024 + 1024;
 constexpr uint32_t GF_IDESC = tc::idesc_bf16_f32(128, 128);
 
 // out[Q, i*nvir + a] = alpha * s_row s_Q (L0 + L1/256 + L2/65536), rows = (i - i0, a).
+template <int BATCH = 0>
 __global__ void __launch_bounds__(192, 1)
     gemm_fx_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                    const GemmFxArgs p) {
@@ -611,7 +790,7 @@ __global__ void __launch_bounds__(192, 1)
         *abort_flag = 0;
         tc::fence_barrier_init();
     }
-    if (warp == 0 && lane == 0) {
+    if (warp == 0 && lane == 0 && !BATCH) {
         tc::prefetch_tmap(&tmA);
         tc::prefetch_tmap(&tmB);
     }
@@ -630,16 +809,20 @@ __global__ void __launch_bounds__(192, 1)
         if (lane == 0) {
             uint32_t g = 0;
             for (int64_t t = blockIdx.x; t < p.tiles && !*abort_flag; t += gridDim.x) {
-                const int tm = (int)(t / p.nTn), tn = (int)(t % p.nTn);
-                for (int kt = 0; kt < p.nk; ++kt, ++g) {
+                const GemmView v = gemm_view<BATCH>(p, &tmA, &tmB, t);
+                if (BATCH) {
+                    tc::tmap_acquire(v.tA);
+                    tc::tmap_acquire(v.tB);
+                }
+                for (int kt = 0; kt < v.nk; ++kt, ++g) {
                     const int s = g % S;
                     const uint32_t u = g / S;
                     if (!tc::mbar_wait(&empty[s], (u & 1) ^ 1, abort_flag, p.err)) goto prod_done;
                     tc::mbar_arrive_expect_tx(&full[s], GF_STAGE);
 #pragma unroll
                     for (int sl = 0; sl < 3; ++sl) {
-                        tc::tma_load_2d(base + (sa(s, sl) - base_u32), &tmA, &full[s], kt * KT, sl * p.M + tm * 128);
-                        tc::tma_load_2d(base + (sb(s, sl) - base_u32), &tmB, &full[s], kt * KT, sl * p.N + tn * 128);
+                        tc::tma_load_2d(base + (sa(s, sl) - base_u32), v.tA, &full[s], kt * KT, sl * v.M + v.tm * 128);
+                        tc::tma_load_2d(base + (sb(s, sl) - base_u32), v.tB, &full[s], kt * KT, sl * v.N + v.tn * 128);
                     }
                 }
             }
@@ -654,9 +837,10 @@ __global__ void __launch_bounds__(192, 1)
         if (lane == 0) {
             uint32_t g = 0, li = 0;
             for (int64_t t = blockIdx.x; t < p.tiles && !*abort_flag; t += gridDim.x, ++li) {
+                const int nk = BATCH ? p.gmols[p.bitems[t].x].nk : p.nk;
                 if (!tc::mbar_wait(tempty, (li & 1) ^ 1, abort_flag, p.err)) break;
                 tc::fence_after_sync();
-                for (int kt = 0; kt < p.nk; ++kt, ++g) {
+                for (int kt = 0; kt < nk; ++kt, ++g) {
                     const int s = g % S;
                     const uint32_t u = g / S;
                     if (!tc::mbar_wait(&full[s], u & 1, abort_flag, p.err)) goto mma_done;
@@ -685,14 +869,14 @@ __global__ void __launch_bounds__(192, 1)
         const int row = q * 32 + lane;
         uint32_t li = 0;
         for (int64_t t = blockIdx.x; t < p.tiles; t += gridDim.x, ++li) {
-            const int tm = (int)(t / p.nTn), tn = (int)(t % p.nTn);
+            const GemmView v = gemm_view<BATCH>(p, &tmA, &tmB, t);
             if (!tc::mbar_wait(tfull, li & 1, abort_flag, p.err)) break;
             tc::fence_after_sync();
-            const int m = tm * 128 + row;           // amplitude row (i - i0, a)
-            const int il = m / p.a_pad, a = m % p.a_pad;
-            const bool vm = a < p.nvir;
-            const double sr = p.alpha * p.rs[m];
-            double* orow = p.out + (int64_t)(p.i0 + il) * p.nvir + a;
+            const int m = v.tm * 128 + row;         // amplitude row (i - i0, a)
+            const int il = m / v.tpad, a = m % v.tpad;
+            const bool vm = a < v.nvir && m < v.rows;
+            const double sr = vm ? p.alpha * v.rs[m] : 0.0;
+            double* orow = v.out + (int64_t)(v.i0 + il) * v.nvir + a;
             const uint32_t tl = tmem_base + ((uint32_t)(q * 32) << 16);
 #pragma unroll 1
             for (int c0 = 0; c0 < 128; c0 += 16) {
@@ -704,10 +888,10 @@ __global__ void __launch_bounds__(192, 1)
                 if (vm) {
 #pragma unroll
                     for (int cc = 0; cc < 16; ++cc) {
-                        const int Q = tn * 128 + c0 + cc;
-                        if (Q < p.naux)
-                            orow[(int64_t)Q * p.nov] =
-                                sr * p.cs[Q] * ((double)l0[cc] + (double)l1[cc] * L1W + (double)l2[cc] * L2W);
+                        const int Q = v.tn * 128 + c0 + cc;
+                        if (Q < v.naux)
+                            orow[(int64_t)Q * v.nov] =
+                                sr * v.cs[Q] * ((double)l0[cc] + (double)l1[cc] * L1W + (double)l2[cc] * L2W);
                     }
                 }
             }
@@ -785,6 +969,160 @@ __global__ void __launch_bounds__(256) fx_reduce_vir_kernel(const double* __rest
     if (lane == 0) acc_vir[v] += 2.0 * r;
 }
 
+// ------------------------------------------------------- batch kernels --
+//
+// One launch covers every molecule of a batch (or of one group of it): the
+// flat block (or thread, or warp) index is mapped to its molecule by a binary
+// search over a per-molecule prefix of that launch's work units.
+
+// Everything the batched split / reduce kernels need about one molecule.
+struct BatchPrep {
+    const double* b;   // B_ov (naux, nocc*nvir)
+    int64_t naux, nocc, nvir, a_pad, q_pad, tpad, ldt, q_rows, M;
+    unsigned long long* cmax;  // [nocc*nvir]
+    double* scl;               // [nocc*a_pad] pair-operand row scales
+    __nv_bfloat16* bt;         // pair-operand slices (rows of this molecule)
+    double* qs;                // [q_rows] Q-row scales (gradient)
+    __nv_bfloat16* bq;         // Q-row slices [3][q_rows][ldt]
+    float* T;                  // amplitudes [nocc*tpad][ldt]
+    double* ts;                // [M] amplitude-row scales
+    __nv_bfloat16* Ts;         // amplitude slices [3][M][ldt]
+    double* de_docc;           // [nocc]
+    double* de_dvir;           // [nvir]
+    int64_t seg0;              // first item of this molecule
+    int64_t items_per_i;       // nocc * tiles per pair (gradient items)
+};
+
+// Largest m in [lo, hi) with pre[m] <= x.
+__device__ __forceinline__ int seg_find(const int64_t* __restrict__ pre, int lo, int hi, int64_t x) {
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (pre[mid] <= x) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+enum BatchPre { PRE_COLMAX, PRE_ROWSCALE, PRE_TRANSPOSE, PRE_QROWS, PRE_TROWS, PRE_OCC, PRE_VIR, PRE_COUNT };
+
+__global__ void __launch_bounds__(256) batch_colmax_kernel(const BatchPrep* __restrict__ mp,
+                                                           const int64_t* __restrict__ pre, int nmol, int* bad) {
+    const int64_t x = blockIdx.x;
+    const int m = seg_find(pre, 0, nmol, x);
+    const BatchPrep& d = mp[m];
+    const int64_t nov = d.nocc * d.nvir, nbx = (nov + 255) / 256, loc = x - pre[m];
+    colmax_body(d.b, d.naux, nov, 64, d.cmax, bad, loc % nbx, loc / nbx);
+}
+
+__global__ void __launch_bounds__(256) batch_row_scale_kernel(const BatchPrep* __restrict__ mp,
+                                                              const int64_t* __restrict__ pre, int nmol) {
+    const int64_t x = (int64_t)blockIdx.x * 256 + threadIdx.x;
+    if (x >= pre[nmol]) return;
+    const int m = seg_find(pre, 0, nmol, x);
+    const BatchPrep& d = mp[m];
+    const int64_t r = x - pre[m], i = r / d.a_pad, a = r % d.a_pad;
+    d.scl[r] = a < d.nvir ? pow2_scale(__longlong_as_double((long long)d.cmax[i * d.nvir + a])) : 1.0;
+}
+
+__global__ void __launch_bounds__(256) batch_transpose_kernel(const BatchPrep* __restrict__ mp,
+                                                              const int64_t* __restrict__ pre, int nmol) {
+    const int64_t x = blockIdx.x;
+    const int m = seg_find(pre, 0, nmol, x);
+    const BatchPrep& d = mp[m];
+    const int64_t nbx = (d.nocc * d.nvir + 63) / 64, loc = x - pre[m];
+    split_fx_transpose_body(d.b, d.naux, d.nocc, d.nvir, d.a_pad, d.q_pad, d.scl, d.bt, loc % nbx, loc / nbx);
+}
+
+__global__ void __launch_bounds__(256) batch_qrows_kernel(const BatchPrep* __restrict__ mp,
+                                                          const int64_t* __restrict__ pre, int nmol) {
+    const int64_t x = blockIdx.x;
+    const int m = seg_find(pre, 0, nmol, x);
+    const BatchPrep& d = mp[m];
+    split_fx_qrows_body(d.b, d.nocc, d.nvir, d.tpad, d.ldt, d.q_rows, d.qs, d.bq, x - pre[m]);
+}
+
+// Amplitude rows of the molecules [m0, m1).
+__global__ void __launch_bounds__(256) batch_trows_kernel(const BatchPrep* __restrict__ mp,
+                                                          const int64_t* __restrict__ pre, int m0, int m1) {
+    const int64_t x = pre[m0] + blockIdx.x;
+    const int m = seg_find(pre, m0, m1, x);
+    const BatchPrep& d = mp[m];
+    split_fx_rows_f32_body(d.T, d.nocc * d.tpad, d.ldt, d.M, d.ts, d.Ts, x - pre[m]);
+}
+
+// dE/deps_i = -2 sum over the items (i, j, tiles) of their t~Tt partials.
+__global__ void __launch_bounds__(256) batch_occ_kernel(const BatchPrep* __restrict__ mp,
+                                                        const int64_t* __restrict__ pre, int m0, int m1,
+                                                        const double* __restrict__ occ_part) {
+    __shared__ double sh[256];
+    const int64_t x = pre[m0] + blockIdx.x;
+    const int m = seg_find(pre, m0, m1, x);
+    const BatchPrep& d = mp[m];
+    const int64_t i = x - pre[m];
+    const double* src = occ_part + d.seg0 + i * d.items_per_i;
+    KSum a;
+    for (int64_t k = threadIdx.x; k < d.items_per_i; k += 256) a.add(src[k]);
+    sh[threadIdx.x] = a.value();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        KSum t;
+        for (int k = 0; k < 256; ++k) t.add(sh[k]);
+        d.de_docc[i] = -2.0 * t.value();
+    }
+}
+
+// dE/deps_v = 2 sum of the row partials of v (tiles with v in the a-tile) and
+// the column partials (mirrored tiles with v in the b-tile); one warp per v.
+// vir_part is indexed from the group's first item g0.
+__global__ void __launch_bounds__(256) batch_vir_kernel(const BatchPrep* __restrict__ mp,
+                                                        const int64_t* __restrict__ pre, int m0, int m1,
+                                                        const int4* __restrict__ items, int64_t g0,
+                                                        const double* __restrict__ vir_part) {
+    const int64_t x = pre[m0] + (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (x >= pre[m1]) return;
+    const int m = seg_find(pre, m0, m1, x);
+    const BatchPrep& d = mp[m];
+    const int v = (int)(x - pre[m]);
+    const int tv = v / fx::BM, rv = v % fx::BM;
+    const int64_t k1 = d.seg0 + d.nocc * d.items_per_i;
+    KSum s;
+    for (int64_t k = d.seg0 + lane; k < k1; k += 32) {
+        const int w = items[k].w;
+        const int ta = w & 0xFFFF, tb = w >> 16;
+        const double* vp = vir_part + (k - g0) * 2 * fx::BM;
+        if (ta == tv) s.add(vp[rv]);
+        if (tb == tv && ta < tb) s.add(vp[fx::BM + rv]);
+    }
+    const double r = warp_sum(s.value());
+    if (lane == 0) d.de_dvir[v] = 2.0 * r;
+}
+
+// Per-molecule (e_os, e_ss) of the molecules [m0, m1): items [seg[m], seg[m+1]).
+__global__ void __launch_bounds__(256) batch_energy_kernel(const double* __restrict__ part,
+                                                           const int64_t* __restrict__ seg, int m0,
+                                                           double* out) {
+    __shared__ double so[256], sn[256];
+    const int m = m0 + blockIdx.x;
+    KSum a, b;
+    for (int64_t k = seg[m] + threadIdx.x; k < seg[m + 1]; k += 256) {
+        a.add(part[2 * k]);
+        b.add(part[2 * k + 1]);
+    }
+    so[threadIdx.x] = a.value();
+    sn[threadIdx.x] = b.value();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        KSum x, y;
+        for (int t = 0; t < 256; ++t) {
+            x.add(so[t]);
+            y.add(sn[t]);
+        }
+        out[2 * m] = x.value();
+        out[2 * m + 1] = y.value();
+    }
+}
+
 // ------------------------------------------------------------------ host --
 
 namespace {
@@ -834,9 +1172,12 @@ fc_status fx_split_pairs(const Rimp2Dev& d, cudaStream_t st, int* bad, FxSplit* 
 fc_status fx_attrs() {
     static bool done = false;
     if (done) return FC_OK;
+    FC_CUDA(cudaFuncSetAttribute(pair_fx_kernel<0, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, fx::SMEM));
     FC_CUDA(cudaFuncSetAttribute(pair_fx_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, fx::SMEM));
     FC_CUDA(cudaFuncSetAttribute(pair_fx_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, fx::SMEM));
-    FC_CUDA(cudaFuncSetAttribute(gemm_fx_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, GF_SMEM));
+    FC_CUDA(cudaFuncSetAttribute(gemm_fx_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, GF_SMEM));
+    FC_CUDA(cudaFuncSetAttribute(gemm_fx_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, GF_SMEM));
+    FC_CUDA(cudaFuncSetAttribute(pair_fx_kernel<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, fx::SMEM));
     done = true;
     return FC_OK;
 }
@@ -1048,7 +1389,7 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
         gargs.out = gamma;
         gargs.err = flags + 1;
         const int g2 = (int)(gargs.tiles < c.sm_count ? gargs.tiles : c.sm_count);
-        gemm_fx_kernel<<<g2, 192, GF_SMEM, st>>>(tmTs, tmBq, gargs);
+        gemm_fx_kernel<0><<<g2, 192, GF_SMEM, st>>>(tmTs, tmBq, gargs);
         FC_TRY(check_launch("gemm_fx_kernel"));
     }
     if (stats) FC_CUDA(cudaEventRecord(c.ev1, st));
@@ -1094,6 +1435,301 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
         stats->h2d_bytes += pairs.size() * sizeof(int2);
         stats->d2h_bytes += h.size() * 8 + sizeof(hf);
     }
+    return FC_OK;
+}
+
+// ---------------------------------------------------------------- batch --
+//
+// Layout of a batch.  Pair operands: all molecules' integer slices in one
+// buffer with a common row pitch (the largest padded aux range); molecule m
+// owns rows row0_m .. row0_m + 3 nocc_m a_pad_m, slice-major.  Items
+// (molecule, i, j, ta | tb << 16) are laid out molecule by molecule, i-major,
+// so a molecule's partials (and one i's) are contiguous; the persistent pair
+// kernel takes them round-robin, so every CTA mixes large and small
+// molecules.  Gradient: amplitudes of a molecule are stored at virtual pitch
+// tpad = nvir rounded up to 8 (not the 128-row tile pitch), and the adjoint
+// contraction reads them and the Q-row slices through per-molecule tensor
+// maps whose inner extent is the exact K = nocc tpad (the TMA zero-fills the
+// K tail).  Molecules are grouped so one group's amplitudes fit group_bytes;
+// groups run one after the other on the same workspace.
+namespace {
+int64_t rup(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+}  // namespace
+
+fc_status rimp2_batch_build_fx(fc_rimp2_batch* b, const std::vector<BatchMolIn>& mols, size_t group_bytes) {
+    FC_TRY(fx_attrs());
+    const int nmol = (int)mols.size();
+    const bool grad = b->grad != 0;
+    Context& c = ctx();
+    int64_t q_pad = fx::KT;
+    for (const auto& d : mols) q_pad = std::max(q_pad, rup(d.naux, fx::KT));
+    const int NP = nmol + 1;
+    std::vector<BatchPrep> hp(nmol);
+    std::vector<BatchMol> hm(nmol);
+    std::vector<int64_t> pre((size_t)PRE_COUNT * NP, 0), seg(NP, 0);
+    auto P = [&](int kind, int m) -> int64_t& { return pre[(size_t)kind * NP + m]; };
+    std::vector<int64_t> scl_off(nmol), cmax_off(nmol), qs_off(nmol), bq_off(nmol), t_off(nmol), ntp(nmol);
+    int64_t rows = 0, nscl = 0, ncmax = 0, nqs = 0, nbq = 0;
+    for (int m = 0; m < nmol; ++m) {
+        const auto& d = mols[m];
+        BatchPrep& x = hp[m];
+        const int64_t nov = d.nocc * d.nvir;
+        x.b = d.b_ov;
+        x.naux = d.naux;
+        x.nocc = d.nocc;
+        x.nvir = d.nvir;
+        x.a_pad = rup(d.nvir, fx::BM);
+        x.q_pad = q_pad;
+        x.tpad = grad ? rup(d.nvir, 8) : x.a_pad;
+        x.ldt = d.nocc * x.tpad;          // a multiple of 8
+        x.q_rows = rup(d.naux, 128);
+        x.M = rup(x.ldt, 128);
+        x.de_docc = d.de_deps_occ;
+        x.de_dvir = d.de_deps_vir;
+        const int64_t nT = x.a_pad / fx::BM;
+        ntp[m] = nT * (nT + 1) / 2;
+        const int64_t npair = grad ? d.nocc * d.nocc : d.nocc * (d.nocc + 1) / 2;
+        x.items_per_i = d.nocc * ntp[m];
+        x.seg0 = seg[m];
+        seg[m + 1] = seg[m] + npair * ntp[m];
+        scl_off[m] = nscl;
+        nscl += d.nocc * x.a_pad;
+        cmax_off[m] = ncmax;
+        ncmax += nov;
+        hm[m].row0 = (int)rows;
+        rows += 3 * d.nocc * x.a_pad;
+        qs_off[m] = nqs;
+        nqs += x.q_rows;
+        bq_off[m] = nbq;
+        nbq += 3 * x.q_rows * x.ldt;
+        P(PRE_COLMAX, m + 1) = P(PRE_COLMAX, m) + (nov + 255) / 256 * ((d.naux + 63) / 64);
+        P(PRE_ROWSCALE, m + 1) = P(PRE_ROWSCALE, m) + d.nocc * x.a_pad;
+        P(PRE_TRANSPOSE, m + 1) = P(PRE_TRANSPOSE, m) + (nov + 63) / 64 * ((d.naux + 63) / 64);
+        P(PRE_QROWS, m + 1) = P(PRE_QROWS, m) + d.naux;
+        P(PRE_TROWS, m + 1) = P(PRE_TROWS, m) + x.ldt;
+        P(PRE_OCC, m + 1) = P(PRE_OCC, m) + d.nocc;
+        P(PRE_VIR, m + 1) = P(PRE_VIR, m) + d.nvir;
+        const double P2 = (double)d.nocc * (d.nocc + 1) / 2.0;
+        b->flops += 2.0 * (double)d.naux * (double)d.nvir * (double)d.nvir * P2;
+        if (grad) b->flops += 2.0 * (double)d.naux * (double)nov * (double)nov;
+    }
+    const int64_t items = seg[nmol];
+    if (rows >= INT32_MAX || items >= INT32_MAX || P(PRE_COLMAX, nmol) >= INT32_MAX ||
+        P(PRE_TRANSPOSE, nmol) >= INT32_MAX || P(PRE_ROWSCALE, nmol) >= (int64_t)INT32_MAX * 256 ||
+        P(PRE_QROWS, nmol) >= INT32_MAX || P(PRE_TROWS, nmol) >= INT32_MAX)
+        return fail(FC_ERR_LAYOUT, "RI-MP2 batch too large for one graph");
+
+    // ---- groups of molecules whose amplitudes share one workspace
+    struct Group {
+        int m0, m1;
+        int64_t i0, i1, t0, t1;
+    };
+    std::vector<Group> groups;
+    size_t gws = 0, gvir = 0;
+    if (grad) {
+        size_t cur = 0;
+        int m0 = 0;
+        for (int m = 0; m < nmol; ++m) {
+            const BatchPrep& x = hp[m];
+            const size_t tb = rup(x.ldt * x.ldt * 4, 256) + rup(x.M * 8, 256) + rup(3 * x.M * x.ldt * 2, 256);
+            if (m > m0 && cur + tb > group_bytes) {
+                groups.push_back({m0, m, seg[m0], seg[m], 0, 0});
+                m0 = m;
+                cur = 0;
+            }
+            t_off[m] = (int64_t)cur;
+            cur += tb;
+            gws = std::max(gws, cur);
+        }
+        groups.push_back({m0, nmol, seg[m0], seg[nmol], 0, 0});
+        for (const auto& g : groups) gvir = std::max(gvir, (size_t)(g.i1 - g.i0) * 2 * fx::BM * 8);
+    }
+
+    // ---- device buffers
+    void *vbt, *vscl, *vcmax, *vmols, *vprep, *vpre, *vseg, *vitems, *vpart;
+    FC_TRY(batch_alloc(b, (size_t)rows * q_pad * 2, &vbt));
+    FC_TRY(batch_alloc(b, (size_t)nscl * 8, &vscl));
+    FC_TRY(batch_alloc(b, (size_t)ncmax * 8, &vcmax));
+    FC_TRY(batch_alloc(b, (size_t)nmol * sizeof(BatchMol), &vmols));
+    FC_TRY(batch_alloc(b, (size_t)nmol * sizeof(BatchPrep), &vprep));
+    FC_TRY(batch_alloc(b, pre.size() * 8, &vpre));
+    FC_TRY(batch_alloc(b, seg.size() * 8, &vseg));
+    FC_TRY(batch_alloc(b, (size_t)items * sizeof(int4), &vitems));
+    FC_TRY(batch_alloc(b, (size_t)items * 16, &vpart));
+    FC_CUDA(cudaMemset(vbt, 0, (size_t)rows * q_pad * 2));
+    void *vocc = nullptr, *vvir = nullptr, *vqs = nullptr, *vbq = nullptr, *vgws = nullptr;
+    void *vgm = nullptr, *vmaps = nullptr, *vgit = nullptr;
+    std::vector<int4> git;
+    if (grad) {
+        FC_TRY(batch_alloc(b, (size_t)items * 8, &vocc));
+        FC_TRY(batch_alloc(b, gvir, &vvir));
+        FC_TRY(batch_alloc(b, (size_t)nqs * 8, &vqs));
+        FC_TRY(batch_alloc(b, (size_t)nbq * 2, &vbq));
+        FC_TRY(batch_alloc(b, gws, &vgws));
+        FC_TRY(batch_alloc(b, (size_t)nmol * sizeof(GemmMol), &vgm));
+        FC_TRY(batch_alloc(b, (size_t)nmol * 2 * sizeof(CUtensorMap), &vmaps));
+        FC_CUDA(cudaMemset(vbq, 0, (size_t)nbq * 2));
+    }
+    // per-molecule pointers
+    std::vector<CUtensorMap> maps(grad ? 2 * nmol : 0);
+    std::vector<GemmMol> gm(grad ? nmol : 0);
+    for (int m = 0; m < nmol; ++m) {
+        BatchPrep& x = hp[m];
+        x.cmax = (unsigned long long*)vcmax + cmax_off[m];
+        x.scl = (double*)vscl + scl_off[m];
+        x.bt = (__nv_bfloat16*)vbt + (int64_t)hm[m].row0 * q_pad;
+        hm[m].eo = mols[m].eps_occ;
+        hm[m].ev = mols[m].eps_vir;
+        hm[m].scl = x.scl;
+        hm[m].nocc = (int)x.nocc;
+        hm[m].nvir = (int)x.nvir;
+        hm[m].a_pad = (int)x.a_pad;
+        hm[m].nk = (int)(rup(x.naux, fx::KT) / fx::KT);
+        hm[m].tpad = (int)x.tpad;
+        hm[m].T = nullptr;
+        hm[m].ldt = x.ldt;
+        if (grad) {
+            char* g0 = (char*)vgws + t_off[m];
+            x.T = (float*)g0;
+            x.ts = (double*)(g0 + rup(x.ldt * x.ldt * 4, 256));
+            x.Ts = (__nv_bfloat16*)(g0 + rup(x.ldt * x.ldt * 4, 256) + rup(x.M * 8, 256));
+            x.qs = (double*)vqs + qs_off[m];
+            x.bq = (__nv_bfloat16*)vbq + bq_off[m];
+            hm[m].T = x.T;
+            FC_TRY(make_tmap_bf16_2d(&maps[2 * m], x.Ts, x.ldt, 3 * x.M, x.ldt * 2, fx::KT, 128));
+            FC_TRY(make_tmap_bf16_2d(&maps[2 * m + 1], x.bq, x.ldt, 3 * x.q_rows, x.ldt * 2, fx::KT, 128));
+            GemmMol& g = gm[m];
+            g.tA = (const CUtensorMap*)vmaps + 2 * m;
+            g.tB = (const CUtensorMap*)vmaps + 2 * m + 1;
+            g.rs = x.ts;
+            g.cs = x.qs;
+            g.M = (int)x.M;
+            g.N = (int)x.q_rows;
+            g.nk = (int)((x.ldt + fx::KT - 1) / fx::KT);
+            g.tpad = (int)x.tpad;
+            g.nvir = (int)x.nvir;
+            g.naux = (int)x.naux;
+            g.rows = (int)x.ldt;
+            g.nov = x.nocc * x.nvir;
+            g.out = mols[m].gamma;
+        }
+    }
+    // work items
+    std::vector<int4> hi;
+    hi.reserve((size_t)items);
+    for (int m = 0; m < nmol; ++m) {
+        const int nocc = hm[m].nocc, nT = hm[m].a_pad / fx::BM;
+        for (int i = 0; i < nocc; ++i)
+            for (int j = grad ? 0 : i; j < nocc; ++j)
+                for (int ta = 0; ta < nT; ++ta)
+                    for (int tb = ta; tb < nT; ++tb) hi.push_back(make_int4(m, i, j, ta | (tb << 16)));
+    }
+    if (grad) {
+        for (auto& g : groups) {
+            g.t0 = (int64_t)git.size();
+            for (int m = g.m0; m < g.m1; ++m) {
+                const int ntm = (int)(hp[m].M / 128), ntn = (int)(hp[m].q_rows / 128);
+                for (int tm = 0; tm < ntm; ++tm)
+                    for (int tn = 0; tn < ntn; ++tn) git.push_back(make_int4(m, tm, tn, 0));
+            }
+            g.t1 = (int64_t)git.size();
+        }
+        FC_TRY(batch_alloc(b, git.size() * sizeof(int4), &vgit));
+        FC_CUDA(cudaMemcpy(vgit, git.data(), git.size() * sizeof(int4), cudaMemcpyHostToDevice));
+        FC_CUDA(cudaMemcpy(vgm, gm.data(), gm.size() * sizeof(GemmMol), cudaMemcpyHostToDevice));
+        FC_CUDA(cudaMemcpy(vmaps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice));
+    }
+    FC_CUDA(cudaMemcpy(vmols, hm.data(), hm.size() * sizeof(BatchMol), cudaMemcpyHostToDevice));
+    FC_CUDA(cudaMemcpy(vprep, hp.data(), hp.size() * sizeof(BatchPrep), cudaMemcpyHostToDevice));
+    FC_CUDA(cudaMemcpy(vpre, pre.data(), pre.size() * 8, cudaMemcpyHostToDevice));
+    FC_CUDA(cudaMemcpy(vseg, seg.data(), seg.size() * 8, cudaMemcpyHostToDevice));
+    FC_CUDA(cudaMemcpy(vitems, hi.data(), hi.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    CUtensorMap tmA, tmB;
+    FC_TRY(make_tmap_bf16_2d(&tmA, vbt, q_pad, rows, q_pad * 2, fx::KT, fx::BM));
+    FC_TRY(make_tmap_bf16_2d(&tmB, vbt, q_pad, rows, q_pad * 2, fx::KT, fx::BN));
+    FC_CUDA(cudaDeviceSynchronize());
+
+    // ---- the recorded sequence
+    cudaStream_t st = b->stream;
+    const BatchPrep* dp = (const BatchPrep*)vprep;
+    const int64_t* dpre = (const int64_t*)vpre;
+    auto PD = [&](int kind) { return dpre + (size_t)kind * NP; };
+    FC_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    fc_status rc = [&]() -> fc_status {
+        int launches = 0;
+        FC_CUDA(cudaMemsetAsync(b->flags, 0, 2 * sizeof(int), st));
+        FC_CUDA(cudaMemsetAsync(vcmax, 0, (size_t)ncmax * 8, st));
+        batch_colmax_kernel<<<(unsigned)P(PRE_COLMAX, nmol), 256, 0, st>>>(dp, PD(PRE_COLMAX), nmol, b->flags);
+        batch_row_scale_kernel<<<(unsigned)((P(PRE_ROWSCALE, nmol) + 255) / 256), 256, 0, st>>>(
+            dp, PD(PRE_ROWSCALE), nmol);
+        batch_transpose_kernel<<<(unsigned)P(PRE_TRANSPOSE, nmol), 256, 0, st>>>(dp, PD(PRE_TRANSPOSE), nmol);
+        launches += 3;
+        if (grad) {
+            batch_qrows_kernel<<<(unsigned)P(PRE_QROWS, nmol), 256, 0, st>>>(dp, PD(PRE_QROWS), nmol);
+            ++launches;
+        }
+        FC_TRY(check_launch("batch split kernels"));
+        PairFxArgs a{};
+        a.bitems = (const int4*)vitems;
+        a.bmols = (const BatchMol*)vmols;
+        a.err = b->flags + 1;
+        if (!grad) {
+            a.items = items;
+            a.part = (double*)vpart;
+            const int grid = (int)std::min<int64_t>(items, c.sm_count);
+            pair_fx_kernel<0, 1><<<grid, 320, fx::SMEM, st>>>(tmA, tmB, a);
+            batch_energy_kernel<<<(unsigned)nmol, 256, 0, st>>>((const double*)vpart, (const int64_t*)vseg, 0,
+                                                                  b->out);
+            FC_TRY(check_launch("batched pair kernel"));
+            launches += 2;
+            b->pair_launches = 1;
+        } else {
+            for (const auto& g : groups) {
+                const int64_t gi = g.i1 - g.i0;
+                a.bitems = (const int4*)vitems + g.i0;
+                a.items = gi;
+                a.part = (double*)vpart + 2 * g.i0;
+                a.occ_part = (double*)vocc + g.i0;
+                a.vir_part = (double*)vvir;
+                const int grid = (int)std::min<int64_t>(gi, c.sm_count);
+                pair_fx_kernel<1, 1><<<grid, 320, fx::SMEM, st>>>(tmA, tmB, a);
+                batch_energy_kernel<<<(unsigned)(g.m1 - g.m0), 256, 0, st>>>((const double*)vpart,
+                                                                               (const int64_t*)vseg, g.m0, b->out);
+                batch_occ_kernel<<<(unsigned)(P(PRE_OCC, g.m1) - P(PRE_OCC, g.m0)), 256, 0, st>>>(
+                    dp, PD(PRE_OCC), g.m0, g.m1, (const double*)vocc);
+                batch_vir_kernel<<<(unsigned)((P(PRE_VIR, g.m1) - P(PRE_VIR, g.m0) + 7) / 8), 256, 0, st>>>(
+                    dp, PD(PRE_VIR), g.m0, g.m1, (const int4*)vitems, g.i0, (const double*)vvir);
+                batch_trows_kernel<<<(unsigned)(P(PRE_TROWS, g.m1) - P(PRE_TROWS, g.m0)), 256, 0, st>>>(
+                    dp, PD(PRE_TROWS), g.m0, g.m1);
+                FC_TRY(check_launch("batched gradient reductions / split"));
+                GemmFxArgs ga{};
+                ga.bitems = (const int4*)vgit + g.t0;
+                ga.gmols = (const GemmMol*)vgm;
+                ga.tiles = g.t1 - g.t0;
+                ga.alpha = 4.0;
+                ga.err = b->flags + 1;
+                const int g2 = (int)std::min<int64_t>(ga.tiles, c.sm_count);
+                gemm_fx_kernel<1><<<g2, 192, GF_SMEM, st>>>(tmA, tmB, ga);
+                FC_TRY(check_launch("batched adjoint contraction"));
+                launches += 6;
+            }
+            b->pair_launches = (int)groups.size();
+        }
+        b->launches = launches;
+        return FC_OK;
+    }();
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(st, &graph);
+    if (rc != FC_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (ec != cudaSuccess) return cuda_fail(ec, "cudaStreamEndCapture");
+    b->graph = graph;
+    FC_CUDA(cudaGraphInstantiate(&b->exec, graph, 0));
+    b->items = items;
+    b->gemm_tiles = (int64_t)git.size();
+    b->groups = grad ? (int)groups.size() : 0;
     return FC_OK;
 }
 

@@ -148,6 +148,63 @@ fc_status fc_rimp2_energy_noalloc(const double* b_ov, int64_t naux, int64_t nocc
                                   int32_t has_kappa, double kappa,
                                   double* e_os, double* e_ss, void* stream);
 
+/* ---- Batched RI-MP2 --------------------------------------------------------
+ * Many molecules of uneven size (naux, nocc, nvir) in one CUDA graph.  The
+ * reference has no batched entry point: its callers loop over
+ * spin_components (ferric-mp2/src/rimp2.rs:1445-1544) and the adjoint
+ * (rimp2.rs:1832-1836) one molecule at a time; this replaces that loop.
+ * All pointers of a descriptor are device pointers and stay valid (and at
+ * the same address) for the life of the batch; their contents may change
+ * between replays.  gamma (naux x nocc*nvir), de_deps_occ [nocc] and
+ * de_deps_vir [nvir] are all set (energy + gradient) or all NULL (energy
+ * only), the same for every molecule.  Only FC_PREC_MIXED (exact integer
+ * slices) is batched; FP64 is one fc_rimp2_energy_grad_dev call per
+ * molecule.  create splits nothing yet: it sizes and allocates the batch's
+ * buffers, builds its work tables and records the launch sequence (split
+ * kernels, persistent pair and adjoint kernels over all molecules' tiles,
+ * reductions) into a graph; replay enqueues that graph on `stream` (NULL =
+ * the batch's own stream); energies waits for the last replay and returns
+ * its per-molecule e_os, e_ss (host arrays of nmol).  The amplitudes of the
+ * gradient are held for a group of molecules at a time; the environment
+ * variable FERRIC_CUDA_BATCH_GROUP_BYTES bounds that workspace (default
+ * 16 GiB).  A batch is used by one thread at a time. */
+typedef struct fc_mol_desc {
+    const double* b_ov;      /* (naux, nocc*nvir), column i*nvir + a */
+    const double* eps_occ;   /* [nocc] */
+    const double* eps_vir;   /* [nvir] */
+    int64_t naux, nocc, nvir;
+    double* gamma;           /* (naux, nocc*nvir) = dE/dB_ov, or NULL */
+    double* de_deps_occ;     /* [nocc], or NULL */
+    double* de_deps_vir;     /* [nvir], or NULL */
+} fc_mol_desc;
+
+typedef struct fc_rimp2_batch fc_rimp2_batch;
+
+typedef struct fc_batch_info {
+    int64_t nmol;
+    int64_t items;           /* pair-kernel work items (molecule, i, j, tile pair) */
+    int64_t gemm_tiles;      /* adjoint-contraction tiles */
+    int32_t launches;        /* kernels recorded in the graph */
+    int32_t groups;          /* amplitude groups (gradient) */
+    int32_t pair_launches;   /* persistent pair-kernel launches */
+    int32_t precision;
+    int32_t grad;
+    int32_t tile_m, tile_n, k_panel;
+    double flops;            /* algorithmic flops of one replay */
+    double last_ms;          /* device time of the last replay read by _energies */
+    uint64_t bytes;          /* device memory held by the batch */
+} fc_batch_info;
+
+fc_status fc_rimp2_batched_create(const fc_mol_desc* mols, int64_t nmol, int32_t precision,
+                                  fc_rimp2_batch** out);
+fc_status fc_rimp2_batched_replay(fc_rimp2_batch* b, void* stream);
+fc_status fc_rimp2_batched_energies(fc_rimp2_batch* b, double* e_os, double* e_ss);
+fc_status fc_rimp2_batched_info(const fc_rimp2_batch* b, fc_batch_info* info);
+fc_status fc_rimp2_batched_destroy(fc_rimp2_batch* b);
+/* create + replay + energies + destroy. */
+fc_status fc_rimp2_batched(const fc_mol_desc* mols, int64_t nmol, int32_t precision,
+                           double* e_os, double* e_ss);
+
 /* ---- DF-JK ----------------------------------------------------------------
  * A handle owns the device copy of the 3-index tensor for the lifetime of a
  * builder (the reference's per-builder DeviceSlot, ferric-scf/src/df_j_gpu.rs:1-5,
