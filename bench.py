@@ -242,6 +242,20 @@ def host_inputs_from(torch, inp):
 
 # ------------------------------------------------------------------ main --
 
+def max_over_ranks(torch, ms, world, dev):
+    """The slowest rank's device time: every rank takes part in one MAX all-reduce."""
+    if world <= 1:
+        return float(ms)
+    t = torch.tensor([float(ms)], device=dev, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world, flops_per_step, ms_step):
+    """Whole-job TFLOP/s of `world` replicas that each ran one step's flops in ms_step."""
+    return world * flops_per_step / (ms_step * 1e-3) / 1e12
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -374,13 +388,9 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
-    ms_total = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms_total], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_total = float(t.item())
+    ms_total = max_over_ranks(torch, e0.elapsed_time(e1), world, dev)
     ms_step = ms_total / args.steps
-    value = world * flops["total"] / (ms_step * 1e-3) / 1e12
+    value = replica_throughput(world, flops["total"], ms_step)
     sc = last["energy"]
 
     # ---- roofline of the dominant kernel (the fused RI-MP2 pair kernel)
