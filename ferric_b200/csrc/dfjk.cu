@@ -256,12 +256,17 @@ fc_status dfjk_prepare_mixed(fc_dfjk* h, cudaStream_t st) {
     FC_CUDA(cudaMemcpyAsync(&bad, vf, sizeof(int), cudaMemcpyDeviceToHost, st));
     FC_CUDA(cudaStreamSynchronize(st));
     if (bad) return fail(FC_ERR_RANGE, "DF-JK: tensor element outside the FP32 range (mixed storage refused)");
+    // square handles also keep the exact-slice split for the tensor-core DF-K
+    if (h->b_sq) FC_TRY(dfk_prepare_split(h, st));
     return FC_OK;
 }
 
 void dfjk_free_mixed(fc_dfjk* h) {
     if (h->pk32) cudaFree(h->pk32);
+    if (h->sq_split) cudaFree(h->sq_split);
     h->pk32 = nullptr;
+    h->sq_split = nullptr;
+    h->sq_scale = nullptr;
 }
 
 fc_status dfk_build_f64(fc_dfjk* h, const double* c_occ, int64_t nocc, double* k, cudaStream_t st,

@@ -11,7 +11,8 @@ struct fc_dfjk {
     double* l_chol = nullptr;  // metric Cholesky factor (raw-Bp form)
     // mixed handles
     float* pk32 = nullptr;     // packed rows, FP32 (DF-J reads 4 B per element)
-    void* sq_split = nullptr;  // square tensor split for the tensor-core stages
+    void* sq_split = nullptr;  // square tensor: three bf16 slices per row (Q, mu) for DF-K
+    double* sq_scale = nullptr;  // their power-of-two row scales (inside the sq_split block)
     uint64_t bytes = 0;        // device bytes owned by the handle
 };
 
@@ -20,6 +21,7 @@ fc_status dfj_build_f64(fc_dfjk* h, const double* d, double* j, cudaStream_t st,
 fc_status dfk_build_f64(fc_dfjk* h, const double* c_occ, int64_t nocc, double* k, cudaStream_t st,
                         fc_stats* stats);
 fc_status dfjk_prepare_mixed(fc_dfjk* h, cudaStream_t st);
+fc_status dfk_prepare_split(fc_dfjk* h, cudaStream_t st);
 void dfjk_free_mixed(fc_dfjk* h);
 fc_status dfj_build_mixed(fc_dfjk* h, const double* d, double* j, cudaStream_t st, fc_stats* stats);
 fc_status dfk_build_mixed(fc_dfjk* h, const double* c_occ, int64_t nocc, double* k, cudaStream_t st,

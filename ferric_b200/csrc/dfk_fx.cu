@@ -1,0 +1,287 @@
+// Split-BF16 DF-K (FC_PREC_MIXED) on the exact-slice tcgen05 GEMM.
+//
+// K = sum_Q (B_Q C)(B_Q C)^T for C = C_occ (n x nocc), no occupation factor
+// (KBuilder::build_from_occ, ferric-scf/src/fock.rs:22-52; the occupied
+// path of ferric-scf/src/df_k.rs:1409-1520, 1575-1660):
+//   once per handle  B rows (Q, mu) split into three bf16 integer slices at a
+//                    power-of-two scale per row (fx_split.cuh)
+//   per build        C^T rows (one per occupied orbital) split the same way
+//   stage 1          W[mu, (Q, i)] = sum_nu B[Q, mu, nu] C[nu, i]: exact-slice
+//                    GEMM, 128 x 64 tiles over the naux*n rows of B (each B
+//                    slice read once: the stage is HBM-bound), FP32 W
+//   split            rows mu of W, three slices at a scale per row
+//   stage 2          K = W W^T: upper 128 x 128 tiles, split over (Q, i) into
+//                    about one item per SM, k-panel flush into FP64 registers
+//                    (xgemm.cuh), FP64 partial tiles
+//   fold             K[mu, nu] = K[nu, mu] = fixed-order sum of the partials
+//                    of the upper element (the final FP64 symmetrisation)
+// Results are deterministic and exactly symmetric.  Error: the slices carry
+// about 24 significant bits of each row; W is rounded to FP32 once.
+#include <algorithm>
+#include <vector>
+
+#include "dfjk.cuh"
+#include "fx_split.cuh"
+#include "tmap.cuh"
+#include "xgemm.cuh"
+
+namespace fc {
+
+namespace {
+
+int64_t rup(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+// Row r = (Q, mu) of the square tensor -> slices [3][rows][ldk], scale s[r].
+__global__ void __launch_bounds__(256) dfk_split_b_kernel(const double* __restrict__ b, int64_t n, int64_t ldk,
+                                                          int64_t rows, double* __restrict__ s,
+                                                          __nv_bfloat16* __restrict__ bs) {
+    split_fx_qrows_body(b, 1, n, ldk, ldk, rows, s, bs, blockIdx.x);
+}
+
+// Column i of C (n x nocc) -> row i of the C^T slices [3][npad][ldk], scale sc[i].
+__global__ void __launch_bounds__(256) dfk_split_c_kernel(const double* __restrict__ c, int64_t n, int64_t nocc,
+                                                          int64_t ldk, int64_t npad, double* __restrict__ sc,
+                                                          __nv_bfloat16* __restrict__ cs, int* bad) {
+    __shared__ double red[32];
+    const int64_t i = blockIdx.x;
+    double m = 0.0;
+    bool nf = false;
+    for (int64_t nu = threadIdx.x; nu < n; nu += 256) {
+        const double v = fabs(c[nu * nocc + i]);
+        nf |= !(v <= 1.0e300);
+        m = fmax(m, v);
+    }
+    if (nf) atomicOr(bad, 1);
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double t = threadIdx.x < 8 ? red[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) t = fmax(t, __shfl_xor_sync(0xffffffffu, t, o));
+        if (threadIdx.x == 0) red[0] = t;
+    }
+    __syncthreads();
+    const double s = pow2_scale(red[0]);
+    if (threadIdx.x == 0) sc[i] = s;
+    const double inv = 1.0 / s;
+    const int64_t ss = npad * ldk;
+    for (int64_t nu = threadIdx.x; nu < n; nu += 256) {
+        __nv_bfloat16 c1, c2, c3;
+        fx_slices(c[nu * nocc + i], inv, c1, c2, c3);
+        cs[i * ldk + nu] = c1;
+        cs[ss + i * ldk + nu] = c2;
+        cs[2 * ss + i * ldk + nu] = c3;
+    }
+}
+
+__global__ void __launch_bounds__(256) dfk_split_w_kernel(const float* __restrict__ w, int64_t ldw, int64_t mp,
+                                                          double* __restrict__ sw, __nv_bfloat16* __restrict__ ws) {
+    split_fx_rows_f32_body(w, ldw, ldw, mp, sw, ws, blockIdx.x);
+}
+
+// Stage 1 store: row r = (Q, mu) of B, column i: W[mu * ldw + Q * nocc_p + i].
+struct EpiW {
+    const double* sa;  // [naux*n] B row scales
+    const double* sc;  // [npad] C^T row scales
+    float* w;
+    int64_t ldw, rows;
+    int n, nocc, nocc_p;
+    __device__ void operator()(int64_t, int4 it, int row, int col0, const double (&acc)[32]) const {
+        const int64_t r = (int64_t)it.x * xg::BM + row;
+        if (r >= rows) return;
+        const int64_t q = r / n, mu = r % n;
+        const int i0 = it.y * 64 + col0;
+        if (i0 >= nocc_p) return;
+        const double s = sa[r];
+        float* dst = w + mu * ldw + q * nocc_p + i0;
+#pragma unroll
+        for (int c4 = 0; c4 < 32; c4 += 4) {
+            if (i0 + c4 >= nocc_p) break;  // nocc_p is a multiple of 8
+            float v[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int i = i0 + c4 + e;
+                v[e] = i < nocc ? (float)(s * sc[i] * acc[c4 + e]) : 0.f;
+            }
+            *reinterpret_cast<float4*>(dst + c4) = make_float4(v[0], v[1], v[2], v[3]);
+        }
+    }
+};
+
+// Stage 2 store: the item's FP64 partial tile [128][128], zero outside n x n.
+struct EpiPart {
+    const double* sw;  // [mp] W row scales
+    double* part;
+    int n;
+    __device__ void operator()(int64_t t, int4 it, int row, int col0, const double (&acc)[32]) const {
+        const int mu = it.x * xg::BM + row;
+        double* dst = part + t * (xg::BM * 128) + row * 128 + col0;
+        const double smu = mu < n ? sw[mu] : 0.0;
+#pragma unroll
+        for (int c2 = 0; c2 < 32; c2 += 2) {
+            const int nu = it.y * 128 + col0 + c2;
+            const double v0 = (mu < n && nu < n) ? smu * sw[nu] * acc[c2] : 0.0;
+            const double v1 = (mu < n && nu + 1 < n) ? smu * sw[nu + 1] * acc[c2 + 1] : 0.0;
+            *reinterpret_cast<double2*>(dst + c2) = make_double2(v0, v1);
+        }
+    }
+};
+
+// K[mu, nu] = K[nu, mu] = sum over the splits (in order) of the upper element.
+__global__ void __launch_bounds__(256) dfk_fold_fx_kernel(const double* __restrict__ part,
+                                                          const int* __restrict__ tix, int nsplit, int nt,
+                                                          int64_t n, double* __restrict__ k) {
+    const int64_t e = (int64_t)blockIdx.x * 256 + threadIdx.x;
+    if (e >= n * n) return;
+    const int64_t r = e / n, c = e % n;
+    const int64_t lo = r < c ? r : c, hi = r < c ? c : r;
+    const int tm = (int)(lo / 128), tn = (int)(hi / 128);
+    const int64_t base = (int64_t)tix[tm * nt + tn] * nsplit;
+    const int64_t off = (lo % 128) * 128 + (hi % 128);
+    double s = 0.0;
+    for (int sp = 0; sp < nsplit; ++sp) s += part[(base + sp) * (128 * 128) + off];
+    k[e] = s;
+}
+
+bool g_attr_done = false;
+
+fc_status xg_attrs() {
+    if (g_attr_done) return FC_OK;
+    FC_CUDA(cudaFuncSetAttribute(xgemm_kernel<64, EpiW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 xg::Cfg<64>::SMEM));
+    FC_CUDA(cudaFuncSetAttribute(xgemm_kernel<128, EpiPart>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 xg::Cfg<128>::SMEM));
+    g_attr_done = true;
+    return FC_OK;
+}
+
+}  // namespace
+
+// Split of the square tensor for the tensor-core stages (mixed square handles).
+fc_status dfk_prepare_split(fc_dfjk* h, cudaStream_t st) {
+    const int64_t rows = h->naux * h->n, ldk = rup(h->n, 8);
+    const size_t sbytes = (size_t)3 * rows * ldk * 2, scl = (size_t)rows * 8;
+    const size_t bytes = rup((int64_t)sbytes, 256) + scl;
+    FC_TRY(pool_reserve(bytes));
+    FC_CUDA(cudaMalloc(&h->sq_split, bytes));
+    h->bytes += bytes;
+    h->sq_scale = (double*)((char*)h->sq_split + rup((int64_t)sbytes, 256));
+    if (ldk != h->n) FC_CUDA(cudaMemsetAsync(h->sq_split, 0, sbytes, st));
+    if (rows > INT32_MAX) return fail(FC_ERR_LAYOUT, "DF-K: naux*n too large");
+    dfk_split_b_kernel<<<(unsigned)rows, 256, 0, st>>>(h->b_sq, h->n, ldk, rows, h->sq_scale,
+                                                       (__nv_bfloat16*)h->sq_split);
+    return check_launch("dfk_split_b_kernel");
+}
+
+fc_status dfk_build_mixed(fc_dfjk* h, const double* c_occ, int64_t nocc, double* kout, cudaStream_t st,
+                          fc_stats* stats) {
+    if (!h->sq_split)
+        return fail(FC_ERR_KERNEL, "DF-K: handle has no split-BF16 copy (created with FC_PREC_F64)");
+    FC_TRY(xg_attrs());
+    Context& cx = ctx();
+    const int64_t n = h->n, naux = h->naux, ldk = rup(n, 8);
+    const int64_t rows = naux * n;
+    const int64_t nocc_p = rup(nocc, 8), npad = rup(nocc, 64), ldw = naux * nocc_p, mp = rup(n, 128);
+    if (rows > INT32_MAX || 3 * rows > (int64_t)UINT32_MAX || mp > 65536 || ldw > INT32_MAX)
+        return fail(FC_ERR_LAYOUT, "DF-K mixed: shape too large");
+    // stage-1 and stage-2 work items
+    std::vector<int4> items;
+    const int ntm1 = (int)((rows + 127) / 128), ntn1 = (int)(npad / 64), nks1 = (int)((n + 63) / 64);
+    for (int tm = 0; tm < ntm1; ++tm)
+        for (int tn = 0; tn < ntn1; ++tn) items.push_back(make_int4(tm, tn, 0, nks1));
+    const int64_t n1 = (int64_t)items.size();
+    const int nt = (int)(mp / 128);
+    const int ntile = nt * (nt + 1) / 2;
+    const int nks2 = (int)((ldw + 63) / 64);
+    int want = std::max(1, cx.sm_count / ntile);
+    const int kps = (nks2 + want - 1) / want;
+    const int nsplit = (nks2 + kps - 1) / kps;
+    std::vector<int> tix((size_t)nt * nt, 0);
+    int tcount = 0;
+    for (int tm = 0; tm < nt; ++tm)
+        for (int tn = tm; tn < nt; ++tn) {
+            tix[tm * nt + tn] = tcount++;
+            for (int sp = 0; sp < nsplit; ++sp) {
+                const int k0 = sp * kps;
+                items.push_back(make_int4(tm, tn, k0, std::min(kps, nks2 - k0)));
+            }
+        }
+    const int64_t n2 = (int64_t)items.size() - n1;
+
+    void *vc, *vout, *vw, *vws, *vsw, *vpart, *vtab;
+    const size_t cs_bytes = (size_t)3 * npad * ldk * 2;
+    FC_TRY(ws_get(WS_MISC, rup((int64_t)cs_bytes, 256) + npad * 8, &vc));
+    FC_TRY(ws_get(WS_OUT, 256, &vout));
+    FC_TRY(ws_get(WS_T, (size_t)n * ldw * 4, &vw));
+    FC_TRY(ws_get(WS_TS, (size_t)3 * mp * ldw * 2, &vws));
+    FC_TRY(ws_get(WS_SCALE, (size_t)mp * 8, &vsw));
+    FC_TRY(ws_get(WS_PART, (size_t)n2 * 128 * 128 * 8, &vpart));
+    FC_TRY(ws_get(WS_PAIRS, items.size() * sizeof(int4) + tix.size() * sizeof(int), &vtab));
+    int* flags = (int*)vout;  // [0] range, [1] timeout
+    double* sc = (double*)((char*)vc + rup((int64_t)cs_bytes, 256));
+    FC_CUDA(cudaMemcpyAsync(vtab, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+    int* dtix = (int*)((int4*)vtab + items.size());
+    FC_CUDA(cudaMemcpyAsync(dtix, tix.data(), tix.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    FC_CUDA(cudaMemsetAsync(vout, 0, 256, st));
+    FC_CUDA(cudaMemsetAsync(vc, 0, cs_bytes, st));
+
+    CUtensorMap tb, tcm, tw;
+    FC_TRY(make_tmap_bf16_2d(&tb, h->sq_split, n, 3 * rows, ldk * 2, 64, 128));
+    FC_TRY(make_tmap_bf16_2d(&tcm, vc, n, 3 * npad, ldk * 2, 64, 64));
+    FC_TRY(make_tmap_bf16_2d(&tw, vws, ldw, 3 * mp, ldw * 2, 64, 128));
+
+    if (stats) FC_CUDA(cudaEventRecord(cx.ev0, st));
+    dfk_split_c_kernel<<<(unsigned)nocc, 256, 0, st>>>(c_occ, n, nocc, ldk, npad, sc, (__nv_bfloat16*)vc, flags);
+    cudaEvent_t* ev = nullptr;
+    if (stats) {
+        FC_TRY(timing_events(2, &ev));
+        FC_CUDA(cudaEventRecord(ev[0], st));
+    }
+    {
+        XArgs a{(const int4*)vtab, n1, (int)rows, (int)npad, flags + 1};
+        EpiW epi{h->sq_scale, sc, (float*)vw, ldw, rows, (int)n, (int)nocc, (int)nocc_p};
+        const int grid = (int)std::min<int64_t>(n1, cx.sm_count);
+        xgemm_kernel<64, EpiW><<<grid, xg::Cfg<64>::THREADS, xg::Cfg<64>::SMEM, st>>>(tb, tcm, a, epi);
+    }
+    if (stats) FC_CUDA(cudaEventRecord(ev[1], st));
+    dfk_split_w_kernel<<<(unsigned)n, 256, 0, st>>>((const float*)vw, ldw, mp, (double*)vsw, (__nv_bfloat16*)vws);
+    if (stats) FC_CUDA(cudaEventRecord(ev[2], st));
+    {
+        XArgs a{(const int4*)vtab + n1, n2, (int)mp, (int)mp, flags + 1};
+        EpiPart epi{(const double*)vsw, (double*)vpart, (int)n};
+        const int grid = (int)std::min<int64_t>(n2, cx.sm_count);
+        xgemm_kernel<128, EpiPart><<<grid, xg::Cfg<128>::THREADS, xg::Cfg<128>::SMEM, st>>>(tw, tw, a, epi);
+    }
+    if (stats) FC_CUDA(cudaEventRecord(ev[3], st));
+    dfk_fold_fx_kernel<<<(unsigned)((n * n + 255) / 256), 256, 0, st>>>((const double*)vpart, dtix, nsplit, nt, n,
+                                                                         kout);
+    FC_TRY(check_launch("split-BF16 DF-K kernels"));
+    if (stats) FC_CUDA(cudaEventRecord(cx.ev1, st));
+    int hf[2];
+    FC_CUDA(cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, st));
+    FC_CUDA(cudaStreamSynchronize(st));
+    if (hf[0]) return fail(FC_ERR_RANGE, "split-BF16 DF-K: C_occ has a non-finite element");
+    if (hf[1]) return fail(FC_ERR_TIMEOUT, "split-BF16 DF-K: a pipeline wait ran out");
+    if (stats) {
+        float ms = 0.f, m1 = 0.f, m2 = 0.f;
+        FC_CUDA(cudaEventElapsedTime(&ms, cx.ev0, cx.ev1));
+        FC_CUDA(cudaEventElapsedTime(&m1, ev[0], ev[1]));
+        FC_CUDA(cudaEventElapsedTime(&m2, ev[2], ev[3]));
+        stats->kernel_ms = ms;
+        stats->flops = 4.0 * (double)naux * (double)n * (double)n * (double)nocc;
+        stats->precision = FC_PREC_MIXED;
+        stats->launches += 5;
+        stats->tile_m = 128;
+        stats->tile_n = 64;
+        stats->k_panel = xg::KP * xg::KT;
+        stats->main_launches = 2;
+        stats->main_ms = (double)m1 + (double)m2;
+        stats->main_flops = stats->flops;
+        stats->main_bytes = 6.0 * (double)rows * (double)n;  // the B slices, read once
+        stats->h2d_bytes += items.size() * sizeof(int4) + tix.size() * sizeof(int);
+        stats->d2h_bytes += sizeof(hf);
+    }
+    return FC_OK;
+}
+
+}  // namespace fc

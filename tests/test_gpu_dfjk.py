@@ -105,3 +105,39 @@ def test_set_precision_refuses_missing_copy(fc):
     jk = DfJK(b, precision="f64")
     with pytest.raises(L.FcError):
         jk.set_precision("mixed")
+
+
+@pytest.mark.parametrize("n,naux,nocc", [(30, 50, 6), (65, 130, 9), (130, 260, 17), (200, 300, 70), (1, 3, 1)])
+def test_mixed_dfk_exact_slices(fc, n, naux, nocc):
+    """Split-BF16 DF-K (tcgen05 exact-slice stages, k-panel FP64 flush):
+    |dK| within the slicing error -- B, C and W rows carry about 24
+    significant bits and W is rounded to FP32 once -- and K exactly
+    symmetric and bit-identical on rebuild."""
+    from ferric_b200.dfjk import DfJK
+    b, c, d = synthetic.dfjk_inputs(n, naux, nocc)
+    ref = orc.df_k_occ(b, c)
+    jk = DfJK(b, precision="mixed")
+    st = {}
+    k = jk.k_from_occ(c, stats=st)
+    assert st["precision"] == 1
+    assert np.array_equal(k, k.T)
+    # |dK_mn| <= 2^-20 sum_Qi |W_m,Qi| |W_n,Qi| with W = B_Q C (four slice / rounding terms of 2^-23 .. 2^-24)
+    w = np.abs(np.einsum("qmn,ni->mqi", b, c)).reshape(n, -1)
+    bound = 2.0 ** -20 * (w @ w.T)
+    err = np.abs(k - ref)
+    assert np.all(err <= bound + 1e-300), float((err / (bound + 1e-300)).max())
+    assert np.array_equal(jk.k_from_occ(c), k)
+    jk.close()
+
+
+def test_mixed_dfk_refuses_nonfinite_c(fc):
+    import ferric_b200._lib as L
+    from ferric_b200.dfjk import DfJK
+    b, c, d = synthetic.dfjk_inputs(30, 50, 6)
+    jk = DfJK(b, precision="mixed")
+    c = c.copy()
+    c[3, 2] = np.nan
+    with pytest.raises(L.FcError) as ei:
+        jk.k_from_occ(c)
+    assert ei.value.name == "FC_ERR_RANGE"
+    jk.close()
