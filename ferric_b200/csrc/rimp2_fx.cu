@@ -189,22 +189,24 @@ struct PairFxArgs {
     int64_t items;
     double* part;  // [item][2]
     int* err;
-    // gradient mode
-    float* T;        // amplitude chunk [ci*a_pad][nocc*a_pad]
-    int64_t ldt;     // nocc * a_pad
-    int i0;
+    // gradient mode: pairs (i, j), i in chunk I (from i0), j in chunk J (from j0)
+    float* T;        // amplitude rows of I: [|I| a_pad][ldt = |J| a_pad]
+    float* T2;       // amplitude rows of J: [|J| a_pad][ldt2 = |I| a_pad] (T when I == J)
+    int64_t ldt, ldt2;
+    int i0, j0;
     double* occ_part;  // [item]
-    double* vir_part;  // [item][128]
+    double* vir_part;  // [item][2][128]: row-virtual and column-virtual sums
 };
 
 // Everything the roles need about item k.
 struct ItemView {
-    int i, j, ta, tb, nk, a_pad, nvir, row0, slice_rows, tpad, i0;
+    int i, j, ta, tb, nk, a_pad, nvir, row0, slice_rows, tpad, i0, j0;
     const double* eo;
     const double* ev;
     const double* scl;
     float* T;
-    int64_t ldt;
+    float* T2;
+    int64_t ldt, ldt2;
 };
 
 template <int BATCH>
@@ -227,8 +229,11 @@ __device__ __forceinline__ ItemView item_view(const PairFxArgs& p, int64_t k) {
         v.scl = m.scl;
         v.tpad = m.tpad;
         v.i0 = 0;
+        v.j0 = 0;
         v.T = m.T;
+        v.T2 = m.T;
         v.ldt = m.ldt;
+        v.ldt2 = m.ldt;
     } else {
         const int2 ij = p.pairs[k / p.ntiles];
         const int2 tt = p.tiles[k % p.ntiles];
@@ -246,8 +251,11 @@ __device__ __forceinline__ ItemView item_view(const PairFxArgs& p, int64_t k) {
         v.scl = p.scl;
         v.tpad = p.a_pad;
         v.i0 = p.i0;
+        v.j0 = p.j0;
         v.T = p.T;
+        v.T2 = p.T2;
         v.ldt = p.ldt;
+        v.ldt2 = p.ldt2;
     }
     return v;
 }
@@ -388,10 +396,14 @@ __global__ void __launch_bounds__(320, 1)
             const bool diag = i == j;
             const int ta = v.ta, tb = v.tb;
             // tiles ta <= tb only: X_ba = Y_ab, so the mirrored tile (tb, ta) is this
-            // tile transposed.  Energy mode weights it 2; gradient mode also
-            // writes its amplitudes (transposed) and its derivative terms.
-            const double wt = (!GRAD && ta < tb) ? 2.0 : 1.0;
+            // tile transposed: its energy terms equal this tile's (weight 2), and
+            // gradient mode writes its amplitudes (transposed) and derivative terms.
+            // Pairs are unordered (i <= j); for i < j the item also stands for the
+            // pair (j, i), whose amplitudes are this item's transposed:
+            // Tt_ji[b, a] = Tt_ij[a, b].
+            const double wt = ta < tb ? 2.0 : 1.0;
             const bool mir = GRAD && ta < tb;
+            const bool both = GRAD && !diag;
             const int a = ta * BM + row;
             const bool va = a < v.nvir;
             const double dA = v.eo[i] + v.eo[j] - (va ? v.ev[a] : 0.0);
@@ -452,55 +464,74 @@ __global__ void __launch_bounds__(320, 1)
                     float tval = 0.f, mval = 0.f, colv = 0.f;
                     if (va && c0 + cc < bmax) {
                         const double r = 1.0 / (dA - evb[c0 + cc]);
-                        if (GRAD) {
-                            const double tt = (2.0 * x - y) * r;   // Tt_ij[a, b]
-                            const double cd = x * r * tt;          // t Tt at (a, b)
-                            tval = (float)tt;
-                            os += x * x * r;
-                            ss += x * (x - y) * r;
-                            oc += cd;
-                            rowc += cd;
-                            if (mir) {
-                                const double tm = (2.0 * y - x) * r;  // Tt_ij[b, a]
-                                const double cm = y * r * tm;         // t Tt at (b, a)
-                                mval = (float)tm;
-                                colv = (float)cm;
-                                os += y * y * r;
-                                ss += y * (y - x) * r;
-                                oc += cm;
-                            }
-                        } else if (diag) {
+                        if (diag) {
                             os += x * x * r;
                         } else {
                             os += (x * x + y * y) * r;
                             ss += (x - y) * (x - y) * r;
+                        }
+                        if (GRAD) {
+                            // t Tt summed over a pair's elements is the pair's share of
+                            // dE/deps_occ; by virtual index, of dE/deps_vir.  Pair (i, j)
+                            // puts its element (a, b) on the row virtual a, pair (j, i)
+                            // on b (its row index); the mirrored tile the other way round.
+                            const double tt = (2.0 * x - y) * r;   // Tt_ij[a, b]
+                            const double cd = x * r * tt;          // t Tt at (a, b)
+                            double cm = 0.0;
+                            tval = (float)tt;
+                            if (mir) {
+                                const double tm = (2.0 * y - x) * r;  // Tt_ij[b, a]
+                                cm = y * r * tm;                      // t Tt at (b, a)
+                                mval = (float)tm;
+                            }
+                            oc += cd + cm;
+                            rowc += both ? cd + cm : cd;
+                            colv = (float)(both ? cd + cm : cm);
                         }
                     }
                     tt8[cc] = tval;
                     mv8[cc] = mval;
                     if (GRAD) xr[c0 + cc] = colv;  // x of this column is consumed: keep cm there
                 }
-                if (GRAD) {
+                if (GRAD && a < v.tpad) {
                     // amplitude rows (i, a) and columns (j, b) at pitch tpad (>= nvir);
-                    // elements with a or b >= tpad belong to no amplitude
-                    float* trow = v.T + ((int64_t)(i - v.i0) * v.tpad) * v.ldt + (int64_t)j * v.tpad;
+                    // elements with a or b >= tpad belong to no amplitude.  Rows of
+                    // i go to T (columns of j from j0), rows of j to T2 (columns of i
+                    // from i0); with one chunk for both, T2 is T.
                     const int bw = v.tpad - (b0 + c0);  // columns of this group inside the pitch
-                    if (a < v.tpad) {
-                        float* d = trow + (int64_t)a * v.ldt + b0 + c0;
-                        if (bw >= 8) {
-                            float4* dst = reinterpret_cast<float4*>(d);
-                            dst[0] = make_float4(tt8[0], tt8[1], tt8[2], tt8[3]);
-                            dst[1] = make_float4(tt8[4], tt8[5], tt8[6], tt8[7]);
-                        } else {
+                    float* trow = v.T + ((int64_t)(i - v.i0) * v.tpad) * v.ldt + (int64_t)(j - v.j0) * v.tpad;
+                    float* d = trow + (int64_t)a * v.ldt + b0 + c0;
+                    if (bw >= 8) {
+                        float4* dst = reinterpret_cast<float4*>(d);
+                        dst[0] = make_float4(tt8[0], tt8[1], tt8[2], tt8[3]);
+                        dst[1] = make_float4(tt8[4], tt8[5], tt8[6], tt8[7]);
+                    } else {
 #pragma unroll
-                            for (int cc = 0; cc < 8; ++cc)
-                                if (cc < bw) d[cc] = tt8[cc];
-                        }
+                        for (int cc = 0; cc < 8; ++cc)
+                            if (cc < bw) d[cc] = tt8[cc];
                     }
-                    if (mir && a < v.tpad) {
+                    if (mir) {
 #pragma unroll
                         for (int cc = 0; cc < 8; ++cc)  // lanes hold consecutive a: coalesced
                             if (cc < bw) trow[(int64_t)(b0 + c0 + cc) * v.ldt + a] = mv8[cc];
+                    }
+                    if (both) {
+                        float* t2 = v.T2 + ((int64_t)(j - v.j0) * v.tpad) * v.ldt2 + (int64_t)(i - v.i0) * v.tpad;
+#pragma unroll
+                        for (int cc = 0; cc < 8; ++cc)  // Tt_ji[b, a] = Tt_ij[a, b]
+                            if (cc < bw) t2[(int64_t)(b0 + c0 + cc) * v.ldt2 + a] = tt8[cc];
+                        if (mir) {                      // Tt_ji[a, b] = Tt_ij[b, a]
+                            float* d2 = t2 + (int64_t)a * v.ldt2 + b0 + c0;
+                            if (bw >= 8) {
+                                float4* dst = reinterpret_cast<float4*>(d2);
+                                dst[0] = make_float4(mv8[0], mv8[1], mv8[2], mv8[3]);
+                                dst[1] = make_float4(mv8[4], mv8[5], mv8[6], mv8[7]);
+                            } else {
+#pragma unroll
+                                for (int cc = 0; cc < 8; ++cc)
+                                    if (cc < bw) d2[cc] = mv8[cc];
+                            }
+                        }
                     }
                 }
             }
@@ -514,7 +545,7 @@ __global__ void __launch_bounds__(320, 1)
                 rb[(warp - 2) * 3 + 2] = vc;
             }
             if (GRAD && h == 1) rowsh[row] = rowc;
-            if (mir) {
+            if (mir || both) {
                 // column sums of the mirrored terms over this warp's 32 rows: a
                 // reduce-scatter butterfly leaves columns 2*lane, 2*lane+1 in xr[0..1]
 #pragma unroll
@@ -532,7 +563,7 @@ __global__ void __launch_bounds__(320, 1)
             }
             asm volatile("bar.sync 1, 256;" ::: "memory");
             if (GRAD && h == 0) p.vir_part[k * 2 * BM + row] = rowc + rowsh[row];
-            if (mir && et < BM) {
+            if ((mir || both) && et < BM) {
                 const int hh = et >> 6, c = et & 63;
                 double cs = 0.0;
 #pragma unroll
@@ -590,6 +621,8 @@ struct GemmFxArgs {
     double alpha;
     double* out;  // Gamma (naux, nov)
     int* err;
+    int kofs;        // first K column of the B operand (Q-row slices)
+    int accumulate;  // out += instead of out =
     // batch mode: tile t is bitems[t] = (molecule, m-tile, n-tile, 0)
     const int4* bitems;
     const GemmMol* gmols;
@@ -718,7 +751,8 @@ __global__ void __launch_bounds__(192, 1)
 #pragma unroll
                     for (int sl = 0; sl < 3; ++sl) {
                         tc::tma_load_2d(base + (sa(s, sl) - base_u32), v.tA, &full[s], kt * KT, sl * v.M + v.tm * 128);
-                        tc::tma_load_2d(base + (sb(s, sl) - base_u32), v.tB, &full[s], kt * KT, sl * v.N + v.tn * 128);
+                        tc::tma_load_2d(base + (sb(s, sl) - base_u32), v.tB, &full[s], p.kofs + kt * KT,
+                                        sl * v.N + v.tn * 128);
                     }
                 }
             }
@@ -785,9 +819,12 @@ __global__ void __launch_bounds__(192, 1)
 #pragma unroll
                     for (int cc = 0; cc < 16; ++cc) {
                         const int Q = v.tn * 128 + c0 + cc;
-                        if (Q < v.naux)
-                            orow[(int64_t)Q * v.nov] =
+                        if (Q < v.naux) {
+                            const double g =
                                 sr * v.cs[Q] * ((double)l0[cc] + (double)l1[cc] * L1W + (double)l2[cc] * L2W);
+                            double* o = orow + (int64_t)Q * v.nov;
+                            *o = p.accumulate ? *o + g : g;
+                        }
                     }
                 }
             }
@@ -828,26 +865,39 @@ __global__ void __launch_bounds__(1024) fx_reduce_pairs_kernel(const double* __r
     }
 }
 
+// acc_occ[o] += sum of the t Tt partials of every item whose pair holds o,
+// for o in I (blocks 0 .. ni-1) and in J (the rest); fixed order.
 __global__ void __launch_bounds__(256) fx_reduce_occ_kernel(const double* __restrict__ occ_part,
-                                                            int64_t items_per_i, int i0, double* de_docc) {
+                                                            const int2* __restrict__ pairs, int64_t npairs,
+                                                            int ntiles, int i0, int ni, int j0,
+                                                            double* acc_occ) {
     __shared__ double sh[256];
-    const int il = blockIdx.x;
-    const double* src = occ_part + (int64_t)il * items_per_i;
+    const int o = (int)blockIdx.x < ni ? i0 + (int)blockIdx.x : j0 + ((int)blockIdx.x - ni);
     KSum a;
-    for (int64_t k = threadIdx.x; k < items_per_i; k += 256) a.add(src[k]);
+    const int64_t n = npairs * ntiles;
+    for (int64_t k = threadIdx.x; k < n; k += 256) {
+        const int2 pr = pairs[k / ntiles];
+        if (pr.x == o || pr.y == o) a.add(occ_part[k]);
+    }
     sh[threadIdx.x] = a.value();
     __syncthreads();
     if (threadIdx.x == 0) {
         KSum x;
         for (int k = 0; k < 256; ++k) x.add(sh[k]);
-        de_docc[i0 + il] = -2.0 * x.value();
+        acc_occ[o] += x.value();
     }
 }
 
-// acc_vir[v] += 2 * (sum over the chunk's items of the row partials of v, from
-// direct tiles (ta, tb) with v in ta, and of the column partials, from the
-// mirrored tiles (tb, ta) with v in tb).  Fixed order: deterministic.
+__global__ void scale_copy_kernel(const double* __restrict__ x, int64_t n, double s, double* __restrict__ y) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) y[k] = s * x[k];
+}
+
+// acc_vir[v] += 2 * (sum over the launch's items of the row-virtual partials
+// of v (v in the a-tile) and of the column-virtual partials (v in the b-tile;
+// present for mirrored tiles and for pairs i < j)).  Fixed order.
 __global__ void __launch_bounds__(256) fx_reduce_vir_kernel(const double* __restrict__ vir_part,
+                                                            const int2* __restrict__ pairs,
                                                             const int2* __restrict__ tiles, int64_t npairs,
                                                             int ntiles, int nvir, double* acc_vir) {
     const int v = blockIdx.x * 8 + (threadIdx.x >> 5);
@@ -859,7 +909,10 @@ __global__ void __launch_bounds__(256) fx_reduce_vir_kernel(const double* __rest
     for (int64_t k = lane; k < nterm; k += 32) {
         const int2 t = tiles[k % ntiles];
         if (t.x == tv) s.add(vir_part[k * 2 * fx::BM + rv]);
-        if (t.y == tv && t.x < t.y) s.add(vir_part[k * 2 * fx::BM + fx::BM + rv]);
+        if (t.y == tv) {
+            const int2 pr = pairs[k / ntiles];
+            if (t.x < t.y || pr.x != pr.y) s.add(vir_part[k * 2 * fx::BM + fx::BM + rv]);
+        }
     }
     const double r = warp_sum(s.value());
     if (lane == 0) acc_vir[v] += 2.0 * r;
@@ -886,7 +939,7 @@ struct BatchPrep {
     double* de_docc;           // [nocc]
     double* de_dvir;           // [nvir]
     int64_t seg0;              // first item of this molecule
-    int64_t items_per_i;       // nocc * tiles per pair (gradient items)
+    int64_t ntp;               // tile pairs (ta <= tb) per occupied pair
 };
 
 // Largest m in [lo, hi) with pre[m] <= x.
@@ -946,7 +999,9 @@ __global__ void __launch_bounds__(256) batch_trows_kernel(const BatchPrep* __res
     split_fx_rows_f32_body(d.T, d.nocc * d.tpad, d.ldt, d.M, d.ts, d.Ts, x - pre[m]);
 }
 
-// dE/deps_i = -2 sum over the items (i, j, tiles) of their t~Tt partials.
+// dE/deps_o = -2 sum of the t Tt partials of the items of every pair holding o.
+// Pairs i <= j are numbered row-major (pidx); partner s gives the pair
+// (min(s, o), max(s, o)).
 __global__ void __launch_bounds__(256) batch_occ_kernel(const BatchPrep* __restrict__ mp,
                                                         const int64_t* __restrict__ pre, int m0, int m1,
                                                         const double* __restrict__ occ_part) {
@@ -954,22 +1009,26 @@ __global__ void __launch_bounds__(256) batch_occ_kernel(const BatchPrep* __restr
     const int64_t x = pre[m0] + blockIdx.x;
     const int m = seg_find(pre, m0, m1, x);
     const BatchPrep& d = mp[m];
-    const int64_t i = x - pre[m];
-    const double* src = occ_part + d.seg0 + i * d.items_per_i;
+    const int64_t o = x - pre[m], n = d.nocc;
     KSum a;
-    for (int64_t k = threadIdx.x; k < d.items_per_i; k += 256) a.add(src[k]);
+    for (int64_t u = threadIdx.x; u < n * d.ntp; u += 256) {
+        const int64_t sp = u / d.ntp, t = u % d.ntp;
+        const int64_t i = sp < o ? sp : o, j = sp < o ? o : sp;
+        const int64_t pidx = i * n - i * (i - 1) / 2 + (j - i);
+        a.add(occ_part[d.seg0 + pidx * d.ntp + t]);
+    }
     sh[threadIdx.x] = a.value();
     __syncthreads();
     if (threadIdx.x == 0) {
         KSum t;
         for (int k = 0; k < 256; ++k) t.add(sh[k]);
-        d.de_docc[i] = -2.0 * t.value();
+        d.de_docc[o] = -2.0 * t.value();
     }
 }
 
-// dE/deps_v = 2 sum of the row partials of v (tiles with v in the a-tile) and
-// the column partials (mirrored tiles with v in the b-tile); one warp per v.
-// vir_part is indexed from the group's first item g0.
+// dE/deps_v = 2 sum of the row-virtual partials of v (v in the a-tile) and
+// the column-virtual partials (v in the b-tile; mirrored tiles and pairs
+// i < j); one warp per v.  vir_part is indexed from the group's first item g0.
 __global__ void __launch_bounds__(256) batch_vir_kernel(const BatchPrep* __restrict__ mp,
                                                         const int64_t* __restrict__ pre, int m0, int m1,
                                                         const int4* __restrict__ items, int64_t g0,
@@ -981,14 +1040,14 @@ __global__ void __launch_bounds__(256) batch_vir_kernel(const BatchPrep* __restr
     const BatchPrep& d = mp[m];
     const int v = (int)(x - pre[m]);
     const int tv = v / fx::BM, rv = v % fx::BM;
-    const int64_t k1 = d.seg0 + d.nocc * d.items_per_i;
+    const int64_t k1 = d.seg0 + d.nocc * (d.nocc + 1) / 2 * d.ntp;
     KSum s;
     for (int64_t k = d.seg0 + lane; k < k1; k += 32) {
-        const int w = items[k].w;
-        const int ta = w & 0xFFFF, tb = w >> 16;
+        const int4 it = items[k];
+        const int ta = it.w & 0xFFFF, tb = it.w >> 16;
         const double* vp = vir_part + (k - g0) * 2 * fx::BM;
         if (ta == tv) s.add(vp[rv]);
-        if (tb == tv && ta < tb) s.add(vp[fx::BM + rv]);
+        if (tb == tv && (ta < tb || it.y != it.z)) s.add(vp[fx::BM + rv]);
     }
     const double r = warp_sum(s.value());
     if (lane == 0) d.de_dvir[v] = 2.0 * r;
@@ -1169,26 +1228,74 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
     FC_TRY(fx_attrs());
     if (d.nocc > (1 << 15)) return fail(FC_ERR_LAYOUT, "split-BF16: nocc too large");
     const int64_t nocc = d.nocc, nvir = d.nvir, naux = d.naux, nov = nocc * nvir;
-    void* vout;
-    FC_TRY(ws_get(WS_OUT, (size_t)(2 * nocc + 16) * 8, &vout));
-    double* e_chunks = (double*)vout;
-    int* flags = (int*)(e_chunks + 2 * nocc + 8);
-    FC_CUDA(cudaMemsetAsync(vout, 0, (size_t)(2 * nocc + 16) * 8, st));
     Context& c = ctx();
-    if (stats) FC_CUDA(cudaEventRecord(c.ev0, st));
     FxSplit sp;
+    void* vout0;
+    FC_TRY(ws_get(WS_OUT, 256, &vout0));
+    int* flags = (int*)vout0;  // [0] range, [1] timeout
+    FC_CUDA(cudaMemsetAsync(vout0, 0, 256, st));
+    if (stats) FC_CUDA(cudaEventRecord(c.ev0, st));
     FC_TRY(fx_split_pairs(d, st, flags, &sp));
     const int64_t a_pad = sp.a_pad;
-    const int64_t K2 = nocc * a_pad;                        // adjoint contraction length (j, b_pad)
+    const int64_t K2 = nocc * a_pad;  // (j, b_pad) columns of the Q-row slices
     const int64_t q_rows = (naux + 127) / 128 * 128;
-    // per-Q-row split of B_ov for the adjoint contraction
-    const int64_t npairs_all = nocc * nocc;
-    const int64_t ntile_all = (a_pad / fx::BM) * (a_pad / fx::BM + 1) / 2;
-    const size_t tab_bytes = (((npairs_all + ntile_all) * sizeof(int2) + 255) / 256) * 256;
-    void *vbq, *vtab;
+    const int nTa = (int)(a_pad / fx::BM);
+    const int ntiles = nTa * (nTa + 1) / 2;  // tiles ta <= tb
+
+    // occupied chunks: a chunk pair (I, J), I <= J, holds the amplitude rows of
+    // I (columns of J) and of J (columns of I) in FP32, plus the slices of one
+    // of them; each unordered pair (i, j) is computed once and feeds both.
+    const int64_t per_c2 = a_pad * a_pad * (4 + 4 + 6);
+    int64_t cc = 1;
+    while (cc < nocc && (cc + 1) * (cc + 1) * per_c2 <= (int64_t)d.chunk_bytes) ++cc;
+    const int64_t nch = (nocc + cc - 1) / cc;
+    struct CP {
+        int64_t i0, ni, j0, nj, p0, np;
+    };
+    std::vector<CP> cps;
+    std::vector<int2> pairs;
+    for (int64_t I = 0; I < nch; ++I)
+        for (int64_t J = I; J < nch; ++J) {
+            CP x;
+            x.i0 = I * cc;
+            x.ni = std::min(cc, nocc - x.i0);
+            x.j0 = J * cc;
+            x.nj = std::min(cc, nocc - x.j0);
+            x.p0 = (int64_t)pairs.size();
+            for (int64_t i = x.i0; i < x.i0 + x.ni; ++i)
+                for (int64_t j = (I == J ? i : x.j0); j < x.j0 + x.nj; ++j) pairs.push_back(make_int2((int)i, (int)j));
+            x.np = (int64_t)pairs.size() - x.p0;
+            cps.push_back(x);
+        }
+    const int64_t npairs_all = (int64_t)pairs.size();
+    for (int ta = 0; ta < nTa; ++ta)
+        for (int tb = ta; tb < nTa; ++tb) pairs.push_back(make_int2(ta, tb));
+    const int64_t ncp = (int64_t)cps.size();
+    int64_t max_items = 0;
+    for (const auto& x : cps) max_items = std::max(max_items, x.np * ntiles);
+
+    void *vbq, *vtab, *vT, *vTs, *vpart;
+    const size_t tab_bytes = ((pairs.size() * sizeof(int2) + 255) / 256) * 256;
     FC_TRY(ws_get(WS_SPLIT2, (size_t)3 * q_rows * K2 * 2, &vbq));
     FC_TRY(ws_get(WS_PAIRS, tab_bytes + q_rows * 8, &vtab));
     double* qs = (double*)((char*)vtab + tab_bytes);
+    const size_t cbytes = (size_t)cc * a_pad * cc * a_pad;  // elements of one amplitude block
+    FC_TRY(ws_get(WS_T, cbytes * 8 + (size_t)cc * a_pad * 8, &vT));
+    FC_TRY(ws_get(WS_TS, cbytes * 6, &vTs));
+    FC_TRY(ws_get(WS_PART, (size_t)max_items * (2 + 1 + 2 * fx::BM) * 8 + (size_t)(2 * ncp + nocc) * 8, &vpart));
+    float* T1 = (float*)vT;
+    float* T2 = T1 + cbytes;
+    double* ts = (double*)(T2 + cbytes);
+    double* part = (double*)vpart;
+    double* occ_part = part + 2 * max_items;
+    double* vir_part = occ_part + max_items;
+    double* e_cp = vir_part + 2 * fx::BM * max_items;  // [ncp][2]
+    double* acc_occ = e_cp + 2 * ncp;                  // [nocc]
+    FC_CUDA(cudaMemcpyAsync(vtab, pairs.data(), pairs.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
+    FC_CUDA(cudaMemsetAsync(de_dvir, 0, nvir * 8, st));
+    FC_CUDA(cudaMemsetAsync(acc_occ, 0, nocc * 8, st));
+    FC_CUDA(cudaMemsetAsync(gamma, 0, (size_t)naux * nov * 8, st));
+    // per-Q-row split of B_ov for the adjoint contraction
     FC_CUDA(cudaMemsetAsync(vbq, 0, (size_t)3 * q_rows * K2 * 2, st));
     fill_kernel<<<(unsigned)((q_rows + 255) / 256), 256, 0, st>>>(qs, q_rows, 1.0);
     split_fx_qrows_kernel<<<(unsigned)naux, 256, 0, st>>>(d.b_ov, naux, nocc, nvir, a_pad, q_rows, qs,
@@ -1196,112 +1303,98 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
     FC_TRY(check_launch("split_fx_qrows_kernel"));
     CUtensorMap tmBq;
     FC_TRY(make_tmap_bf16_2d(&tmBq, vbq, K2, 3 * q_rows, K2 * 2, fx::KT, 128));
+    const int2* dpairs = (const int2*)vtab;
+    const int2* dtiles = dpairs + npairs_all;
 
-    // occupied chunk: ci rows of amplitudes, FP32 (written by the pair kernel)
-    // and as three slices (read by the adjoint contraction)
-    const int64_t per_i = a_pad * K2 * (4 + 6);
-    int64_t ci = d.chunk_bytes / (per_i > 0 ? per_i : 1);
-    if (ci < 1) ci = 1;
-    if (ci > nocc) ci = nocc;
-    const int nTa = (int)(a_pad / fx::BM), nTb = (int)(a_pad / fx::BN);
-    const int ntiles = nTa * (nTa + 1) / 2;  // tiles ta <= tb (nTa == nTb)
-    const int64_t items_per_i = nocc * (int64_t)ntiles;
-    const size_t t_bytes = (size_t)ci * a_pad * K2 * 4;
-    void *vT, *vTs, *vpart;
-    FC_TRY(ws_get(WS_T, t_bytes + (size_t)ci * a_pad * 8, &vT));
-    FC_TRY(ws_get(WS_TS, (size_t)3 * ci * a_pad * K2 * 2, &vTs));
-    FC_TRY(ws_get(WS_PART, (size_t)ci * items_per_i * (2 + 1 + 2 * fx::BM) * 8, &vpart));
-    float* T = (float*)vT;
-    double* ts = (double*)((char*)vT + t_bytes);
-    void* ts_slices = vTs;
-    double* occ_part = (double*)vpart + ci * items_per_i * 2;
-    double* vir_part = occ_part + ci * items_per_i;
-    // pair table: ordered pairs, row-major by i; then every (a-tile, b-tile)
-    std::vector<int2> pairs((size_t)npairs_all);
-    for (int i = 0; i < nocc; ++i)
-        for (int j = 0; j < nocc; ++j) pairs[(size_t)i * nocc + j] = make_int2(i, j);
-    for (int ta = 0; ta < nTa; ++ta)
-        for (int tb = ta; tb < nTb; ++tb) pairs.push_back(make_int2(ta, tb));
-    FC_CUDA(cudaMemcpyAsync(vtab, pairs.data(), pairs.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
-    FC_CUDA(cudaMemsetAsync(de_dvir, 0, nvir * 8, st));
-
-    CUtensorMap tmTs;
-    FC_TRY(make_tmap_bf16_2d(&tmTs, ts_slices, K2, 3 * ci * a_pad, K2 * 2, fx::KT, 128));
-    const int64_t nchunks = (nocc + ci - 1) / ci;
     cudaEvent_t* ev = nullptr;
-    if (stats) FC_TRY(timing_events((int)(2 * nchunks), &ev));
-    for (int64_t ch = 0; ch < nchunks; ++ch) {
-        const int64_t i0 = ch * ci;
-        const int64_t cn = i0 + ci <= nocc ? ci : nocc - i0;
+    if (stats) FC_TRY(timing_events((int)ncp, &ev));
+    // Gamma[:, rows] += 4 Bq[:, cols] T^T for one amplitude block
+    auto adjoint = [&](float* T, int64_t r0, int64_t nr, int64_t k0, int64_t nk) -> fc_status {
+        const int64_t ldk = nk * a_pad, rows = nr * a_pad;
+        split_fx_rows_f32_kernel<<<(unsigned)rows, 256, 0, st>>>(T, ldk, rows, ts, (__nv_bfloat16*)vTs);
+        CUtensorMap tmTs;
+        FC_TRY(make_tmap_bf16_2d(&tmTs, vTs, ldk, 3 * rows, ldk * 2, fx::KT, 128));
+        GemmFxArgs g{};
+        g.rs = ts;
+        g.cs = qs;
+        g.M = (int)rows;
+        g.N = (int)q_rows;
+        g.nk = (int)(ldk / fx::KT);
+        g.nTm = (int)(rows / 128);
+        g.nTn = (int)(q_rows / 128);
+        g.tiles = (int64_t)g.nTm * g.nTn;
+        g.a_pad = (int)a_pad;
+        g.nvir = (int)nvir;
+        g.naux = (int)naux;
+        g.i0 = (int)r0;
+        g.nov = nov;
+        g.alpha = 4.0;
+        g.out = gamma;
+        g.err = flags + 1;
+        g.kofs = (int)(k0 * a_pad);
+        g.accumulate = 1;
+        const int g2 = (int)(g.tiles < c.sm_count ? g.tiles : c.sm_count);
+        gemm_fx_kernel<0><<<g2, 192, GF_SMEM, st>>>(tmTs, tmBq, g);
+        return check_launch("gemm_fx_kernel");
+    };
+    for (int64_t x = 0; x < ncp; ++x) {
+        const CP& cp = cps[x];
+        const bool same = cp.i0 == cp.j0;
         PairFxArgs a{};
         a.eo = d.eps_occ;
         a.ev = d.eps_vir;
         a.scl = sp.scl;
-        a.pairs = (const int2*)vtab + i0 * nocc;
-        a.tiles = (const int2*)vtab + npairs_all;
+        a.pairs = dpairs + cp.p0;
+        a.tiles = dtiles;
         a.ntiles = ntiles;
-        a.npairs = (int)(cn * nocc);
+        a.npairs = (int)cp.np;
         a.nocc = (int)nocc;
         a.nvir = (int)nvir;
         a.a_pad = (int)a_pad;
         a.nTa = nTa;
-        a.nTb = nTb;
+        a.nTb = nTa;
         a.nk = (int)(sp.q_pad / fx::KT);
-        a.items = cn * items_per_i;
-        a.part = (double*)vpart;
+        a.items = cp.np * ntiles;
+        a.part = part;
         a.err = flags + 1;
-        a.T = T;
-        a.ldt = K2;
-        a.i0 = (int)i0;
+        a.T = T1;
+        a.ldt = cp.nj * a_pad;
+        a.T2 = same ? T1 : T2;
+        a.ldt2 = same ? a.ldt : cp.ni * a_pad;
+        a.i0 = (int)cp.i0;
+        a.j0 = (int)cp.j0;
         a.occ_part = occ_part;
         a.vir_part = vir_part;
         const int grid = (int)(a.items < c.sm_count ? a.items : c.sm_count);
-        if (stats) FC_CUDA(cudaEventRecord(ev[2 * ch], st));
+        if (stats) FC_CUDA(cudaEventRecord(ev[2 * x], st));
         pair_fx_kernel<1><<<grid, 320, fx::SMEM, st>>>(sp.tmA, sp.tmB, a);
         FC_TRY(check_launch("pair_fx_kernel<grad>"));
-        if (stats) FC_CUDA(cudaEventRecord(ev[2 * ch + 1], st));
-        fx_reduce_pairs_kernel<<<1, 1024, 0, st>>>((const double*)vpart, a.items, e_chunks + 2 * ch);
-        fx_reduce_occ_kernel<<<(unsigned)cn, 256, 0, st>>>(occ_part, items_per_i, (int)i0, de_docc);
-        fx_reduce_vir_kernel<<<(unsigned)((nvir + 7) / 8), 256, 0, st>>>(
-            vir_part, (const int2*)vtab + npairs_all, cn * nocc, ntiles, (int)nvir, de_dvir);
-        split_fx_rows_f32_kernel<<<(unsigned)(cn * a_pad), 256, 0, st>>>(T, K2, ci * a_pad, ts,
-                                                                          (__nv_bfloat16*)ts_slices);
-        FC_TRY(check_launch("gradient chunk reductions / split"));
-        GemmFxArgs gargs{};
-        gargs.rs = ts;
-        gargs.cs = qs;
-        gargs.M = (int)(ci * a_pad);   // slice stride of the chunk tensor map
-        gargs.N = (int)q_rows;
-        gargs.nk = (int)(K2 / fx::KT);
-        gargs.nTm = (int)(cn * a_pad / 128);
-        gargs.nTn = (int)(q_rows / 128);
-        gargs.tiles = (int64_t)gargs.nTm * gargs.nTn;
-        gargs.a_pad = (int)a_pad;
-        gargs.nvir = (int)nvir;
-        gargs.naux = (int)naux;
-        gargs.i0 = (int)i0;
-        gargs.nov = nov;
-        gargs.alpha = 4.0;
-        gargs.out = gamma;
-        gargs.err = flags + 1;
-        const int g2 = (int)(gargs.tiles < c.sm_count ? gargs.tiles : c.sm_count);
-        gemm_fx_kernel<0><<<g2, 192, GF_SMEM, st>>>(tmTs, tmBq, gargs);
-        FC_TRY(check_launch("gemm_fx_kernel"));
+        if (stats) FC_CUDA(cudaEventRecord(ev[2 * x + 1], st));
+        fx_reduce_pairs_kernel<<<1, 1024, 0, st>>>(part, a.items, e_cp + 2 * x);
+        fx_reduce_occ_kernel<<<(unsigned)(same ? cp.ni : cp.ni + cp.nj), 256, 0, st>>>(
+            occ_part, dpairs + cp.p0, cp.np, ntiles, (int)cp.i0, (int)cp.ni, (int)cp.j0, acc_occ);
+        fx_reduce_vir_kernel<<<(unsigned)((nvir + 7) / 8), 256, 0, st>>>(vir_part, dpairs + cp.p0, dtiles, cp.np,
+                                                                          ntiles, (int)nvir, de_dvir);
+        FC_TRY(check_launch("gradient reductions"));
+        FC_TRY(adjoint(T1, cp.i0, cp.ni, cp.j0, cp.nj));
+        if (!same) FC_TRY(adjoint(T2, cp.j0, cp.nj, cp.i0, cp.ni));
     }
+    scale_copy_kernel<<<(unsigned)((nocc + 255) / 256), 256, 0, st>>>(acc_occ, nocc, -2.0, de_docc);
+    FC_TRY(check_launch("scale_copy_kernel"));
     if (stats) FC_CUDA(cudaEventRecord(c.ev1, st));
-    std::vector<double> h((size_t)(2 * nchunks));
+    std::vector<double> h((size_t)(2 * ncp));
     int hf[2];
-    FC_CUDA(cudaMemcpyAsync(h.data(), e_chunks, h.size() * 8, cudaMemcpyDeviceToHost, st));
+    FC_CUDA(cudaMemcpyAsync(h.data(), e_cp, h.size() * 8, cudaMemcpyDeviceToHost, st));
     FC_CUDA(cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, st));
     FC_CUDA(cudaStreamSynchronize(st));
     if (hf[0]) return fail(FC_ERR_RANGE, "split-BF16: B_ov has a non-finite element");
     if (hf[1]) return fail(FC_ERR_TIMEOUT, "split-BF16 gradient kernels: a pipeline wait ran out");
-    double eo = 0.0, co = 0.0, es = 0.0, cs2 = 0.0;
-    for (int64_t ch = 0; ch < nchunks; ++ch) {
-        double v = h[2 * ch], t = eo + v;
+    double eo = 0.0, co = 0.0, es = 0.0, cs2 = 0.0;  // Neumaier sums over the chunk pairs
+    for (int64_t x = 0; x < ncp; ++x) {
+        double v = h[2 * x], t = eo + v;
         co += fabs(eo) >= fabs(v) ? (eo - t) + v : (v - t) + eo;
         eo = t;
-        v = h[2 * ch + 1];
+        v = h[2 * x + 1];
         t = es + v;
         cs2 += fabs(es) >= fabs(v) ? (es - t) + v : (v - t) + es;
         es = t;
@@ -1315,19 +1408,19 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
         const double P = (double)nocc * (nocc + 1) / 2.0;
         stats->flops = 2.0 * naux * (double)nvir * nvir * P + 2.0 * naux * (double)nov * nov;
         stats->precision = FC_PREC_MIXED;
-        stats->launches += (int)(6 * nchunks + 5);
+        stats->launches += (int)(5 * ncp + 6 * (ncp - nch) + 6);
         stats->tile_m = fx::BM;
         stats->tile_n = fx::BN;
-        stats->main_launches = (int)nchunks;
+        stats->main_launches = (int)ncp;
         double tsum = 0.0;
-        for (int64_t ch = 0; ch < nchunks; ++ch) {
-            float x = 0.f;
-            FC_CUDA(cudaEventElapsedTime(&x, ev[2 * ch], ev[2 * ch + 1]));
-            tsum += x;
+        for (int64_t x = 0; x < ncp; ++x) {
+            float t = 0.f;
+            FC_CUDA(cudaEventElapsedTime(&t, ev[2 * x], ev[2 * x + 1]));
+            tsum += t;
         }
         stats->main_ms = tsum;
-        stats->main_flops = 2.0 * naux * (double)nov * nov;
-        stats->main_bytes = 6.0 * naux * (double)nov * (double)nchunks;
+        stats->main_flops = 2.0 * naux * (double)nvir * nvir * P;  // G_ij over unordered pairs
+        stats->main_bytes = 6.0 * naux * (double)nov * (double)nch;
         stats->h2d_bytes += pairs.size() * sizeof(int2);
         stats->d2h_bytes += h.size() * 8 + sizeof(hf);
     }
@@ -1384,8 +1477,8 @@ fc_status rimp2_batch_build_fx(fc_rimp2_batch* b, const std::vector<BatchMolIn>&
         x.de_dvir = d.de_deps_vir;
         const int64_t nT = x.a_pad / fx::BM;
         ntp[m] = nT * (nT + 1) / 2;
-        const int64_t npair = grad ? d.nocc * d.nocc : d.nocc * (d.nocc + 1) / 2;
-        x.items_per_i = d.nocc * ntp[m];
+        const int64_t npair = d.nocc * (d.nocc + 1) / 2;  // unordered pairs in both modes
+        x.ntp = ntp[m];
         x.seg0 = seg[m];
         seg[m + 1] = seg[m] + npair * ntp[m];
         scl_off[m] = nscl;
@@ -1516,7 +1609,7 @@ fc_status rimp2_batch_build_fx(fc_rimp2_batch* b, const std::vector<BatchMolIn>&
     for (int m = 0; m < nmol; ++m) {
         const int nocc = hm[m].nocc, nT = hm[m].a_pad / fx::BM;
         for (int i = 0; i < nocc; ++i)
-            for (int j = grad ? 0 : i; j < nocc; ++j)
+            for (int j = i; j < nocc; ++j)
                 for (int ta = 0; ta < nT; ++ta)
                     for (int tb = ta; tb < nT; ++tb) hi.push_back(make_int4(m, i, j, ta | (tb << 16)));
     }
