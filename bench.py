@@ -266,13 +266,18 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the one FP64-plain reference step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--size", choices=["full", "small"], default="full",
+    ap.add_argument("--size", choices=["full", "small", "c5"], default="full",
                     help="small: naux 2400, nocc 60, nvir 550 + n 300, naux 1200, nocc 30 "
-                         "(the profiling case; inputs still larger than L2)")
+                         "(the profiling case; inputs still larger than L2); c5: the shapes of "
+                         "all-trans C20H42 in def2-TZVP (naux 2150 def2-TZVP-RIFIT, nocc 81, nvir 791 + "
+                         "n 872, naux 2256 def2-universal-jkfit, nocc 81) with the synthetic distributions")
     args = ap.parse_args()
     if args.size == "small":
         RIMP2.update(naux=2400, nocc=60, nvir=550)
         DFJK.update(n=300, naux=1200, nocc=30)
+    elif args.size == "c5":
+        RIMP2.update(naux=2150, nocc=81, nvir=791)
+        DFJK.update(n=872, naux=2256, nocc=81)
 
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -282,7 +287,9 @@ def main():
     config = {"workload": f"synthetic RI-MP2 E+grad (naux {RIMP2['naux']}, nocc {RIMP2['nocc']}, "
                           f"nvir {RIMP2['nvir']}) + DF-JK build (n {DFJK['n']}, naux {DFJK['naux']}, "
                           f"nocc {DFJK['nocc']}), one replica per GPU",
-              "rimp2": RIMP2, "dfjk": DFJK, "l2": "inputs larger than L2 (B_ov 5.07 GB, B_JK 6.91 GB)",
+              "rimp2": RIMP2, "dfjk": DFJK,
+              "l2": "inputs larger than L2 (B_ov %.2f GB, B_JK %.2f GB)" % (
+                  8e-9 * RIMP2["naux"] * RIMP2["nocc"] * RIMP2["nvir"], 8e-9 * DFJK["naux"] * DFJK["n"] ** 2),
               "parallelism": f"replica x{world}"}
 
     if args.impl == "reference":
