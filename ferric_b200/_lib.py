@@ -52,6 +52,7 @@ SIGNATURES = {
     "fc_rimp2_batched_replay": (_I32, [_P, _P]),
     "fc_rimp2_batched_energies": (_I32, [_P, _DP, _DP]),
     "fc_rimp2_batched_info": (_I32, [_P, _P]),
+    "fc_rimp2_batched_plan": (_c.c_size_t, [_P, _c.c_char_p, _c.c_size_t]),
     "fc_rimp2_batched_destroy": (_I32, [_P]),
     "fc_rimp2_batched": (_I32, [_P, _I64, _I32, _DP, _DP]),
 }

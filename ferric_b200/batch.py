@@ -85,6 +85,15 @@ class Rimp2Batch:
         check(_lib.lib.fc_rimp2_batched_info(self._h, ctypes.byref(r)))
         return r.as_dict()
 
+    def plan(self):
+        """Per size bucket: tile shape, the diagonal-tile exchange choice and
+        whether it was measured (autotuner), defaulted or forced."""
+        import json
+        n = _lib.lib.fc_rimp2_batched_plan(self._h, None, 0)
+        buf = ctypes.create_string_buffer(n + 1)
+        _lib.lib.fc_rimp2_batched_plan(self._h, buf, n + 1)
+        return json.loads(buf.value.decode())
+
     def close(self):
         if getattr(self, "_h", None):
             _lib.lib.fc_rimp2_batched_destroy(self._h)

@@ -2,6 +2,7 @@
 // their operands split once per run, persistent launches over all of them,
 // the whole sequence captured into one CUDA graph and replayed.
 #pragma once
+#include <string>
 #include <vector>
 
 #include "fc_internal.cuh"
@@ -25,6 +26,7 @@ struct fc_rimp2_batch {
     int pair_launches = 0;      // persistent pair-kernel launches in the graph
     double flops = 0.0;         // algorithmic flops of one run
     double ms = 0.0;            // device time of the last timed replay
+    std::string plan_json;      // per size bucket: the exchange choice and where it came from
 };
 
 namespace fc {
@@ -41,5 +43,11 @@ fc_status batch_alloc(fc_rimp2_batch* b, size_t bytes, void** out);
 // Builds the batch's tables and records its launch sequence into b->graph
 // (split-BF16 exact-slice kernels).  group_bytes bounds the amplitude
 // workspace of one group of molecules (gradient).
-fc_status rimp2_batch_build_fx(fc_rimp2_batch* b, const std::vector<BatchMolIn>& mols, size_t group_bytes);
+// The default choice of the diagonal-tile exchange for items with nk k-steps
+// (FERRIC_CUDA_XT=0/1 forces it).
+int fx_exchange_choice(int nk, int grad);
+// plan[m] (or the default when plan is null): 1 = diagonal tiles of molecule m
+// in one phase with the transpose exchanged in shared memory.
+fc_status rimp2_batch_build_fx(fc_rimp2_batch* b, const std::vector<BatchMolIn>& mols, size_t group_bytes,
+                               const int* plan);
 }  // namespace fc

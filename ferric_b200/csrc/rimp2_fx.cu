@@ -30,6 +30,7 @@
 // and the dE/deps partials; the adjoint contraction Gamma = 4 B Tt^T runs in
 // gemm_fx_kernel with the same exact-level scheme.
 #include <algorithm>
+#include <cstdlib>
 
 #include "batch.cuh"
 #include "fc_internal.cuh"
@@ -48,7 +49,9 @@ constexpr int B_BYTES = BN * KT * 2;  // 16 KiB
 constexpr int NSL = 3;
 constexpr int STAGE_BYTES = NSL * (A_BYTES + B_BYTES);  // 96 KiB
 constexpr int STAGES = 2;
-constexpr int SMEM = STAGES * STAGE_BYTES + 1024 + 7168;
+constexpr int XP = BM + 1;                       // pitch of the exchange rows (floats)
+constexpr int XBUF_BYTES = 32 * XP * 4;          // one lane quarter of a parked X tile
+constexpr int SMEM = STAGES * STAGE_BYTES + 1024 + 7168 + XBUF_BYTES;
 constexpr uint32_t IDESC = tc::idesc_bf16_f32(128, 128);
 constexpr double L1W = 1.0 / 256.0, L2W = 1.0 / 65536.0;
 
@@ -170,6 +173,7 @@ struct BatchMol {
     const double* scl;
     int nocc, nvir, a_pad, nk;
     int row0, tpad;  // tpad: virtual pitch of the amplitude rows/columns (gradient)
+    int xt, pad2_;   // exchange (one phase) on diagonal tiles
     float* T;        // amplitudes [nocc*tpad][ldt] (gradient)
     int64_t ldt;
 };
@@ -186,6 +190,7 @@ struct PairFxArgs {
     int ntiles;         // tiles per pair
     int npairs;
     int nocc, nvir, a_pad, nTa, nTb, nk;
+    int xt;        // exchange (one phase) on diagonal tiles
     int64_t items;
     double* part;  // [item][2]
     int* err;
@@ -201,6 +206,7 @@ struct PairFxArgs {
 // Everything the roles need about item k.
 struct ItemView {
     int i, j, ta, tb, nk, a_pad, nvir, row0, slice_rows, tpad, i0, j0;
+    int xt;  // diagonal tile, i != j: Y = X^T exchanged in shared memory, no Y phase
     const double* eo;
     const double* ev;
     const double* scl;
@@ -228,6 +234,7 @@ __device__ __forceinline__ ItemView item_view(const PairFxArgs& p, int64_t k) {
         v.ev = m.ev;
         v.scl = m.scl;
         v.tpad = m.tpad;
+        v.xt = m.xt && v.ta == v.tb && v.i != v.j;
         v.i0 = 0;
         v.j0 = 0;
         v.T = m.T;
@@ -250,6 +257,7 @@ __device__ __forceinline__ ItemView item_view(const PairFxArgs& p, int64_t k) {
         v.ev = p.ev;
         v.scl = p.scl;
         v.tpad = p.a_pad;
+        v.xt = p.xt && v.ta == v.tb && v.i != v.j;
         v.i0 = p.i0;
         v.j0 = p.j0;
         v.T = p.T;
@@ -281,6 +289,7 @@ __global__ void __launch_bounds__(320, 1)
     double* red = reinterpret_cast<double*>(bars + 2 * S + 4);  // [2][8][3]
     double* rowsh = red + 48;                                    // [128] row sums of the upper column half
     double* colsh = rowsh + 128;                                 // [4 quadrants][2 halves][64] column sums
+    float* xbuf = reinterpret_cast<float*>(base + S * STAGE_BYTES + 7168);  // [32][XP] exchange rows
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (tid == 0) {
@@ -319,7 +328,7 @@ __global__ void __launch_bounds__(320, 1)
             uint32_t g = 0;
             for (int64_t k = blockIdx.x; k < p.items && !*abort_flag; k += gridDim.x) {
                 const ItemView v = item_view<BATCH>(p, k);
-                const int nph = v.i == v.j ? 1 : 2;
+                const int nph = (v.i == v.j || v.xt) ? 1 : 2;
                 for (int ph = 0; ph < nph; ++ph) {
                     const int ia = ph == 0 ? v.i : v.j, ib = ph == 0 ? v.j : v.i;
                     for (int kt = 0; kt < v.nk; ++kt, ++g) {
@@ -350,7 +359,7 @@ __global__ void __launch_bounds__(320, 1)
             uint32_t g = 0, pc = 0;  // pc: phases issued (TMEM hand-overs)
             for (int64_t k = blockIdx.x; k < p.items && !*abort_flag; k += gridDim.x) {
                 const ItemView v = item_view<BATCH>(p, k);
-                const int nph = v.i == v.j ? 1 : 2;
+                const int nph = (v.i == v.j || v.xt) ? 1 : 2;
                 for (int ph = 0; ph < nph; ++ph, ++pc) {
                     if (!tc::mbar_wait(tempty, (pc & 1) ^ 1, abort_flag, p.err)) goto mma_done;
                     tc::fence_after_sync();
@@ -434,33 +443,22 @@ __global__ void __launch_bounds__(320, 1)
             tc::fence_before_sync();
             tc::mbar_arrive(tempty);
             ++pc;
-            if (!diag) {
+            const bool xt = v.xt;          // the same for every thread of the CTA
+            const bool two = !diag && !xt;  // a Y phase follows in TMEM
+            if (two) {
                 if (!tc::mbar_wait(tfull, pc & 1, abort_flag, p.err)) break;
                 tc::fence_after_sync();
             }
             // plain FP64 sums over this thread's 64 terms (relative error <= 64 u);
             // the tile partials are summed compensated
             double os = 0.0, ss = 0.0, oc = 0.0, rowc = 0.0;
-#pragma unroll
-            for (int c0 = 0; c0 < HC; c0 += 8) {
-                float y0[8], y1[8], y2[8];
-                if (!diag) {
-                    tc::tmem_ld8(tl + c0, y0);
-                    tc::tmem_ld8(tl + BN + c0, y1);
-                    tc::tmem_ld8(tl + 2 * BN + c0, y2);
-                    tc::tmem_wait_ld();
-                    if (c0 + 8 == HC) {  // every level of this phase is read: release TMEM
-                        tc::fence_before_sync();
-                        tc::mbar_arrive(tempty);
-                    }
-                }
+            // the terms of this thread's columns c0 .. c0 + 7, given their Y values
+            auto proc8 = [&](const int c0, const double (&yv)[8]) {
                 float tt8[8], mv8[8];
 #pragma unroll
                 for (int cc = 0; cc < 8; ++cc) {
                     const double x = (double)xr[c0 + cc];
-                    const double y = diag ? x
-                                          : sya * syb[c0 + cc] *
-                                                ((double)y0[cc] + (double)y1[cc] * L1W + (double)y2[cc] * L2W);
+                    const double y = yv[cc];
                     float tval = 0.f, mval = 0.f, colv = 0.f;
                     if (va && c0 + cc < bmax) {
                         const double r = 1.0 / (dA - evb[c0 + cc]);
@@ -475,6 +473,8 @@ __global__ void __launch_bounds__(320, 1)
                             // dE/deps_occ; by virtual index, of dE/deps_vir.  Pair (i, j)
                             // puts its element (a, b) on the row virtual a, pair (j, i)
                             // on b (its row index); the mirrored tile the other way round.
+                            // On an exchanged diagonal tile the thread of row a also
+                            // holds (b, a)'s term and puts it on a directly.
                             const double tt = (2.0 * x - y) * r;   // Tt_ij[a, b]
                             const double cd = x * r * tt;          // t Tt at (a, b)
                             double cm = 0.0;
@@ -485,13 +485,17 @@ __global__ void __launch_bounds__(320, 1)
                                 mval = (float)tm;
                             }
                             oc += cd + cm;
-                            rowc += both ? cd + cm : cd;
-                            colv = (float)(both ? cd + cm : cm);
+                            if (xt) {
+                                rowc += cd + y * r * ((2.0 * y - x) * r);  // t Tt at (b, a)
+                            } else {
+                                rowc += both ? cd + cm : cd;
+                                colv = (float)(both ? cd + cm : cm);
+                            }
                         }
                     }
                     tt8[cc] = tval;
                     mv8[cc] = mval;
-                    if (GRAD) xr[c0 + cc] = colv;  // x of this column is consumed: keep cm there
+                    if (GRAD && !xt) xr[c0 + cc] = colv;  // x of this column is consumed: keep cm there
                 }
                 if (GRAD && a < v.tpad) {
                     // amplitude rows (i, a) and columns (j, b) at pitch tpad (>= nvir);
@@ -534,8 +538,65 @@ __global__ void __launch_bounds__(320, 1)
                         }
                     }
                 }
+            };
+            if (!xt) {
+#pragma unroll
+                for (int c0 = 0; c0 < HC; c0 += 8) {
+                    double yv[8];
+                    if (two) {
+                        float y0[8], y1[8], y2[8];
+                        tc::tmem_ld8(tl + c0, y0);
+                        tc::tmem_ld8(tl + BN + c0, y1);
+                        tc::tmem_ld8(tl + 2 * BN + c0, y2);
+                        tc::tmem_wait_ld();
+                        if (c0 + 8 == HC) {  // every level of this phase is read: release TMEM
+                            tc::fence_before_sync();
+                            tc::mbar_arrive(tempty);
+                        }
+#pragma unroll
+                        for (int cc = 0; cc < 8; ++cc)
+                            yv[cc] = sya * syb[c0 + cc] * ((double)y0[cc] + (double)y1[cc] * L1W + (double)y2[cc] * L2W);
+                    } else {
+#pragma unroll
+                        for (int cc = 0; cc < 8; ++cc) yv[cc] = (double)xr[c0 + cc];
+                    }
+                    proc8(c0, yv);
+                }
+                if (two) ++pc;
+            } else {
+                // Y = X^T inside a diagonal tile: in round r the parked X of lane
+                // quarter r passes through shared memory, and the threads whose 64
+                // columns hold quarter r (half r / 2) take Y[a, b] = X[b, a] of those
+                // 32 columns from it.
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    if (q == r) {
+#pragma unroll
+                        for (int c = 0; c < HC; ++c) xbuf[lane * XP + h * HC + c] = xr[c];
+                    }
+                    asm volatile("bar.sync 1, 256;" ::: "memory");
+                    if (h == (r >> 1)) {
+                        if (r & 1) {
+#pragma unroll
+                            for (int c0 = 0; c0 < 32; c0 += 8) {
+                                double yv[8];
+#pragma unroll
+                                for (int cc = 0; cc < 8; ++cc) yv[cc] = (double)xbuf[(c0 + cc) * XP + row];
+                                proc8(32 + c0, yv);
+                            }
+                        } else {
+#pragma unroll
+                            for (int c0 = 0; c0 < 32; c0 += 8) {
+                                double yv[8];
+#pragma unroll
+                                for (int cc = 0; cc < 8; ++cc) yv[cc] = (double)xbuf[(c0 + cc) * XP + row];
+                                proc8(c0, yv);
+                            }
+                        }
+                    }
+                    asm volatile("bar.sync 1, 256;" ::: "memory");
+                }
             }
-            if (!diag) ++pc;
             const double vo = warp_sum(os), vs = warp_sum(ss);
             const double vc = GRAD ? warp_sum(oc) : 0.0;
             double* rb = red + (li & 1) * 24;
@@ -545,7 +606,7 @@ __global__ void __launch_bounds__(320, 1)
                 rb[(warp - 2) * 3 + 2] = vc;
             }
             if (GRAD && h == 1) rowsh[row] = rowc;
-            if (mir || both) {
+            if ((mir || both) && !xt) {
                 // column sums of the mirrored terms over this warp's 32 rows: a
                 // reduce-scatter butterfly leaves columns 2*lane, 2*lane+1 in xr[0..1]
 #pragma unroll
@@ -563,12 +624,12 @@ __global__ void __launch_bounds__(320, 1)
             }
             asm volatile("bar.sync 1, 256;" ::: "memory");
             if (GRAD && h == 0) p.vir_part[k * 2 * BM + row] = rowc + rowsh[row];
-            if ((mir || both) && et < BM) {
+            if ((mir || both) && et < BM) {  // an exchanged tile put its column terms on the rows
                 const int hh = et >> 6, c = et & 63;
                 double cs = 0.0;
 #pragma unroll
                 for (int qq = 0; qq < 4; ++qq) cs += colsh[(qq * 2 + hh) * 64 + c];
-                p.vir_part[k * 2 * BM + BM + et] = cs;
+                p.vir_part[k * 2 * BM + BM + et] = xt ? 0.0 : cs;
             }
             if (et == 0) {
                 KSum so, sn, sc;
@@ -1082,6 +1143,12 @@ __global__ void __launch_bounds__(256) batch_energy_kernel(const double* __restr
 
 namespace {
 
+// k-steps of 64 from which the exchange is the default (measured on B200:
+// energy items gain from nk = 4 on; gradient items, whose epilogue also
+// writes amplitudes, lose up to nk = 11 and gain a little at nk = 76)
+constexpr int XT_MIN_NK_ENERGY = 4;
+constexpr int XT_MIN_NK_GRAD = 32;
+
 struct FxSplit {
     __nv_bfloat16* bt;
     double* scl;
@@ -1139,6 +1206,17 @@ fc_status fx_attrs() {
 
 }  // namespace
 
+// Diagonal tiles (ta == tb, i != j) in one tensor-core phase with the
+// transpose exchanged in shared memory (1), or in two phases (0).  The
+// exchange saves a phase of MMAs and costs the epilogue two passes over
+// shared memory with half the threads busy in each: it pays when the phase
+// is long (many k-steps).  FERRIC_CUDA_XT=0/1 forces it.
+int fx_exchange_choice(int nk, int grad) {
+    const char* e = std::getenv("FERRIC_CUDA_XT");
+    if (e && (e[0] == '0' || e[0] == '1')) return e[0] == '1';
+    return nk >= (grad ? XT_MIN_NK_GRAD : XT_MIN_NK_ENERGY);
+}
+
 fc_status rimp2_energy_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double* e_ss, fc_stats* stats) {
     FC_TRY(fx_attrs());
     if (d.nocc > (1 << 15)) return fail(FC_ERR_LAYOUT, "split-BF16: nocc too large");
@@ -1176,6 +1254,7 @@ fc_status rimp2_energy_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, doub
     a.nTa = (int)(sp.a_pad / fx::BM);
     a.nTb = (int)(sp.a_pad / fx::BN);
     a.nk = (int)(sp.q_pad / fx::KT);
+    a.xt = fx_exchange_choice(a.nk, 0);
     a.items = (int64_t)a.npairs * a.ntiles;
     void* vpart;
     FC_TRY(ws_get(WS_PART, a.items * 2 * sizeof(double), &vpart));
@@ -1354,6 +1433,7 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
         a.nTa = nTa;
         a.nTb = nTa;
         a.nk = (int)(sp.q_pad / fx::KT);
+        a.xt = fx_exchange_choice(a.nk, 1);
         a.items = cp.np * ntiles;
         a.part = part;
         a.err = flags + 1;
@@ -1445,7 +1525,8 @@ namespace {
 int64_t rup(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 }  // namespace
 
-fc_status rimp2_batch_build_fx(fc_rimp2_batch* b, const std::vector<BatchMolIn>& mols, size_t group_bytes) {
+fc_status rimp2_batch_build_fx(fc_rimp2_batch* b, const std::vector<BatchMolIn>& mols, size_t group_bytes,
+                               const int* plan) {
     FC_TRY(fx_attrs());
     const int nmol = (int)mols.size();
     const bool grad = b->grad != 0;
@@ -1575,6 +1656,7 @@ fc_status rimp2_batch_build_fx(fc_rimp2_batch* b, const std::vector<BatchMolIn>&
         hm[m].a_pad = (int)x.a_pad;
         hm[m].nk = (int)(rup(x.naux, fx::KT) / fx::KT);
         hm[m].tpad = (int)x.tpad;
+        hm[m].xt = plan ? plan[m] : fx_exchange_choice(hm[m].nk, grad);
         hm[m].T = nullptr;
         hm[m].ldt = x.ldt;
         if (grad) {

@@ -200,6 +200,13 @@ fc_status fc_rimp2_batched_create(const fc_mol_desc* mols, int64_t nmol, int32_t
 fc_status fc_rimp2_batched_replay(fc_rimp2_batch* b, void* stream);
 fc_status fc_rimp2_batched_energies(fc_rimp2_batch* b, double* e_os, double* e_ss);
 fc_status fc_rimp2_batched_info(const fc_rimp2_batch* b, fc_batch_info* info);
+/* The batch's schedule per size bucket, as a JSON array (NUL-terminated
+ * into buf, returns the full length): bucket key ("grad"/"energy", virtual
+ * tiles of 128, k-steps of 64), molecules, tile shape, the diagonal-tile
+ * exchange choice and its source ("tuned": measured by the autotuner when
+ * FERRIC_CUDA_AUTOTUNE=1, or read from FERRIC_CUDA_AUTOTUNE_CACHE;
+ * "default"; "forced" by FERRIC_CUDA_XT), with the measured times. */
+size_t fc_rimp2_batched_plan(const fc_rimp2_batch* b, char* buf, size_t len);
 fc_status fc_rimp2_batched_destroy(fc_rimp2_batch* b);
 /* create + replay + energies + destroy. */
 fc_status fc_rimp2_batched(const fc_mol_desc* mols, int64_t nmol, int32_t precision,

@@ -163,3 +163,52 @@ def test_batch_refusals(fc):
     with pytest.raises(ValueError):
         Rimp2Batch([(dev[0][0], dev[1][1], dev[0][2])])
     torch.cuda.synchronize()
+
+
+def test_batch_autotuner_plan(fc, monkeypatch, tmp_path):
+    """FERRIC_CUDA_AUTOTUNE=1: every size bucket's exchange choice is measured
+    (both choices timed on a trial sub-batch), reported by plan(), written to
+    the cache file, and the results stay within the mixed bars whichever
+    choice won."""
+    import json
+    from ferric_b200.batch import Rimp2Batch
+    cache = tmp_path / "tune.json"
+    monkeypatch.setenv("FERRIC_CUDA_AUTOTUNE", "1")
+    monkeypatch.setenv("FERRIC_CUDA_AUTOTUNE_CACHE", str(cache))
+    mols = _mols([1, 6, 1, 6], seed0=400)
+    bt = Rimp2Batch(_to_dev(mols), grad=True)
+    plan = bt.plan()
+    assert sum(p["molecules"] for p in plan) == 4 and len(plan) == 2
+    for p in plan:
+        assert p["source"] == "tuned" and p["exchange"] in (0, 1)
+        assert p["ms_two_phase"] > 0 and p["ms_exchange"] > 0
+        assert p["exchange"] == int(p["ms_exchange"] < p["ms_two_phase"])
+    bt.run()
+    e_os, e_ss = bt.energies()
+    for m, (b, eo, ev) in enumerate(mols):
+        r_os, r_ss, gamma, d_o, d_v = orc.energy_gamma_deps(b, eo, ev)
+        assert abs(e_os[m] + e_ss[m] - (r_os + r_ss)) <= MIXED_E_REL * abs(r_os + r_ss)
+        assert np.abs(bt.gamma[m].cpu().numpy() - gamma).max() <= MIXED_G_REL * np.abs(gamma).max()
+        assert np.abs(bt.de_dvir[m].cpu().numpy() - d_v).max() <= MIXED_D_REL * np.abs(d_v).max()
+    bt.close()
+    if cache.exists():  # written unless an earlier batch of this process tuned these buckets
+        data = json.loads(cache.read_text())
+        assert all(k.startswith(("grad_", "energy_")) for k in data)
+
+
+@pytest.mark.parametrize("grad", [False, True])
+def test_batch_exchange_forced(fc, monkeypatch, grad):
+    """Both schedules of the diagonal tiles give the same energies (to the
+    FP32 parking of the exchanged Y values)."""
+    from ferric_b200.batch import Rimp2Batch
+    mols = _to_dev(_mols([2, 5, 3], seed0=500))
+    res = {}
+    for xt in ("0", "1"):
+        monkeypatch.setenv("FERRIC_CUDA_XT", xt)
+        bt = Rimp2Batch(mols, grad=grad)
+        assert all(p["source"] == "forced" and p["exchange"] == int(xt) for p in bt.plan())
+        bt.run()
+        res[xt] = bt.energies()
+        bt.close()
+    assert np.allclose(res["0"][0], res["1"][0], rtol=1e-9, atol=0)
+    assert np.allclose(res["0"][1], res["1"][1], rtol=1e-8, atol=0)

@@ -41,12 +41,13 @@ def emulate_fixed_slices(b):
     return np.outer(s, s) * (l0 + l1 / 256.0 + l2 / 65536.0)
 
 
-def energy_from_g(g, eo, ev, tile=128):
+def energy_from_g(g, eo, ev, tile=128, xt=False):
     """The device's energy from the exact level sums.  Per pair i <= j the
     device visits 128 x 128 tiles (ta, tb) with ta <= tb (weight 2 off the tile
     diagonal: the summands are symmetric under a <-> b); in each the X element
     (ia|jb) is parked in FP32 (round to nearest) between the two tensor-core
-    phases and the Y element (ib|ja) stays FP64; i == j uses X only."""
+    phases and the Y element (ib|ja) stays FP64; i == j uses X only.  With the
+    exchange (xt) a diagonal tile's Y is the parked X transposed (FP32)."""
     nocc, nvir = len(eo), len(ev)
     nt = (nvir + tile - 1) // tile
     e_os = e_ss = 0.0
@@ -65,6 +66,8 @@ def energy_from_g(g, eo, ev, tile=128):
                         e_os += w * np.sum(x * x / d)
                     else:
                         y = gy[sa, sb]
+                        if xt and ta == tb:
+                            y = y.astype(np.float32).astype(np.float64)
                         e_os += w * np.sum((x * x + y * y) / d)
                         e_ss += w * np.sum((x - y) ** 2 / d)
     return e_os, e_ss
@@ -73,24 +76,29 @@ def energy_from_g(g, eo, ev, tile=128):
 SHAPES = [(96, 5, 23), (84, 5, 19), (200, 7, 65), (300, 4, 130), (130, 3, 128), (480, 12, 110)]
 
 
+@pytest.mark.parametrize("xt", ["0", "1"])
 @pytest.mark.parametrize("naux,nocc,nvir", SHAPES)
-def test_mixed_energy_matches_oracle_and_emulation(fc, naux, nocc, nvir):
+def test_mixed_energy_matches_oracle_and_emulation(fc, monkeypatch, naux, nocc, nvir, xt):
+    """xt = 1: diagonal tiles in one phase, Y = X^T exchanged in shared memory."""
     from ferric_b200 import rimp2
+    monkeypatch.setenv("FERRIC_CUDA_XT", xt)
     b, eo, ev = synthetic.rimp2_inputs(naux, nocc, nvir)
     ref = orc.spin_components(b, np.concatenate([eo, ev]), nocc, nvir)
     st = {}
     e_os, e_ss = rimp2.rimp2_energy(b, eo, ev, precision="mixed", stats=st)
     assert st["precision"] == 1 and st["launches"] > 0
     assert abs(e_os + e_ss - ref[2]) <= MIXED_E_REL * abs(ref[2]) + 1e-12
-    em = energy_from_g(emulate_fixed_slices(b), eo, ev)
+    em = energy_from_g(emulate_fixed_slices(b), eo, ev, xt=xt == "1")
     # exact accumulation: device == emulation (incl. the FP32 parking of X) to summation rounding
     assert abs(e_os - em[0]) <= 1e-12 * abs(em[0]) + 1e-15
     assert abs(e_ss - em[1]) <= 1e-12 * abs(em[0]) + 1e-15
 
 
-@pytest.mark.parametrize("naux,nocc,nvir", [(96, 5, 23), (200, 7, 65), (300, 4, 130)])
-def test_mixed_gradient_matches_oracle(fc, naux, nocc, nvir):
+@pytest.mark.parametrize("xt", ["0", "1"])
+@pytest.mark.parametrize("naux,nocc,nvir", [(96, 5, 23), (200, 7, 65), (300, 4, 130), (520, 6, 300)])
+def test_mixed_gradient_matches_oracle(fc, monkeypatch, naux, nocc, nvir, xt):
     from ferric_b200 import rimp2
+    monkeypatch.setenv("FERRIC_CUDA_XT", xt)
     b, eo, ev = synthetic.rimp2_inputs(naux, nocc, nvir)
     e_os, e_ss, gamma, d_o, d_v = orc.energy_gamma_deps(b, eo, ev)
     sc, g, go, gv = rimp2.rimp2_energy_grad(b, eo, ev, precision="mixed")
@@ -165,3 +173,19 @@ def test_mixed_fast_has_no_adjoint(fc):
     with pytest.raises(L.FcError) as ei:
         rimp2.rimp2_energy_grad(b, eo, ev, precision="mixed_fast")
     assert ei.value.name == "FC_ERR_KERNEL"
+
+
+def test_exchange_matches_two_phases(fc, monkeypatch):
+    """The diagonal-tile exchange changes only which Y values are parked in
+    FP32 (those of diagonal tiles): energy to ~1e-9, Gamma to the FP32 rounding
+    of the amplitudes."""
+    from ferric_b200 import rimp2
+    b, eo, ev = synthetic.rimp2_inputs(520, 7, 300)
+    out = {}
+    for xt in ("0", "1"):
+        monkeypatch.setenv("FERRIC_CUDA_XT", xt)
+        out[xt] = rimp2.rimp2_energy_grad(b, eo, ev, precision="mixed")
+    e0, e1 = out["0"][0].e_total, out["1"][0].e_total
+    assert abs(e0 - e1) <= 1e-9 * abs(e0)
+    for k in (1, 2, 3):
+        assert np.abs(out["0"][k] - out["1"][k]).max() <= 1e-6 * np.abs(out["0"][k]).max()
