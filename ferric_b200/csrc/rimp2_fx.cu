@@ -51,7 +51,8 @@ constexpr int STAGE_BYTES = NSL * (A_BYTES + B_BYTES);  // 96 KiB
 constexpr int STAGES = 2;
 constexpr int XP = BM + 1;                       // pitch of the exchange rows (floats)
 constexpr int XBUF_BYTES = 32 * XP * 4;          // one lane quarter of a parked X tile
-constexpr int SMEM = STAGES * STAGE_BYTES + 1024 + 7168 + XBUF_BYTES;
+constexpr int COL_BYTES = 3 * BN * 8;             // a tile's virtual energies and column scales
+constexpr int SMEM = STAGES * STAGE_BYTES + 1024 + 7168 + XBUF_BYTES + COL_BYTES;
 constexpr uint32_t IDESC = tc::idesc_bf16_f32(128, 128);
 constexpr double L1W = 1.0 / 256.0, L2W = 1.0 / 65536.0;
 
@@ -149,11 +150,11 @@ __global__ void fill_kernel(double* __restrict__ x, int64_t n, double v) {
 // Per-Q-row split of B_ov over (j, b) with b padded to a_pad:
 // Bq[s][q][j*a_pad + b] (q < q_rows), scale qs[q].  One CTA per Q row.
 
-__global__ void __launch_bounds__(256) split_fx_qrows_kernel(const double* __restrict__ B, int64_t naux,
-                                                             int64_t nocc, int64_t nvir, int64_t a_pad,
+__global__ void __launch_bounds__(256) split_fx_qrows_kernel(const double* __restrict__ B, int64_t nocc,
+                                                             int64_t nvir, int64_t tpad, int64_t K,
                                                              int64_t q_rows, double* __restrict__ qs,
                                                              __nv_bfloat16* __restrict__ Bq) {
-    split_fx_qrows_body(B, nocc, nvir, a_pad, nocc * a_pad, q_rows, qs, Bq, blockIdx.x);
+    split_fx_qrows_body(B, nocc, nvir, tpad, K, q_rows, qs, Bq, blockIdx.x);
 }
 
 
@@ -190,6 +191,7 @@ struct PairFxArgs {
     int ntiles;         // tiles per pair
     int npairs;
     int nocc, nvir, a_pad, nTa, nTb, nk;
+    int tpad;      // pitch of the amplitude rows and columns (>= nvir, multiple of 8)
     int xt;        // exchange (one phase) on diagonal tiles
     int64_t items;
     double* part;  // [item][2]
@@ -256,7 +258,7 @@ __device__ __forceinline__ ItemView item_view(const PairFxArgs& p, int64_t k) {
         v.eo = p.eo;
         v.ev = p.ev;
         v.scl = p.scl;
-        v.tpad = p.a_pad;
+        v.tpad = p.tpad;
         v.xt = p.xt && v.ta == v.tb && v.i != v.j;
         v.i0 = p.i0;
         v.j0 = p.j0;
@@ -290,6 +292,7 @@ __global__ void __launch_bounds__(320, 1)
     double* rowsh = red + 48;                                    // [128] row sums of the upper column half
     double* colsh = rowsh + 128;                                 // [4 quadrants][2 halves][64] column sums
     float* xbuf = reinterpret_cast<float*>(base + S * STAGE_BYTES + 7168);  // [32][XP] exchange rows
+    double* colb = reinterpret_cast<double*>(base + S * STAGE_BYTES + 7168 + XBUF_BYTES);  // [3][BN]
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (tid == 0) {
@@ -419,13 +422,28 @@ __global__ void __launch_bounds__(320, 1)
             const double sxa = v.scl[(int64_t)i * v.a_pad + a];
             const double sya = v.scl[(int64_t)j * v.a_pad + a];
             const int b0 = tb * BN + h * HC;  // first column of this thread
-            const double* sxb = v.scl + (int64_t)j * v.a_pad + b0;
-            const double* syb = v.scl + (int64_t)i * v.a_pad + b0;
-            const double* evb = v.ev + b0;
+            // the tile's columns (virtual energies, scales of (j, b) and (i, b)) in
+            // shared memory: every lane of a warp reads the same column (broadcast)
+            {
+                const int cb = tb * BN + (et & (BN - 1));
+                if (et < BN) {
+                    colb[et] = cb < v.nvir ? v.ev[cb] : 0.0;
+                    colb[BN + et] = v.scl[(int64_t)j * v.a_pad + cb];
+                } else {
+                    colb[2 * BN + (et - BN)] = v.scl[(int64_t)i * v.a_pad + cb];
+                }
+            }
+            asm volatile("bar.sync 1, 256;" ::: "memory");
+            const double* evb = colb + h * HC;
+            const double* sxb = colb + BN + h * HC;
+            const double* syb = colb + 2 * BN + h * HC;
             const int bmax = v.nvir - b0;    // columns c < bmax are real virtuals
 
-            // X phase: park (ia|jb) of this half row in registers (FP32, round to nearest)
-            if (!tc::mbar_wait(tfull, pc & 1, abort_flag, p.err)) break;
+            // X phase: park (ia|jb) of this half row in registers (FP32, round to nearest).
+            // One thread waits (bounded); the 256 epilogue threads leave together
+            // if it gave up, since named barriers follow.
+            if (!tc::bar_and<1, 256>(et != 0 || tc::mbar_wait(tfull, pc & 1, abort_flag, p.err))) break;
+            if (et != 0) tc::mbar_wait(tfull, pc & 1, abort_flag, p.err);  // phase complete: returns at once
             tc::fence_after_sync();
             float xr[HC];
 #pragma unroll
@@ -446,7 +464,8 @@ __global__ void __launch_bounds__(320, 1)
             const bool xt = v.xt;          // the same for every thread of the CTA
             const bool two = !diag && !xt;  // a Y phase follows in TMEM
             if (two) {
-                if (!tc::mbar_wait(tfull, pc & 1, abort_flag, p.err)) break;
+                if (!tc::bar_and<1, 256>(et != 0 || tc::mbar_wait(tfull, pc & 1, abort_flag, p.err))) break;
+                if (et != 0) tc::mbar_wait(tfull, pc & 1, abort_flag, p.err);
                 tc::fence_after_sync();
             }
             // plain FP64 sums over this thread's 64 terms (relative error <= 64 u);
@@ -677,7 +696,8 @@ struct GemmFxArgs {
     int M, N, nk;      // padded to 128; nk = K / 64
     int nTm, nTn;
     int64_t tiles;
-    int a_pad, nvir, naux, i0;
+    int a_pad, nvir, naux, i0;  // a_pad: pitch of the amplitude rows (i, a)
+    int rows;                   // real amplitude rows
     int64_t nov;
     double alpha;
     double* out;  // Gamma (naux, nov)
@@ -737,7 +757,7 @@ __device__ __forceinline__ GemmView gemm_view(const GemmFxArgs& p, const CUtenso
         v.tpad = p.a_pad;
         v.nvir = p.nvir;
         v.naux = p.naux;
-        v.rows = p.nTm * 128;
+        v.rows = p.rows;
         v.i0 = p.i0;
     }
     return v;
@@ -1254,6 +1274,7 @@ fc_status rimp2_energy_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, doub
     a.nTa = (int)(sp.a_pad / fx::BM);
     a.nTb = (int)(sp.a_pad / fx::BN);
     a.nk = (int)(sp.q_pad / fx::KT);
+    a.tpad = a.a_pad;
     a.xt = fx_exchange_choice(a.nk, 0);
     a.items = (int64_t)a.npairs * a.ntiles;
     void* vpart;
@@ -1316,7 +1337,8 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
     if (stats) FC_CUDA(cudaEventRecord(c.ev0, st));
     FC_TRY(fx_split_pairs(d, st, flags, &sp));
     const int64_t a_pad = sp.a_pad;
-    const int64_t K2 = nocc * a_pad;  // (j, b_pad) columns of the Q-row slices
+    const int64_t tp = (nvir + 7) / 8 * 8;  // amplitude pitch: rows (i, a) and columns (j, b), a, b < tp
+    const int64_t K2 = nocc * tp;           // (j, b) columns of the Q-row slices
     const int64_t q_rows = (naux + 127) / 128 * 128;
     const int nTa = (int)(a_pad / fx::BM);
     const int ntiles = nTa * (nTa + 1) / 2;  // tiles ta <= tb
@@ -1324,7 +1346,7 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
     // occupied chunks: a chunk pair (I, J), I <= J, holds the amplitude rows of
     // I (columns of J) and of J (columns of I) in FP32, plus the slices of one
     // of them; each unordered pair (i, j) is computed once and feeds both.
-    const int64_t per_c2 = a_pad * a_pad * (4 + 4 + 6);
+    const int64_t per_c2 = tp * tp * (4 + 4 + 6) + 1024 * tp;
     int64_t cc = 1;
     while (cc < nocc && (cc + 1) * (cc + 1) * per_c2 <= (int64_t)d.chunk_bytes) ++cc;
     const int64_t nch = (nocc + cc - 1) / cc;
@@ -1358,9 +1380,10 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
     FC_TRY(ws_get(WS_SPLIT2, (size_t)3 * q_rows * K2 * 2, &vbq));
     FC_TRY(ws_get(WS_PAIRS, tab_bytes + q_rows * 8, &vtab));
     double* qs = (double*)((char*)vtab + tab_bytes);
-    const size_t cbytes = (size_t)cc * a_pad * cc * a_pad;  // elements of one amplitude block
-    FC_TRY(ws_get(WS_T, cbytes * 8 + (size_t)cc * a_pad * 8, &vT));
-    FC_TRY(ws_get(WS_TS, cbytes * 6, &vTs));
+    const size_t cbytes = (size_t)cc * tp * cc * tp;  // elements of one amplitude block
+    const int64_t mp_max = (cc * tp + 127) / 128 * 128;
+    FC_TRY(ws_get(WS_T, cbytes * 8 + (size_t)mp_max * 8, &vT));
+    FC_TRY(ws_get(WS_TS, (size_t)3 * mp_max * cc * tp * 2, &vTs));
     FC_TRY(ws_get(WS_PART, (size_t)max_items * (2 + 1 + 2 * fx::BM) * 8 + (size_t)(2 * ncp + nocc) * 8, &vpart));
     float* T1 = (float*)vT;
     float* T2 = T1 + cbytes;
@@ -1377,7 +1400,7 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
     // per-Q-row split of B_ov for the adjoint contraction
     FC_CUDA(cudaMemsetAsync(vbq, 0, (size_t)3 * q_rows * K2 * 2, st));
     fill_kernel<<<(unsigned)((q_rows + 255) / 256), 256, 0, st>>>(qs, q_rows, 1.0);
-    split_fx_qrows_kernel<<<(unsigned)naux, 256, 0, st>>>(d.b_ov, naux, nocc, nvir, a_pad, q_rows, qs,
+    split_fx_qrows_kernel<<<(unsigned)naux, 256, 0, st>>>(d.b_ov, nocc, nvir, tp, K2, q_rows, qs,
                                                           (__nv_bfloat16*)vbq);
     FC_TRY(check_launch("split_fx_qrows_kernel"));
     CUtensorMap tmBq;
@@ -1389,20 +1412,21 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
     if (stats) FC_TRY(timing_events((int)ncp, &ev));
     // Gamma[:, rows] += 4 Bq[:, cols] T^T for one amplitude block
     auto adjoint = [&](float* T, int64_t r0, int64_t nr, int64_t k0, int64_t nk) -> fc_status {
-        const int64_t ldk = nk * a_pad, rows = nr * a_pad;
-        split_fx_rows_f32_kernel<<<(unsigned)rows, 256, 0, st>>>(T, ldk, rows, ts, (__nv_bfloat16*)vTs);
+        const int64_t ldk = nk * tp, rows = nr * tp, mp = (rows + 127) / 128 * 128;
+        split_fx_rows_f32_kernel<<<(unsigned)rows, 256, 0, st>>>(T, ldk, mp, ts, (__nv_bfloat16*)vTs);
         CUtensorMap tmTs;
-        FC_TRY(make_tmap_bf16_2d(&tmTs, vTs, ldk, 3 * rows, ldk * 2, fx::KT, 128));
+        FC_TRY(make_tmap_bf16_2d(&tmTs, vTs, ldk, 3 * mp, ldk * 2, fx::KT, 128));
         GemmFxArgs g{};
         g.rs = ts;
         g.cs = qs;
-        g.M = (int)rows;
+        g.M = (int)mp;
         g.N = (int)q_rows;
-        g.nk = (int)(ldk / fx::KT);
-        g.nTm = (int)(rows / 128);
+        g.nk = (int)((ldk + fx::KT - 1) / fx::KT);
+        g.nTm = (int)(mp / 128);
+        g.rows = (int)rows;
         g.nTn = (int)(q_rows / 128);
         g.tiles = (int64_t)g.nTm * g.nTn;
-        g.a_pad = (int)a_pad;
+        g.a_pad = (int)tp;
         g.nvir = (int)nvir;
         g.naux = (int)naux;
         g.i0 = (int)r0;
@@ -1410,7 +1434,7 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
         g.alpha = 4.0;
         g.out = gamma;
         g.err = flags + 1;
-        g.kofs = (int)(k0 * a_pad);
+        g.kofs = (int)(k0 * tp);
         g.accumulate = 1;
         const int g2 = (int)(g.tiles < c.sm_count ? g.tiles : c.sm_count);
         gemm_fx_kernel<0><<<g2, 192, GF_SMEM, st>>>(tmTs, tmBq, g);
@@ -1433,14 +1457,15 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
         a.nTa = nTa;
         a.nTb = nTa;
         a.nk = (int)(sp.q_pad / fx::KT);
+        a.tpad = (int)tp;
         a.xt = fx_exchange_choice(a.nk, 1);
         a.items = cp.np * ntiles;
         a.part = part;
         a.err = flags + 1;
         a.T = T1;
-        a.ldt = cp.nj * a_pad;
+        a.ldt = cp.nj * tp;
         a.T2 = same ? T1 : T2;
-        a.ldt2 = same ? a.ldt : cp.ni * a_pad;
+        a.ldt2 = same ? a.ldt : cp.ni * tp;
         a.i0 = (int)cp.i0;
         a.j0 = (int)cp.j0;
         a.occ_part = occ_part;

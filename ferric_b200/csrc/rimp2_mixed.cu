@@ -267,7 +267,11 @@ __global__ void __launch_bounds__(192, 1)
         for (int64_t k = blockIdx.x; k < p.items; k += gridDim.x, ++li) {
             const ItemDesc d = decode_item(p, k);
             const int buf = li & 1;
-            if (!tc::mbar_wait(&tfull[buf], (li >> 1) & 1, abort_flag, p.err)) break;
+            // one thread waits (bounded); the 128 epilogue threads leave together if
+            // it gave up, since a named barrier follows
+            if (!tc::bar_and<1, 128>(et != 0 || tc::mbar_wait(&tfull[buf], (li >> 1) & 1, abort_flag, p.err)))
+                break;
+            if (et != 0) tc::mbar_wait(&tfull[buf], (li >> 1) & 1, abort_flag, p.err);
             tc::fence_after_sync();
             const int a = d.ta * TC_TILE + row;
             const bool va = a < p.nvir;

@@ -76,6 +76,20 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volati
     }
 }
 
+// AND of `v` over the `nthreads` threads of named barrier `id` (a barrier
+// itself): lets a group of warps take one decision, e.g. to leave a loop that
+// has named barriers in it together.
+template <int ID, int NTHREADS>
+__device__ __forceinline__ bool bar_and(bool v) {
+    uint32_t r;
+    asm volatile(
+        "{ .reg .pred p, q; setp.ne.u32 q, %1, 0; bar.red.and.pred p, %2, %3, q; selp.u32 %0, 1, 0, p; }"
+        : "=r"(r)
+        : "r"((uint32_t)v), "n"(ID), "n"(NTHREADS)
+        : "memory");
+    return r != 0;
+}
+
 // ----------------------------------------------------------------- TMA --
 
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {

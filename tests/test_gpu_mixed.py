@@ -113,16 +113,16 @@ def test_mixed_gradient_matches_oracle(fc, monkeypatch, naux, nocc, nvir, xt):
 
 
 def test_mixed_gradient_chunked(fc, monkeypatch):
-    """Occupied chunks of 2 (9 = 2+2+2+2+1): 15 chunk pairs, 10 of them off
-    the diagonal (each unordered pair feeds the amplitude rows of both its
-    chunks).  The amplitudes are the same; each amplitude block is split at
+    """A small chunk budget: several occupied chunks (the last one shorter),
+    most chunk pairs off the diagonal (each unordered pair feeds the
+    amplitude rows of both its chunks).  The amplitudes are the same; each amplitude block is split at
     its own row scales (the row maximum over the block's columns), so Gamma
     differs from the one-chunk Gamma by the slicing error; dE/deps come from
     the pair kernel in FP64 and differ only in summation order."""
     from ferric_b200 import rimp2
     b, eo, ev = synthetic.rimp2_inputs(160, 9, 40)
     one = rimp2.rimp2_energy_grad(b, eo, ev, precision="mixed")
-    monkeypatch.setenv("FERRIC_CUDA_CHUNK_BYTES", str(3 * 3 * 128 * 128 * 14 - 1))
+    monkeypatch.setenv("FERRIC_CUDA_CHUNK_BYTES", str(9 * (40 * 40 * 14 + 1024 * 40) - 1))  # chunks of 2
     many = rimp2.rimp2_energy_grad(b, eo, ev, precision="mixed")
     assert abs(one[0].e_total - many[0].e_total) <= 1e-14 * abs(one[0].e_total)
     assert np.abs(one[1] - many[1]).max() <= 4e-6 * np.abs(one[1]).max()
