@@ -32,7 +32,7 @@ def test_autograd_f64_matches_fd_and_identities(fc):
     # central differences of the oracle energy at h = 1e-5 on seeded entries
     eps = np.concatenate([eo, ev])
     h = 1e-5
-    rows, cols = synthetic.fd_entries(naux, nocc * nvir, count=16)
+    rows, cols = synthetic.fd_entries(naux, nocc * nvir, count=64)
     for p, ia in zip(rows, cols):
         bp = b.copy(); bp[p, ia] += h
         bm = b.copy(); bm[p, ia] -= h
@@ -67,7 +67,7 @@ def test_autograd_mixed_matches_fd_of_fp64_oracle(fc):
     ref = orc.spin_components(b, eps, nocc, nvir)[2]
     assert abs(e.item() - ref) <= 5e-8 * abs(ref)
     h = 1e-5
-    rows, cols = synthetic.fd_entries(naux, nocc * nvir, count=16)
+    rows, cols = synthetic.fd_entries(naux, nocc * nvir, count=64)
     scale = np.abs(gb).max()
     for p, ia in zip(rows, cols):
         bp = b.copy(); bp[p, ia] += h

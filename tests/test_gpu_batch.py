@@ -212,3 +212,21 @@ def test_batch_exchange_forced(fc, monkeypatch, grad):
         bt.close()
     assert np.allclose(res["0"][0], res["1"][0], rtol=1e-9, atol=0)
     assert np.allclose(res["0"][1], res["1"][1], rtol=1e-8, atol=0)
+
+
+def test_batch_single_and_degenerate_molecules(fc):
+    """A batch of one, and molecules with one occupied / one virtual orbital."""
+    from ferric_b200.batch import Rimp2Batch
+    mols = [synthetic.rimp2_inputs(17, 1, 1, seed_b=61, seed_eps=62),
+            synthetic.rimp2_inputs(40, 1, 30, seed_b=63, seed_eps=64),
+            synthetic.rimp2_inputs(90, 6, 2, seed_b=65, seed_eps=66)]
+    for group in (mols[:1], mols):
+        bt = Rimp2Batch(_to_dev(group), grad=True)
+        bt.run()
+        e_os, e_ss = bt.energies()
+        for m, (b, eo, ev) in enumerate(group):
+            r_os, r_ss, gamma, d_o, d_v = orc.energy_gamma_deps(b, eo, ev)
+            assert abs(e_os[m] + e_ss[m] - (r_os + r_ss)) <= MIXED_E_REL * abs(r_os + r_ss) + 1e-12
+            assert np.abs(bt.gamma[m].cpu().numpy() - gamma).max() <= MIXED_G_REL * np.abs(gamma).max()
+            assert np.abs(bt.de_docc[m].cpu().numpy() - d_o).max() <= MIXED_D_REL * np.abs(d_o).max()
+        bt.close()

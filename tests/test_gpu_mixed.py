@@ -19,6 +19,7 @@ pytestmark = pytest.mark.gpu
 MIXED_E_REL = 5e-8
 MIXED_G_REL = 1e-5
 MIXED_D_REL = 1e-6
+# absolute floor (Eh) for tiny systems, where one product carries the full 2^-23 slice error
 FAST_E_REL = 2e-4     # hi+lo, FP32 accumulation (accumulation-bound)
 
 
@@ -189,3 +190,32 @@ def test_exchange_matches_two_phases(fc, monkeypatch):
     assert abs(e0 - e1) <= 1e-9 * abs(e0)
     for k in (1, 2, 3):
         assert np.abs(out["0"][k] - out["1"][k]).max() <= 1e-6 * np.abs(out["0"][k]).max()
+
+
+EDGE = [
+    (17, 1, 1),       # one occupied, one virtual
+    (1, 3, 4),        # one aux function
+    (65, 2, 129),     # one virtual past a 128-row tile: two tiles, ragged
+    (64, 4, 128),     # exact tile and k-step edges
+    (700, 33, 169),   # the largest batched alkane (C8H18 in cc-pVDZ / -RI)
+]
+
+
+@pytest.mark.parametrize("naux,nocc,nvir", EDGE)
+def test_mixed_edge_shapes(fc, naux, nocc, nvir):
+    from ferric_b200 import rimp2
+    b, eo, ev = synthetic.rimp2_inputs(naux, nocc, nvir, seed_b=11, seed_eps=12)
+    e_os, e_ss, gamma, d_o, d_v = orc.energy_gamma_deps(b, eo, ev)
+    e = rimp2.rimp2_energy(b, eo, ev, precision="mixed")
+    assert abs(sum(e) - (e_os + e_ss)) <= MIXED_E_REL * abs(e_os + e_ss) + 1e-12
+    sc, g, go, gv = rimp2.rimp2_energy_grad(b, eo, ev, precision="mixed")
+    assert abs(sc.e_total - (e_os + e_ss)) <= MIXED_E_REL * abs(e_os + e_ss) + 1e-12
+    assert np.abs(g - gamma).max() <= MIXED_G_REL * np.abs(gamma).max()
+    assert np.abs(go - d_o).max() <= MIXED_D_REL * np.abs(d_o).max()
+    assert np.abs(gv - d_v).max() <= MIXED_D_REL * np.abs(d_v).max()
+
+
+def test_mixed_zero_sizes(fc):
+    from ferric_b200 import rimp2
+    e_os, e_ss = rimp2.rimp2_energy(np.zeros((10, 0)), np.zeros(0), np.zeros(5), precision="mixed")
+    assert e_os == 0.0 and e_ss == 0.0
