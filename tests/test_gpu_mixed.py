@@ -20,6 +20,7 @@ MIXED_E_REL = 5e-8
 MIXED_G_REL = 1e-5
 MIXED_D_REL = 1e-6
 # absolute floor (Eh) for tiny systems, where one product carries the full 2^-23 slice error
+MIXED_E_ABS = 1e-12
 FAST_E_REL = 2e-4     # hi+lo, FP32 accumulation (accumulation-bound)
 
 
@@ -88,7 +89,7 @@ def test_mixed_energy_matches_oracle_and_emulation(fc, monkeypatch, naux, nocc, 
     st = {}
     e_os, e_ss = rimp2.rimp2_energy(b, eo, ev, precision="mixed", stats=st)
     assert st["precision"] == 1 and st["launches"] > 0
-    assert abs(e_os + e_ss - ref[2]) <= MIXED_E_REL * abs(ref[2]) + 1e-12
+    assert abs(e_os + e_ss - ref[2]) <= MIXED_E_REL * abs(ref[2]) + MIXED_E_ABS
     em = energy_from_g(emulate_fixed_slices(b), eo, ev, xt=xt == "1")
     # exact accumulation: device == emulation (incl. the FP32 parking of X) to summation rounding
     assert abs(e_os - em[0]) <= 1e-12 * abs(em[0]) + 1e-15
@@ -103,7 +104,7 @@ def test_mixed_gradient_matches_oracle(fc, monkeypatch, naux, nocc, nvir, xt):
     b, eo, ev = synthetic.rimp2_inputs(naux, nocc, nvir)
     e_os, e_ss, gamma, d_o, d_v = orc.energy_gamma_deps(b, eo, ev)
     sc, g, go, gv = rimp2.rimp2_energy_grad(b, eo, ev, precision="mixed")
-    assert abs(sc.e_total - (e_os + e_ss)) <= MIXED_E_REL * abs(e_os + e_ss) + 1e-12
+    assert abs(sc.e_total - (e_os + e_ss)) <= MIXED_E_REL * abs(e_os + e_ss) + MIXED_E_ABS
     assert np.abs(g - gamma).max() <= MIXED_G_REL * np.abs(gamma).max()
     assert np.abs(go - d_o).max() <= MIXED_D_REL * np.abs(d_o).max()
     assert np.abs(gv - d_v).max() <= MIXED_D_REL * np.abs(d_v).max()
@@ -207,9 +208,9 @@ def test_mixed_edge_shapes(fc, naux, nocc, nvir):
     b, eo, ev = synthetic.rimp2_inputs(naux, nocc, nvir, seed_b=11, seed_eps=12)
     e_os, e_ss, gamma, d_o, d_v = orc.energy_gamma_deps(b, eo, ev)
     e = rimp2.rimp2_energy(b, eo, ev, precision="mixed")
-    assert abs(sum(e) - (e_os + e_ss)) <= MIXED_E_REL * abs(e_os + e_ss) + 1e-12
+    assert abs(sum(e) - (e_os + e_ss)) <= MIXED_E_REL * abs(e_os + e_ss) + MIXED_E_ABS
     sc, g, go, gv = rimp2.rimp2_energy_grad(b, eo, ev, precision="mixed")
-    assert abs(sc.e_total - (e_os + e_ss)) <= MIXED_E_REL * abs(e_os + e_ss) + 1e-12
+    assert abs(sc.e_total - (e_os + e_ss)) <= MIXED_E_REL * abs(e_os + e_ss) + MIXED_E_ABS
     assert np.abs(g - gamma).max() <= MIXED_G_REL * np.abs(gamma).max()
     assert np.abs(go - d_o).max() <= MIXED_D_REL * np.abs(d_o).max()
     assert np.abs(gv - d_v).max() <= MIXED_D_REL * np.abs(d_v).max()
