@@ -107,8 +107,10 @@ struct EpiStore {
     double* C;
     int64_t ldc;
     double alpha;
+    int accumulate;  // C += alpha v instead of C = alpha v
     __device__ __forceinline__ void operator()(int m, int n, double v, int) const {
-        C[(int64_t)m * ldc + n] = alpha * v;
+        double* c = C + (int64_t)m * ldc + n;
+        *c = accumulate ? *c + alpha * v : alpha * v;
     }
 };
 

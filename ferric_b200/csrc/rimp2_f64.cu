@@ -18,6 +18,8 @@
 // Tt_ij[a, b] = (2X - Y)/D into the chunk's amplitude rows and the partials
 // of c = t Tt for dE/d eps (ferric-mp2/src/oo_rimp2.rs:1170-1191); the second
 // contraction Gamma_i = 4 B Tt_i^T runs in dgemm_tn.
+#include <algorithm>
+
 #include "fc_internal.cuh"
 #include "dmma.cuh"
 #include "dgemm_tn.cuh"
@@ -40,12 +42,13 @@ struct PairArgs {
     int has_kappa;
     double kappa;
     double* part;  // [item][2] energy partials
-    // gradient mode
-    double* T;
-    int64_t ldt;
-    int i0;
-    double* occ_part;  // [item]
-    double* vir_part;  // [item][64]
+    // gradient mode: unordered pairs (i, j), i in chunk I (from i0), j in chunk J (from j0)
+    double* T;         // amplitude rows of I: [|I| nvir][ldt = |J| nvir]
+    double* T2;        // amplitude rows of J: [|J| nvir][ldt2 = |I| nvir] (T when I == J)
+    int64_t ldt, ldt2;
+    int i0, j0;
+    double* occ_part;  // [item][2]: t Tt summed for the orderings (i, j) and (j, i)
+    double* vir_part;  // [item][64]: row-virtual sums of both orderings
 };
 
 template <int GRAD>
@@ -137,7 +140,7 @@ __global__ void __launch_bounds__(256, 2) pair_f64_kernel(PairArgs p) {
     cp_async_wait<0>();
 
     const double eij = p.eo[i] + p.eo[j];
-    KSum os, ss, oc;
+    KSum os, ss, oc, oc2;
     double rowsum[2] = {0.0, 0.0};
 #pragma unroll
     for (int mt = 0; mt < 2; ++mt) {
@@ -153,13 +156,25 @@ __global__ void __launch_bounds__(256, 2) pair_f64_kernel(PairArgs p) {
                     const double x = X[mt][nt][h], y = Y[mt][nt][h];
                     double f = 1.0 / D;
                     if (GRAD) {
+                        // pair (i, j): Tt_ij[a, b] into the rows of i; for i < j also
+                        // pair (j, i): Tt_ji[a, b] = (2 G_ji - G_ij)[a, b] / D into the
+                        // rows of j.  Both orderings put t Tt on the row virtual a.
                         const double tt = (2.0 * x - y) * f;
-                        p.T[((int64_t)(i - p.i0) * nvir + a) * p.ldt + (int64_t)j * nvir + b] = tt;
+                        p.T[((int64_t)(i - p.i0) * nvir + a) * p.ldt + (int64_t)(j - p.j0) * nvir + b] = tt;
                         const double c = x * f * tt;
                         os.add(x * x * f);
                         ss.add(x * (x - y) * f);
                         oc.add(c);
                         rowsum[mt] += c;
+                        if (i != j) {
+                            const double t2 = (2.0 * y - x) * f;
+                            p.T2[((int64_t)(j - p.j0) * nvir + a) * p.ldt2 + (int64_t)(i - p.i0) * nvir + b] = t2;
+                            const double c2 = y * f * t2;
+                            os.add(y * y * f);
+                            ss.add(y * (y - x) * f);
+                            oc2.add(c2);
+                            rowsum[mt] += c2;
+                        }
                     } else {
                         if (p.has_kappa) {
                             const double d1 = 1.0 - exp(p.kappa * D);
@@ -182,7 +197,11 @@ __global__ void __launch_bounds__(256, 2) pair_f64_kernel(PairArgs p) {
     }
     if (GRAD) {
         const double voc = block_sum(oc.value(), red);
-        if (tid == 0) p.occ_part[item] = voc;
+        const double voc2 = block_sum(oc2.value(), red);
+        if (tid == 0) {
+            p.occ_part[2 * item] = voc;
+            p.occ_part[2 * item + 1] = voc2;
+        }
 #pragma unroll
         for (int mt = 0; mt < 2; ++mt) {
             double r = rowsum[mt];
@@ -218,22 +237,34 @@ __global__ void __launch_bounds__(1024) reduce_pairs_kernel(const double* __rest
     }
 }
 
-// de_docc[i0 + il] = -2 * sum of the occ partials of occupied il of the chunk.
+// acc_occ[o] += sum of the t Tt partials of the ordering (o, *) of every item
+// whose pair holds o (slot 0 when o is i, slot 1 when o is j != i), for o in
+// I (blocks 0 .. ni-1) and J (the rest); fixed order.
 __global__ void __launch_bounds__(256) reduce_occ_kernel(const double* __restrict__ occ_part,
-                                                         int64_t items_per_i, int i0,
-                                                         double* de_docc) {
+                                                         const int2* __restrict__ pairs, int64_t npairs,
+                                                         int ntile2, int i0, int ni, int j0,
+                                                         double* acc_occ) {
     __shared__ double sh[256];
-    const int il = blockIdx.x;
-    const double* src = occ_part + (int64_t)il * items_per_i;
+    const int o = (int)blockIdx.x < ni ? i0 + (int)blockIdx.x : j0 + ((int)blockIdx.x - ni);
     KSum a;
-    for (int64_t k = threadIdx.x; k < items_per_i; k += 256) a.add(src[k]);
+    const int64_t n = npairs * ntile2;
+    for (int64_t k = threadIdx.x; k < n; k += 256) {
+        const int2 pr = pairs[k / ntile2];
+        if (pr.x == o) a.add(occ_part[2 * k]);
+        else if (pr.y == o) a.add(occ_part[2 * k + 1]);
+    }
     sh[threadIdx.x] = a.value();
     __syncthreads();
     if (threadIdx.x == 0) {
         KSum x;
         for (int k = 0; k < 256; ++k) x.add(sh[k]);
-        de_docc[i0 + il] = -2.0 * x.value();
+        acc_occ[o] += x.value();
     }
+}
+
+__global__ void scale_copy_f64_kernel(const double* __restrict__ x, int64_t n, double s, double* __restrict__ y) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) y[k] = s * x[k];
 }
 
 // acc_vir[a] += 2 * sum over the chunk's items with a in their a-tile.
@@ -337,40 +368,76 @@ fc_status rimp2_grad_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, doubl
     FC_TRY(set_smem_once());
     const int64_t nocc = d.nocc, nvir = d.nvir, naux = d.naux, nov = nocc * nvir;
     const int ntile = (int)((nvir + PR_T - 1) / PR_T);
-    // Amplitude chunk: ci occupied rows of Tt (ci*nvir x nov doubles), sized to
-    // a fixed budget so the call fits beside B and Gamma.
-    const int64_t per_i = nvir * nov * (int64_t)sizeof(double);
-    int64_t ci = d.chunk_bytes / (per_i > 0 ? per_i : 1);
-    if (ci < 1) ci = 1;
-    if (ci > nocc) ci = nocc;
-    const int64_t items_per_i = nocc * (int64_t)ntile * ntile;
-    const int64_t items = ci * items_per_i;
-    if (items > INT32_MAX) return fail(FC_ERR_LAYOUT, "RI-MP2 gradient: too many pair tiles per chunk");
-
-    void *vpairs, *vpart, *vT, *vocc, *vvir, *vout;
-    FC_TRY(ws_get(WS_PAIRS, (nocc * nocc + (int64_t)ntile * ntile) * sizeof(int2), &vpairs));
-    FC_TRY(ws_get(WS_T, ci * per_i, &vT));
-    FC_TRY(ws_get(WS_PART, items * (2 + 1 + PR_T) * sizeof(double), &vpart));
-    FC_TRY(ws_get(WS_OUT, ((nocc + 63) / 64 * 64 + 2) * 2 * sizeof(double) + 64, &vout));
-    vocc = (double*)vpart + items * 2;
-    vvir = (double*)vocc + items;
-    double* e_chunks = (double*)vout;  // [nchunks][2]
-    std::vector<int2> hp((size_t)(nocc * nocc));
-    for (int i = 0; i < nocc; ++i)
-        for (int j = 0; j < nocc; ++j) hp[(size_t)i * nocc + j] = make_int2(i, j);
+    const int ntile2 = ntile * ntile;  // every tile (ta, tb) of a pair, ta-major
+    // Occupied chunks processed as chunk pairs (I, J), I <= J: each unordered
+    // pair (i, j) is computed once and writes the amplitude rows of i (columns
+    // of J) and of j (columns of I); both blocks (c nvir)^2 doubles fit the
+    // chunk budget beside B and Gamma.
+    int64_t cc = 1;
+    while (cc < nocc && 2 * (cc + 1) * nvir * (cc + 1) * nvir * 8 <= (int64_t)d.chunk_bytes) ++cc;
+    const int64_t nch = (nocc + cc - 1) / cc;
+    struct CP {
+        int64_t i0, ni, j0, nj, p0, np;
+    };
+    std::vector<CP> cps;
+    std::vector<int2> hp;
+    for (int64_t I = 0; I < nch; ++I)
+        for (int64_t J = I; J < nch; ++J) {
+            CP x;
+            x.i0 = I * cc;
+            x.ni = std::min(cc, nocc - x.i0);
+            x.j0 = J * cc;
+            x.nj = std::min(cc, nocc - x.j0);
+            x.p0 = (int64_t)hp.size();
+            for (int64_t i = x.i0; i < x.i0 + x.ni; ++i)
+                for (int64_t j = (I == J ? i : x.j0); j < x.j0 + x.nj; ++j) hp.push_back(make_int2((int)i, (int)j));
+            x.np = (int64_t)hp.size() - x.p0;
+            cps.push_back(x);
+        }
+    const int64_t npairs_all = (int64_t)hp.size();
     for (int ta = 0; ta < ntile; ++ta)
-        for (int tb = 0; tb < ntile; ++tb) hp.push_back(make_int2(ta, tb));  // every tile: ta-major
+        for (int tb = 0; tb < ntile; ++tb) hp.push_back(make_int2(ta, tb));
+    const int64_t ncp = (int64_t)cps.size();
+    int64_t max_items = 0;
+    for (const auto& x : cps) max_items = std::max(max_items, x.np * ntile2);
+    if (max_items > INT32_MAX) return fail(FC_ERR_LAYOUT, "RI-MP2 gradient: too many pair tiles per chunk pair");
+
+    void *vpairs, *vpart, *vT, *vout;
+    const size_t blk = (size_t)cc * nvir * cc * nvir;  // doubles of one amplitude block
+    FC_TRY(ws_get(WS_PAIRS, hp.size() * sizeof(int2), &vpairs));
+    FC_TRY(ws_get(WS_T, 2 * blk * sizeof(double), &vT));
+    FC_TRY(ws_get(WS_PART, (size_t)max_items * (2 + 2 + PR_T) * sizeof(double), &vpart));
+    FC_TRY(ws_get(WS_OUT, (size_t)(2 * ncp + nocc) * sizeof(double) + 64, &vout));
+    double* part = (double*)vpart;
+    double* occ = part + 2 * max_items;
+    double* vir = occ + 2 * max_items;
+    double* T1 = (double*)vT;
+    double* T2 = T1 + blk;
+    double* e_cp = (double*)vout;     // [ncp][2]
+    double* acc_occ = e_cp + 2 * ncp;  // [nocc]
     FC_CUDA(cudaMemcpyAsync(vpairs, hp.data(), hp.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
     FC_CUDA(cudaMemsetAsync(de_dvir, 0, nvir * sizeof(double), st));
+    FC_CUDA(cudaMemsetAsync(acc_occ, 0, nocc * sizeof(double), st));
+    FC_CUDA(cudaMemsetAsync(gamma, 0, (size_t)naux * nov * sizeof(double), st));
+    const int2* dpairs = (const int2*)vpairs;
 
     Context& c = ctx();
-    const int64_t nchunks = (nocc + ci - 1) / ci;
     cudaEvent_t* ev = nullptr;
-    if (stats) FC_TRY(timing_events((int)nchunks, &ev));
+    if (stats) FC_TRY(timing_events((int)ncp, &ev));
     if (stats) FC_CUDA(cudaEventRecord(c.ev0, st));
-    for (int64_t ch = 0; ch < nchunks; ++ch) {
-        const int64_t i0 = ch * ci;
-        const int64_t cn = (i0 + ci <= nocc) ? ci : nocc - i0;
+    // Gamma[:, rows of R] += 4 B_ov[:, columns of K] . T^T
+    auto adjoint = [&](const double* T, int64_t r0, int64_t nr, int64_t k0, int64_t nk) -> fc_status {
+        const int N = (int)(nr * nvir);
+        dim3 grid((N + DG_BN - 1) / DG_BN, (unsigned)((naux + DG_BM - 1) / DG_BM), 1);
+        EpiStore epi{gamma + r0 * nvir, nov, 4.0, 1};
+        const int64_t K = nk * nvir;
+        dgemm_tn_kernel<EpiStore><<<grid, 256, DG_SMEM, st>>>(d.b_ov + k0 * nvir, nov, T, K, (int)naux, N, K, K, 0,
+                                                               epi);
+        return check_launch("dgemm_tn_kernel<gamma>");
+    };
+    for (int64_t x = 0; x < ncp; ++x) {
+        const CP& cp = cps[x];
+        const bool same = cp.i0 == cp.j0;
         PairArgs a{};
         a.B = d.b_ov;
         a.ldb = nov;
@@ -378,43 +445,43 @@ fc_status rimp2_grad_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, doubl
         a.nvir = (int)nvir;
         a.eo = d.eps_occ;
         a.ev = d.eps_vir;
-        a.pairs = (const int2*)vpairs + i0 * nocc;
-        a.tiles = (const int2*)vpairs + nocc * nocc;
-        a.ntiles = ntile * ntile;
-        a.part = (double*)vpart;
-        a.T = (double*)vT;
-        a.ldt = nov;
-        a.i0 = (int)i0;
-        a.occ_part = (double*)vocc;
-        a.vir_part = (double*)vvir;
-        const int64_t nit = cn * items_per_i;
-        if (stats) FC_CUDA(cudaEventRecord(ev[2 * ch], st));
+        a.pairs = dpairs + cp.p0;
+        a.tiles = dpairs + npairs_all;
+        a.ntiles = ntile2;
+        a.part = part;
+        a.T = T1;
+        a.ldt = cp.nj * nvir;
+        a.T2 = same ? T1 : T2;
+        a.ldt2 = same ? a.ldt : cp.ni * nvir;
+        a.i0 = (int)cp.i0;
+        a.j0 = (int)cp.j0;
+        a.occ_part = occ;
+        a.vir_part = vir;
+        const int64_t nit = cp.np * ntile2;
+        if (stats) FC_CUDA(cudaEventRecord(ev[2 * x], st));
         pair_f64_kernel<1><<<(unsigned)nit, 256, PR_SMEM, st>>>(a);
         FC_TRY(check_launch("pair_f64_kernel<grad>"));
-        if (stats) FC_CUDA(cudaEventRecord(ev[2 * ch + 1], st));
-        reduce_pairs_kernel<<<1, 1024, 0, st>>>((const double*)vpart, nit, e_chunks + 2 * ch);
-        reduce_occ_kernel<<<(unsigned)cn, 256, 0, st>>>((const double*)vocc, items_per_i, (int)i0, de_docc);
-        reduce_vir_kernel<<<(unsigned)((nvir + 7) / 8), 256, 0, st>>>((const double*)vvir, cn * nocc, ntile,
-                                                                      (int)nvir, de_dvir);
+        if (stats) FC_CUDA(cudaEventRecord(ev[2 * x + 1], st));
+        reduce_pairs_kernel<<<1, 1024, 0, st>>>(part, nit, e_cp + 2 * x);
+        reduce_occ_kernel<<<(unsigned)(same ? cp.ni : cp.ni + cp.nj), 256, 0, st>>>(
+            occ, dpairs + cp.p0, cp.np, ntile2, (int)cp.i0, (int)cp.ni, (int)cp.j0, acc_occ);
+        reduce_vir_kernel<<<(unsigned)((nvir + 7) / 8), 256, 0, st>>>(vir, cp.np, ntile, (int)nvir, de_dvir);
         FC_TRY(check_launch("rimp2 gradient reductions"));
-        // Gamma[:, i0*nvir : (i0+cn)*nvir] = 4 * B_ov . Tt_chunk^T
-        const int N = (int)(cn * nvir);
-        dim3 grid((N + DG_BN - 1) / DG_BN, (unsigned)((naux + DG_BM - 1) / DG_BM), 1);
-        EpiStore epi{gamma + i0 * nvir, nov, 4.0};
-        dgemm_tn_kernel<EpiStore><<<grid, 256, DG_SMEM, st>>>(d.b_ov, nov, (const double*)vT, nov,
-                                                               (int)naux, N, nov, nov, 0, epi);
-        FC_TRY(check_launch("dgemm_tn_kernel<gamma>"));
+        FC_TRY(adjoint(T1, cp.i0, cp.ni, cp.j0, cp.nj));
+        if (!same) FC_TRY(adjoint(T2, cp.j0, cp.nj, cp.i0, cp.ni));
     }
+    scale_copy_f64_kernel<<<(unsigned)((nocc + 255) / 256), 256, 0, st>>>(acc_occ, nocc, -2.0, de_docc);
+    FC_TRY(check_launch("scale_copy_f64_kernel"));
     if (stats) FC_CUDA(cudaEventRecord(c.ev1, st));
-    std::vector<double> h((size_t)(2 * nchunks));
-    FC_CUDA(cudaMemcpyAsync(h.data(), e_chunks, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    std::vector<double> h((size_t)(2 * ncp));
+    FC_CUDA(cudaMemcpyAsync(h.data(), e_cp, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
     FC_CUDA(cudaStreamSynchronize(st));
     double eo = 0.0, co = 0.0, es = 0.0, cs = 0.0;
-    for (int64_t ch = 0; ch < nchunks; ++ch) {  // ascending-chunk compensated sum
-        double v = h[2 * ch], tt = eo + v;
+    for (int64_t x = 0; x < ncp; ++x) {  // chunk-pair order, compensated
+        double v = h[2 * x], tt = eo + v;
         co += (fabs(eo) >= fabs(v)) ? (eo - tt) + v : (v - tt) + eo;
         eo = tt;
-        v = h[2 * ch + 1];
+        v = h[2 * x + 1];
         tt = es + v;
         cs += (fabs(es) >= fabs(v)) ? (es - tt) + v : (v - tt) + es;
         es = tt;
@@ -428,18 +495,18 @@ fc_status rimp2_grad_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, doubl
         const double P = (double)nocc * (nocc + 1) / 2.0;
         stats->flops = 2.0 * naux * (double)nvir * nvir * P + 2.0 * naux * (double)nov * nov;
         stats->precision = FC_PREC_F64;
-        stats->launches += (int)(5 * nchunks);
+        stats->launches += (int)(5 * ncp + (ncp - nch) + 5);
         stats->tile_m = PR_T;
         stats->tile_n = PR_T;
         stats->k_panel = 0;
         stats->d2h_bytes += h.size() * sizeof(double);
         stats->h2d_bytes += hp.size() * sizeof(int2);
-        // dominant kernel: the fused pair kernel, one launch per chunk, forming
-        // the G_ij blocks of every ordered pair (i in chunk, all j)
-        stats->main_launches = (int)nchunks;
-        FC_TRY(timing_sum((int)nchunks, &stats->main_ms));
-        stats->main_flops = 2.0 * naux * (double)nov * nov;
-        stats->main_bytes = 8.0 * naux * (double)nov * (double)nchunks + 8.0 * (double)nov * nov;
+        // dominant kernel: the fused pair kernel, one launch per chunk pair,
+        // forming G_ij and G_ji of every unordered pair
+        stats->main_launches = (int)ncp;
+        FC_TRY(timing_sum((int)ncp, &stats->main_ms));
+        stats->main_flops = 4.0 * naux * (double)nvir * nvir * P;
+        stats->main_bytes = 8.0 * naux * (double)nov * (double)nch + 8.0 * (double)nov * nov;
     }
     return FC_OK;
 }
