@@ -212,6 +212,24 @@ fc_status fc_rimp2_batched_destroy(fc_rimp2_batch* b);
 fc_status fc_rimp2_batched(const fc_mol_desc* mols, int64_t nmol, int32_t precision,
                            double* e_os, double* e_ss);
 
+/* ---- MO transform and metric dressing (the step before the RI-MP2 path) -----
+ * B[P, l*nright + r] = sum_Q M[P, Q] (Q|lr),
+ * (Q|lr) = sum_{mu nu} C_left[mu, l] (Q|mu nu) C_right[nu, r]
+ * (stream_dressed_mo_band, ferric-mp2/src/rimp2.rs:648-737; with C_left = C_occ
+ * and C_right = C_vir, B is the B_ov of the RI-MP2 entry points).  eri3:
+ * (naux, n, n) row-major, symmetric in (mu, nu); m: (naux, naux) row-major
+ * (V^-1/2 or L^-1); c_left (n x nleft), c_right (n x nright) row-major;
+ * b: (naux, nleft*nright).  FC_PREC_F64: FP64 throughout; FC_PREC_MIXED:
+ * the two half transforms in FP64 and the dressing GEMM (2 naux^2 nleft
+ * nright flops, the dominant term) as exact-slice split-BF16 on the tensor
+ * cores.  The host variant copies eri3 in aux chunks. */
+fc_status fc_mo_dress(const double* eri3, int64_t naux, int64_t n, const double* m,
+                      const double* c_left, int64_t nleft, const double* c_right, int64_t nright,
+                      int32_t precision, double* b, fc_stats* stats);
+fc_status fc_mo_dress_dev(const double* eri3, int64_t naux, int64_t n, const double* m,
+                          const double* c_left, int64_t nleft, const double* c_right, int64_t nright,
+                          int32_t precision, double* b, void* stream, fc_stats* stats);
+
 /* ---- DF-JK ----------------------------------------------------------------
  * A handle owns the device copy of the 3-index tensor for the lifetime of a
  * builder (the reference's per-builder DeviceSlot, ferric-scf/src/df_j_gpu.rs:1-5,

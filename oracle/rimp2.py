@@ -193,3 +193,20 @@ def energy_gamma_deps(b_ov, eps_occ, eps_vir, occ=None):
         de_dvir += 2.0 * np.sum(c, axis=(1, 2))
         gamma[:, i * nvir:(i + 1) * nvir] = 4.0 * (b_ov @ tt.reshape(nvir, nov).T)
     return e_os, e_ss, gamma, de_docc, de_dvir
+
+
+def stream_dressed_mo(t3, m, c_left, c_right, chunk=256):
+    """B[P, l*nr + r] = sum_Q M[P, Q] (Q|lr), (Q|lr) = C_left^T (Q|mu nu) C_right,
+    streamed over aux chunks with an accumulating GEMM into B
+    (stream_dressed_mo_band_budgeted, ferric-mp2/src/rimp2.rs:665-737:
+    occupied-side contraction first, then the right index, then
+    ``b += V^-1/2[:, chunk] . mo_blk``)."""
+    naux = t3.shape[0]
+    nl, nr = c_left.shape[1], c_right.shape[1]
+    b = np.zeros((naux, nl * nr))
+    for q0 in range(0, naux, chunk):
+        q1 = min(naux, q0 + chunk)
+        half = np.einsum("ml,qmn->qln", c_left, t3[q0:q1], optimize=True)   # (qc, nl, nao)
+        mo = np.einsum("qln,nr->qlr", half, c_right, optimize=True).reshape(q1 - q0, nl * nr)
+        b += m[:, q0:q1] @ mo
+    return b

@@ -49,7 +49,7 @@ def build(name):
     enuc = scf.nuclear_repulsion(zs, rs)
     nocc = int(g["nocc"])
     e_rhf, eps, C = scf.rhf(S, T + V, nocc, enuc, scf.exact_jk(eri))
-    b, _, _ = scf.dressed(basis.shells_for(atoms, aux), sh)
+    b, v_aux, t3_aux = scf.dressed(basis.shells_for(atoms, aux), sh)
     bov = scf.b_ov(b, C, nocc)
     nvir = C.shape[1] - nocc
     e_os, e_ss, _ = orc.spin_components(bov, eps, nocc, nvir)
@@ -67,8 +67,9 @@ def build(name):
         e_df, eps_df, c_df = scf.rhf(S, T + V, nocc, enuc, scf.df_jk(bjk))
         bov_df = scf.b_ov(b, c_df, nocc)
         d_os, d_ss, _ = orc.spin_components(bov_df, eps_df, nocc, nvir)
+        # raw (P|mn), the metric and the exact-JK orbitals: inputs of the MO dressing
         out.update(b_jk=bjk, b_ri=b, h_core=T + V, s=S, e_nuc=enuc, oracle_e_dfrhf=e_df,
-                   oracle_dfrhf_e_os=d_os, oracle_dfrhf_e_ss=d_ss)
+                   oracle_dfrhf_e_os=d_os, oracle_dfrhf_e_ss=d_ss, t3_ri=t3_aux, v_ri=v_aux, c=C)
     print(f"{name}: n {C.shape[0]} naux {bov.shape[0]} E_rhf {e_rhf:.12f} (golden {g['e_rhf']:.12f}) "
           f"E_os {e_os:.14f} (golden {g['dfmp2']['e_os']:.14f}) {time.time() - t0:.1f} s", flush=True)
     np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
