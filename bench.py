@@ -298,6 +298,47 @@ def batch_leg(torch, dev, nmol):
     return out
 
 
+def dress_leg(torch, dev, naux=2150, n=872, nocc=81):
+    """MO transform + metric dressing at config 5's shapes (C20H42 in def2-TZVP
+    / def2-TZVP-RIFIT): synthetic (Q|mu nu) symmetric in mu nu (the config-2
+    distribution), M = L^-1 of a seeded SPD metric, orthonormal orbitals;
+    FP64 and split-BF16 dressing timed once each (after a warm-up at small
+    size), the mixed result's error against FP64 stated."""
+    from ferric_b200.dress import mo_dress
+    g = torch.Generator(device=dev)
+    g.manual_seed(5)
+    idx = torch.arange(n, device=dev, dtype=torch.float64)
+    env = 0.05 * torch.exp(-(idx[:, None] - idx[None, :]).abs() / 50.0)
+    t3 = torch.empty((naux, n, n), device=dev, dtype=torch.float64)
+    for q0 in range(0, naux, 128):
+        x = torch.randn((min(128, naux - q0), n, n), generator=g, device=dev, dtype=torch.float64) * env
+        t3[q0:q0 + x.shape[0]] = (x + x.transpose(1, 2)) / (2.0 ** 0.5)
+    a = torch.randn((naux, naux), generator=g, device=dev, dtype=torch.float64)
+    v = a @ a.T / naux + torch.eye(naux, device=dev, dtype=torch.float64)
+    m = torch.linalg.inv(torch.linalg.cholesky(v))
+    c, _ = torch.linalg.qr(torch.randn((n, n), generator=g, device=dev, dtype=torch.float64))
+    cl, cr = c[:, :nocc].contiguous(), c[:, nocc:].contiguous()
+    mo_dress(t3[:8, :64, :64].contiguous(), m[:8, :8].contiguous(), cl[:64].contiguous(), cr[:64].contiguous(),
+             precision="mixed")
+    out = {"naux": naux, "n": n, "nocc": nocc, "nvir": n - nocc,
+           "data": "synthetic (Q|mu nu), seeded SPD metric, orthonormal orbitals"}
+    res = {}
+    for prec in ("f64", "mixed"):
+        st = {}
+        b = mo_dress(t3, m, cl, cr, precision=prec, stats=st)
+        torch.cuda.synchronize()
+        res[prec] = b
+        out[prec] = {"ms": st["kernel_ms"], "tflops": st["flops"] / (st["kernel_ms"] * 1e-3) / 1e12,
+                     "dressing_gemm_ms": st["main_ms"],
+                     "dressing_gemm_tflops": st["main_flops"] / (st["main_ms"] * 1e-3) / 1e12}
+    out["flops"] = st["flops"]
+    out["mixed_b_max_rel_err"] = float((res["mixed"] - res["f64"]).abs().max() / res["f64"].abs().max())
+    out["speedup_mixed_vs_f64"] = out["f64"]["ms"] / out["mixed"]["ms"]
+    del t3, res
+    torch.cuda.empty_cache()
+    return out
+
+
 def max_over_ranks(torch, ms, world, dev):
     """The slowest rank's device time: every rank takes part in one MAX all-reduce."""
     if world <= 1:
@@ -324,6 +365,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched config-4 leg")
     ap.add_argument("--batch-mols", type=int, default=512)
+    ap.add_argument("--no-dress", action="store_true", help="skip the MO-dressing leg")
     ap.add_argument("--size", choices=["full", "small", "c5"], default="full",
                     help="small: naux 2400, nocc 60, nvir 550 + n 300, naux 1200, nocc 30 "
                          "(the profiling case; inputs still larger than L2); c5: the shapes of "
@@ -569,6 +611,11 @@ def main():
         torch.cuda.empty_cache()
         batch = batch_leg(torch, dev, args.batch_mols)
 
+    # ---- the step before the path: MO transform + metric dressing, config-5 shapes
+    dress = None
+    if prec == "mixed" and not args.no_dress:
+        dress = dress_leg(torch, dev)
+
     if rank == 0:
         out = {
             "metric": "RI-MP2 E+grad & DF-JK step throughput (algorithmic TFLOP/s)",
@@ -584,7 +631,7 @@ def main():
             "roofline": roofline, "roofline_dfj": roof_dfj,
             "plain_f64": plain,
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
-            "config4_batch": batch,
+            "config4_batch": batch, "mo_dressing": dress,
         }
         print(json.dumps(out))
     jk.close()
