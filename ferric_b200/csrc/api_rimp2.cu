@@ -179,3 +179,94 @@ fc_status fc_rimp2_energy_grad(const double* b_ov, int64_t naux, int64_t nocc, i
 }
 
 }  // extern "C"
+
+namespace {
+
+// Unrestricted RI-MP2 energy components (u_rimp2.rs:693-753): same-spin from
+// the closed-shell kernels (E_ss of one spin's B = 2 E_sigma-sigma, the
+// pair sum of same_spin_block_energy), opposite-spin from the cross kernels.
+fc_status ump2_dispatch(const UmpSpin& a, const UmpSpin& b, int64_t naux, int32_t precision, cudaStream_t st,
+                        double* e_aa, double* e_bb, double* e_ab, fc_stats* stats) {
+    *e_aa = *e_bb = *e_ab = 0.0;
+    if (naux == 0) return FC_OK;
+    const UmpSpin* sp[2] = {&a, &b};
+    double* out[2] = {e_aa, e_bb};
+    for (int k = 0; k < 2; ++k) {
+        const UmpSpin& x = *sp[k];
+        if (x.nocc < 2 || x.nvir == 0) continue;  // one occupied orbital: no same-spin pair
+        Rimp2Dev d{x.b_ov, x.eps_occ, x.eps_vir, naux, x.nocc, x.nvir, 0, 0.0, chunk_budget()};
+        double os = 0.0, ss = 0.0;
+        fc_stats st1{};
+        FC_TRY(energy_dispatch(d, precision, st, &os, &ss, stats ? &st1 : nullptr));
+        *out[k] = 0.5 * ss;
+        if (stats) {
+            stats->main_ms += st1.main_ms;
+            stats->main_flops += st1.main_flops;
+            stats->main_launches += st1.main_launches;
+            stats->launches += st1.launches;
+        }
+    }
+    if (a.nocc && a.nvir && b.nocc && b.nvir) {
+        if (precision == FC_PREC_F64) FC_TRY(ump2_cross_f64(a, b, naux, st, e_ab, stats));
+        else FC_TRY(ump2_cross_fx(a, b, naux, st, e_ab, stats));
+    }
+    if (stats) stats->precision = precision == FC_PREC_F64 ? FC_PREC_F64 : FC_PREC_MIXED;
+    return FC_OK;
+}
+
+fc_status ump2_checks(int64_t naux, int64_t noa, int64_t nva, int64_t nob, int64_t nvb, int32_t precision,
+                      const void* ba, const void* bb, const void* e1, const void* e2, const void* e3) {
+    if (!e1 || !e2 || !e3) return fail(FC_ERR_INVALID, "U-RI-MP2: null output pointer");
+    if (precision != FC_PREC_F64 && precision != FC_PREC_MIXED)
+        return fail(FC_ERR_INVALID, "U-RI-MP2: precision is FC_PREC_F64 or FC_PREC_MIXED");
+    FC_TRY(check_shapes(ba, naux, noa, nva, ba, ba, FC_PREC_F64, 0, 0.0, e1, e2));
+    FC_TRY(check_shapes(bb, naux, nob, nvb, bb, bb, FC_PREC_F64, 0, 0.0, e1, e2));
+    return FC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+fc_status fc_ump2_energy_dev(const double* b_a, int64_t nocc_a, int64_t nvir_a, const double* eps_occ_a,
+                             const double* eps_vir_a, const double* b_b, int64_t nocc_b, int64_t nvir_b,
+                             const double* eps_occ_b, const double* eps_vir_b, int64_t naux, int32_t precision,
+                             double* e_aa, double* e_bb, double* e_ab, void* stream, fc_stats* stats) {
+    FC_TRY(ump2_checks(naux, nocc_a, nvir_a, nocc_b, nvir_b, precision, b_a, b_b, e_aa, e_bb, e_ab));
+    FC_TRY(require_init());
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (stats) *stats = fc_stats{};
+    UmpSpin a{b_a, eps_occ_a, eps_vir_a, nocc_a, nvir_a}, b{b_b, eps_occ_b, eps_vir_b, nocc_b, nvir_b};
+    return ump2_dispatch(a, b, naux, precision, pick_stream(stream), e_aa, e_bb, e_ab, stats);
+}
+
+fc_status fc_ump2_energy(const double* b_a, int64_t nocc_a, int64_t nvir_a, const double* eps_occ_a,
+                         const double* eps_vir_a, const double* b_b, int64_t nocc_b, int64_t nvir_b,
+                         const double* eps_occ_b, const double* eps_vir_b, int64_t naux, int32_t precision,
+                         double* e_aa, double* e_bb, double* e_ab, fc_stats* stats) {
+    FC_TRY(ump2_checks(naux, nocc_a, nvir_a, nocc_b, nvir_b, precision, b_a, b_b, e_aa, e_bb, e_ab));
+    FC_TRY(require_init());
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (stats) *stats = fc_stats{};
+    cudaStream_t st = ctx().stream;
+    const size_t na = (size_t)naux * nocc_a * nvir_a * 8, nb = (size_t)naux * nocc_b * nvir_b * 8;
+    void *da, *db, *ea, *eb;
+    FC_TRY(ws_get(WS_B, na, &da));
+    FC_TRY(ws_get(WS_GAMMA, nb, &db));
+    FC_TRY(ws_get(WS_EPS, (nocc_a + nvir_a) * 8, &ea));
+    FC_TRY(ws_get(WS_HOSTOUT, (nocc_b + nvir_b) * 8, &eb));
+    if (na) FC_CUDA(cudaMemcpyAsync(da, b_a, na, cudaMemcpyHostToDevice, st));
+    if (nb) FC_CUDA(cudaMemcpyAsync(db, b_b, nb, cudaMemcpyHostToDevice, st));
+    if (nocc_a) FC_CUDA(cudaMemcpyAsync(ea, eps_occ_a, nocc_a * 8, cudaMemcpyHostToDevice, st));
+    if (nvir_a) FC_CUDA(cudaMemcpyAsync((double*)ea + nocc_a, eps_vir_a, nvir_a * 8, cudaMemcpyHostToDevice, st));
+    if (nocc_b) FC_CUDA(cudaMemcpyAsync(eb, eps_occ_b, nocc_b * 8, cudaMemcpyHostToDevice, st));
+    if (nvir_b) FC_CUDA(cudaMemcpyAsync((double*)eb + nocc_b, eps_vir_b, nvir_b * 8, cudaMemcpyHostToDevice, st));
+    UmpSpin a{(const double*)da, (const double*)ea, (const double*)ea + nocc_a, nocc_a, nvir_a};
+    UmpSpin b{(const double*)db, (const double*)eb, (const double*)eb + nocc_b, nocc_b, nvir_b};
+    FC_TRY(ump2_dispatch(a, b, naux, precision, st, e_aa, e_bb, e_ab, stats));
+    FC_CUDA(cudaStreamSynchronize(st));
+    if (stats) stats->h2d_bytes += na + nb + (nocc_a + nvir_a + nocc_b + nvir_b) * 8;
+    return FC_OK;
+}
+
+}  // extern "C"

@@ -29,4 +29,18 @@ fc_status rimp2_energy_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, doub
 fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double* e_ss, double* gamma,
                         double* de_docc, double* de_dvir, fc_stats* stats);
 
+// One spin channel of unrestricted RI-MP2 (device pointers).
+struct UmpSpin {
+    const double* b_ov;     // (naux, nocc*nvir)
+    const double* eps_occ;  // [nocc]
+    const double* eps_vir;  // [nvir]
+    int64_t nocc, nvir;
+};
+// Opposite-spin energy sum_{i a J B} (ia|JB)^2 / D: FP64 DMMA, or exact
+// slices on tcgen05.
+fc_status ump2_cross_f64(const UmpSpin& a, const UmpSpin& b, int64_t naux, cudaStream_t st, double* e_ab,
+                         fc_stats* stats);
+fc_status ump2_cross_fx(const UmpSpin& a, const UmpSpin& b, int64_t naux, cudaStream_t st, double* e_ab,
+                        fc_stats* stats);
+
 }  // namespace fc

@@ -49,10 +49,19 @@ struct PairArgs {
     int i0, j0;
     double* occ_part;  // [item][2]: t Tt summed for the orderings (i, j) and (j, i)
     double* vir_part;  // [item][64]: row-virtual sums of both orderings
+    // cross-spin mode (MODE 2): pairs (i alpha, J beta), G = B_alpha_i^T B_beta_J
+    const double* B2;
+    int64_t ldb2;
+    int nvir2;
+    const double* eo2;
+    const double* ev2;
 };
 
+// GRAD: 0 energy (unique pairs, X and Y = G_ji), 1 gradient, 2 cross-spin
+// energy (X = G_iJ of B_alpha and B_beta only, E_ab += X^2 / D).
 template <int GRAD>
 __global__ void __launch_bounds__(256, 2) pair_f64_kernel(PairArgs p) {
+    constexpr bool CROSS = GRAD == 2;
     extern __shared__ __align__(16) double sm[];
     __shared__ double red[32];
     __shared__ double vsum[2][PR_T];
@@ -69,9 +78,11 @@ __global__ void __launch_bounds__(256, 2) pair_f64_kernel(PairArgs p) {
     const int A0 = ta * PR_T, B0 = tb * PR_T;
     const int nvir = p.nvir, naux = p.naux;
     const int64_t ldb = p.ldb;
+    const int nvb = CROSS ? p.nvir2 : nvir;  // virtuals of the column side
+    const int64_t ldb2 = CROSS ? p.ldb2 : ldb;
     const double* gAi = p.B + (int64_t)i * nvir + A0;
     const double* gAj = p.B + (int64_t)j * nvir + A0;
-    const double* gBj = p.B + (int64_t)j * nvir + B0;
+    const double* gBj = (CROSS ? p.B2 : p.B) + (int64_t)j * nvb + B0;
     const double* gBi = p.B + (int64_t)i * nvir + B0;
     const int nk = (naux + PR_BK - 1) / PR_BK;
 
@@ -82,13 +93,15 @@ __global__ void __launch_bounds__(256, 2) pair_f64_kernel(PairArgs p) {
             const int idx = tid + 256 * e, r = idx >> 6, c = idx & 63;
             const int q = kt * PR_BK + r;
             const bool okA = q < naux && A0 + c < nvir;
-            const bool okB = q < naux && B0 + c < nvir;
+            const bool okB = q < naux && B0 + c < nvb;
             const int64_t off = (int64_t)q * ldb + c;
             const int so = r * PR_LD + c;
             cp_async8(s + 0 * PR_BK * PR_LD + so, okA ? gAi + off : p.B, okA);
-            cp_async8(s + 1 * PR_BK * PR_LD + so, okA ? gAj + off : p.B, okA);
-            cp_async8(s + 2 * PR_BK * PR_LD + so, okB ? gBj + off : p.B, okB);
-            cp_async8(s + 3 * PR_BK * PR_LD + so, okB ? gBi + off : p.B, okB);
+            cp_async8(s + 2 * PR_BK * PR_LD + so, okB ? gBj + (int64_t)q * ldb2 + c : p.B, okB);
+            if (!CROSS) {
+                cp_async8(s + 1 * PR_BK * PR_LD + so, okA ? gAj + off : p.B, okA);
+                cp_async8(s + 3 * PR_BK * PR_LD + so, okB ? gBi + off : p.B, okB);
+            }
         }
     };
 
@@ -133,13 +146,13 @@ __global__ void __launch_bounds__(256, 2) pair_f64_kernel(PairArgs p) {
 #pragma unroll
                 for (int nt = 0; nt < 4; ++nt) {
                     dmma_8x8x4(X[mt][nt], ax[mt], bx[nt]);
-                    dmma_8x8x4(Y[mt][nt], ay[mt], by[nt]);
+                    if (!CROSS) dmma_8x8x4(Y[mt][nt], ay[mt], by[nt]);
                 }
         }
     }
     cp_async_wait<0>();
 
-    const double eij = p.eo[i] + p.eo[j];
+    const double eij = p.eo[i] + (CROSS ? p.eo2[j] : p.eo[j]);
     KSum os, ss, oc, oc2;
     double rowsum[2] = {0.0, 0.0};
 #pragma unroll
@@ -151,11 +164,13 @@ __global__ void __launch_bounds__(256, 2) pair_f64_kernel(PairArgs p) {
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int b = B0 + wc * 32 + nt * 8 + 2 * t + h;
-                if (a < nvir && b < nvir) {
-                    const double D = eij - ea - p.ev[b];
+                if (a < nvir && b < nvb) {
+                    const double D = eij - ea - (CROSS ? p.ev2[b] : p.ev[b]);
                     const double x = X[mt][nt][h], y = Y[mt][nt][h];
                     double f = 1.0 / D;
-                    if (GRAD) {
+                    if (CROSS) {
+                        os.add(x * x * f);
+                    } else if (GRAD) {
                         // pair (i, j): Tt_ij[a, b] into the rows of i; for i < j also
                         // pair (j, i): Tt_ji[a, b] = (2 G_ji - G_ij)[a, b] / D into the
                         // rows of j.  Both orderings put t Tt on the row virtual a.
@@ -188,14 +203,14 @@ __global__ void __launch_bounds__(256, 2) pair_f64_kernel(PairArgs p) {
     }
     // energy mode visits tiles ta <= tb only: the summands are symmetric under
     // a <-> b (X_ba = Y_ab), so an off-diagonal tile counts twice
-    const double w = GRAD ? 1.0 : (i == j ? 0.5 : 1.0) * (ta < tb ? 2.0 : 1.0);
+    const double w = GRAD ? 1.0 : (i == j ? 0.5 : 1.0) * (ta < tb ? 2.0 : 1.0);  // (CROSS: 1)
     const double vos = block_sum(os.value(), red);
     const double vss = block_sum(ss.value(), red);
     if (tid == 0) {
         p.part[item * 2 + 0] = w * vos;
         p.part[item * 2 + 1] = w * vss;
     }
-    if (GRAD) {
+    if (GRAD == 1) {
         const double voc = block_sum(oc.value(), red);
         const double voc2 = block_sum(oc2.value(), red);
         if (tid == 0) {
@@ -291,6 +306,7 @@ static fc_status set_smem_once() {
     if (done) return FC_OK;
     FC_CUDA(cudaFuncSetAttribute(pair_f64_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, PR_SMEM));
     FC_CUDA(cudaFuncSetAttribute(pair_f64_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, PR_SMEM));
+    FC_CUDA(cudaFuncSetAttribute(pair_f64_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, PR_SMEM));
     FC_CUDA(cudaFuncSetAttribute(dgemm_tn_kernel<EpiStore>, cudaFuncAttributeMaxDynamicSharedMemorySize, DG_SMEM));
     done = true;
     return FC_OK;
@@ -507,6 +523,70 @@ fc_status rimp2_grad_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, doubl
         FC_TRY(timing_sum((int)ncp, &stats->main_ms));
         stats->main_flops = 4.0 * naux * (double)nvir * nvir * P;
         stats->main_bytes = 8.0 * naux * (double)nov * (double)nch + 8.0 * (double)nov * nov;
+    }
+    return FC_OK;
+}
+
+// Opposite-spin (alpha-beta) energy of unrestricted RI-MP2 in FP64: every
+// (i alpha, J beta) pair, every (a-tile, b-tile), X = G_iJ only
+// (opposite_spin_block_energy, ferric-mp2/src/u_rimp2.rs:731-753).
+fc_status ump2_cross_f64(const UmpSpin& A, const UmpSpin& Bs, int64_t naux, cudaStream_t st, double* e_ab,
+                         fc_stats* stats) {
+    FC_TRY(set_smem_once());
+    const int nta = (int)((A.nvir + PR_T - 1) / PR_T), ntb = (int)((Bs.nvir + PR_T - 1) / PR_T);
+    const int64_t npairs = A.nocc * Bs.nocc;
+    const int ntiles = nta * ntb;
+    const int64_t items = npairs * ntiles;
+    if (items > INT32_MAX) return fail(FC_ERR_LAYOUT, "U-RI-MP2: too many pair tiles for one launch");
+    void *vpairs, *vpart, *vout;
+    FC_TRY(ws_get(WS_PAIRS, (npairs + ntiles) * sizeof(int2), &vpairs));
+    FC_TRY(ws_get(WS_PART, items * 2 * sizeof(double), &vpart));
+    FC_TRY(ws_get(WS_OUT, 64 * sizeof(double), &vout));
+    std::vector<int2> hp;
+    for (int i = 0; i < A.nocc; ++i)
+        for (int j = 0; j < Bs.nocc; ++j) hp.push_back(make_int2(i, j));
+    for (int ta = 0; ta < nta; ++ta)
+        for (int tb = 0; tb < ntb; ++tb) hp.push_back(make_int2(ta, tb));
+    FC_CUDA(cudaMemcpyAsync(vpairs, hp.data(), hp.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
+    PairArgs a{};
+    a.B = A.b_ov;
+    a.ldb = A.nocc * A.nvir;
+    a.naux = (int)naux;
+    a.nvir = (int)A.nvir;
+    a.eo = A.eps_occ;
+    a.ev = A.eps_vir;
+    a.pairs = (const int2*)vpairs;
+    a.tiles = (const int2*)vpairs + npairs;
+    a.ntiles = ntiles;
+    a.part = (double*)vpart;
+    a.B2 = Bs.b_ov;
+    a.ldb2 = Bs.nocc * Bs.nvir;
+    a.nvir2 = (int)Bs.nvir;
+    a.eo2 = Bs.eps_occ;
+    a.ev2 = Bs.eps_vir;
+    Context& c = ctx();
+    cudaEvent_t* ev = nullptr;
+    if (stats) {
+        FC_TRY(timing_events(1, &ev));
+        FC_CUDA(cudaEventRecord(ev[0], st));
+    }
+    pair_f64_kernel<2><<<(unsigned)items, 256, PR_SMEM, st>>>(a);
+    FC_TRY(check_launch("pair_f64_kernel<cross>"));
+    if (stats) FC_CUDA(cudaEventRecord(ev[1], st));
+    reduce_pairs_kernel<<<1, 1024, 0, st>>>((const double*)vpart, items, (double*)vout);
+    FC_TRY(check_launch("reduce_pairs_kernel"));
+    double h[2];
+    FC_CUDA(cudaMemcpyAsync(h, vout, sizeof(h), cudaMemcpyDeviceToHost, st));
+    FC_CUDA(cudaStreamSynchronize(st));
+    *e_ab = h[0];
+    if (stats) {
+        double ms = 0.0;
+        FC_TRY(timing_sum(1, &ms));
+        stats->main_ms += ms;
+        stats->main_launches += 1;
+        stats->main_flops += 2.0 * (double)naux * (double)(A.nocc * A.nvir) * (double)(Bs.nocc * Bs.nvir);
+        stats->launches += 2;
+        (void)c;
     }
     return FC_OK;
 }

@@ -38,6 +38,7 @@
 #include "rimp2.cuh"
 #include "tc.cuh"
 #include "tmap.cuh"
+#include "xgemm.cuh"
 
 namespace fc {
 
@@ -1528,6 +1529,145 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
         stats->main_bytes = 6.0 * naux * (double)nov * (double)nch;
         stats->h2d_bytes += pairs.size() * sizeof(int2);
         stats->d2h_bytes += h.size() * 8 + sizeof(hf);
+    }
+    return FC_OK;
+}
+
+// ------------------------------------------------- unrestricted RI-MP2 --
+//
+// Opposite-spin energy E_ab = sum_{i a J B} (ia|JB)^2 / D on the exact-slice
+// tensor-core GEMM: G = B_alpha^T B_beta over rows (i, a) and (J, B) with no
+// padding per occupied orbital (no exchange partner is needed, so tiles need
+// not hold whole (i, J) blocks); the epilogue forms g^2 / D and leaves one
+// partial per warp and tile, summed in fixed order.
+
+namespace {
+
+struct EpiOS {
+    const double* sa;  // [nov_a] row scales (rows (i, a))
+    const double* sb;  // [nov_b] row scales (rows (J, B))
+    const double* eoa;
+    const double* eva;
+    const double* eob;
+    const double* evb;
+    int nva, nvb;
+    int64_t rows_a, rows_b;
+    double* part;  // [tile][16] per epilogue warp
+    __device__ void operator()(int64_t t, int4 it, int row, int col0, const double (&acc)[32]) const {
+        const int64_t p = (int64_t)it.x * 128 + row;
+        double s = 0.0;
+        if (p < rows_a) {
+            const int i = (int)(p / nva), a = (int)(p % nva);
+            const double da = eoa[i] - eva[a];
+            const double sp = sa[p];
+            const int64_t w0 = (int64_t)it.y * 128 + col0;
+            int J = (int)(w0 / nvb), B = (int)(w0 % nvb);
+#pragma unroll
+            for (int c = 0; c < 32; ++c) {
+                const int64_t w = w0 + c;
+                if (w < rows_b) {
+                    const double g = sp * sb[w] * acc[c];
+                    s += g * g / (da + eob[J] - evb[B]);
+                }
+                if (++B == nvb) {
+                    B = 0;
+                    ++J;
+                }
+            }
+        }
+        s = warp_sum(s);
+        if ((threadIdx.x & 31) == 0) part[t * 16 + ((threadIdx.x >> 5) - 2)] = s;
+    }
+};
+
+// B_ov of one spin -> exact slices, rows (i, a) unpadded, K = q_pad.
+fc_status ump2_split(const UmpSpin& x, int64_t naux, int64_t q_pad, cudaStream_t st, int* bad, int slot_split,
+                     int slot_scale, __nv_bfloat16** bt, double** scl) {
+    const int64_t nov = x.nocc * x.nvir;
+    void *vbt, *vsc;
+    FC_TRY(ws_get(slot_split, (size_t)3 * nov * q_pad * 2, &vbt));
+    FC_TRY(ws_get(slot_scale, (size_t)nov * 16 + 256, &vsc));
+    unsigned long long* cmax = (unsigned long long*)vsc;
+    double* s = (double*)vsc + nov;
+    FC_CUDA(cudaMemsetAsync(cmax, 0, nov * 8, st));
+    dim3 g1((unsigned)((nov + 255) / 256), (unsigned)((naux + 63) / 64));
+    colmax_kernel<<<g1, 256, 0, st>>>(x.b_ov, naux, nov, 64, cmax, bad);
+    row_scale_kernel<<<(unsigned)((nov + 255) / 256), 256, 0, st>>>(cmax, x.nocc, x.nvir, x.nvir, s);
+    dim3 g3((unsigned)((nov + 63) / 64), (unsigned)((naux + 63) / 64));
+    if (g3.y > 65535) return fail(FC_ERR_LAYOUT, "U-RI-MP2 split: naux too large");
+    split_fx_transpose_kernel<<<g3, 256, 0, st>>>(x.b_ov, naux, x.nocc, x.nvir, x.nvir, q_pad, s,
+                                                  (__nv_bfloat16*)vbt);
+    *bt = (__nv_bfloat16*)vbt;
+    *scl = s;
+    return check_launch("U-RI-MP2 split kernels");
+}
+
+bool g_os_attr = false;
+
+}  // namespace
+
+fc_status ump2_cross_fx(const UmpSpin& A, const UmpSpin& Bs, int64_t naux, cudaStream_t st, double* e_ab,
+                        fc_stats* stats) {
+    if (!g_os_attr) {
+        FC_CUDA(cudaFuncSetAttribute(xgemm_kernel<128, EpiOS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     xg::Cfg<128>::SMEM));
+        g_os_attr = true;
+    }
+    Context& c = ctx();
+    const int64_t nova = A.nocc * A.nvir, novb = Bs.nocc * Bs.nvir;
+    const int64_t q_pad = (naux + fx::KT - 1) / fx::KT * fx::KT;
+    if (3 * nova > (int64_t)UINT32_MAX || 3 * novb > (int64_t)UINT32_MAX || nova > INT32_MAX)
+        return fail(FC_ERR_LAYOUT, "U-RI-MP2: too many operand rows");
+    void* vout;
+    FC_TRY(ws_get(WS_OUT, 256, &vout));
+    int* flags = (int*)vout;
+    double* res = (double*)vout + 4;
+    FC_CUDA(cudaMemsetAsync(vout, 0, 256, st));
+    __nv_bfloat16 *bta, *btb;
+    double *sa, *sb;
+    FC_TRY(ump2_split(A, naux, q_pad, st, flags, WS_SPLIT, WS_SCALE, &bta, &sa));
+    FC_TRY(ump2_split(Bs, naux, q_pad, st, flags, WS_SPLIT2, WS_MISC, &btb, &sb));
+    std::vector<int4> items;
+    const int ntm = (int)((nova + 127) / 128), ntn = (int)((novb + 127) / 128), nks = (int)(q_pad / fx::KT);
+    for (int tn = 0; tn < ntn; ++tn)
+        for (int tm = 0; tm < ntm; ++tm) items.push_back(make_int4(tm, tn, 0, nks));
+    void *vtab, *vpart;
+    FC_TRY(ws_get(WS_PAIRS, items.size() * sizeof(int4), &vtab));
+    FC_TRY(ws_get(WS_PART, items.size() * 16 * 8, &vpart));
+    FC_CUDA(cudaMemcpyAsync(vtab, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+    CUtensorMap ta, tb;
+    FC_TRY(make_tmap_bf16_2d(&ta, bta, q_pad, 3 * nova, q_pad * 2, fx::KT, 128));
+    FC_TRY(make_tmap_bf16_2d(&tb, btb, q_pad, 3 * novb, q_pad * 2, fx::KT, 128));
+    XArgs a{(const int4*)vtab, (int64_t)items.size(), (int)nova, (int)novb, flags + 1};
+    EpiOS epi{sa, sb, A.eps_occ, A.eps_vir, Bs.eps_occ, Bs.eps_vir, (int)A.nvir, (int)Bs.nvir, nova, novb,
+              (double*)vpart};
+    cudaEvent_t* ev = nullptr;
+    if (stats) {
+        FC_TRY(timing_events(1, &ev));
+        FC_CUDA(cudaEventRecord(ev[0], st));
+    }
+    const int grid = (int)std::min<int64_t>((int64_t)items.size(), c.sm_count);
+    xgemm_kernel<128, EpiOS><<<grid, xg::Cfg<128>::THREADS, xg::Cfg<128>::SMEM, st>>>(ta, tb, a, epi);
+    FC_TRY(check_launch("opposite-spin exact-slice GEMM"));
+    if (stats) FC_CUDA(cudaEventRecord(ev[1], st));
+    // the partials as (even, odd) pairs: out = (sum of even, sum of odd)
+    fx_reduce_pairs_kernel<<<1, 1024, 0, st>>>((const double*)vpart, (int64_t)items.size() * 8, res);
+    FC_TRY(check_launch("fx_reduce_pairs_kernel"));
+    double h[2];
+    int hf[2];
+    FC_CUDA(cudaMemcpyAsync(h, res, sizeof(h), cudaMemcpyDeviceToHost, st));
+    FC_CUDA(cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, st));
+    FC_CUDA(cudaStreamSynchronize(st));
+    if (hf[0]) return fail(FC_ERR_RANGE, "split-BF16: B_ov has a non-finite element");
+    if (hf[1]) return fail(FC_ERR_TIMEOUT, "opposite-spin GEMM: a pipeline wait ran out");
+    *e_ab = h[0] + h[1];
+    if (stats) {
+        double ms = 0.0;
+        FC_TRY(timing_sum(1, &ms));
+        stats->main_ms += ms;
+        stats->main_launches += 1;
+        stats->main_flops += 2.0 * (double)naux * (double)nova * (double)novb;
+        stats->launches += 8;
     }
     return FC_OK;
 }

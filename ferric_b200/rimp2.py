@@ -180,3 +180,31 @@ def ri_densities(b_ov, eps_occ, eps_vir, precision="f64"):
     ``x_ov = Gamma / 4``; the P diagonals enter as ``dE/deps / 2``."""
     sc, gamma, d_o, d_v = rimp2_energy_grad(b_ov, eps_occ, eps_vir, precision)
     return gamma / 4.0, d_o, d_v, sc.e_total
+
+
+def ump2_energy(b_a, eps_occ_a, eps_vir_a, b_b, eps_occ_b, eps_vir_b, precision="f64", stats=None):
+    """Unrestricted RI-MP2 energy components ``(e_aa, e_bb, e_ab)``
+    (same_spin_block_energy / opposite_spin_block_energy,
+    ferric-mp2/src/u_rimp2.rs:693-753); SCS/SOS weighting is the caller's."""
+    _lib.ensure_init()
+    noa, nva, nob, nvb = (int(x.shape[0]) for x in (eps_occ_a, eps_vir_a, eps_occ_b, eps_vir_b))
+    naux = int(b_a.shape[0])
+    if b_b.shape[0] != naux:
+        raise ValueError("b_a and b_b must share naux")
+    e1, e2, e3 = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    st = FcStats()
+    prec = _precision(precision)
+    if _is_torch_cuda(b_a):
+        ts = [t.contiguous() for t in (b_a, eps_occ_a, eps_vir_a, b_b, eps_occ_b, eps_vir_b)]
+        check(_lib.lib.fc_ump2_energy_dev(ptr(ts[0]), noa, nva, ptr(ts[1]), ptr(ts[2]), ptr(ts[3]), nob, nvb,
+                                          ptr(ts[4]), ptr(ts[5]), naux, prec, ctypes.byref(e1), ctypes.byref(e2),
+                                          ctypes.byref(e3), _stream_of(ts[0]), ctypes.byref(st)))
+    else:
+        ts = [np.ascontiguousarray(x, dtype=np.float64)
+              for x in (b_a, eps_occ_a, eps_vir_a, b_b, eps_occ_b, eps_vir_b)]
+        check(_lib.lib.fc_ump2_energy(ptr(ts[0]), noa, nva, ptr(ts[1]), ptr(ts[2]), ptr(ts[3]), nob, nvb,
+                                      ptr(ts[4]), ptr(ts[5]), naux, prec, ctypes.byref(e1), ctypes.byref(e2),
+                                      ctypes.byref(e3), ctypes.byref(st)))
+    if stats is not None:
+        stats.update(st.as_dict())
+    return e1.value, e2.value, e3.value

@@ -124,6 +124,23 @@ fc_status fc_rimp2_energy_grad_dev(const double* b_ov, int64_t naux, int64_t noc
                                    double* de_docc, double* de_dvir, void* stream,
                                    fc_stats* stats);
 
+/* Unrestricted RI-MP2 energy components (alpha-alpha, beta-beta,
+ * alpha-beta), the device part of u_ri_mp2: same_spin_block_energy and
+ * opposite_spin_block_energy (ferric-mp2/src/u_rimp2.rs:693-753), with the
+ * reference's device path try_u_{same,opposite}_spin_on_device
+ * (ferric-mp2/src/rimp2_gpu.rs:884-1038).  b_a (naux, nocc_a*nvir_a) and
+ * b_b (naux, nocc_b*nvir_b) share naux; SCS/SOS weights are applied by the
+ * caller (e_corr = c_os e_ab + c_ss (e_aa + e_bb)).  FC_PREC_F64 or
+ * FC_PREC_MIXED (exact slices). */
+fc_status fc_ump2_energy(const double* b_a, int64_t nocc_a, int64_t nvir_a, const double* eps_occ_a,
+                         const double* eps_vir_a, const double* b_b, int64_t nocc_b, int64_t nvir_b,
+                         const double* eps_occ_b, const double* eps_vir_b, int64_t naux, int32_t precision,
+                         double* e_aa, double* e_bb, double* e_ab, fc_stats* stats);
+fc_status fc_ump2_energy_dev(const double* b_a, int64_t nocc_a, int64_t nvir_a, const double* eps_occ_a,
+                             const double* eps_vir_a, const double* b_b, int64_t nocc_b, int64_t nvir_b,
+                             const double* eps_occ_b, const double* eps_vir_b, int64_t naux, int32_t precision,
+                             double* e_aa, double* e_bb, double* e_ab, void* stream, fc_stats* stats);
+
 /* FP64 RI-MP2 energy that allocates no device memory.  No counterpart in the
  * reference: it is for callers that cannot call cudaMalloc -- callers whose
  * device memory belongs to another allocator (ferric's device-pool ledger

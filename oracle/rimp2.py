@@ -210,3 +210,33 @@ def stream_dressed_mo(t3, m, c_left, c_right, chunk=256):
         mo = np.einsum("qln,nr->qlr", half, c_right, optimize=True).reshape(q1 - q0, nl * nr)
         b += m[:, q0:q1] @ mo
     return b
+
+
+def u_same_spin(b_ov, eps_occ, eps_vir):
+    """Same-spin (alpha-alpha or beta-beta) RI-MP2 energy of one spin channel:
+    0.25 * sum_i sum_{j>=i} fac_ij sum_ab (g_ab - g_ba)^2 / D, fac 1 on i == j
+    and 2 off (same_spin_block_energy, ferric-mp2/src/u_rimp2.rs:693-724)."""
+    nocc, nvir = len(eps_occ), len(eps_vir)
+    e = 0.0
+    for i in range(nocc):
+        bi = b_ov[:, i * nvir:(i + 1) * nvir]
+        for j in range(i, nocc):
+            g = bi.T @ b_ov[:, j * nvir:(j + 1) * nvir]          # (ia|jb)
+            k = g - g.T
+            d = eps_occ[i] + eps_occ[j] - eps_vir[:, None] - eps_vir[None, :]
+            e += (1.0 if i == j else 2.0) * np.sum(k * k / d)
+    return 0.25 * e
+
+
+def u_opposite_spin(b_a, eps_occ_a, eps_vir_a, b_b, eps_occ_b, eps_vir_b):
+    """Opposite-spin (alpha-beta) RI-MP2 energy: sum_{i a J B} (ia|JB)^2 / D
+    (opposite_spin_block_energy, ferric-mp2/src/u_rimp2.rs:731-753)."""
+    noa, nva = len(eps_occ_a), len(eps_vir_a)
+    nob, nvb = len(eps_occ_b), len(eps_vir_b)
+    e = 0.0
+    for i in range(noa):
+        g = b_a[:, i * nva:(i + 1) * nva].T @ b_b                      # (nva, nob*nvb)
+        d = (eps_occ_a[i] + np.repeat(eps_occ_b, nvb)[None, :]
+             - eps_vir_a[:, None] - np.tile(eps_vir_b, nob)[None, :])
+        e += np.sum(g * g / d)
+    return e

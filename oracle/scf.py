@@ -93,3 +93,54 @@ def dressed(aux, shells):
 def b_ov(b, C, nocc):
     co, cv = C[:, :nocc], C[:, nocc:]
     return np.einsum("qmn,mi,na->qia", b, co, cv, optimize=True).reshape(b.shape[0], -1)
+
+
+def uhf(S, H, na, nb, e_nuc, eri, tol=1e-11, max_iter=300, guess=None):
+    """Unrestricted HF with exact J/K and DIIS on both spins' commutators
+    (F_s = H + J(D_a + D_b) - K(D_s)); returns (E, (eps_a, eps_b), (C_a, C_b)).
+    The reference's UMP2 goldens were made with PySCF scf.UHF at conv_tol
+    1e-11 (testdata/reference/validation/u_rimp2/*.json provenance)."""
+    s, u = np.linalg.eigh(S)
+    X = u / np.sqrt(s)
+    if guess is None:
+        e, c = np.linalg.eigh(X.T @ H @ X)
+        Ca = Cb = X @ c
+    else:
+        Ca, Cb = guess
+    jk = exact_jk(eri)
+    focks, errs = [], []
+    e_old = 0.0
+    for it in range(max_iter):
+        Da = Ca[:, :na] @ Ca[:, :na].T
+        Db = Cb[:, :nb] @ Cb[:, :nb].T
+        Ja, Ka = jk(Da)
+        Jb, Kb = jk(Db)
+        Fa = H + Ja + Jb - Ka
+        Fb = H + Ja + Jb - Kb
+        E = 0.5 * (np.sum(Da * (H + Fa)) + np.sum(Db * (H + Fb))) + e_nuc
+        ea = X.T @ (Fa @ Da @ S - S @ Da @ Fa) @ X
+        eb = X.T @ (Fb @ Db @ S - S @ Db @ Fb) @ X
+        focks.append((Fa, Fb))
+        errs.append(np.concatenate([ea.ravel(), eb.ravel()]))
+        if len(focks) > 10:
+            focks.pop(0)
+            errs.pop(0)
+        if np.abs(errs[-1]).max() < tol * 100 and abs(E - e_old) < tol:
+            break
+        e_old = E
+        m = len(focks)
+        Bm = -np.ones((m + 1, m + 1))
+        Bm[m, m] = 0.0
+        for a in range(m):
+            for b in range(m):
+                Bm[a, b] = errs[a] @ errs[b]
+        rhs = np.zeros(m + 1)
+        rhs[m] = -1.0
+        coef = np.linalg.lstsq(Bm, rhs, rcond=None)[0][:m]
+        Fda = sum(cf * f[0] for cf, f in zip(coef, focks))
+        Fdb = sum(cf * f[1] for cf, f in zip(coef, focks))
+        Ca = X @ np.linalg.eigh(X.T @ Fda @ X)[1]
+        Cb = X @ np.linalg.eigh(X.T @ Fdb @ X)[1]
+    epa, ca = np.linalg.eigh(X.T @ Fa @ X)
+    epb, cb = np.linalg.eigh(X.T @ Fb @ X)
+    return E, (epa, epb), (X @ ca, X @ cb)

@@ -75,6 +75,50 @@ def build(name):
     np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
 
 
+# open-shell systems: UHF (exact J/K) then unrestricted RI-MP2 (alpha-alpha,
+# beta-beta, alpha-beta) against the reference's u_rimp2 goldens
+U_SYSTEMS = {
+    "oh_ump2": "u_rimp2/oh_cc-pvdz.json",
+    "nh2_ump2": "u_rimp2/nh2_cc-pvdz.json",
+}
+
+
+def build_u(name):
+    g = json.load(open(os.path.join(REF, U_SYSTEMS[name])))
+    atoms = [(s, (x, y, z)) for s, x, y, z in g["provenance"]["geometry_bohr"]]
+    zs = [basis.SYMBOLS[s] for s, _ in atoms]
+    rs = [c for _, c in atoms]
+    t0 = time.time()
+    sh = basis.shells_for(atoms, g["basis"])
+    S, T = integrals.overlap_kinetic(sh)
+    V = integrals.nuclear(sh, zs, rs)
+    eri = integrals.eri4(sh)
+    enuc = scf.nuclear_repulsion(zs, rs)
+    na, nb = int(g["uhf"]["nelec_alpha"]), int(g["uhf"]["nelec_beta"])
+    # several starting orbitals (core Hamiltonian; RHF of the n-electron
+    # cation- and anion-like closed shells), keep the lowest UHF solution, as
+    # the goldens' generator scans guesses ("3 guesses + stability loop")
+    tries = [scf.uhf(S, T + V, na, nb, enuc, eri)]
+    for nc in sorted({nb, na}):
+        _, _, c0 = scf.rhf(S, T + V, nc, enuc, scf.exact_jk(eri), tol=1e-9)
+        tries.append(scf.uhf(S, T + V, na, nb, enuc, eri, guess=(c0, c0)))
+    e_uhf, (epa, epb), (ca, cb) = min(tries, key=lambda r: r[0])
+    b, _, _ = scf.dressed(basis.shells_for(atoms, g["aux_basis"]), sh)
+    ba, bb = scf.b_ov(b, ca, na), scf.b_ov(b, cb, nb)
+    e_aa = orc.u_same_spin(ba, epa[:na], epa[na:])
+    e_bb = orc.u_same_spin(bb, epb[:nb], epb[nb:])
+    e_ab = orc.u_opposite_spin(ba, epa[:na], epa[na:], bb, epb[:nb], epb[nb:])
+    u = g["ump2"]
+    out = dict(b_a=ba, b_b=bb, eps_a=epa, eps_b=epb, na=na, nb=nb,
+               golden_e_uhf=g["uhf"]["energy"], golden_e_aa=u["e_aa"], golden_e_bb=u["e_bb"],
+               golden_e_ab=u["e_ab"], oracle_e_uhf=e_uhf, oracle_e_aa=e_aa, oracle_e_bb=e_bb,
+               oracle_e_ab=e_ab)
+    print(f"{name}: E_uhf {e_uhf:.12f} (golden {g['uhf']['energy']:.12f}) e_aa {e_aa:.14f} "
+          f"({u['e_aa']:.14f}) e_bb {e_bb:.14f} ({u['e_bb']:.14f}) e_ab {e_ab:.14f} ({u['e_ab']:.14f}) "
+          f"{time.time() - t0:.1f} s", flush=True)
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+
+
 if __name__ == "__main__":
-    for n in (sys.argv[1:] or SYSTEMS):
-        build(n)
+    for n in (sys.argv[1:] or list(SYSTEMS) + list(U_SYSTEMS)):
+        (build_u if n in U_SYSTEMS else build)(n)

@@ -143,3 +143,24 @@ def test_density_weights_nonsymmetric():
     w = dfjk.packed_density_weights(d)
     b = rng.standard_normal((7, 7)); b = b + b.T
     assert abs(np.sum(b * d) - np.dot(dfjk.pack_lower(b[None])[0], w)) < 1e-13
+
+
+def test_ump2_oracle_closed_shell_identities():
+    """u_rimp2.rs's same/opposite-spin sums at alpha = beta reproduce the
+    closed-shell E_SS / 2 and E_OS (rimp2.rs:1399-1544)."""
+    from oracle import rimp2 as orc
+    from oracle import synthetic
+    b, eo, ev = synthetic.rimp2_inputs(60, 4, 11)
+    e_os, e_ss, _ = orc.spin_components(b, np.concatenate([eo, ev]), 4, 11)
+    assert abs(2 * orc.u_same_spin(b, eo, ev) - e_ss) < 1e-14 * abs(e_ss) + 1e-18
+    assert abs(orc.u_opposite_spin(b, eo, ev, b, eo, ev) - e_os) < 1e-13 * abs(e_os)
+
+
+def test_ump2_fixtures_pinned_to_golden():
+    import os
+    here = os.path.dirname(os.path.abspath(__file__))
+    for name in ("oh_ump2", "nh2_ump2"):
+        d = np.load(os.path.join(here, "golden", name + ".npz"))
+        assert abs(float(d["oracle_e_uhf"]) - float(d["golden_e_uhf"])) < 1e-9
+        for k in ("e_aa", "e_bb", "e_ab"):
+            assert abs(float(d["oracle_" + k]) - float(d["golden_" + k])) < 1e-9
