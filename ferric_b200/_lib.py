@@ -51,6 +51,8 @@ SIGNATURES = {
     "fc_ump2_energy": (_I32, [_P, _I64, _I64, _P, _P, _P, _I64, _I64, _P, _P, _I64, _I32, _DP, _DP, _DP, _P]),
     "fc_ump2_energy_dev": (_I32, [_P, _I64, _I64, _P, _P, _P, _I64, _I64, _P, _P, _I64, _I32, _DP, _DP, _DP, _P,
                                   _P]),
+    "fc_rimp2_imat": (_I32, [_P, _P, _I64, _I64, _I64, _I64, _I64, _I32, _P, _P]),
+    "fc_rimp2_imat_dev": (_I32, [_P, _P, _I64, _I64, _I64, _I64, _I64, _I32, _P, _P, _P]),
     "fc_mo_dress": (_I32, [_P, _I64, _I64, _P, _P, _I64, _P, _I64, _I32, _P, _P]),
     "fc_mo_dress_dev": (_I32, [_P, _I64, _I64, _P, _P, _I64, _P, _I64, _I32, _P, _P, _P]),
     "fc_rimp2_batched_create": (_I32, [_P, _I64, _I32, _c.POINTER(_P)]),

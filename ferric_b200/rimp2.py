@@ -208,3 +208,28 @@ def ump2_energy(b_a, eps_occ_a, eps_vir_a, b_b, eps_occ_b, eps_vir_b, precision=
     if stats is not None:
         stats.update(st.as_dict())
     return e1.value, e2.value, e3.value
+
+
+def rimp2_imat(x_ov, b_full, nocc, nvir, first_occ=0, precision="f64", stats=None):
+    """RI Lagrangian Imat (nmo x nmo) from x_ov = Gamma / 4 and the dressed MO
+    3-index tensor b_full (naux, nmo, nmo) (build_imat_ri,
+    ferric-mp2/src/zvector.rs:735-832)."""
+    _lib.ensure_init()
+    naux, nmo = int(b_full.shape[0]), int(b_full.shape[1])
+    st = FcStats()
+    prec = _precision(precision)
+    if _is_torch_cuda(b_full):
+        import torch
+        x, b = x_ov.contiguous(), b_full.contiguous()
+        out = torch.empty((nmo, nmo), dtype=torch.float64, device=b.device)
+        check(_lib.lib.fc_rimp2_imat_dev(ptr(x), ptr(b), naux, nmo, nocc, nvir, first_occ, prec, ptr(out),
+                                         _stream_of(b), ctypes.byref(st)))
+    else:
+        x = np.ascontiguousarray(x_ov, dtype=np.float64)
+        b = np.ascontiguousarray(b_full, dtype=np.float64)
+        out = np.empty((nmo, nmo))
+        check(_lib.lib.fc_rimp2_imat(ptr(x), ptr(b), naux, nmo, nocc, nvir, first_occ, prec, ptr(out),
+                                     ctypes.byref(st)))
+    if stats is not None:
+        stats.update(st.as_dict())
+    return out

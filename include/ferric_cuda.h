@@ -141,6 +141,20 @@ fc_status fc_ump2_energy_dev(const double* b_a, int64_t nocc_a, int64_t nvir_a, 
                              const double* eps_occ_b, const double* eps_vir_b, int64_t naux, int32_t precision,
                              double* e_aa, double* e_bb, double* e_ab, void* stream, fc_stats* stats);
 
+/* RI Lagrangian Imat (nmo x nmo, row-major), the first consumer of the
+ * RI-MP2 adjoint in the analytic gradient (build_imat_ri / imat_fill_rows,
+ * ferric-mp2/src/zvector.rs:735-832):
+ *   Imat[q, fo + i] = -2 sum_{P,a} x_ov[P, i*nvir + a] b_full[P, q, fo + nocc + a]
+ *   Imat[q, fo + nocc + a] = -2 sum_{P,i} x_ov[P, i*nvir + a] b_full[P, q, fo + i]
+ * with x_ov = Gamma / 4 (naux, nocc*nvir) and b_full the dressed MO 3-index
+ * tensor (naux, nmo, nmo); fo = first_occ, frozen-core columns zero.
+ * FC_PREC_F64 or FC_PREC_MIXED (exact slices, k-panel FP64 flush). */
+fc_status fc_rimp2_imat(const double* x_ov, const double* b_full, int64_t naux, int64_t nmo, int64_t nocc,
+                        int64_t nvir, int64_t first_occ, int32_t precision, double* imat, fc_stats* stats);
+fc_status fc_rimp2_imat_dev(const double* x_ov, const double* b_full, int64_t naux, int64_t nmo, int64_t nocc,
+                            int64_t nvir, int64_t first_occ, int32_t precision, double* imat, void* stream,
+                            fc_stats* stats);
+
 /* FP64 RI-MP2 energy that allocates no device memory.  No counterpart in the
  * reference: it is for callers that cannot call cudaMalloc -- callers whose
  * device memory belongs to another allocator (ferric's device-pool ledger

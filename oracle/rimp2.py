@@ -240,3 +240,38 @@ def u_opposite_spin(b_a, eps_occ_a, eps_vir_a, b_b, eps_occ_b, eps_vir_b):
              - eps_vir_a[:, None] - np.tile(eps_vir_b, nob)[None, :])
         e += np.sum(g * g / d)
     return e
+
+
+def imat_ri(x_ov, b_full, nocc, nvir, first_occ=0):
+    """RI Lagrangian Imat (build_imat_ri / imat_fill_rows,
+    ferric-mp2/src/zvector.rs:735-832): for every MO row q,
+    Imat[q, first_occ + i] = -2 sum_{P,a} x_ov[P, i*nvir + a] b_full[P, q, nocc_total + a],
+    Imat[q, nocc_total + a] = -2 sum_{P,i} x_ov[P, i*nvir + a] b_full[P, q, first_occ + i];
+    frozen-core columns stay zero."""
+    naux, nmo = b_full.shape[0], b_full.shape[1]
+    nt = first_occ + nocc
+    x = x_ov.reshape(naux, nocc, nvir)
+    imat = np.zeros((nmo, nmo))
+    imat[:, first_occ:nt] = -2.0 * np.einsum("pqa,pia->qi", b_full[:, :, nt:nt + nvir], x, optimize=True)
+    imat[:, nt:nt + nvir] = -2.0 * np.einsum("pqi,pia->qa", b_full[:, :, first_occ:nt], x, optimize=True)
+    return imat
+
+
+def imat_scalar(x_ov, b_full, nocc, nvir, first_occ=0):
+    """The scalar definition of Imat and the sum of |terms| per element (the
+    reference's known-answer test, zvector.rs:1245-1290)."""
+    naux, nmo = b_full.shape[0], b_full.shape[1]
+    nt = first_occ + nocc
+    want = np.zeros((nmo, nmo))
+    absum = np.zeros((nmo, nmo))
+    for q in range(nmo):
+        for i in range(nocc):
+            for p in range(naux):
+                for a in range(nvir):
+                    t = x_ov[p, i * nvir + a] * b_full[p, q, nt + a]
+                    want[q, first_occ + i] -= 2.0 * t
+                    absum[q, first_occ + i] += 2.0 * abs(t)
+                    t2 = x_ov[p, i * nvir + a] * b_full[p, q, first_occ + i]
+                    want[q, nt + a] -= 2.0 * t2
+                    absum[q, nt + a] += 2.0 * abs(t2)
+    return want, absum

@@ -164,3 +164,21 @@ def test_ump2_fixtures_pinned_to_golden():
         assert abs(float(d["oracle_e_uhf"]) - float(d["golden_e_uhf"])) < 1e-9
         for k in ("e_aa", "e_bb", "e_ab"):
             assert abs(float(d["oracle_" + k]) - float(d["golden_" + k])) < 1e-9
+
+
+def test_imat_gemm_matches_scalar_definition():
+    """zvector.rs:1245-1290 restated: the GEMM form of Imat equals its scalar
+    definition within (n_max + 2) eps of the absolute sums, frozen-core
+    columns zero."""
+    from oracle import rimp2 as orc
+    naux, nocc, nvir, fo = 9, 4, 7, 2
+    nmo = fo + nocc + nvir
+    rng = np.random.default_rng(0x9E37)
+    x = rng.uniform(-1, 1, (naux, nocc * nvir))
+    bf = rng.uniform(-1, 1, (naux, nmo, nmo))
+    got = orc.imat_ri(x, bf, nocc, nvir, fo)
+    want, absum = orc.imat_scalar(x, bf, nocc, nvir, fo)
+    bar = (naux * max(nocc, nvir) + 2.0) * np.finfo(float).eps
+    assert np.all(np.abs(got - want) <= bar * absum)
+    assert np.all(got[:, :fo] == 0.0)
+    assert np.any(got != 0.0)
