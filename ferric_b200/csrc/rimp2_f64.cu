@@ -14,10 +14,15 @@
 // which is the reference's pair loop over the (i, j) and (j, i) orderings
 // (ferric-mp2/src/rimp2.rs:1399-1441, 1506-1544).
 //
-// Gradient mode (ordered pairs, i in the current chunk): the item writes
-// Tt_ij[a, b] = (2X - Y)/D into the chunk's amplitude rows and the partials
-// of c = t Tt for dE/d eps (ferric-mp2/src/oo_rimp2.rs:1170-1191); the second
-// contraction Gamma_i = 4 B Tt_i^T runs in dgemm_tn.
+// Gradient mode (unordered pairs of an occupied chunk pair (I, J)): the item
+// writes Tt_ij[a, b] = (2X - Y)/D into the amplitude rows of i and, for
+// i < j, Tt_ji[a, b] = (2Y - X)/D into the rows of j, plus the partials of
+// c = t Tt of both orderings for dE/d eps (ferric-mp2/src/oo_rimp2.rs:1170-1191);
+// the second contraction Gamma[:, I] += 4 B[:, J] Tt_IJ^T (and the same for J)
+// runs in dgemm_tn.
+//
+// Cross-spin mode (unrestricted alpha-beta energy): X = G_iJ of two tensors,
+// E_ab += X^2 / D (ferric-mp2/src/u_rimp2.rs:731-753).
 #include <algorithm>
 
 #include "fc_internal.cuh"

@@ -26,9 +26,12 @@
 // than an SM delivers).  Energy mode: unordered pairs, E_OS += (X^2 + Y^2)/D,
 // E_SS += (X - Y)^2/D (i == j: X phase only, E_SS = 0), the reference pair
 // loop of ferric-mp2/src/rimp2.rs:1399-1544 over both orderings.  Gradient
-// mode: ordered pairs of an occupied chunk; writes Tt_ij = (2X - Y)/D (FP32)
-// and the dE/deps partials; the adjoint contraction Gamma = 4 B Tt^T runs in
-// gemm_fx_kernel with the same exact-level scheme.
+// mode: unordered pairs of an occupied chunk pair (I, J); the item writes
+// Tt_ij = (2X - Y)/D (FP32) into the rows of i and Tt_ji = Tt_ij^T into the
+// rows of j, and the dE/deps partials of both orderings; the adjoint
+// contraction Gamma[:, I] += 4 Bq[:, J] Tt_IJ^T runs in gemm_fx_kernel with
+// the same exact-level scheme.  Diagonal tiles (ta == tb, i != j) may run in
+// one phase, Y = X^T passed through shared memory (the exchange schedule).
 #include <algorithm>
 #include <cstdlib>
 
@@ -769,7 +772,8 @@ constexpr int GF_STAGES = 2;
 constexpr int GF_SMEM = GF_STAGES * GF_STAGE + 1024 + 1024;
 constexpr uint32_t GF_IDESC = tc::idesc_bf16_f32(128, 128);
 
-// out[Q, i*nvir + a] = alpha * s_row s_Q (L0 + L1/256 + L2/65536), rows = (i - i0, a).
+// out[Q, (i0 + il)*nvir + a] (+)= alpha * s_row s_Q (L0 + L1/256 + L2/65536)
+// for amplitude rows m = il*tpad + a (a < nvir).
 template <int BATCH = 0>
 __global__ void __launch_bounds__(192, 1)
     gemm_fx_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
