@@ -33,6 +33,19 @@ fc_status check_shapes(const void* b_ov, int64_t naux, int64_t nocc, int64_t nvi
     return FC_OK;
 }
 
+// The context's copy stream and event for Gamma blocks (created once).
+fc_status copy_stream(cudaStream_t* s, cudaEvent_t* e) {
+    static cudaStream_t cs = nullptr;
+    static cudaEvent_t ce = nullptr;
+    if (!cs) {
+        FC_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        FC_CUDA(cudaEventCreateWithFlags(&ce, cudaEventDisableTiming));
+    }
+    *s = cs;
+    *e = ce;
+    return FC_OK;
+}
+
 int64_t chunk_budget() {
     int64_t b = int64_t(8) << 30;
     if (const char* s = std::getenv("FERRIC_CUDA_CHUNK_BYTES")) {
@@ -56,14 +69,28 @@ fc_status energy_dispatch(const Rimp2Dev& d, int32_t precision, cudaStream_t st,
 
 fc_status grad_dispatch(const Rimp2Dev& d, int32_t precision, cudaStream_t st, double* e_os,
                         double* e_ss, double* gamma, double* de_docc, double* de_dvir,
-                        fc_stats* stats) {
+                        fc_stats* stats, const GammaSink* sink = nullptr) {
     if (precision == FC_PREC_F64)
-        return rimp2_grad_f64(d, st, e_os, e_ss, gamma, de_docc, de_dvir, stats);
-    if (precision == FC_PREC_MIXED) return rimp2_grad_fx(d, st, e_os, e_ss, gamma, de_docc, de_dvir, stats);
+        return rimp2_grad_f64(d, st, e_os, e_ss, gamma, de_docc, de_dvir, stats, sink);
+    if (precision == FC_PREC_MIXED)
+        return rimp2_grad_fx(d, st, e_os, e_ss, gamma, de_docc, de_dvir, stats, sink);
     return fail(FC_ERR_KERNEL, "FC_PREC_MIXED_FAST has no adjoint kernel; use FC_PREC_MIXED");
 }
 
 }  // namespace
+
+namespace fc {
+
+fc_status gamma_sink_block(const GammaSink* sink, const double* gamma, int64_t naux, int64_t nov, int64_t nvir,
+                           int64_t r0, int64_t nr, cudaStream_t st) {
+    FC_CUDA(cudaEventRecord(sink->ready, st));
+    FC_CUDA(cudaStreamWaitEvent(sink->stream, sink->ready, 0));
+    FC_CUDA(cudaMemcpy2DAsync(sink->host + r0 * nvir, nov * 8, gamma + r0 * nvir, nov * 8, nr * nvir * 8, naux,
+                              cudaMemcpyDeviceToHost, sink->stream));
+    return FC_OK;
+}
+
+}  // namespace fc
 
 extern "C" {
 
@@ -166,11 +193,25 @@ fc_status fc_rimp2_energy_grad(const double* b_ov, int64_t naux, int64_t nocc, i
     FC_CUDA(cudaMemcpyAsync((double*)de + nocc, eps_vir, nvir * 8, cudaMemcpyHostToDevice, st));
     Rimp2Dev d{(const double*)db, (const double*)de, (const double*)de + nocc, naux, nocc, nvir,
                0, 0.0, chunk_budget()};
-    FC_TRY(grad_dispatch(d, precision, st, e_os, e_ss, (double*)dg, (double*)dd, (double*)dd + nocc, stats));
-    FC_CUDA(cudaMemcpyAsync(gamma, dg, nel * 8, cudaMemcpyDeviceToHost, st));
+    // A pinned Gamma receives its column blocks while the gradient still runs
+    // (a pageable one is copied at the end: an async copy from pageable memory
+    // would hold the host thread that issues the kernels).
+    cudaPointerAttributes pa{};
+    const bool pinned = cudaPointerGetAttributes(&pa, gamma) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    Context& c = ctx();
+    GammaSink sink{gamma, nullptr, nullptr};
+    if (pinned && precision != FC_PREC_MIXED_FAST) {
+        FC_TRY(copy_stream(&sink.stream, &sink.ready));
+    }
+    FC_TRY(grad_dispatch(d, precision, st, e_os, e_ss, (double*)dg, (double*)dd, (double*)dd + nocc, stats,
+                         sink.stream ? &sink : nullptr));
+    if (!sink.stream) FC_CUDA(cudaMemcpyAsync(gamma, dg, nel * 8, cudaMemcpyDeviceToHost, st));
     FC_CUDA(cudaMemcpyAsync(de_docc, dd, nocc * 8, cudaMemcpyDeviceToHost, st));
     FC_CUDA(cudaMemcpyAsync(de_dvir, (double*)dd + nocc, nvir * 8, cudaMemcpyDeviceToHost, st));
     FC_CUDA(cudaStreamSynchronize(st));
+    if (sink.stream) FC_CUDA(cudaStreamSynchronize(sink.stream));
+    (void)c;
     if (stats) {
         stats->h2d_bytes += nel * 8 + (nocc + nvir) * 8;
         stats->d2h_bytes += nel * 8 + (nocc + nvir) * 8;

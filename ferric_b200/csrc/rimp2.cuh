@@ -14,10 +14,21 @@ struct Rimp2Dev {
     int64_t chunk_bytes;    // amplitude-chunk budget of the gradient
 };
 
+// Where the gradient's Gamma goes as its column blocks become final: a
+// pinned host array (naux x nov, row-major) and a copy stream; the block of
+// occupied chunk I is final once every chunk pair (I, J >= I) has run, and is
+// copied out on `stream` while later chunk pairs compute.
+struct GammaSink {
+    double* host;
+    cudaStream_t stream;
+    cudaEvent_t ready;
+};
+
 fc_status rimp2_energy_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, double* e_ss,
                            fc_stats* stats);
 fc_status rimp2_grad_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, double* e_ss,
-                         double* gamma, double* de_docc, double* de_dvir, fc_stats* stats);
+                         double* gamma, double* de_docc, double* de_dvir, fc_stats* stats,
+                         const GammaSink* sink = nullptr);
 
 // Split-BF16 (tcgen05) kernel sets.  _fx: integer-valued slices with exact
 // FP32 accumulation (FC_PREC_MIXED).  _mixed: floating hi+lo split, 3
@@ -27,7 +38,11 @@ fc_status rimp2_energy_mixed(const Rimp2Dev& d, int terms, cudaStream_t st, doub
 fc_status rimp2_energy_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double* e_ss,
                           fc_stats* stats);
 fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double* e_ss, double* gamma,
-                        double* de_docc, double* de_dvir, fc_stats* stats);
+                        double* de_docc, double* de_dvir, fc_stats* stats, const GammaSink* sink = nullptr);
+// Copy Gamma's columns of occupied rows [r0, r0 + nr) to the sink once `st`
+// has reached this point.
+fc_status gamma_sink_block(const GammaSink* sink, const double* gamma, int64_t naux, int64_t nov, int64_t nvir,
+                           int64_t r0, int64_t nr, cudaStream_t st);
 
 // One spin channel of unrestricted RI-MP2 (device pointers).
 struct UmpSpin {

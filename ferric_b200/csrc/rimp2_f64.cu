@@ -385,7 +385,8 @@ fc_status rimp2_energy_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, dou
 }
 
 fc_status rimp2_grad_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, double* e_ss,
-                         double* gamma, double* de_docc, double* de_dvir, fc_stats* stats) {
+                         double* gamma, double* de_docc, double* de_dvir, fc_stats* stats,
+                         const GammaSink* sink) {
     FC_TRY(set_smem_once());
     const int64_t nocc = d.nocc, nvir = d.nvir, naux = d.naux, nov = nocc * nvir;
     const int ntile = (int)((nvir + PR_T - 1) / PR_T);
@@ -490,6 +491,8 @@ fc_status rimp2_grad_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, doubl
         FC_TRY(check_launch("rimp2 gradient reductions"));
         FC_TRY(adjoint(T1, cp.i0, cp.ni, cp.j0, cp.nj));
         if (!same) FC_TRY(adjoint(T2, cp.j0, cp.nj, cp.i0, cp.ni));
+        // row I of the chunk pairs is done: Gamma's columns of chunk I are final
+        if (sink && cp.j0 + cp.nj == nocc) FC_TRY(gamma_sink_block(sink, gamma, naux, nov, nvir, cp.i0, cp.ni, st));
     }
     scale_copy_f64_kernel<<<(unsigned)((nocc + 255) / 256), 256, 0, st>>>(acc_occ, nocc, -2.0, de_docc);
     FC_TRY(check_launch("scale_copy_f64_kernel"));

@@ -1329,7 +1329,7 @@ fc_status rimp2_energy_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, doub
 }
 
 fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double* e_ss, double* gamma,
-                        double* de_docc, double* de_dvir, fc_stats* stats) {
+                        double* de_docc, double* de_dvir, fc_stats* stats, const GammaSink* sink) {
     FC_TRY(fx_attrs());
     if (d.nocc > (1 << 15)) return fail(FC_ERR_LAYOUT, "split-BF16: nocc too large");
     const int64_t nocc = d.nocc, nvir = d.nvir, naux = d.naux, nov = nocc * nvir;
@@ -1488,6 +1488,8 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
         FC_TRY(check_launch("gradient reductions"));
         FC_TRY(adjoint(T1, cp.i0, cp.ni, cp.j0, cp.nj));
         if (!same) FC_TRY(adjoint(T2, cp.j0, cp.nj, cp.i0, cp.ni));
+        // row I of the chunk pairs is done: Gamma's columns of chunk I are final
+        if (sink && cp.j0 + cp.nj == nocc) FC_TRY(gamma_sink_block(sink, gamma, naux, nov, nvir, cp.i0, cp.ni, st));
     }
     scale_copy_kernel<<<(unsigned)((nocc + 255) / 256), 256, 0, st>>>(acc_occ, nocc, -2.0, de_docc);
     FC_TRY(check_launch("scale_copy_kernel"));

@@ -220,3 +220,26 @@ def test_mixed_zero_sizes(fc):
     from ferric_b200 import rimp2
     e_os, e_ss = rimp2.rimp2_energy(np.zeros((10, 0)), np.zeros(0), np.zeros(5), precision="mixed")
     assert e_os == 0.0 and e_ss == 0.0
+
+
+@pytest.mark.parametrize("precision", ["mixed", "f64"])
+def test_gamma_streamed_to_pinned_host(fc, monkeypatch, precision):
+    """With a pinned host Gamma the host API copies each occupied chunk's
+    columns out while later chunk pairs still run; the result is the same
+    bits as the copy-at-the-end path (pageable Gamma)."""
+    import ctypes
+    import torch
+    import ferric_b200._lib as L
+    from ferric_b200 import rimp2
+    b, eo, ev = synthetic.rimp2_inputs(160, 9, 40)
+    monkeypatch.setenv("FERRIC_CUDA_CHUNK_BYTES", str(9 * (40 * 40 * 14 + 1024 * 40) - 1))
+    ref = rimp2.rimp2_energy_grad(b, eo, ev, precision=precision)
+    g = torch.empty(b.shape, dtype=torch.float64, pin_memory=True)
+    g.fill_(np.nan)
+    do, dv = np.empty(9), np.empty(40)
+    e1, e2 = ctypes.c_double(), ctypes.c_double()
+    L.check(L.lib.fc_rimp2_energy_grad(L.ptr(b), 160, 9, 40, L.ptr(eo), L.ptr(ev), L.PRECISIONS[precision],
+                                       ctypes.byref(e1), ctypes.byref(e2), ctypes.c_void_p(g.data_ptr()),
+                                       L.ptr(do), L.ptr(dv), None))
+    assert np.array_equal(g.numpy(), ref[1])
+    assert np.array_equal(do, ref[2]) and np.array_equal(dv, ref[3])
