@@ -2,7 +2,7 @@
 //
 // DF-J (ferric-scf/src/df_j.rs:1199-1245, 1459-1572) is two GEMV passes over
 // the packed lower triangle of B, HBM-bound:
-//   pass 1  d_P = sum_k Bp[P, k] w_k      (one CTA per aux row, fixed-order sum)
+//   pass 1  d_P = sum_k Bp[P, k] w_k      (CTAs over row segments, fixed-order sums)
 //   solve   c = V^-1 d                     (FP64 Cholesky solves, when a metric is set)
 //   pass 2  J_k = sum_P Bp[P, k] c_P       (column-parallel over k, split over P,
 //                                           fixed-order fold of the splits)
@@ -41,23 +41,40 @@ __global__ void density_weights_kernel(const double* __restrict__ d, int64_t n,
 
 // ---------------------------------------------------------- DF-J passes --
 
+// Pass 1 reads each aux row in segments of DFJ_SEG_BYTES, one CTA per
+// (row, segment): a row per CTA left a near-empty last wave (2400 rows are
+// 2.03 waves of 148 x 8 CTAs) that ran latency-bound.  Segment partials land
+// in part[row * nseg + seg] and dfj_seg_sum_kernel adds them in fixed order.
+constexpr int64_t DFJ_SEG_BYTES = 65536;
+
 template <typename TB>
-__global__ void __launch_bounds__(256) dfj_pass1_kernel(const TB* __restrict__ bp, int64_t pair,
+__global__ void __launch_bounds__(256) dfj_pass1_kernel(const TB* __restrict__ bp, int64_t pair, int64_t seg,
                                                         const double* __restrict__ w,
-                                                        double* __restrict__ dp) {
+                                                        double* __restrict__ part) {
     __shared__ double red[32];
     const TB* row = bp + (int64_t)blockIdx.x * pair;
+    const int64_t k0 = (int64_t)blockIdx.y * seg;
+    const int64_t k1 = k0 + seg < pair ? k0 + seg : pair;
     double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-    int64_t k = threadIdx.x;
-    for (; k + 768 < pair; k += 1024) {
+    int64_t k = k0 + threadIdx.x;
+    for (; k + 768 < k1; k += 1024) {
         s0 += (double)row[k] * w[k];
         s1 += (double)row[k + 256] * w[k + 256];
         s2 += (double)row[k + 512] * w[k + 512];
         s3 += (double)row[k + 768] * w[k + 768];
     }
-    for (; k < pair; k += 256) s0 += (double)row[k] * w[k];
+    for (; k < k1; k += 256) s0 += (double)row[k] * w[k];
     const double v = block_sum((s0 + s1) + (s2 + s3), red);
-    if (threadIdx.x == 0) dp[blockIdx.x] = v;
+    if (threadIdx.x == 0) part[(int64_t)blockIdx.x * gridDim.y + blockIdx.y] = v;
+}
+
+__global__ void dfj_seg_sum_kernel(const double* __restrict__ part, int nseg, int64_t naux,
+                                   double* __restrict__ dp) {
+    const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= naux) return;
+    double s = 0.0;
+    for (int g = 0; g < nseg; ++g) s += part[q * nseg + g];
+    dp[q] = s;
 }
 
 template <typename TB>
@@ -79,18 +96,148 @@ __global__ void __launch_bounds__(256) dfj_pass2_kernel(const TB* __restrict__ b
     part[(int64_t)blockIdx.y * pair + k] = s0 + s1;
 }
 
-// FP64 -> FP32 (round to nearest) copy of the packed rows; flags values
-// outside the FP32 range (the reference's F32Range check,
-// ferric-core/src/gpu/kernels/round_f64_to_f32.cu semantics).
-__global__ void round_f32_kernel(const double* __restrict__ x, int64_t n, float* __restrict__ y, int* bad) {
-    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    const double v = x[k];
-    if (!(fabs(v) <= 3.4028234663852886e38)) atomicOr(bad, 1);
-    y[k] = __double2float_rn(v);
+// Exact FP32 -> FP64 widening.  The hardware conversion issues at a few per
+// clock per SM, which alone held the FP32 passes to ~3.6 TB/s; widen_f32 does
+// the same on the integer pipe, and the passes convert DFJ_HW_WIDEN of each
+// float4's four elements in hardware and the rest here, so the two pipes
+// share the load (measured best at 2 of 4).  widen_f32 is the IEEE 754 field
+// mapping for normal numbers: an arithmetic shift by 3 moves sign, 8-bit
+// exponent and the top 20 fraction bits into the high word (the sign lands
+// in bits 31..28; the mask keeps bit 31), adding 896 << 20 rebiases the
+// exponent (1023 - 127), and the low 3 fraction bits go to the top of the low
+// word.  +-0 widen to +0 (a product's zero sign is all that differs).
+// SUB = true also widens subnormals, through the hardware conversion; the
+// FP32 copy records whether it holds any, so the usual tensor takes the
+// branch-free form.  No Inf/NaN reaches here: the FP32 copy is refused when a
+// value overflows.
+constexpr int DFJ_HW_WIDEN = 2;
+
+template <bool SUB>
+__device__ __forceinline__ double widen_f32(float f) {
+    const uint32_t u = __float_as_uint(f);
+    if constexpr (SUB) {
+        if ((u & 0x7f800000u) == 0u) return (double)f;
+    }
+    const uint32_t hi = ((uint32_t)((int32_t)u >> 3) & 0x8fffffffu) + 0x38000000u;
+    return __hiloint2double((u << 1) ? (int)hi : 0, (int)(u << 29));
 }
 
-__global__ void dfj_unpack_kernel(const double* __restrict__ part, int nsplit, int64_t pair, int64_t n,
+template <int I, bool SUB>
+__device__ __forceinline__ double widen_at(float f) {
+    if constexpr (I < DFJ_HW_WIDEN) return (double)f;
+    else return widen_f32<SUB>(f);
+}
+
+template <bool SUB>
+__device__ __forceinline__ double dot4(const float4& a, const double* w) {
+    return widen_at<0, SUB>(a.x) * w[0] + widen_at<1, SUB>(a.y) * w[1] + widen_at<2, SUB>(a.z) * w[2] +
+           widen_at<3, SUB>(a.w) * w[3];
+}
+
+// Pass 1 over the FP32 rows (pitch ld = pair rounded up to 4, zero padded):
+// one CTA per (group of DFJ_ROWS rows, segment); each float4's FP64 weights
+// (32 B of w, from L2) serve DFJ_ROWS rows, so L2 -> SM traffic is 1.25x the
+// HBM stream instead of 3x it (one row per CTA), and the DFJ_ROWS loads per
+// thread in flight cover HBM latency.  Rows past naux re-read the last row;
+// their sums are dropped.
+constexpr int DFJ_ROWS = 8;
+
+template <bool SUB>
+__global__ void __launch_bounds__(256, 3) dfj_pass1_f32v_kernel(const float* __restrict__ bp, int64_t naux,
+                                                                int64_t ld, int64_t seg4,
+                                                                const double* __restrict__ w,
+                                                                double* __restrict__ part) {
+    __shared__ double red[DFJ_ROWS][8];
+    const int64_t r0 = (int64_t)blockIdx.x * DFJ_ROWS;
+    const int64_t n4 = ld / 4;
+    const float4* rows[DFJ_ROWS];
+#pragma unroll
+    for (int r = 0; r < DFJ_ROWS; ++r)
+        rows[r] = reinterpret_cast<const float4*>(bp + (r0 + r < naux ? r0 + r : naux - 1) * ld);
+    const int64_t k0 = (int64_t)blockIdx.y * seg4;
+    const int64_t k1 = k0 + seg4 < n4 ? k0 + seg4 : n4;
+    double s[DFJ_ROWS] = {};
+    for (int64_t k = k0 + threadIdx.x; k < k1; k += 256) {
+        float4 a[DFJ_ROWS];
+#pragma unroll
+        for (int r = 0; r < DFJ_ROWS; ++r) a[r] = rows[r][k];
+        const double* wa = w + 4 * k;
+#pragma unroll
+        for (int r = 0; r < DFJ_ROWS; ++r) s[r] += dot4<SUB>(a[r], wa);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int r = 0; r < DFJ_ROWS; ++r) {
+        double v = s[r];
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) red[r][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < DFJ_ROWS && r0 + threadIdx.x < naux) {
+        double v = 0.0;
+        for (int i = 0; i < 8; ++i) v += red[threadIdx.x][i];
+        part[(r0 + threadIdx.x) * gridDim.y + blockIdx.y] = v;
+    }
+}
+
+// Pass 2 over the FP32 rows: each thread owns four columns (one float4) and
+// keeps four rows' loads in flight.
+template <bool SUB>
+__global__ void __launch_bounds__(256) dfj_pass2_f32v_kernel(const float* __restrict__ bp, int64_t naux, int64_t ld,
+                                                             const double* __restrict__ c, int64_t rows_per_split,
+                                                             double* __restrict__ part) {
+    const int64_t k4 = (int64_t)blockIdx.x * 256 + threadIdx.x;
+    if (k4 >= ld / 4) return;
+    const int64_t p0 = (int64_t)blockIdx.y * rows_per_split;
+    const int64_t p1 = p0 + rows_per_split < naux ? p0 + rows_per_split : naux;
+    double s[4] = {0.0, 0.0, 0.0, 0.0}, t[4] = {0.0, 0.0, 0.0, 0.0};
+    const float4* col = reinterpret_cast<const float4*>(bp) + k4;
+    const int64_t l4 = ld / 4;
+    int64_t p = p0;
+    for (; p + 3 < p1; p += 4) {
+        const float4 a = col[p * l4], b = col[(p + 1) * l4], e = col[(p + 2) * l4], f = col[(p + 3) * l4];
+        const double ca = c[p], cb = c[p + 1], ce = c[p + 2], cf = c[p + 3];
+        s[0] += widen_at<0, SUB>(a.x) * ca + widen_at<0, SUB>(b.x) * cb;
+        s[1] += widen_at<1, SUB>(a.y) * ca + widen_at<1, SUB>(b.y) * cb;
+        s[2] += widen_at<2, SUB>(a.z) * ca + widen_at<2, SUB>(b.z) * cb;
+        s[3] += widen_at<3, SUB>(a.w) * ca + widen_at<3, SUB>(b.w) * cb;
+        t[0] += widen_at<0, SUB>(e.x) * ce + widen_at<0, SUB>(f.x) * cf;
+        t[1] += widen_at<1, SUB>(e.y) * ce + widen_at<1, SUB>(f.y) * cf;
+        t[2] += widen_at<2, SUB>(e.z) * ce + widen_at<2, SUB>(f.z) * cf;
+        t[3] += widen_at<3, SUB>(e.w) * ce + widen_at<3, SUB>(f.w) * cf;
+    }
+    for (; p < p1; ++p) {
+        const float4 a = col[p * l4];
+        const double ca = c[p];
+        s[0] += widen_at<0, SUB>(a.x) * ca;
+        s[1] += widen_at<1, SUB>(a.y) * ca;
+        s[2] += widen_at<2, SUB>(a.z) * ca;
+        s[3] += widen_at<3, SUB>(a.w) * ca;
+    }
+    double2* dst = reinterpret_cast<double2*>(part + (int64_t)blockIdx.y * ld + 4 * k4);
+    dst[0] = make_double2(s[0] + t[0], s[1] + t[1]);
+    dst[1] = make_double2(s[2] + t[2], s[3] + t[3]);
+}
+
+// FP64 -> FP32 (round to nearest) copy of the packed rows, row p of x (pitch
+// pair) to row p of y (pitch ld); flags values outside the FP32 range (bit 0,
+// the reference's F32Range check, ferric-core/src/gpu/kernels/round_f64_to_f32.cu
+// semantics) and subnormal results, which are kept as the reference keeps
+// them (bit 1).
+__global__ void round_f32_kernel(const double* __restrict__ x, int64_t rows, int64_t pair, int64_t ld,
+                                 float* __restrict__ y, int* bad) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= rows * pair) return;
+    const int64_t p = e / pair, k = e % pair;
+    const double v = x[e];
+    if (!(fabs(v) <= 3.4028234663852886e38)) atomicOr(bad, 1);
+    const float f = __double2float_rn(v);
+    if (f != 0.0f && fabsf(f) < 1.17549435e-38f) atomicOr(bad, 2);
+    y[p * ld + k] = f;
+}
+
+// part: [nsplit][ld] pass-2 partials of the packed J (ld >= pair).
+__global__ void dfj_unpack_kernel(const double* __restrict__ part, int nsplit, int64_t ld, int64_t n,
                                   double* __restrict__ j) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= n * n) return;
@@ -98,7 +245,7 @@ __global__ void dfj_unpack_kernel(const double* __restrict__ part, int nsplit, i
     const int64_t hi = r > c ? r : c, lo = r > c ? c : r;
     const int64_t k = hi * (hi + 1) / 2 + lo;
     double s = 0.0;
-    for (int sp = 0; sp < nsplit; ++sp) s += part[(int64_t)sp * pair + k];
+    for (int sp = 0; sp < nsplit; ++sp) s += part[(int64_t)sp * ld + k];
     j[idx] = s;
 }
 
@@ -200,21 +347,44 @@ template <typename TB>
 static fc_status dfj_build_t(fc_dfjk* h, const TB* bp, int prec, const double* d, double* j, cudaStream_t st,
                              fc_stats* stats) {
     const int64_t naux = h->naux, n = h->n, pair = h->pair;
+    constexpr bool F32 = sizeof(TB) == 4;
+    const int64_t ld = F32 ? h->ld32 : pair;  // row pitch of bp
     void *vw, *vpart;
     const int nsplit = 4;
-    FC_TRY(ws_get(WS_MISC, (pair + naux + 64) * 8, &vw));
-    FC_TRY(ws_get(WS_PART, (int64_t)nsplit * pair * 8, &vpart));
+    const int64_t seg = F32 ? DFJ_SEG_BYTES / 2 / 16 : DFJ_SEG_BYTES / (int64_t)sizeof(TB);  // float4 or TB units
+    const int64_t nseg = ((F32 ? ld / 4 : pair) + seg - 1) / seg;
+    FC_TRY(ws_get(WS_MISC, (ld + naux * (nseg + 1) + 64) * 8, &vw));
+    FC_TRY(ws_get(WS_PART, (int64_t)nsplit * ld * 8, &vpart));
     double* w = (double*)vw;
-    double* dp = w + pair;
+    double* dp = w + ld;
+    double* segp = dp + naux;
     Context& c = ctx();
     if (stats) FC_CUDA(cudaEventRecord(c.ev0, st));
+    if (ld > pair) FC_CUDA(cudaMemsetAsync(w + pair, 0, (ld - pair) * 8, st));
     density_weights_kernel<<<(unsigned)n, 128, 0, st>>>(d, n, w);
-    dfj_pass1_kernel<TB><<<(unsigned)naux, 256, 0, st>>>(bp, pair, w, dp);
+    if constexpr (F32) {
+        const dim3 g1((unsigned)((naux + DFJ_ROWS - 1) / DFJ_ROWS), (unsigned)nseg);
+        if (h->pk32_subnormal)
+            dfj_pass1_f32v_kernel<true><<<g1, 256, 0, st>>>((const float*)bp, naux, ld, seg, w, segp);
+        else
+            dfj_pass1_f32v_kernel<false><<<g1, 256, 0, st>>>((const float*)bp, naux, ld, seg, w, segp);
+    } else {
+        dfj_pass1_kernel<TB><<<dim3((unsigned)naux, (unsigned)nseg), 256, 0, st>>>(bp, pair, seg, w, segp);
+    }
+    dfj_seg_sum_kernel<<<(unsigned)((naux + 255) / 256), 256, 0, st>>>(segp, (int)nseg, naux, dp);
     if (h->l_chol) chol_solve_kernel<<<1, 1024, 0, st>>>(h->l_chol, naux, dp);
     const int64_t rps = (naux + nsplit - 1) / nsplit;
-    dim3 g2((unsigned)((pair + 255) / 256), nsplit);
-    dfj_pass2_kernel<TB><<<g2, 256, 0, st>>>(bp, naux, pair, dp, rps, (double*)vpart);
-    dfj_unpack_kernel<<<(unsigned)((n * n + 255) / 256), 256, 0, st>>>((const double*)vpart, nsplit, pair, n, j);
+    if constexpr (F32) {
+        dim3 g2((unsigned)((ld / 4 + 255) / 256), nsplit);
+        if (h->pk32_subnormal)
+            dfj_pass2_f32v_kernel<true><<<g2, 256, 0, st>>>((const float*)bp, naux, ld, dp, rps, (double*)vpart);
+        else
+            dfj_pass2_f32v_kernel<false><<<g2, 256, 0, st>>>((const float*)bp, naux, ld, dp, rps, (double*)vpart);
+    } else {
+        dim3 g2((unsigned)((pair + 255) / 256), nsplit);
+        dfj_pass2_kernel<TB><<<g2, 256, 0, st>>>(bp, naux, pair, dp, rps, (double*)vpart);
+    }
+    dfj_unpack_kernel<<<(unsigned)((n * n + 255) / 256), 256, 0, st>>>((const double*)vpart, nsplit, ld, n, j);
     FC_TRY(check_launch("DF-J kernels"));
     if (stats) {
         FC_CUDA(cudaEventRecord(c.ev1, st));
@@ -224,7 +394,7 @@ static fc_status dfj_build_t(fc_dfjk* h, const TB* bp, int prec, const double* d
         stats->kernel_ms = ms;
         stats->flops = 4.0 * (double)naux * (double)pair;
         stats->precision = prec;
-        stats->launches += 4 + (h->l_chol ? 1 : 0);
+        stats->launches += 5 + (h->l_chol ? 1 : 0);
         stats->main_launches = 2;
         stats->main_ms = ms;
         stats->main_flops = stats->flops;
@@ -243,19 +413,23 @@ fc_status dfj_build_mixed(fc_dfjk* h, const double* d, double* j, cudaStream_t s
 }
 
 fc_status dfjk_prepare_mixed(fc_dfjk* h, cudaStream_t st) {
-    const int64_t npk = h->naux * h->pair;
+    h->ld32 = (h->pair + 3) / 4 * 4;
+    const int64_t npk = h->naux * h->ld32;
     FC_TRY(pool_reserve((uint64_t)npk * 4));
     FC_CUDA(cudaMalloc(&h->pk32, (size_t)npk * 4));
     h->bytes += (uint64_t)npk * 4;
+    if (h->ld32 != h->pair) FC_CUDA(cudaMemsetAsync(h->pk32, 0, (size_t)npk * 4, st));
     void* vf;
     FC_TRY(ws_get(WS_OUT, 256, &vf));
     FC_CUDA(cudaMemsetAsync(vf, 0, 256, st));
-    round_f32_kernel<<<(unsigned)((npk + 255) / 256), 256, 0, st>>>(h->b_pk, npk, h->pk32, (int*)vf);
+    round_f32_kernel<<<(unsigned)((h->naux * h->pair + 255) / 256), 256, 0, st>>>(h->b_pk, h->naux, h->pair, h->ld32,
+                                                                                 h->pk32, (int*)vf);
     FC_TRY(check_launch("round_f32_kernel"));
     int bad = 0;
     FC_CUDA(cudaMemcpyAsync(&bad, vf, sizeof(int), cudaMemcpyDeviceToHost, st));
     FC_CUDA(cudaStreamSynchronize(st));
-    if (bad) return fail(FC_ERR_RANGE, "DF-JK: tensor element outside the FP32 range (mixed storage refused)");
+    if (bad & 1) return fail(FC_ERR_RANGE, "DF-JK: tensor element outside the FP32 range (mixed storage refused)");
+    h->pk32_subnormal = (bad & 2) != 0;
     // square handles also keep the exact-slice split for the tensor-core DF-K
     if (h->b_sq) FC_TRY(dfk_prepare_split(h, st));
     return FC_OK;

@@ -10,7 +10,9 @@ struct fc_dfjk {
     double* b_pk = nullptr;    // (naux, n(n+1)/2) packed lower rows
     double* l_chol = nullptr;  // metric Cholesky factor (raw-Bp form)
     // mixed handles
-    float* pk32 = nullptr;     // packed rows, FP32 (DF-J reads 4 B per element)
+    float* pk32 = nullptr;     // packed rows, FP32 (DF-J reads 4 B per element), row pitch ld32
+    int64_t ld32 = 0;          // pair rounded up to 4 (16-byte rows for float4 loads), zero padded
+    bool pk32_subnormal = false;  // the FP32 copy holds subnormals: DF-J widens them exactly (slower)
     void* sq_split = nullptr;  // square tensor: three bf16 slices per row (Q, mu) for DF-K
     double* sq_scale = nullptr;  // their power-of-two row scales (inside the sq_split block)
     uint64_t bytes = 0;        // device bytes owned by the handle

@@ -98,6 +98,36 @@ def test_mixed_dfj_fp32_storage(fc):
     assert np.array_equal(jk.j(d), j)
 
 
+@pytest.mark.parametrize("sub", [False, True])
+@pytest.mark.parametrize("n,naux", [(65, 30), (190, 40)])
+def test_mixed_dfj_widening_exact(fc, n, naux, sub):
+    """The FP32 passes widen each stored element to FP64 exactly: J equals the
+    FP64 build of the FP32-rounded tensor to FP64 rounding.  Zeros (+0 and
+    -0) and negatives are planted, and with ``sub`` FP32 subnormals, which
+    the copy keeps (round_f64_to_f32.cu: no flush) and the passes then widen
+    through their exact variant; n = 65 gives a pair count that is not a
+    multiple of 4 (padded pitch), n = 190 more than one pass-1 segment."""
+    from ferric_b200.dfjk import DfJK
+    b, _, d = synthetic.dfjk_inputs(n, naux, 23)
+    b = b.copy()
+    rng = np.random.default_rng(8)
+    q = rng.integers(0, naux, 600)
+    m = rng.integers(0, n, 600)
+    k = rng.integers(0, n, 600)
+    tiny = rng.choice([-1.0, 1.0], 200) * 10.0 ** (rng.uniform(-44, -39, 200) if sub else rng.uniform(-37, -30, 200))
+    vals = np.concatenate([np.zeros(100), -np.zeros(100), tiny, -np.abs(rng.standard_normal(200))])
+    b[q, m, k] = vals
+    lo, hi = np.tril_indices(n, -1)
+    b[:, hi, lo] = b[:, lo, hi]        # symmetric again (planted pairs may collide)
+    b32 = b.astype(np.float32).astype(np.float64)
+    assert np.any((b32 != 0) & (np.abs(b32) < np.finfo(np.float32).tiny)) == sub
+    ref = orc.df_j_square(b32, d)
+    jk = DfJK(b, precision="mixed")
+    j = jk.j(d)
+    assert np.abs(j - ref).max() <= 1e-12 * np.abs(ref).max()
+    jk.close()
+
+
 def test_set_precision_refuses_missing_copy(fc):
     import ferric_b200._lib as L
     from ferric_b200.dfjk import DfJK
