@@ -894,12 +894,22 @@ __global__ void __launch_bounds__(192, 1)
             const double sr = vm ? p.alpha * v.rs[m] : 0.0;
             double* orow = v.out + (int64_t)(v.i0 + il) * v.nvir + a;
             const uint32_t tl = tmem_base + ((uint32_t)(q * 32) << 16);
+            // The 16 old Gamma values of a column chunk (nov apart) are loaded
+            // together before the TMEM wait: issued one by one between the
+            // stores, each was a DRAM round trip that the next tile's MMAs
+            // (single TMEM accumulator) waited for.
 #pragma unroll 1
             for (int c0 = 0; c0 < 128; c0 += 16) {
                 float l0[16], l1[16], l2[16];
                 tc::tmem_ld16(tl + c0, l0);
                 tc::tmem_ld16(tl + 128 + c0, l1);
                 tc::tmem_ld16(tl + 256 + c0, l2);
+                double old[16];
+#pragma unroll
+                for (int cc = 0; cc < 16; ++cc) {
+                    const int Q = v.tn * 128 + c0 + cc;
+                    old[cc] = vm && p.accumulate && Q < v.naux ? orow[(int64_t)Q * v.nov] : 0.0;
+                }
                 tc::tmem_wait_ld();
                 if (vm) {
 #pragma unroll
@@ -908,8 +918,7 @@ __global__ void __launch_bounds__(192, 1)
                         if (Q < v.naux) {
                             const double g =
                                 sr * v.cs[Q] * ((double)l0[cc] + (double)l1[cc] * L1W + (double)l2[cc] * L2W);
-                            double* o = orow + (int64_t)Q * v.nov;
-                            *o = p.accumulate ? *o + g : g;
+                            orow[(int64_t)Q * v.nov] = p.accumulate ? old[cc] + g : g;
                         }
                     }
                 }
