@@ -46,7 +46,7 @@ void batch_free(fc_rimp2_batch* b) {
 
 // ------------------------------------------------------------ autotuner --
 //
-// Per size bucket (gradient or energy, virtual tiles of 128, k-steps of 64)
+// Per size bucket (gradient or energy, virtual tiles of 128, k-steps of the pair kernel's K tile, 128)
 // the one schedule choice that is not fixed by the shapes: diagonal tiles in
 // one tensor-core phase with the transpose exchanged in shared memory, or in
 // two phases.  Which wins depends on the bucket (the exchange shortens the
@@ -175,7 +175,7 @@ fc_status make_plan(fc_rimp2_batch* b, const std::vector<BatchMolIn>& in, std::v
     std::vector<std::string> keys(in.size());
     std::vector<int64_t> nks(in.size());
     for (size_t m = 0; m < in.size(); ++m) {
-        const int64_t nt = (in[m].nvir + 127) / 128, nk = (in[m].naux + 63) / 64;
+        const int64_t nt = (in[m].nvir + 127) / 128, nk = fx_ksteps(in[m].naux);
         keys[m] = bucket_key(grad, nt, nk);
         nks[m] = nk;
         members[keys[m]].push_back((int64_t)m);

@@ -46,6 +46,8 @@ fc_status batch_alloc(fc_rimp2_batch* b, size_t bytes, void** out);
 // The default choice of the diagonal-tile exchange for items with nk k-steps
 // (FERRIC_CUDA_XT=0/1 forces it).
 int fx_exchange_choice(int nk, int grad);
+// k-steps of the pair kernel over naux (its K tile).
+int fx_ksteps(int64_t naux);
 // plan[m] (or the default when plan is null): 1 = diagonal tiles of molecule m
 // in one phase with the transpose exchanged in shared memory.
 fc_status rimp2_batch_build_fx(fc_rimp2_batch* b, const std::vector<BatchMolIn>& mols, size_t group_bytes,

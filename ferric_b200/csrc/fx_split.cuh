@@ -1,39 +1,67 @@
-// Exact integer-slice split shared by the split-BF16 kernels: every operand
-// row r gets a power of two s_r with max|x| / s_r in [64, 128) and three
-// bf16 slices holding integers in [-128, 128],
-//     x / s_r = c1 + c2 / 256 + c3 / 65536 + eps,   |eps| <= 2^-17,
-// so tensor-core sums of slice products are exact integers in FP32 while
-// they stay below 2^24.
+// Exact integer-slice splits.  Every operand row r gets a power of two s_r
+// and three integer slices,
+//     x / s_r = c1 + c2 / W + c3 / W^2 + eps,   |eps| <= 1 / (2 W^2),
+// so tensor-core sums of slice products are exact integers.  Two formats:
+//   SliceBf16  bf16 integers in [-128, 128], W = 256, max|x| / s in [64, 128);
+//              FP32 accumulation, exact while sums stay below 2^24 (the
+//              DF-K, dressing and Imat GEMMs, which drain to FP64 in panels);
+//   SliceI8    int8 integers in [-127, 127], W = 254, max|x| / s in (63.5, 127];
+//              int32 accumulation (tcgen05.mma kind::i8), exact for
+//              K <= 2^31 / (3 127^2) = 44382 (the RI-MP2 pair kernel and the
+//              adjoint contraction).
+// Both carry about 23 significant bits of each element relative to its row
+// maximum.
 #pragma once
 #include <cuda_bf16.h>
 #include <cstdint>
 
 namespace fc {
 
-// Power-of-two scale with max / s in [64, 128).
-__device__ __forceinline__ double pow2_scale(double mx) {
-    if (!(mx > 0.0) || !(mx <= 1.0e300)) return 1.0;
-    int k;
-    frexp(mx, &k);           // mx = m 2^k, m in [0.5, 1)
-    return ldexp(1.0, k - 7);
-}
+struct SliceBf16 {
+    using T = __nv_bfloat16;
+    static constexpr double W = 256.0;
+    // power of two with max / s in [64, 128)
+    __device__ static double scale(double mx) {
+        if (!(mx > 0.0) || !(mx <= 1.0e300)) return 1.0;
+        int k;
+        frexp(mx, &k);  // mx = m 2^k, m in [0.5, 1)
+        return ldexp(1.0, k - 7);
+    }
+    __device__ static T cast(double v) { return __double2bfloat16(v); }
+};
 
-__device__ __forceinline__ void fx_slices(double x, double inv_s, __nv_bfloat16& c1, __nv_bfloat16& c2,
-                                          __nv_bfloat16& c3) {
+struct SliceI8 {
+    using T = int8_t;
+    static constexpr double W = 254.0;
+    // power of two with max / s in (63.5, 127]
+    __device__ static double scale(double mx) {
+        const double s = SliceBf16::scale(mx);
+        return mx > 127.0 * s ? 2.0 * s : s;
+    }
+    __device__ static T cast(double v) { return (int8_t)(int)v; }
+};
+
+// Power-of-two scale of the BF16 format (DF-K, dressing, Imat).
+__device__ __forceinline__ double pow2_scale(double mx) { return SliceBf16::scale(mx); }
+
+template <class SL = SliceBf16>
+__device__ __forceinline__ void fx_slices(double x, double inv_s, typename SL::T& c1, typename SL::T& c2,
+                                          typename SL::T& c3) {
     const double y = x * inv_s;
     const double a = rint(y);
-    const double y2 = (y - a) * 256.0;
+    const double y2 = (y - a) * SL::W;
     const double b = rint(y2);
-    const double c = rint((y2 - b) * 256.0);
-    c1 = __double2bfloat16(a);
-    c2 = __double2bfloat16(b);
-    c3 = __double2bfloat16(c);
+    const double c = rint((y2 - b) * SL::W);
+    c1 = SL::cast(a);
+    c2 = SL::cast(b);
+    c3 = SL::cast(c);
 }
 
 // Row q of B_ov -> Bq[s][q][j*tpad + b] (row pitch K) at the row's scale qs[q].
+template <class SL = SliceBf16>
 __device__ __forceinline__ void split_fx_qrows_body(const double* __restrict__ B, int64_t nocc, int64_t nvir,
                                                     int64_t tpad, int64_t K, int64_t q_rows,
-                                                    double* __restrict__ qs, __nv_bfloat16* __restrict__ Bq,
+                                                    double* __restrict__ qs, typename SL::T* __restrict__ Bq,
                                                     int64_t q) {
     __shared__ double red[32];
     const int64_t nov = nocc * nvir;
@@ -50,15 +78,15 @@ __device__ __forceinline__ void split_fx_qrows_body(const double* __restrict__ B
         if (threadIdx.x == 0) red[0] = t;
     }
     __syncthreads();
-    const double s = pow2_scale(red[0]);
+    const double s = SL::scale(red[0]);
     if (threadIdx.x == 0) qs[q] = s;
     const double inv = 1.0 / s;
     const int64_t ss = q_rows * K;
-    __nv_bfloat16* o0 = Bq + q * K;
+    typename SL::T* o0 = Bq + q * K;
     for (int64_t k = threadIdx.x; k < nov; k += 256) {
         const int64_t j = k / nvir, b = k % nvir;
-        __nv_bfloat16 c1, c2, c3;
-        fx_slices(row[k], inv, c1, c2, c3);
+        typename SL::T c1, c2, c3;
+        fx_slices<SL>(row[k], inv, c1, c2, c3);
         const int64_t d = j * tpad + b;
         o0[d] = c1;
         o0[ss + d] = c2;
@@ -69,9 +97,11 @@ __device__ __forceinline__ void split_fx_qrows_body(const double* __restrict__ B
 // Per-row split of the FP32 amplitude chunk T[rows][pitch] (first Kv columns)
 // -> Ts[s][rows][pitch], ts[row].  One CTA per row; the row is read twice
 // (max, then slices).  Kv and pitch are multiples of 4.
+template <class SL = SliceBf16>
 __device__ __forceinline__ void split_fx_rows_f32_body(const float* __restrict__ T, int64_t Kv, int64_t K,
                                                        int64_t slice_rows, double* __restrict__ ts,
-                                                       __nv_bfloat16* __restrict__ Ts, int64_t r) {
+                                                       typename SL::T* __restrict__ Ts, int64_t r) {
+    using E = typename SL::T;
     __shared__ double red[32];
     const float4* row = reinterpret_cast<const float4*>(T + r * K);
     const int64_t K4 = Kv / 4;
@@ -89,33 +119,30 @@ __device__ __forceinline__ void split_fx_rows_f32_body(const float* __restrict__
         if (threadIdx.x == 0) red[0] = t;
     }
     __syncthreads();
-    const double s = pow2_scale(red[0]);
+    const double s = SL::scale(red[0]);
     if (threadIdx.x == 0) ts[r] = s;
     const double inv = 1.0 / s;
     const int64_t ss = slice_rows * K;
-    __nv_bfloat16* o0 = Ts + r * K;
+    E* o0 = Ts + r * K;
     for (int64_t k = threadIdx.x; k < K4; k += 256) {
         const float4 v = row[k];
-        __nv_bfloat16 a[4], b[4], c[4];
-        fx_slices(v.x, inv, a[0], b[0], c[0]);
-        fx_slices(v.y, inv, a[1], b[1], c[1]);
-        fx_slices(v.z, inv, a[2], b[2], c[2]);
-        fx_slices(v.w, inv, a[3], b[3], c[3]);
-        uint2 pa, pb, pc;
-        __nv_bfloat162 t0 = __halves2bfloat162(a[0], a[1]), t1 = __halves2bfloat162(a[2], a[3]);
-        pa.x = *reinterpret_cast<uint32_t*>(&t0);
-        pa.y = *reinterpret_cast<uint32_t*>(&t1);
-        t0 = __halves2bfloat162(b[0], b[1]);
-        t1 = __halves2bfloat162(b[2], b[3]);
-        pb.x = *reinterpret_cast<uint32_t*>(&t0);
-        pb.y = *reinterpret_cast<uint32_t*>(&t1);
-        t0 = __halves2bfloat162(c[0], c[1]);
-        t1 = __halves2bfloat162(c[2], c[3]);
-        pc.x = *reinterpret_cast<uint32_t*>(&t0);
-        pc.y = *reinterpret_cast<uint32_t*>(&t1);
-        reinterpret_cast<uint2*>(o0)[k] = pa;
-        reinterpret_cast<uint2*>(o0 + ss)[k] = pb;
-        reinterpret_cast<uint2*>(o0 + 2 * ss)[k] = pc;
+        E a[4], b[4], c[4];
+        fx_slices<SL>(v.x, inv, a[0], b[0], c[0]);
+        fx_slices<SL>(v.y, inv, a[1], b[1], c[1]);
+        fx_slices<SL>(v.z, inv, a[2], b[2], c[2]);
+        fx_slices<SL>(v.w, inv, a[3], b[3], c[3]);
+        // four elements of each slice in one store (8 B for bf16, 4 B for int8)
+        struct alignas(4 * sizeof(E)) Q4 { E e[4]; };
+        Q4 pa, pb, pc;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            pa.e[u] = a[u];
+            pb.e[u] = b[u];
+            pc.e[u] = c[u];
+        }
+        reinterpret_cast<Q4*>(o0)[k] = pa;
+        reinterpret_cast<Q4*>(o0 + ss)[k] = pb;
+        reinterpret_cast<Q4*>(o0 + 2 * ss)[k] = pc;
     }
 }
 

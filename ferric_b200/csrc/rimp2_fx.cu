@@ -1,37 +1,39 @@
-// Split-BF16 RI-MP2 with exact tensor-core accumulation (FC_PREC_MIXED).
+// Exact integer-slice RI-MP2 on the int8 tensor cores (FC_PREC_MIXED).
 //
 // Why: the tcgen05 FP32 accumulator does not round to nearest -- measured on
 // B200, every accumulation step loses about 2^-24 of the running sum toward
 // zero, so a floating hi/lo split accumulated over naux = 4800 is biased by
 // ~1e-5 relative in E (the effect the reference measured for its f32 path,
-// ferric-core/src/gpu/mixed.rs:18-21).  Here every FP32 partial sum is an
-// integer below 2^24, which FP32 holds exactly whatever the rounding mode.
+// ferric-core/src/gpu/mixed.rs:18-21).  Here the operands are split into
+// integer slices and multiplied on tcgen05.mma kind::i8 with int32
+// accumulation, exact whatever the magnitudes (K <= 44382).  The int8 MMA
+// covers twice the K of a bf16 one per instruction and its operands are half
+// the bytes, so the six products cost what three bf16 products would.
 //
-// Split.  Each operand row r (an (i, a) column of B_ov over Q for the pair
-// products, a Q row over (j, b) for the adjoint contraction) gets a power of
-// two s_r with max|x| / s_r in [64, 128), and three bf16 slices holding
-// integers in [-128, 128]:
-//     x / s_r = c1 + c2 / 256 + c3 / 65536 + eps,   |eps| <= 2^-17.
-// Products.  Three levels, one TMEM accumulator each, exact in FP32:
+// Split (SliceI8).  Each operand row r (an (i, a) column of B_ov over Q for
+// the pair products, a Q row over (j, b) for the adjoint contraction) gets a
+// power of two s_r with max|x| / s_r in (63.5, 127], and three int8 slices
+// holding integers in [-127, 127]:
+//     x / s_r = c1 + c2 / 254 + c3 / 254^2 + eps,   |eps| <= 2^-17.
+// Products.  Three levels, one TMEM accumulator each, exact in int32:
 //     L0 = c1 c1',  L1 = c1 c2' + c2 c1',  L2 = c1 c3' + c2 c2' + c3 c1'
-// (6 bf16 tensor-core products), combined in FP64 in the epilogue:
-//     g = s_r s_r' (L0 + L1 / 256 + L2 / 65536).
+// (6 int8 tensor-core products), combined in FP64 in the epilogue:
+//     g = s_r s_r' ((L0 254 + L1) 254 + L2) / 254^2.
 //
 // Pair kernel (this file): item = (pair, a-tile 128, b-tile 128); the X phase
 // accumulates (ia|jb) into the three level accumulators (3 x 128 TMEM
 // columns), the epilogue parks it in registers (FP32, round to nearest), and
 // the Y phase accumulates (ib|ja) = G_ji[a, b] into the same columns, so each
-// thread holds an element and its exchange partner.  128 x 128 UMMAs keep the
-// shared-memory operand reads at 128 B/clk (128 x 64 ones need 192 B/clk, more
-// than an SM delivers).  Energy mode: unordered pairs, E_OS += (X^2 + Y^2)/D,
-// E_SS += (X - Y)^2/D (i == j: X phase only, E_SS = 0), the reference pair
-// loop of ferric-mp2/src/rimp2.rs:1399-1544 over both orderings.  Gradient
-// mode: unordered pairs of an occupied chunk pair (I, J); the item writes
-// Tt_ij = (2X - Y)/D (FP32) into the rows of i and Tt_ji = Tt_ij^T into the
-// rows of j, and the dE/deps partials of both orderings; the adjoint
-// contraction Gamma[:, I] += 4 Bq[:, J] Tt_IJ^T runs in gemm_fx_kernel with
-// the same exact-level scheme.  Diagonal tiles (ta == tb, i != j) may run in
-// one phase, Y = X^T passed through shared memory (the exchange schedule).
+// thread holds an element and its exchange partner.  Energy mode: unordered
+// pairs, E_OS += (X^2 + Y^2)/D, E_SS += (X - Y)^2/D (i == j: X phase only,
+// E_SS = 0), the reference pair loop of ferric-mp2/src/rimp2.rs:1399-1544
+// over both orderings.  Gradient mode: unordered pairs of an occupied chunk
+// pair (I, J); the item writes Tt_ij = (2X - Y)/D (FP32) into the rows of i
+// and Tt_ji = Tt_ij^T into the rows of j, and the dE/deps partials of both
+// orderings; the adjoint contraction Gamma[:, I] += 4 Bq[:, J] Tt_IJ^T runs
+// in gemm_fx_kernel with the same exact-level scheme.  Diagonal tiles
+// (ta == tb, i != j) may run in one phase, Y = X^T passed through shared
+// memory (the exchange schedule).
 #include <algorithm>
 #include <cstdlib>
 
@@ -47,9 +49,12 @@ namespace fc {
 
 namespace fx {
 
-constexpr int BM = 128, BN = 128, KT = 64;
-constexpr int A_BYTES = BM * KT * 2;  // 16 KiB
-constexpr int B_BYTES = BN * KT * 2;  // 16 KiB
+constexpr int BM = 128, BN = 128;
+constexpr int KT = 128;       // int8 elements (128 B) of K per pipeline stage
+constexpr int KT_BF16 = 64;   // bf16 elements per stage of the exact-slice xgemm (opposite-spin UMP2)
+constexpr int64_t KMAX = 32768;  // K per int32 accumulation (< 44382: 3 * 127^2 * K < 2^31)
+constexpr int A_BYTES = BM * KT;  // 16 KiB of int8
+constexpr int B_BYTES = BN * KT;  // 16 KiB of int8
 constexpr int NSL = 3;
 constexpr int STAGE_BYTES = NSL * (A_BYTES + B_BYTES);  // 96 KiB
 constexpr int STAGES = 2;
@@ -57,14 +62,16 @@ constexpr int XP = BM + 1;                       // pitch of the exchange rows (
 constexpr int XBUF_BYTES = 32 * XP * 4;          // one lane quarter of a parked X tile
 constexpr int COL_BYTES = 3 * BN * 8;             // a tile's virtual energies and column scales
 constexpr int SMEM = STAGES * STAGE_BYTES + 1024 + 7168 + XBUF_BYTES + COL_BYTES;
-constexpr uint32_t IDESC = tc::idesc_bf16_f32(128, 128);
-constexpr double L1W = 1.0 / 256.0, L2W = 1.0 / 65536.0;
+constexpr uint32_t IDESC = tc::idesc_i8_s32(128, 128);
+constexpr double LW = 254.0, LW2INV = 1.0 / (254.0 * 254.0);
 
-// products: (A slice, B slice, level)
-__constant__ int8_t kPA[6] = {0, 0, 1, 0, 1, 2};
-__constant__ int8_t kPB[6] = {0, 1, 0, 2, 1, 0};
-__constant__ int8_t kPL[6] = {0, 1, 1, 2, 2, 2};
-__constant__ int8_t kPFirst[6] = {1, 1, 0, 1, 0, 0};  // first product of its level
+// s (L0 + L1 / 254 + L2 / 254^2) from the three int32 TMEM words of a level
+// set: the integer combination (L0 254 + L1) 254 + L2 is exact in FP64.
+__device__ __forceinline__ double level_value(float w0, float w1, float w2, double s) {
+    const double v = (tc::i32_to_f64(w0) * LW + tc::i32_to_f64(w1)) * LW + tc::i32_to_f64(w2);
+    return v * (s * LW2INV);
+}
+
 
 }  // namespace fx
 
@@ -96,20 +103,24 @@ __global__ void __launch_bounds__(256) colmax_kernel(const double* __restrict__ 
 
 
 // scl[i*a_pad + a] from the column maxima of B_ov (1 for padding rows).
+template <class SL>
 __global__ void row_scale_kernel(const unsigned long long* __restrict__ cmax, int64_t nocc, int64_t nvir,
                                  int64_t a_pad, double* __restrict__ scl) {
     const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= nocc * a_pad) return;
     const int64_t i = r / a_pad, a = r % a_pad;
-    scl[r] = a < nvir ? pow2_scale(__longlong_as_double((long long)cmax[i * nvir + a])) : 1.0;
+    scl[r] = a < nvir ? SL::scale(__longlong_as_double((long long)cmax[i * nvir + a])) : 1.0;
 }
 
 
 // B[q, ia] -> Bt[s][i][a][q] (q < q_pad) integer slices at scale scl[i*a_pad+a].
+template <class SL>
 __device__ __forceinline__ void split_fx_transpose_body(const double* __restrict__ B, int64_t naux, int64_t nocc,
                                                         int64_t nvir, int64_t a_pad, int64_t q_pad,
                                                         const double* __restrict__ scl,
-                                                        __nv_bfloat16* __restrict__ Bt, int64_t bx, int64_t by) {
+                                                        typename SL::T* __restrict__ Bt, int64_t bx, int64_t by) {
+    using E = typename SL::T;
+    struct alignas(2 * sizeof(E)) P2 { E e[2]; };
     __shared__ double tile[64][65];
     const int64_t nov = nocc * nvir;
     const int64_t q0 = by * 64, ia0 = bx * 64;
@@ -129,21 +140,22 @@ __device__ __forceinline__ void split_fx_transpose_body(const double* __restrict
         if (ia >= nov) continue;
         const int64_t i = ia / nvir, a = ia % nvir;
         const double inv = 1.0 / scl[i * a_pad + a];
-        __nv_bfloat16 a0, b0, c0, a1, b1, c1;
-        fx_slices(tile[qq][c], inv, a0, b0, c0);
-        fx_slices(tile[qq + 1][c], inv, a1, b1, c1);
+        P2 pa, pb, pc;
+        fx_slices<SL>(tile[qq][c], inv, pa.e[0], pb.e[0], pc.e[0]);
+        fx_slices<SL>(tile[qq + 1][c], inv, pa.e[1], pb.e[1], pc.e[1]);
         const int64_t off = (i * a_pad + a) * q_pad + q0 + qq;
-        *reinterpret_cast<__nv_bfloat162*>(Bt + off) = __halves2bfloat162(a0, a1);
-        *reinterpret_cast<__nv_bfloat162*>(Bt + ss + off) = __halves2bfloat162(b0, b1);
-        *reinterpret_cast<__nv_bfloat162*>(Bt + 2 * ss + off) = __halves2bfloat162(c0, c1);
+        *reinterpret_cast<P2*>(Bt + off) = pa;
+        *reinterpret_cast<P2*>(Bt + ss + off) = pb;
+        *reinterpret_cast<P2*>(Bt + 2 * ss + off) = pc;
     }
 }
 
+template <class SL>
 __global__ void __launch_bounds__(256) split_fx_transpose_kernel(const double* __restrict__ B, int64_t naux,
                                                                  int64_t nocc, int64_t nvir, int64_t a_pad,
                                                                  int64_t q_pad, const double* __restrict__ scl,
-                                                                 __nv_bfloat16* __restrict__ Bt) {
-    split_fx_transpose_body(B, naux, nocc, nvir, a_pad, q_pad, scl, Bt, blockIdx.x, blockIdx.y);
+                                                                 typename SL::T* __restrict__ Bt) {
+    split_fx_transpose_body<SL>(B, naux, nocc, nvir, a_pad, q_pad, scl, Bt, blockIdx.x, blockIdx.y);
 }
 
 __global__ void fill_kernel(double* __restrict__ x, int64_t n, double v) {
@@ -157,15 +169,36 @@ __global__ void fill_kernel(double* __restrict__ x, int64_t n, double v) {
 __global__ void __launch_bounds__(256) split_fx_qrows_kernel(const double* __restrict__ B, int64_t nocc,
                                                              int64_t nvir, int64_t tpad, int64_t K,
                                                              int64_t q_rows, double* __restrict__ qs,
-                                                             __nv_bfloat16* __restrict__ Bq) {
-    split_fx_qrows_body(B, nocc, nvir, tpad, K, q_rows, qs, Bq, blockIdx.x);
+                                                             int8_t* __restrict__ Bq) {
+    split_fx_qrows_body<SliceI8>(B, nocc, nvir, tpad, K, q_rows, qs, Bq, blockIdx.x);
 }
 
 
 __global__ void __launch_bounds__(256) split_fx_rows_f32_kernel(const float* __restrict__ T, int64_t K,
                                                                 int64_t slice_rows, double* __restrict__ ts,
-                                                                __nv_bfloat16* __restrict__ Ts) {
-    split_fx_rows_f32_body(T, K, K, slice_rows, ts, Ts, blockIdx.x);
+                                                                int8_t* __restrict__ Ts) {
+    split_fx_rows_f32_body<SliceI8>(T, K, K, slice_rows, ts, Ts, blockIdx.x);
+}
+
+// The 6 products of one k-step (4 MMAs of K = 32 each) from the stage whose
+// A slice 0 has descriptor `da`; the three A slices are A_BYTES apart and the
+// B slices start BOFS bytes after A slice 0.  Offsets are compile-time: the
+// descriptor start-address field is linear in the address.
+template <int BOFS>
+__device__ __forceinline__ void issue_products(uint64_t da, uint32_t tmem_base, int kt) {
+    using namespace fx;
+    constexpr int PA[6] = {0, 0, 1, 0, 1, 2};
+    constexpr int PB[6] = {0, 1, 0, 2, 1, 0};
+    constexpr int PL[6] = {0, 1, 1, 2, 2, 2};
+    constexpr int PF[6] = {1, 1, 0, 1, 0, 0};  // first product of its level
+#pragma unroll
+    for (int pr = 0; pr < 6; ++pr) {
+#pragma unroll
+        for (int kk = 0; kk < KT / 32; ++kk)
+            tc::umma_i8(tmem_base + PL[pr] * BN, da + (uint64_t)((PA[pr] * A_BYTES + kk * 32) >> 4),
+                        da + (uint64_t)((BOFS + PB[pr] * B_BYTES + kk * 32) >> 4), IDESC,
+                        (kt > 0 || kk > 0 || !PF[pr]) ? 1u : 0u);
+    }
 }
 
 // ------------------------------------------------------------ pair kernel --
@@ -363,6 +396,9 @@ __global__ void __launch_bounds__(320, 1)
     } else if (warp == 1) {
         // ------------------------------------------------------ UMMA issuer
         if (lane == 0) {
+            // the operand descriptors of both stages, computed once: rebuilding
+            // them every k-step delayed the MMA issue by ~9% (measured)
+            const uint64_t da0 = tc::sdesc_k128(sa(0, 0)), da1 = tc::sdesc_k128(sa(1, 0));
             uint32_t g = 0, pc = 0;  // pc: phases issued (TMEM hand-overs)
             for (int64_t k = blockIdx.x; k < p.items && !*abort_flag; k += gridDim.x) {
                 const ItemView v = item_view<BATCH>(p, k);
@@ -375,15 +411,7 @@ __global__ void __launch_bounds__(320, 1)
                         const uint32_t u = g / S;
                         if (!tc::mbar_wait(&full[s], u & 1, abort_flag, p.err)) goto mma_done;
                         tc::fence_after_sync();
-#pragma unroll
-                        for (int pr = 0; pr < 6; ++pr) {
-                            const uint32_t a0 = sa(s, kPA[pr]), b0 = sb(s, kPB[pr]);
-                            const uint32_t dcol = tmem_base + kPL[pr] * BN;
-#pragma unroll
-                            for (int kk = 0; kk < KT / 16; ++kk)
-                                tc::umma_bf16(dcol, tc::sdesc_k128(a0 + kk * 32), tc::sdesc_k128(b0 + kk * 32),
-                                              IDESC, (kt > 0 || kk > 0 || !kPFirst[pr]) ? 1u : 0u);
-                        }
+                        issue_products<NSL * A_BYTES>(s ? da1 : da0, tmem_base, kt);
                         tc::umma_commit(&empty[s]);
                     }
                     tc::umma_commit(tfull);
@@ -458,9 +486,7 @@ __global__ void __launch_bounds__(320, 1)
                 tc::tmem_ld16(tl + 2 * BN + c0, l2);
                 tc::tmem_wait_ld();
 #pragma unroll
-                for (int cc = 0; cc < 16; ++cc)
-                    xr[c0 + cc] = (float)(sxa * sxb[c0 + cc] *
-                                          ((double)l0[cc] + (double)l1[cc] * L1W + (double)l2[cc] * L2W));
+                for (int cc = 0; cc < 16; ++cc) xr[c0 + cc] = (float)level_value(l0[cc], l1[cc], l2[cc], sxa * sxb[c0 + cc]);
             }
             tc::fence_before_sync();
             tc::mbar_arrive(tempty);
@@ -577,8 +603,7 @@ __global__ void __launch_bounds__(320, 1)
                             tc::mbar_arrive(tempty);
                         }
 #pragma unroll
-                        for (int cc = 0; cc < 8; ++cc)
-                            yv[cc] = sya * syb[c0 + cc] * ((double)y0[cc] + (double)y1[cc] * L1W + (double)y2[cc] * L2W);
+                        for (int cc = 0; cc < 8; ++cc) yv[cc] = level_value(y0[cc], y1[cc], y2[cc], sya * syb[c0 + cc]);
                     } else {
 #pragma unroll
                         for (int cc = 0; cc < 8; ++cc) yv[cc] = (double)xr[c0 + cc];
@@ -707,6 +732,7 @@ struct GemmFxArgs {
     double* out;  // Gamma (naux, nov)
     int* err;
     int kofs;        // first K column of the B operand (Q-row slices)
+    int aofs;        // first K column of the A operand (a K segment of the amplitude slices)
     int accumulate;  // out += instead of out =
     // batch mode: tile t is bitems[t] = (molecule, m-tile, n-tile, 0)
     const int4* bitems;
@@ -770,9 +796,8 @@ __device__ __forceinline__ GemmView gemm_view(const GemmFxArgs& p, const CUtenso
 constexpr int GF_STAGE = 3 * (16384 + 16384);  // 96 KiB
 constexpr int GF_STAGES = 2;
 constexpr int GF_SMEM = GF_STAGES * GF_STAGE + 1024 + 1024;
-constexpr uint32_t GF_IDESC = tc::idesc_bf16_f32(128, 128);
 
-// out[Q, (i0 + il)*nvir + a] (+)= alpha * s_row s_Q (L0 + L1/256 + L2/65536)
+// out[Q, (i0 + il)*nvir + a] (+)= alpha * s_row s_Q (L0 + L1/254 + L2/254^2)
 // for amplitude rows m = il*tpad + a (a < nvir).
 template <int BATCH = 0>
 __global__ void __launch_bounds__(192, 1)
@@ -836,7 +861,8 @@ __global__ void __launch_bounds__(192, 1)
                     tc::mbar_arrive_expect_tx(&full[s], GF_STAGE);
 #pragma unroll
                     for (int sl = 0; sl < 3; ++sl) {
-                        tc::tma_load_2d(base + (sa(s, sl) - base_u32), v.tA, &full[s], kt * KT, sl * v.M + v.tm * 128);
+                        tc::tma_load_2d(base + (sa(s, sl) - base_u32), v.tA, &full[s], p.aofs + kt * KT,
+                                        sl * v.M + v.tm * 128);
                         tc::tma_load_2d(base + (sb(s, sl) - base_u32), v.tB, &full[s], p.kofs + kt * KT,
                                         sl * v.N + v.tn * 128);
                     }
@@ -851,6 +877,7 @@ __global__ void __launch_bounds__(192, 1)
         }
     } else if (warp == 1) {
         if (lane == 0) {
+            const uint64_t da0 = tc::sdesc_k128(sa(0, 0)), da1 = tc::sdesc_k128(sa(1, 0));
             uint32_t g = 0, li = 0;
             for (int64_t t = blockIdx.x; t < p.tiles && !*abort_flag; t += gridDim.x, ++li) {
                 const int nk = BATCH ? p.gmols[p.bitems[t].x].nk : p.nk;
@@ -861,15 +888,7 @@ __global__ void __launch_bounds__(192, 1)
                     const uint32_t u = g / S;
                     if (!tc::mbar_wait(&full[s], u & 1, abort_flag, p.err)) goto mma_done;
                     tc::fence_after_sync();
-#pragma unroll
-                    for (int pr = 0; pr < 6; ++pr) {
-                        const uint32_t a0 = sa(s, kPA[pr]), b0 = sb(s, kPB[pr]);
-                        const uint32_t dcol = tmem_base + kPL[pr] * 128;
-#pragma unroll
-                        for (int kk = 0; kk < KT / 16; ++kk)
-                            tc::umma_bf16(dcol, tc::sdesc_k128(a0 + kk * 32), tc::sdesc_k128(b0 + kk * 32), GF_IDESC,
-                                          (kt > 0 || kk > 0 || !kPFirst[pr]) ? 1u : 0u);
-                    }
+                    issue_products<3 * 16384>(s ? da1 : da0, tmem_base, kt);
                     tc::umma_commit(&empty[s]);
                 }
                 tc::umma_commit(tfull);
@@ -916,8 +935,7 @@ __global__ void __launch_bounds__(192, 1)
                     for (int cc = 0; cc < 16; ++cc) {
                         const int Q = v.tn * 128 + c0 + cc;
                         if (Q < v.naux) {
-                            const double g =
-                                sr * v.cs[Q] * ((double)l0[cc] + (double)l1[cc] * L1W + (double)l2[cc] * L2W);
+                            const double g = level_value(l0[cc], l1[cc], l2[cc], sr * v.cs[Q]);
                             orow[(int64_t)Q * v.nov] = p.accumulate ? old[cc] + g : g;
                         }
                     }
@@ -1025,12 +1043,12 @@ struct BatchPrep {
     int64_t naux, nocc, nvir, a_pad, q_pad, tpad, ldt, q_rows, M;
     unsigned long long* cmax;  // [nocc*nvir]
     double* scl;               // [nocc*a_pad] pair-operand row scales
-    __nv_bfloat16* bt;         // pair-operand slices (rows of this molecule)
+    int8_t* bt;                // pair-operand slices (rows of this molecule)
     double* qs;                // [q_rows] Q-row scales (gradient)
-    __nv_bfloat16* bq;         // Q-row slices [3][q_rows][ldt]
+    int8_t* bq;                // Q-row slices [3][q_rows][ldt]
     float* T;                  // amplitudes [nocc*tpad][ldt]
     double* ts;                // [M] amplitude-row scales
-    __nv_bfloat16* Ts;         // amplitude slices [3][M][ldt]
+    int8_t* Ts;                // amplitude slices [3][M][ldt]
     double* de_docc;           // [nocc]
     double* de_dvir;           // [nvir]
     int64_t seg0;              // first item of this molecule
@@ -1065,7 +1083,7 @@ __global__ void __launch_bounds__(256) batch_row_scale_kernel(const BatchPrep* _
     const int m = seg_find(pre, 0, nmol, x);
     const BatchPrep& d = mp[m];
     const int64_t r = x - pre[m], i = r / d.a_pad, a = r % d.a_pad;
-    d.scl[r] = a < d.nvir ? pow2_scale(__longlong_as_double((long long)d.cmax[i * d.nvir + a])) : 1.0;
+    d.scl[r] = a < d.nvir ? SliceI8::scale(__longlong_as_double((long long)d.cmax[i * d.nvir + a])) : 1.0;
 }
 
 __global__ void __launch_bounds__(256) batch_transpose_kernel(const BatchPrep* __restrict__ mp,
@@ -1074,7 +1092,8 @@ __global__ void __launch_bounds__(256) batch_transpose_kernel(const BatchPrep* _
     const int m = seg_find(pre, 0, nmol, x);
     const BatchPrep& d = mp[m];
     const int64_t nbx = (d.nocc * d.nvir + 63) / 64, loc = x - pre[m];
-    split_fx_transpose_body(d.b, d.naux, d.nocc, d.nvir, d.a_pad, d.q_pad, d.scl, d.bt, loc % nbx, loc / nbx);
+    split_fx_transpose_body<SliceI8>(d.b, d.naux, d.nocc, d.nvir, d.a_pad, d.q_pad, d.scl, d.bt, loc % nbx,
+                                     loc / nbx);
 }
 
 __global__ void __launch_bounds__(256) batch_qrows_kernel(const BatchPrep* __restrict__ mp,
@@ -1082,7 +1101,7 @@ __global__ void __launch_bounds__(256) batch_qrows_kernel(const BatchPrep* __res
     const int64_t x = blockIdx.x;
     const int m = seg_find(pre, 0, nmol, x);
     const BatchPrep& d = mp[m];
-    split_fx_qrows_body(d.b, d.nocc, d.nvir, d.tpad, d.ldt, d.q_rows, d.qs, d.bq, x - pre[m]);
+    split_fx_qrows_body<SliceI8>(d.b, d.nocc, d.nvir, d.tpad, d.ldt, d.q_rows, d.qs, d.bq, x - pre[m]);
 }
 
 // Amplitude rows of the molecules [m0, m1).
@@ -1091,7 +1110,7 @@ __global__ void __launch_bounds__(256) batch_trows_kernel(const BatchPrep* __res
     const int64_t x = pre[m0] + blockIdx.x;
     const int m = seg_find(pre, m0, m1, x);
     const BatchPrep& d = mp[m];
-    split_fx_rows_f32_body(d.T, d.nocc * d.tpad, d.ldt, d.M, d.ts, d.Ts, x - pre[m]);
+    split_fx_rows_f32_body<SliceI8>(d.T, d.nocc * d.tpad, d.ldt, d.M, d.ts, d.Ts, x - pre[m]);
 }
 
 // dE/deps_o = -2 sum of the t Tt partials of the items of every pair holding o.
@@ -1177,14 +1196,18 @@ __global__ void __launch_bounds__(256) batch_energy_kernel(const double* __restr
 
 namespace {
 
-// k-steps of 64 from which the exchange is the default (measured on B200:
-// energy items gain from nk = 4 on; gradient items, whose epilogue also
-// writes amplitudes, lose up to nk = 11 and gain a little at nk = 76)
-constexpr int XT_MIN_NK_ENERGY = 4;
-constexpr int XT_MIN_NK_GRAD = 32;
+// k-steps (of fx::KT) from which the exchange is the default: it pays when
+// a phase is long against the epilogue (energy items gain from K = 256 on;
+// gradient items, whose epilogue also writes amplitudes, from K ~ 2048)
+constexpr int XT_MIN_NK_ENERGY = 2;
+constexpr int XT_MIN_NK_GRAD = 16;
+
+// naux up to which the int32 level sums of the pair kernel are exact:
+// 3 * 127^2 * naux < 2^31.
+constexpr int64_t PAIR_KMAX = 44382;
 
 struct FxSplit {
-    __nv_bfloat16* bt;
+    int8_t* bt;
     double* scl;
     int64_t a_pad, q_pad;
     CUtensorMap tmA, tmB;
@@ -1195,30 +1218,33 @@ fc_status fx_split_pairs(const Rimp2Dev& d, cudaStream_t st, int* bad, FxSplit* 
     const int64_t q_pad = (d.naux + fx::KT - 1) / fx::KT * fx::KT;
     const int64_t nov = d.nocc * d.nvir;
     const int64_t rows = (int64_t)fx::NSL * d.nocc * a_pad;
+    if (d.naux > PAIR_KMAX)
+        return fail(FC_ERR_LAYOUT, "mixed RI-MP2: naux > 44382 exceeds the exact int32 level sums (use FP64)");
     void *vbt, *vscl;
-    FC_TRY(ws_get(WS_SPLIT, (size_t)rows * q_pad * 2, &vbt));
+    FC_TRY(ws_get(WS_SPLIT, (size_t)rows * q_pad, &vbt));
     FC_TRY(ws_get(WS_SCALE, (size_t)(nov + d.nocc * a_pad) * 8 + 256, &vscl));
     unsigned long long* cmax = (unsigned long long*)vscl;
     double* scl = (double*)vscl + nov;
     FC_CUDA(cudaMemsetAsync(cmax, 0, nov * 8, st));
-    FC_CUDA(cudaMemsetAsync(vbt, 0, (size_t)rows * q_pad * 2, st));
+    FC_CUDA(cudaMemsetAsync(vbt, 0, (size_t)rows * q_pad, st));
     {
         const int64_t rps = 64;
         dim3 g((unsigned)((nov + 255) / 256), (unsigned)((d.naux + rps - 1) / rps));
         colmax_kernel<<<g, 256, 0, st>>>(d.b_ov, d.naux, nov, rps, cmax, bad);
     }
-    row_scale_kernel<<<(unsigned)((d.nocc * a_pad + 255) / 256), 256, 0, st>>>(cmax, d.nocc, d.nvir, a_pad, scl);
+    row_scale_kernel<SliceI8><<<(unsigned)((d.nocc * a_pad + 255) / 256), 256, 0, st>>>(cmax, d.nocc, d.nvir,
+                                                                                        a_pad, scl);
     {
         dim3 g((unsigned)((nov + 63) / 64), (unsigned)((d.naux + 63) / 64));
         if (g.y > 65535) return fail(FC_ERR_LAYOUT, "split: naux too large");
-        split_fx_transpose_kernel<<<g, 256, 0, st>>>(d.b_ov, d.naux, d.nocc, d.nvir, a_pad, q_pad, scl,
-                                                     (__nv_bfloat16*)vbt);
+        split_fx_transpose_kernel<SliceI8><<<g, 256, 0, st>>>(d.b_ov, d.naux, d.nocc, d.nvir, a_pad, q_pad, scl,
+                                                              (int8_t*)vbt);
     }
     FC_TRY(check_launch("fixed-point split kernels"));
     if (rows > (int64_t)UINT32_MAX) return fail(FC_ERR_LAYOUT, "split: too many operand rows");
-    FC_TRY(make_tmap_bf16_2d(&o->tmA, vbt, q_pad, rows, q_pad * 2, fx::KT, fx::BM));
-    FC_TRY(make_tmap_bf16_2d(&o->tmB, vbt, q_pad, rows, q_pad * 2, fx::KT, fx::BN));
-    o->bt = (__nv_bfloat16*)vbt;
+    FC_TRY(make_tmap_i8_2d(&o->tmA, vbt, q_pad, rows, q_pad, fx::KT, fx::BM));
+    FC_TRY(make_tmap_i8_2d(&o->tmB, vbt, q_pad, rows, q_pad, fx::KT, fx::BN));
+    o->bt = (int8_t*)vbt;
     o->scl = scl;
     o->a_pad = a_pad;
     o->q_pad = q_pad;
@@ -1245,6 +1271,8 @@ fc_status fx_attrs() {
 // exchange saves a phase of MMAs and costs the epilogue two passes over
 // shared memory with half the threads busy in each: it pays when the phase
 // is long (many k-steps).  FERRIC_CUDA_XT=0/1 forces it.
+int fx_ksteps(int64_t naux) { return (int)((naux + fx::KT - 1) / fx::KT); }
+
 int fx_exchange_choice(int nk, int grad) {
     const char* e = std::getenv("FERRIC_CUDA_XT");
     if (e && (e[0] == '0' || e[0] == '1')) return e[0] == '1';
@@ -1351,7 +1379,8 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
     if (stats) FC_CUDA(cudaEventRecord(c.ev0, st));
     FC_TRY(fx_split_pairs(d, st, flags, &sp));
     const int64_t a_pad = sp.a_pad;
-    const int64_t tp = (nvir + 7) / 8 * 8;  // amplitude pitch: rows (i, a) and columns (j, b), a, b < tp
+    const int64_t tp = (nvir + 15) / 16 * 16;  // amplitude pitch: rows (i, a) and columns (j, b), a, b < tp
+                                               // (16: int8 slice columns of a chunk start 16-byte aligned)
     const int64_t K2 = nocc * tp;           // (j, b) columns of the Q-row slices
     const int64_t q_rows = (naux + 127) / 128 * 128;
     const int nTa = (int)(a_pad / fx::BM);
@@ -1360,7 +1389,7 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
     // occupied chunks: a chunk pair (I, J), I <= J, holds the amplitude rows of
     // I (columns of J) and of J (columns of I) in FP32, plus the slices of one
     // of them; each unordered pair (i, j) is computed once and feeds both.
-    const int64_t per_c2 = tp * tp * (4 + 4 + 6) + 1024 * tp;
+    const int64_t per_c2 = tp * tp * (4 + 4 + 3) + 1024 * tp;  // two FP32 amplitude blocks, int8 slices
     int64_t cc = 1;
     while (cc < nocc && (cc + 1) * (cc + 1) * per_c2 <= (int64_t)d.chunk_bytes) ++cc;
     const int64_t nch = (nocc + cc - 1) / cc;
@@ -1391,13 +1420,13 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
 
     void *vbq, *vtab, *vT, *vTs, *vpart;
     const size_t tab_bytes = ((pairs.size() * sizeof(int2) + 255) / 256) * 256;
-    FC_TRY(ws_get(WS_SPLIT2, (size_t)3 * q_rows * K2 * 2, &vbq));
+    FC_TRY(ws_get(WS_SPLIT2, (size_t)3 * q_rows * K2, &vbq));
     FC_TRY(ws_get(WS_PAIRS, tab_bytes + q_rows * 8, &vtab));
     double* qs = (double*)((char*)vtab + tab_bytes);
     const size_t cbytes = (size_t)cc * tp * cc * tp;  // elements of one amplitude block
     const int64_t mp_max = (cc * tp + 127) / 128 * 128;
     FC_TRY(ws_get(WS_T, cbytes * 8 + (size_t)mp_max * 8, &vT));
-    FC_TRY(ws_get(WS_TS, (size_t)3 * mp_max * cc * tp * 2, &vTs));
+    FC_TRY(ws_get(WS_TS, (size_t)3 * mp_max * cc * tp, &vTs));
     FC_TRY(ws_get(WS_PART, (size_t)max_items * (2 + 1 + 2 * fx::BM) * 8 + (size_t)(2 * ncp + nocc) * 8, &vpart));
     float* T1 = (float*)vT;
     float* T2 = T1 + cbytes;
@@ -1412,30 +1441,35 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
     FC_CUDA(cudaMemsetAsync(acc_occ, 0, nocc * 8, st));
     FC_CUDA(cudaMemsetAsync(gamma, 0, (size_t)naux * nov * 8, st));
     // per-Q-row split of B_ov for the adjoint contraction
-    FC_CUDA(cudaMemsetAsync(vbq, 0, (size_t)3 * q_rows * K2 * 2, st));
+    FC_CUDA(cudaMemsetAsync(vbq, 0, (size_t)3 * q_rows * K2, st));
     fill_kernel<<<(unsigned)((q_rows + 255) / 256), 256, 0, st>>>(qs, q_rows, 1.0);
-    split_fx_qrows_kernel<<<(unsigned)naux, 256, 0, st>>>(d.b_ov, nocc, nvir, tp, K2, q_rows, qs,
-                                                          (__nv_bfloat16*)vbq);
+    split_fx_qrows_kernel<<<(unsigned)naux, 256, 0, st>>>(d.b_ov, nocc, nvir, tp, K2, q_rows, qs, (int8_t*)vbq);
     FC_TRY(check_launch("split_fx_qrows_kernel"));
     CUtensorMap tmBq;
-    FC_TRY(make_tmap_bf16_2d(&tmBq, vbq, K2, 3 * q_rows, K2 * 2, fx::KT, 128));
+    FC_TRY(make_tmap_i8_2d(&tmBq, vbq, K2, 3 * q_rows, K2, fx::KT, 128));
     const int2* dpairs = (const int2*)vtab;
     const int2* dtiles = dpairs + npairs_all;
 
     cudaEvent_t* ev = nullptr;
     if (stats) FC_TRY(timing_events((int)ncp, &ev));
+    // K segment of the adjoint contraction: fx::KMAX, or FERRIC_CUDA_KSEG (a
+    // positive multiple of fx::KT up to fx::KMAX; tests use short segments)
+    int64_t kseg = fx::KMAX;
+    if (const char* e = std::getenv("FERRIC_CUDA_KSEG")) {
+        const long long v = std::atoll(e);
+        if (v > 0 && v % fx::KT == 0 && v <= fx::KMAX) kseg = v;
+    }
     // Gamma[:, rows] += 4 Bq[:, cols] T^T for one amplitude block
     auto adjoint = [&](float* T, int64_t r0, int64_t nr, int64_t k0, int64_t nk) -> fc_status {
         const int64_t ldk = nk * tp, rows = nr * tp, mp = (rows + 127) / 128 * 128;
-        split_fx_rows_f32_kernel<<<(unsigned)rows, 256, 0, st>>>(T, ldk, mp, ts, (__nv_bfloat16*)vTs);
+        split_fx_rows_f32_kernel<<<(unsigned)rows, 256, 0, st>>>(T, ldk, mp, ts, (int8_t*)vTs);
         CUtensorMap tmTs;
-        FC_TRY(make_tmap_bf16_2d(&tmTs, vTs, ldk, 3 * mp, ldk * 2, fx::KT, 128));
+        FC_TRY(make_tmap_i8_2d(&tmTs, vTs, ldk, 3 * mp, ldk, fx::KT, 128));
         GemmFxArgs g{};
         g.rs = ts;
         g.cs = qs;
         g.M = (int)mp;
         g.N = (int)q_rows;
-        g.nk = (int)((ldk + fx::KT - 1) / fx::KT);
         g.nTm = (int)(mp / 128);
         g.rows = (int)rows;
         g.nTn = (int)(q_rows / 128);
@@ -1448,11 +1482,19 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
         g.alpha = 4.0;
         g.out = gamma;
         g.err = flags + 1;
-        g.kofs = (int)(k0 * tp);
         g.accumulate = 1;
         const int g2 = (int)(g.tiles < c.sm_count ? g.tiles : c.sm_count);
-        gemm_fx_kernel<0><<<g2, 192, GF_SMEM, st>>>(tmTs, tmBq, g);
-        return check_launch("gemm_fx_kernel");
+        // K segments of at most kseg (a multiple of KT) keep the int32 level
+        // sums exact; each segment adds its part into Gamma
+        for (int64_t ks = 0; ks < ldk; ks += kseg) {
+            const int64_t kl = std::min<int64_t>(kseg, ldk - ks);
+            g.aofs = (int)ks;
+            g.kofs = (int)(k0 * tp + ks);
+            g.nk = (int)((kl + fx::KT - 1) / fx::KT);
+            gemm_fx_kernel<0><<<g2, 192, GF_SMEM, st>>>(tmTs, tmBq, g);
+            FC_TRY(check_launch("gemm_fx_kernel"));
+        }
+        return FC_OK;
     };
     for (int64_t x = 0; x < ncp; ++x) {
         const CP& cp = cps[x];
@@ -1598,6 +1640,7 @@ struct EpiOS {
 // B_ov of one spin -> exact slices, rows (i, a) unpadded, K = q_pad.
 fc_status ump2_split(const UmpSpin& x, int64_t naux, int64_t q_pad, cudaStream_t st, int* bad, int slot_split,
                      int slot_scale, __nv_bfloat16** bt, double** scl) {
+    // consumed by the bf16 exact-slice xgemm (FP32 accumulation, panel drains)
     const int64_t nov = x.nocc * x.nvir;
     void *vbt, *vsc;
     FC_TRY(ws_get(slot_split, (size_t)3 * nov * q_pad * 2, &vbt));
@@ -1607,11 +1650,11 @@ fc_status ump2_split(const UmpSpin& x, int64_t naux, int64_t q_pad, cudaStream_t
     FC_CUDA(cudaMemsetAsync(cmax, 0, nov * 8, st));
     dim3 g1((unsigned)((nov + 255) / 256), (unsigned)((naux + 63) / 64));
     colmax_kernel<<<g1, 256, 0, st>>>(x.b_ov, naux, nov, 64, cmax, bad);
-    row_scale_kernel<<<(unsigned)((nov + 255) / 256), 256, 0, st>>>(cmax, x.nocc, x.nvir, x.nvir, s);
+    row_scale_kernel<SliceBf16><<<(unsigned)((nov + 255) / 256), 256, 0, st>>>(cmax, x.nocc, x.nvir, x.nvir, s);
     dim3 g3((unsigned)((nov + 63) / 64), (unsigned)((naux + 63) / 64));
     if (g3.y > 65535) return fail(FC_ERR_LAYOUT, "U-RI-MP2 split: naux too large");
-    split_fx_transpose_kernel<<<g3, 256, 0, st>>>(x.b_ov, naux, x.nocc, x.nvir, x.nvir, q_pad, s,
-                                                  (__nv_bfloat16*)vbt);
+    split_fx_transpose_kernel<SliceBf16><<<g3, 256, 0, st>>>(x.b_ov, naux, x.nocc, x.nvir, x.nvir, q_pad, s,
+                                                             (__nv_bfloat16*)vbt);
     *bt = (__nv_bfloat16*)vbt;
     *scl = s;
     return check_launch("U-RI-MP2 split kernels");
@@ -1630,7 +1673,7 @@ fc_status ump2_cross_fx(const UmpSpin& A, const UmpSpin& Bs, int64_t naux, cudaS
     }
     Context& c = ctx();
     const int64_t nova = A.nocc * A.nvir, novb = Bs.nocc * Bs.nvir;
-    const int64_t q_pad = (naux + fx::KT - 1) / fx::KT * fx::KT;
+    const int64_t q_pad = (naux + fx::KT_BF16 - 1) / fx::KT_BF16 * fx::KT_BF16;
     if (3 * nova > (int64_t)UINT32_MAX || 3 * novb > (int64_t)UINT32_MAX || nova > INT32_MAX)
         return fail(FC_ERR_LAYOUT, "U-RI-MP2: too many operand rows");
     void* vout;
@@ -1643,7 +1686,7 @@ fc_status ump2_cross_fx(const UmpSpin& A, const UmpSpin& Bs, int64_t naux, cudaS
     FC_TRY(ump2_split(A, naux, q_pad, st, flags, WS_SPLIT, WS_SCALE, &bta, &sa));
     FC_TRY(ump2_split(Bs, naux, q_pad, st, flags, WS_SPLIT2, WS_MISC, &btb, &sb));
     std::vector<int4> items;
-    const int ntm = (int)((nova + 127) / 128), ntn = (int)((novb + 127) / 128), nks = (int)(q_pad / fx::KT);
+    const int ntm = (int)((nova + 127) / 128), ntn = (int)((novb + 127) / 128), nks = (int)(q_pad / fx::KT_BF16);
     for (int tn = 0; tn < ntn; ++tn)
         for (int tm = 0; tm < ntm; ++tm) items.push_back(make_int4(tm, tn, 0, nks));
     void *vtab, *vpart;
@@ -1651,8 +1694,8 @@ fc_status ump2_cross_fx(const UmpSpin& A, const UmpSpin& Bs, int64_t naux, cudaS
     FC_TRY(ws_get(WS_PART, items.size() * 16 * 8, &vpart));
     FC_CUDA(cudaMemcpyAsync(vtab, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
     CUtensorMap ta, tb;
-    FC_TRY(make_tmap_bf16_2d(&ta, bta, q_pad, 3 * nova, q_pad * 2, fx::KT, 128));
-    FC_TRY(make_tmap_bf16_2d(&tb, btb, q_pad, 3 * novb, q_pad * 2, fx::KT, 128));
+    FC_TRY(make_tmap_bf16_2d(&ta, bta, q_pad, 3 * nova, q_pad * 2, fx::KT_BF16, 128));
+    FC_TRY(make_tmap_bf16_2d(&tb, btb, q_pad, 3 * novb, q_pad * 2, fx::KT_BF16, 128));
     XArgs a{(const int4*)vtab, (int64_t)items.size(), (int)nova, (int)novb, flags + 1};
     EpiOS epi{sa, sb, A.eps_occ, A.eps_vir, Bs.eps_occ, Bs.eps_vir, (int)A.nvir, (int)Bs.nvir, nova, novb,
               (double*)vpart};
@@ -1730,8 +1773,8 @@ fc_status rimp2_batch_build_fx(fc_rimp2_batch* b, const std::vector<BatchMolIn>&
         x.nvir = d.nvir;
         x.a_pad = rup(d.nvir, fx::BM);
         x.q_pad = q_pad;
-        x.tpad = grad ? rup(d.nvir, 8) : x.a_pad;
-        x.ldt = d.nocc * x.tpad;          // a multiple of 8
+        x.tpad = grad ? rup(d.nvir, 16) : x.a_pad;
+        x.ldt = d.nocc * x.tpad;          // a multiple of 16 (16-byte int8 slice rows)
         x.q_rows = rup(d.naux, 128);
         x.M = rup(x.ldt, 128);
         x.de_docc = d.de_deps_occ;
@@ -1764,6 +1807,9 @@ fc_status rimp2_batch_build_fx(fc_rimp2_batch* b, const std::vector<BatchMolIn>&
         if (grad) b->flops += 2.0 * (double)d.naux * (double)nov * (double)nov;
     }
     const int64_t items = seg[nmol];
+    for (const auto& x : hp)
+        if (x.naux > PAIR_KMAX || (grad && x.ldt > fx::KMAX))
+            return fail(FC_ERR_LAYOUT, "RI-MP2 batch: a molecule exceeds the exact int32 level-sum range");
     if (rows >= INT32_MAX || items >= INT32_MAX || P(PRE_COLMAX, nmol) >= INT32_MAX ||
         P(PRE_TRANSPOSE, nmol) >= INT32_MAX || P(PRE_ROWSCALE, nmol) >= (int64_t)INT32_MAX * 256 ||
         P(PRE_QROWS, nmol) >= INT32_MAX || P(PRE_TROWS, nmol) >= INT32_MAX)
@@ -1781,7 +1827,7 @@ fc_status rimp2_batch_build_fx(fc_rimp2_batch* b, const std::vector<BatchMolIn>&
         int m0 = 0;
         for (int m = 0; m < nmol; ++m) {
             const BatchPrep& x = hp[m];
-            const size_t tb = rup(x.ldt * x.ldt * 4, 256) + rup(x.M * 8, 256) + rup(3 * x.M * x.ldt * 2, 256);
+            const size_t tb = rup(x.ldt * x.ldt * 4, 256) + rup(x.M * 8, 256) + rup(3 * x.M * x.ldt, 256);
             if (m > m0 && cur + tb > group_bytes) {
                 groups.push_back({m0, m, seg[m0], seg[m], 0, 0});
                 m0 = m;
@@ -1797,7 +1843,7 @@ fc_status rimp2_batch_build_fx(fc_rimp2_batch* b, const std::vector<BatchMolIn>&
 
     // ---- device buffers
     void *vbt, *vscl, *vcmax, *vmols, *vprep, *vpre, *vseg, *vitems, *vpart;
-    FC_TRY(batch_alloc(b, (size_t)rows * q_pad * 2, &vbt));
+    FC_TRY(batch_alloc(b, (size_t)rows * q_pad, &vbt));
     FC_TRY(batch_alloc(b, (size_t)nscl * 8, &vscl));
     FC_TRY(batch_alloc(b, (size_t)ncmax * 8, &vcmax));
     FC_TRY(batch_alloc(b, (size_t)nmol * sizeof(BatchMol), &vmols));
@@ -1806,7 +1852,7 @@ fc_status rimp2_batch_build_fx(fc_rimp2_batch* b, const std::vector<BatchMolIn>&
     FC_TRY(batch_alloc(b, seg.size() * 8, &vseg));
     FC_TRY(batch_alloc(b, (size_t)items * sizeof(int4), &vitems));
     FC_TRY(batch_alloc(b, (size_t)items * 16, &vpart));
-    FC_CUDA(cudaMemset(vbt, 0, (size_t)rows * q_pad * 2));
+    FC_CUDA(cudaMemset(vbt, 0, (size_t)rows * q_pad));
     void *vocc = nullptr, *vvir = nullptr, *vqs = nullptr, *vbq = nullptr, *vgws = nullptr;
     void *vgm = nullptr, *vmaps = nullptr, *vgit = nullptr;
     std::vector<int4> git;
@@ -1814,11 +1860,11 @@ fc_status rimp2_batch_build_fx(fc_rimp2_batch* b, const std::vector<BatchMolIn>&
         FC_TRY(batch_alloc(b, (size_t)items * 8, &vocc));
         FC_TRY(batch_alloc(b, gvir, &vvir));
         FC_TRY(batch_alloc(b, (size_t)nqs * 8, &vqs));
-        FC_TRY(batch_alloc(b, (size_t)nbq * 2, &vbq));
+        FC_TRY(batch_alloc(b, (size_t)nbq, &vbq));
         FC_TRY(batch_alloc(b, gws, &vgws));
         FC_TRY(batch_alloc(b, (size_t)nmol * sizeof(GemmMol), &vgm));
         FC_TRY(batch_alloc(b, (size_t)nmol * 2 * sizeof(CUtensorMap), &vmaps));
-        FC_CUDA(cudaMemset(vbq, 0, (size_t)nbq * 2));
+        FC_CUDA(cudaMemset(vbq, 0, (size_t)nbq));
     }
     // per-molecule pointers
     std::vector<CUtensorMap> maps(grad ? 2 * nmol : 0);
@@ -1827,7 +1873,7 @@ fc_status rimp2_batch_build_fx(fc_rimp2_batch* b, const std::vector<BatchMolIn>&
         BatchPrep& x = hp[m];
         x.cmax = (unsigned long long*)vcmax + cmax_off[m];
         x.scl = (double*)vscl + scl_off[m];
-        x.bt = (__nv_bfloat16*)vbt + (int64_t)hm[m].row0 * q_pad;
+        x.bt = (int8_t*)vbt + (int64_t)hm[m].row0 * q_pad;
         hm[m].eo = mols[m].eps_occ;
         hm[m].ev = mols[m].eps_vir;
         hm[m].scl = x.scl;
@@ -1843,12 +1889,12 @@ fc_status rimp2_batch_build_fx(fc_rimp2_batch* b, const std::vector<BatchMolIn>&
             char* g0 = (char*)vgws + t_off[m];
             x.T = (float*)g0;
             x.ts = (double*)(g0 + rup(x.ldt * x.ldt * 4, 256));
-            x.Ts = (__nv_bfloat16*)(g0 + rup(x.ldt * x.ldt * 4, 256) + rup(x.M * 8, 256));
+            x.Ts = (int8_t*)(g0 + rup(x.ldt * x.ldt * 4, 256) + rup(x.M * 8, 256));
             x.qs = (double*)vqs + qs_off[m];
-            x.bq = (__nv_bfloat16*)vbq + bq_off[m];
+            x.bq = (int8_t*)vbq + bq_off[m];
             hm[m].T = x.T;
-            FC_TRY(make_tmap_bf16_2d(&maps[2 * m], x.Ts, x.ldt, 3 * x.M, x.ldt * 2, fx::KT, 128));
-            FC_TRY(make_tmap_bf16_2d(&maps[2 * m + 1], x.bq, x.ldt, 3 * x.q_rows, x.ldt * 2, fx::KT, 128));
+            FC_TRY(make_tmap_i8_2d(&maps[2 * m], x.Ts, x.ldt, 3 * x.M, x.ldt, fx::KT, 128));
+            FC_TRY(make_tmap_i8_2d(&maps[2 * m + 1], x.bq, x.ldt, 3 * x.q_rows, x.ldt, fx::KT, 128));
             GemmMol& g = gm[m];
             g.tA = (const CUtensorMap*)vmaps + 2 * m;
             g.tB = (const CUtensorMap*)vmaps + 2 * m + 1;
@@ -1896,8 +1942,8 @@ fc_status rimp2_batch_build_fx(fc_rimp2_batch* b, const std::vector<BatchMolIn>&
     FC_CUDA(cudaMemcpy(vseg, seg.data(), seg.size() * 8, cudaMemcpyHostToDevice));
     FC_CUDA(cudaMemcpy(vitems, hi.data(), hi.size() * sizeof(int4), cudaMemcpyHostToDevice));
     CUtensorMap tmA, tmB;
-    FC_TRY(make_tmap_bf16_2d(&tmA, vbt, q_pad, rows, q_pad * 2, fx::KT, fx::BM));
-    FC_TRY(make_tmap_bf16_2d(&tmB, vbt, q_pad, rows, q_pad * 2, fx::KT, fx::BN));
+    FC_TRY(make_tmap_i8_2d(&tmA, vbt, q_pad, rows, q_pad, fx::KT, fx::BM));
+    FC_TRY(make_tmap_i8_2d(&tmB, vbt, q_pad, rows, q_pad, fx::KT, fx::BN));
     FC_CUDA(cudaDeviceSynchronize());
 
     // ---- the recorded sequence

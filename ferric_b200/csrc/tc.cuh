@@ -196,6 +196,31 @@ __host__ __device__ constexpr uint32_t idesc_bf16_f32(int m, int n) {
            | ((uint32_t)(m >> 4) << 24);   // M / 16
 }
 
+// Instruction descriptor: signed int8 x signed int8 -> int32, both operands K-major.
+__host__ __device__ constexpr uint32_t idesc_i8_s32(int m, int n) {
+    return (2u << 4)                       // D format S32
+           | (1u << 7)                     // A format signed 8-bit
+           | (1u << 10)                    // B format signed 8-bit
+           | ((uint32_t)(n >> 3) << 17)    // N / 8
+           | ((uint32_t)(m >> 4) << 24);   // M / 16
+}
+
+// D[128 x N] (+)= A[128 x 32] B[N x 32]^T in exact int32 (K = 32 bytes of
+// each operand row per instruction).
+__device__ __forceinline__ void umma_i8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                        uint32_t accumulate) {
+    asm volatile(
+        "{ .reg .pred p; setp.ne.b32 p, %4, 0; "
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p; }" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
+// Exact int32 (a TMEM word) -> double on the FP64 pipe:
+// (2^52 + 2^31 + i) - (2^52 + 2^31).
+__device__ __forceinline__ double i32_to_f64(float word) {
+    return __hiloint2double(0x43300000, __float_as_int(word) ^ (int)0x80000000) - 4503601774854144.0;
+}
+
 __device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
                                           uint32_t accumulate) {
     asm volatile(

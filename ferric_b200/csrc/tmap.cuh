@@ -8,4 +8,7 @@ namespace fc {
 // `outer` rows `row_bytes` apart, boxes of box_inner x box_outer.
 fc_status make_tmap_bf16_2d(CUtensorMap* map, const void* base, uint64_t inner, uint64_t outer,
                             uint64_t row_bytes, uint32_t box_inner, uint32_t box_outer);
+// The same for 8-bit elements (the int8 integer slices).
+fc_status make_tmap_i8_2d(CUtensorMap* map, const void* base, uint64_t inner, uint64_t outer, uint64_t row_bytes,
+                          uint32_t box_inner, uint32_t box_outer);
 }  // namespace fc

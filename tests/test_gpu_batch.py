@@ -17,7 +17,12 @@ from oracle import synthetic
 pytestmark = pytest.mark.gpu
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-MIXED_E_REL = 5e-8
+# Energy bound of the split: each element of G carries 23-24 bits relative
+# to its row maximum, so for small systems, where a few elements dominate E,
+# E's relative error reaches ~2.6e-7 (largest of 120 seeded random systems
+# of 2-4 occupied orbitals; either integer-slice format, emulated exactly);
+# large systems sit near 1e-10.
+MIXED_E_REL = 3e-7
 MIXED_G_REL = 1e-5
 MIXED_D_REL = 1e-6
 MIXED_E_ABS = 1e-12  # Eh, tiny systems
