@@ -149,6 +149,30 @@ def measured_peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
 
 
+def measure_i8_tops(torch, dev, seconds=2.0):
+    """Int8 tensor peak for the integer-slice kernels: cuBLAS int8 GEMM
+    (torch._int_mm, 8192^3, int32 accumulation) back to back for `seconds`
+    (sustained under the power cap, like the kernels it is compared with)."""
+    g = torch.Generator(device=dev).manual_seed(5)
+    a = torch.randint(-127, 128, (8192, 8192), generator=g, device=dev, dtype=torch.int8)
+    b = torch.randint(-127, 128, (8192, 8192), generator=g, device=dev, dtype=torch.int8).t()
+    for _ in range(3):
+        torch._int_mm(a, b)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    torch._int_mm(a, b)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    reps = max(3, int(seconds * 1e3 / max(e0.elapsed_time(e1), 1e-3)))
+    e0.record()
+    for _ in range(reps):
+        torch._int_mm(a, b)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    return 2.0 * 8192 ** 3 * reps / (e0.elapsed_time(e1) * 1e-3) / 1e12
+
+
 def measure_dgemm_tflops(torch, dev):
     """FP64 peak for the plain set: cuBLAS DGEMM 8192^3, best of 5 (CUDA events)."""
     a = torch.randn((8192, 8192), device=dev, dtype=torch.float64)
@@ -509,12 +533,18 @@ def main():
         peak = measure_dgemm_tflops(torch, dev)
         peak_note = "measured in this run: cuBLAS DGEMM 8192^3 (FP64 tensor path)"
         achieved = flops_per_launch / (avg_launch_ms * 1e-3) / 1e12
+    elif prec == "mixed":
+        peak = measure_i8_tops(torch, dev)
+        peak_note = ("measured in this run: cuBLAS int8 GEMM 8192^3 sustained (torch._int_mm); "
+                     f"executed = {executed} x algorithmic int8 ops")
+        achieved = executed * flops_per_launch / (avg_launch_ms * 1e-3) / 1e12
     else:
         peak = peaks.get("bf16_tflops_sustained", peaks["bf16_tflops"])
         peak_note = f"{peak_src} bf16 dense (sustained), executed = {executed} x algorithmic flops"
         achieved = executed * flops_per_launch / (avg_launch_ms * 1e-3) / 1e12
     roofline = {"bound": "tensor", "kernel": "rimp2 pair kernel (fused G_ij + denominator epilogue)",
-                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "achieved": achieved, "peak": peak, "unit": "TOP/s" if prec == "mixed" else "TFLOP/s",
+                "frac": achieved / peak,
                 "peak_source": peak_note, "flops_per_launch": flops_per_launch,
                 "avg_launch_ms": avg_launch_ms,
                 "traffic": read_traffic(f"rimp2_pair_{prec}")}
@@ -622,7 +652,7 @@ def main():
             "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": {"f64": "f64",
-                      "mixed": "bf16 x3 integer slices, 6 products, exact f32 accumulation, f64 epilogue"}[prec],
+                      "mixed": "int8 x3 integer slices, 6 products, exact int32 accumulation, f64 epilogue"}[prec],
             "precision": prec, "dfj_precision": dfj_prec, "dfk_precision": dfk_prec,
             "data": "synthetic (seeded, generated on device)", "config": config,
             "components_ms": {"rimp2_e_grad": last["rimp2"]["kernel_ms"], "dfj": last["dfj"]["kernel_ms"],
