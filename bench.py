@@ -455,7 +455,7 @@ def main():
     prec = args.precision
     if prec == "auto":
         prec = os.environ.get("FERRIC_BENCH_PRECISION", "mixed")
-        try:  # the split-BF16 kernels; FP64 plain when this build has none
+        try:  # the integer-slice kernels; FP64 plain when this build has none
             tb = torch.zeros((64, 2), dtype=torch.float64, device=dev)
             rimp2.rimp2_energy(tb, torch.zeros(1, dtype=torch.float64, device=dev) - 1,
                                torch.ones(2, dtype=torch.float64, device=dev), precision=prec)

@@ -244,7 +244,7 @@ fc_status fc_rimp2_batched_create(const fc_mol_desc* mols, int64_t nmol, int32_t
     *out = nullptr;
     if (precision != FC_PREC_MIXED)
         return fail(FC_ERR_KERNEL,
-                    "fc_rimp2_batched_create: the batched launch runs the split-BF16 exact-slice kernels "
+                    "fc_rimp2_batched_create: the batched launch runs the exact integer-slice kernels "
                     "(FC_PREC_MIXED) only; call fc_rimp2_energy_grad_dev per molecule for FP64");
     if (nmol > (1 << 30)) return fail(FC_ERR_LAYOUT, "fc_rimp2_batched_create: too many molecules");
     int with_grad = -1;

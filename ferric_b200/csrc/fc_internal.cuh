@@ -57,8 +57,8 @@ enum WsSlot {
     WS_OUT,        // small results and error flags
     WS_T,          // amplitude chunk (FP64 or FP32) + row scales
     WS_TS,         // amplitude chunk slices
-    WS_SPLIT,      // split-BF16 pair operands
-    WS_SPLIT2,     // split-BF16 adjoint operand (Q rows)
+    WS_SPLIT,      // integer-slice pair operands
+    WS_SPLIT2,     // integer-slice adjoint operand (Q rows)
     WS_SCALE,      // column maxima + operand-row scales
     WS_MISC,       // DF-J weights / d_P, DF-K C^T
     WS_COUNT

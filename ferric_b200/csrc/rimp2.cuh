@@ -30,8 +30,8 @@ fc_status rimp2_grad_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, doubl
                          double* gamma, double* de_docc, double* de_dvir, fc_stats* stats,
                          const GammaSink* sink = nullptr);
 
-// Split-BF16 (tcgen05) kernel sets.  _fx: integer-valued slices with exact
-// FP32 accumulation (FC_PREC_MIXED).  _mixed: floating hi+lo split, 3
+// Tensor-core (tcgen05) kernel sets.  _fx: int8 integer slices with exact
+// int32 accumulation (FC_PREC_MIXED).  _mixed: floating bf16 hi+lo split, 3
 // products, FP32 accumulation (FC_PREC_MIXED_FAST; energy only).
 fc_status rimp2_energy_mixed(const Rimp2Dev& d, int terms, cudaStream_t st, double* e_os,
                              double* e_ss, fc_stats* stats);

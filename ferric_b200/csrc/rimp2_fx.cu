@@ -1281,7 +1281,7 @@ int fx_exchange_choice(int nk, int grad) {
 
 fc_status rimp2_energy_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double* e_ss, fc_stats* stats) {
     FC_TRY(fx_attrs());
-    if (d.nocc > (1 << 15)) return fail(FC_ERR_LAYOUT, "split-BF16: nocc too large");
+    if (d.nocc > (1 << 15)) return fail(FC_ERR_LAYOUT, "mixed RI-MP2: nocc too large");
     void* vout;
     FC_TRY(ws_get(WS_OUT, 256, &vout));
     double* out = (double*)vout;
@@ -1340,8 +1340,8 @@ fc_status rimp2_energy_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, doub
     FC_CUDA(cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, st));
     FC_CUDA(cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, st));
     FC_CUDA(cudaStreamSynchronize(st));
-    if (hf[0]) return fail(FC_ERR_RANGE, "split-BF16: B_ov has a non-finite element");
-    if (hf[1]) return fail(FC_ERR_TIMEOUT, "split-BF16 pair kernel: a pipeline wait ran out");
+    if (hf[0]) return fail(FC_ERR_RANGE, "mixed RI-MP2: B_ov has a non-finite element");
+    if (hf[1]) return fail(FC_ERR_TIMEOUT, "mixed pair kernel: a pipeline wait ran out");
     *e_os = h[0];
     *e_ss = h[1];
     if (stats) {
@@ -1368,7 +1368,7 @@ fc_status rimp2_energy_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, doub
 fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double* e_ss, double* gamma,
                         double* de_docc, double* de_dvir, fc_stats* stats, const GammaSink* sink) {
     FC_TRY(fx_attrs());
-    if (d.nocc > (1 << 15)) return fail(FC_ERR_LAYOUT, "split-BF16: nocc too large");
+    if (d.nocc > (1 << 15)) return fail(FC_ERR_LAYOUT, "mixed RI-MP2: nocc too large");
     const int64_t nocc = d.nocc, nvir = d.nvir, naux = d.naux, nov = nocc * nvir;
     Context& c = ctx();
     FxSplit sp;
@@ -1550,8 +1550,8 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
     FC_CUDA(cudaMemcpyAsync(h.data(), e_cp, h.size() * 8, cudaMemcpyDeviceToHost, st));
     FC_CUDA(cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, st));
     FC_CUDA(cudaStreamSynchronize(st));
-    if (hf[0]) return fail(FC_ERR_RANGE, "split-BF16: B_ov has a non-finite element");
-    if (hf[1]) return fail(FC_ERR_TIMEOUT, "split-BF16 gradient kernels: a pipeline wait ran out");
+    if (hf[0]) return fail(FC_ERR_RANGE, "mixed RI-MP2: B_ov has a non-finite element");
+    if (hf[1]) return fail(FC_ERR_TIMEOUT, "mixed gradient kernels: a pipeline wait ran out");
     double eo = 0.0, co = 0.0, es = 0.0, cs2 = 0.0;  // Neumaier sums over the chunk pairs
     for (int64_t x = 0; x < ncp; ++x) {
         double v = h[2 * x], t = eo + v;
@@ -1716,7 +1716,7 @@ fc_status ump2_cross_fx(const UmpSpin& A, const UmpSpin& Bs, int64_t naux, cudaS
     FC_CUDA(cudaMemcpyAsync(h, res, sizeof(h), cudaMemcpyDeviceToHost, st));
     FC_CUDA(cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, st));
     FC_CUDA(cudaStreamSynchronize(st));
-    if (hf[0]) return fail(FC_ERR_RANGE, "split-BF16: B_ov has a non-finite element");
+    if (hf[0]) return fail(FC_ERR_RANGE, "mixed RI-MP2: B_ov has a non-finite element");
     if (hf[1]) return fail(FC_ERR_TIMEOUT, "opposite-spin GEMM: a pipeline wait ran out");
     *e_ab = h[0] + h[1];
     if (stats) {

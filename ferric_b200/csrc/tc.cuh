@@ -1,6 +1,6 @@
-// Blackwell (sm_100a) tensor-core plumbing for the split-BF16 kernels:
+// Blackwell (sm_100a) tensor-core plumbing for the integer-slice kernels:
 // mbarriers with time-bounded waits, TMA tile loads, TMEM allocation and
-// loads, UMMA (tcgen05.mma kind::f16) issue and commit, descriptors.
+// loads, UMMA (tcgen05.mma kind::f16 and kind::i8) issue and commit, descriptors.
 //
 // Every wait is bounded by the global timer: a wait that runs out sets the
 // kernel's error word and the CTA-wide abort flag, and the roles leave their

@@ -34,16 +34,19 @@ typedef int32_t fc_status;
 #define FC_ERR_LAYOUT     5  /* GpuError::Layout: bad shape, size or overflow      */
 #define FC_ERR_CUDA       6  /* GpuError::Cuda: a CUDA call failed                 */
 #define FC_ERR_KERNEL     7  /* GpuError::Kernel: kernel image or launch refused   */
-#define FC_ERR_RANGE      8  /* GpuError::F32Range: operand outside split-BF16 range*/
+#define FC_ERR_RANGE      8  /* GpuError::F32Range: operand outside the mixed range*/
 #define FC_ERR_TIMEOUT    9  /* a bounded device wait ran out                      */
 #define FC_ERR_INVALID   10  /* null pointer, bad enum, library not initialised   */
 
 /* Arithmetic of the contraction kernels. */
 #define FC_PREC_F64        0  /* all-FP64 "plain" kernels: the drop-in             */
-#define FC_PREC_MIXED      1  /* split-BF16, exact accumulation: each operand row   */
-                              /* scaled by a power of two and split into 3 bf16    */
-                              /* slices holding integers; 6 tensor-core products   */
-                              /* into 3 FP32 accumulators that never round         */
+#define FC_PREC_MIXED      1  /* exact integer slices: each operand row scaled by  */
+                              /* a power of two and split into 3 integer slices;   */
+                              /* 6 tensor-core products into 3 accumulators that   */
+                              /* never round.  RI-MP2 pair/adjoint kernels: int8   */
+                              /* slices, int32 sums (tcgen05 kind::i8); DF-K,      */
+                              /* dressing, Imat: bf16 slices, FP32 sums drained    */
+                              /* to FP64 before they could round                   */
 #define FC_PREC_MIXED_FAST 2  /* split-BF16 hi+lo, 3 products, FP32 accumulation   */
                               /* (energy only; ~1e-5 relative, accumulation-bound) */
 
