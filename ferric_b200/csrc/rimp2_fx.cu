@@ -22,9 +22,11 @@
 //
 // Pair kernel (this file): item = (pair, a-tile 128, b-tile 128); the X phase
 // accumulates (ia|jb) into the three level accumulators (3 x 128 TMEM
-// columns), the epilogue parks it in registers (FP32, round to nearest), and
-// the Y phase accumulates (ib|ja) = G_ji[a, b] into the same columns, so each
-// thread holds an element and its exchange partner.  Energy mode: unordered
+// columns), the epilogue parks it in FP32 (round to nearest) in the spare
+// TMEM columns 384..511, the Y phase accumulates (ib|ja) = G_ji[a, b] into
+// the level columns, and the epilogue takes Y into registers (FP32) and hands
+// the level columns back before its FP64 work, which then runs under the
+// next item's X phase; each thread holds an element and its exchange partner.  Energy mode: unordered
 // pairs, E_OS += (X^2 + Y^2)/D, E_SS += (X - Y)^2/D (i == j: X phase only,
 // E_SS = 0), the reference pair loop of ferric-mp2/src/rimp2.rs:1399-1544
 // over both orderings.  Gradient mode: unordered pairs of an occupied chunk
@@ -471,13 +473,21 @@ __global__ void __launch_bounds__(320, 1)
             const double* syb = colb + 2 * BN + h * HC;
             const int bmax = v.nvir - b0;    // columns c < bmax are real virtuals
 
-            // X phase: park (ia|jb) of this half row in registers (FP32, round to nearest).
+            // X phase: park (ia|jb) of this half row in FP32 (round to nearest).
             // One thread waits (bounded); the 256 epilogue threads leave together
             // if it gave up, since named barriers follow.
             if (!tc::bar_and<1, 256>(et != 0 || tc::mbar_wait(tfull, pc & 1, abort_flag, p.err))) break;
             if (et != 0) tc::mbar_wait(tfull, pc & 1, abort_flag, p.err);  // phase complete: returns at once
             tc::fence_after_sync();
-            float xr[HC];
+            const bool xt = v.xt;          // the same for every thread of the CTA
+            const bool two = !diag && !xt;  // a Y phase follows in TMEM
+            // pk: this thread's 64 parked values -- X of a one-phase item, Y of a
+            // two-phase item (whose X waits in TMEM columns 3 BN + h HC .., beyond
+            // the three levels the MMAs write) -- then its column terms.  Both
+            // phases of a two-phase item are out of the level columns before the
+            // heavy FP64 work below, which runs under the next item's X phase.
+            float pk[HC];
+            const uint32_t tpk = tmem_base + ((uint32_t)(q * 32) << 16) + 3 * BN + h * HC;
 #pragma unroll
             for (int c0 = 0; c0 < HC; c0 += 16) {
                 float l0[16], l1[16], l2[16];
@@ -486,27 +496,42 @@ __global__ void __launch_bounds__(320, 1)
                 tc::tmem_ld16(tl + 2 * BN + c0, l2);
                 tc::tmem_wait_ld();
 #pragma unroll
-                for (int cc = 0; cc < 16; ++cc) xr[c0 + cc] = (float)level_value(l0[cc], l1[cc], l2[cc], sxa * sxb[c0 + cc]);
+                for (int cc = 0; cc < 16; ++cc) pk[c0 + cc] = (float)level_value(l0[cc], l1[cc], l2[cc], sxa * sxb[c0 + cc]);
+                if (two) tc::tmem_st16(tpk + c0, pk + c0);
             }
+            if (two) tc::tmem_wait_st();
             tc::fence_before_sync();
             tc::mbar_arrive(tempty);
             ++pc;
-            const bool xt = v.xt;          // the same for every thread of the CTA
-            const bool two = !diag && !xt;  // a Y phase follows in TMEM
             if (two) {
+                // Y phase: (ib|ja) = G_ji[a, b] of this half row, FP32 like X
                 if (!tc::bar_and<1, 256>(et != 0 || tc::mbar_wait(tfull, pc & 1, abort_flag, p.err))) break;
                 if (et != 0) tc::mbar_wait(tfull, pc & 1, abort_flag, p.err);
                 tc::fence_after_sync();
+#pragma unroll
+                for (int c0 = 0; c0 < HC; c0 += 16) {
+                    float l0[16], l1[16], l2[16];
+                    tc::tmem_ld16(tl + c0, l0);
+                    tc::tmem_ld16(tl + BN + c0, l1);
+                    tc::tmem_ld16(tl + 2 * BN + c0, l2);
+                    tc::tmem_wait_ld();
+#pragma unroll
+                    for (int cc = 0; cc < 16; ++cc)
+                        pk[c0 + cc] = (float)level_value(l0[cc], l1[cc], l2[cc], sya * syb[c0 + cc]);
+                }
+                tc::fence_before_sync();
+                tc::mbar_arrive(tempty);  // the level columns are free for the next item
+                ++pc;
             }
             // plain FP64 sums over this thread's 64 terms (relative error <= 64 u);
             // the tile partials are summed compensated
             double os = 0.0, ss = 0.0, oc = 0.0, rowc = 0.0;
             // the terms of this thread's columns c0 .. c0 + 7, given their Y values
-            auto proc8 = [&](const int c0, const double (&yv)[8]) {
+            auto proc8 = [&](const int c0, const float (&xv)[8], const double (&yv)[8]) {
                 float tt8[8], mv8[8];
 #pragma unroll
                 for (int cc = 0; cc < 8; ++cc) {
-                    const double x = (double)xr[c0 + cc];
+                    const double x = (double)xv[cc];
                     const double y = yv[cc];
                     float tval = 0.f, mval = 0.f, colv = 0.f;
                     if (va && c0 + cc < bmax) {
@@ -544,7 +569,7 @@ __global__ void __launch_bounds__(320, 1)
                     }
                     tt8[cc] = tval;
                     mv8[cc] = mval;
-                    if (GRAD && !xt) xr[c0 + cc] = colv;  // x of this column is consumed: keep cm there
+                    if (GRAD && !xt) pk[c0 + cc] = colv;  // this column's value is consumed: keep cm there
                 }
                 if (GRAD && a < v.tpad) {
                     // amplitude rows (i, a) and columns (j, b) at pitch tpad (>= nvir);
@@ -591,26 +616,19 @@ __global__ void __launch_bounds__(320, 1)
             if (!xt) {
 #pragma unroll
                 for (int c0 = 0; c0 < HC; c0 += 8) {
+                    float xv[8];
                     double yv[8];
                     if (two) {
-                        float y0[8], y1[8], y2[8];
-                        tc::tmem_ld8(tl + c0, y0);
-                        tc::tmem_ld8(tl + BN + c0, y1);
-                        tc::tmem_ld8(tl + 2 * BN + c0, y2);
+                        tc::tmem_ld8(tpk + c0, xv);  // X back from its TMEM columns
                         tc::tmem_wait_ld();
-                        if (c0 + 8 == HC) {  // every level of this phase is read: release TMEM
-                            tc::fence_before_sync();
-                            tc::mbar_arrive(tempty);
-                        }
-#pragma unroll
-                        for (int cc = 0; cc < 8; ++cc) yv[cc] = level_value(y0[cc], y1[cc], y2[cc], sya * syb[c0 + cc]);
                     } else {
 #pragma unroll
-                        for (int cc = 0; cc < 8; ++cc) yv[cc] = (double)xr[c0 + cc];
+                        for (int cc = 0; cc < 8; ++cc) xv[cc] = pk[c0 + cc];  // i == j: Y = X
                     }
-                    proc8(c0, yv);
+#pragma unroll
+                    for (int cc = 0; cc < 8; ++cc) yv[cc] = (double)pk[c0 + cc];
+                    proc8(c0, xv, yv);
                 }
-                if (two) ++pc;
             } else {
                 // Y = X^T inside a diagonal tile: in round r the parked X of lane
                 // quarter r passes through shared memory, and the threads whose 64
@@ -620,25 +638,33 @@ __global__ void __launch_bounds__(320, 1)
                 for (int r = 0; r < 4; ++r) {
                     if (q == r) {
 #pragma unroll
-                        for (int c = 0; c < HC; ++c) xbuf[lane * XP + h * HC + c] = xr[c];
+                        for (int c = 0; c < HC; ++c) xbuf[lane * XP + h * HC + c] = pk[c];
                     }
                     asm volatile("bar.sync 1, 256;" ::: "memory");
                     if (h == (r >> 1)) {
                         if (r & 1) {
 #pragma unroll
                             for (int c0 = 0; c0 < 32; c0 += 8) {
+                                float xv[8];
                                 double yv[8];
 #pragma unroll
-                                for (int cc = 0; cc < 8; ++cc) yv[cc] = (double)xbuf[(c0 + cc) * XP + row];
-                                proc8(32 + c0, yv);
+                                for (int cc = 0; cc < 8; ++cc) {
+                                    xv[cc] = pk[32 + c0 + cc];
+                                    yv[cc] = (double)xbuf[(c0 + cc) * XP + row];
+                                }
+                                proc8(32 + c0, xv, yv);
                             }
                         } else {
 #pragma unroll
                             for (int c0 = 0; c0 < 32; c0 += 8) {
+                                float xv[8];
                                 double yv[8];
 #pragma unroll
-                                for (int cc = 0; cc < 8; ++cc) yv[cc] = (double)xbuf[(c0 + cc) * XP + row];
-                                proc8(c0, yv);
+                                for (int cc = 0; cc < 8; ++cc) {
+                                    xv[cc] = pk[c0 + cc];
+                                    yv[cc] = (double)xbuf[(c0 + cc) * XP + row];
+                                }
+                                proc8(c0, xv, yv);
                             }
                         }
                     }
@@ -656,19 +682,19 @@ __global__ void __launch_bounds__(320, 1)
             if (GRAD && h == 1) rowsh[row] = rowc;
             if ((mir || both) && !xt) {
                 // column sums of the mirrored terms over this warp's 32 rows: a
-                // reduce-scatter butterfly leaves columns 2*lane, 2*lane+1 in xr[0..1]
+                // reduce-scatter butterfly leaves columns 2*lane, 2*lane+1 in pk[0..1]
 #pragma unroll
                 for (int half = HC / 2, off = 16; off > 0; half >>= 1, off >>= 1) {
                     const bool up = (lane & off) != 0;
 #pragma unroll
                     for (int c = 0; c < half; ++c) {
-                        const float send = up ? xr[c] : xr[c + half];
+                        const float send = up ? pk[c] : pk[c + half];
                         const float recv = __shfl_xor_sync(0xffffffffu, send, off);
-                        xr[c] = (up ? xr[c + half] : xr[c]) + recv;
+                        pk[c] = (up ? pk[c + half] : pk[c]) + recv;
                     }
                 }
-                colsh[(q * 2 + h) * 64 + 2 * lane] = (double)xr[0];
-                colsh[(q * 2 + h) * 64 + 2 * lane + 1] = (double)xr[1];
+                colsh[(q * 2 + h) * 64 + 2 * lane] = (double)pk[0];
+                colsh[(q * 2 + h) * 64 + 2 * lane + 1] = (double)pk[1];
             }
             asm volatile("bar.sync 1, 256;" ::: "memory");
             if (GRAD && h == 0) p.vir_part[k * 2 * BM + row] = rowc + rowsh[row];

@@ -64,9 +64,10 @@ def energy_from_g(g, eo, ev, tile=128, xt=False):
     """The device's energy from the exact level sums.  Per pair i <= j the
     device visits 128 x 128 tiles (ta, tb) with ta <= tb (weight 2 off the tile
     diagonal: the summands are symmetric under a <-> b); in each the X element
-    (ia|jb) is parked in FP32 (round to nearest) between the two tensor-core
-    phases and the Y element (ib|ja) stays FP64; i == j uses X only.  With the
-    exchange (xt) a diagonal tile's Y is the parked X transposed (FP32)."""
+    (ia|jb) and the Y element (ib|ja) are held in FP32 (round to nearest)
+    between the tensor-core phases and the FP64 epilogue; i == j uses X only.
+    With the exchange (xt) a diagonal tile's Y is the parked X transposed, the
+    same FP32 values."""
     nocc, nvir = len(eo), len(ev)
     nt = (nvir + tile - 1) // tile
     e_os = e_ss = 0.0
@@ -84,9 +85,7 @@ def energy_from_g(g, eo, ev, tile=128, xt=False):
                     if i == j:
                         e_os += w * np.sum(x * x / d)
                     else:
-                        y = gy[sa, sb]
-                        if xt and ta == tb:
-                            y = y.astype(np.float32).astype(np.float64)
+                        y = gy[sa, sb].astype(np.float32).astype(np.float64)
                         e_os += w * np.sum((x * x + y * y) / d)
                         e_ss += w * np.sum((x - y) ** 2 / d)
     return e_os, e_ss
