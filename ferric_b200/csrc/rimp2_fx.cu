@@ -486,6 +486,11 @@ __global__ void __launch_bounds__(320, 1)
             // the three levels the MMAs write) -- then its column terms.  Both
             // phases of a two-phase item are out of the level columns before the
             // heavy FP64 work below, which runs under the next item's X phase.
+            // Batched items (small molecules, phases of a few k-steps) are
+            // epilogue-bound: there X stays in registers and Y streams out of
+            // the level columns group by group (measured 8% faster for the
+            // 512-molecule batch), the same FP32 values either way.
+            constexpr bool PARK = !BATCH;
             float pk[HC];
             const uint32_t tpk = tmem_base + ((uint32_t)(q * 32) << 16) + 3 * BN + h * HC;
 #pragma unroll
@@ -497,9 +502,9 @@ __global__ void __launch_bounds__(320, 1)
                 tc::tmem_wait_ld();
 #pragma unroll
                 for (int cc = 0; cc < 16; ++cc) pk[c0 + cc] = (float)level_value(l0[cc], l1[cc], l2[cc], sxa * sxb[c0 + cc]);
-                if (two) tc::tmem_st16(tpk + c0, pk + c0);
+                if (PARK && two) tc::tmem_st16(tpk + c0, pk + c0);
             }
-            if (two) tc::tmem_wait_st();
+            if (PARK && two) tc::tmem_wait_st();
             tc::fence_before_sync();
             tc::mbar_arrive(tempty);
             ++pc;
@@ -508,6 +513,8 @@ __global__ void __launch_bounds__(320, 1)
                 if (!tc::bar_and<1, 256>(et != 0 || tc::mbar_wait(tfull, pc & 1, abort_flag, p.err))) break;
                 if (et != 0) tc::mbar_wait(tfull, pc & 1, abort_flag, p.err);
                 tc::fence_after_sync();
+            }
+            if (PARK && two) {
 #pragma unroll
                 for (int c0 = 0; c0 < HC; c0 += 16) {
                     float l0[16], l1[16], l2[16];
@@ -618,17 +625,36 @@ __global__ void __launch_bounds__(320, 1)
                 for (int c0 = 0; c0 < HC; c0 += 8) {
                     float xv[8];
                     double yv[8];
-                    if (two) {
+                    if (PARK && two) {
                         tc::tmem_ld8(tpk + c0, xv);  // X back from its TMEM columns
                         tc::tmem_wait_ld();
+#pragma unroll
+                        for (int cc = 0; cc < 8; ++cc) yv[cc] = (double)pk[c0 + cc];
+                    } else if (two) {
+                        float y0[8], y1[8], y2[8];
+                        tc::tmem_ld8(tl + c0, y0);
+                        tc::tmem_ld8(tl + BN + c0, y1);
+                        tc::tmem_ld8(tl + 2 * BN + c0, y2);
+                        tc::tmem_wait_ld();
+                        if (c0 + 8 == HC) {  // every level of this phase is read: release TMEM
+                            tc::fence_before_sync();
+                            tc::mbar_arrive(tempty);
+                        }
+#pragma unroll
+                        for (int cc = 0; cc < 8; ++cc) {
+                            xv[cc] = pk[c0 + cc];
+                            yv[cc] = (double)(float)level_value(y0[cc], y1[cc], y2[cc], sya * syb[c0 + cc]);
+                        }
                     } else {
 #pragma unroll
-                        for (int cc = 0; cc < 8; ++cc) xv[cc] = pk[c0 + cc];  // i == j: Y = X
+                        for (int cc = 0; cc < 8; ++cc) {
+                            xv[cc] = pk[c0 + cc];  // i == j: Y = X
+                            yv[cc] = (double)pk[c0 + cc];
+                        }
                     }
-#pragma unroll
-                    for (int cc = 0; cc < 8; ++cc) yv[cc] = (double)pk[c0 + cc];
                     proc8(c0, xv, yv);
                 }
+                if (!PARK && two) ++pc;
             } else {
                 // Y = X^T inside a diagonal tile: in round r the parked X of lane
                 // quarter r passes through shared memory, and the threads whose 64
@@ -1034,27 +1060,39 @@ __global__ void scale_copy_kernel(const double* __restrict__ x, int64_t n, doubl
 
 // acc_vir[v] += 2 * (sum over the launch's items of the row-virtual partials
 // of v (v in the a-tile) and of the column-virtual partials (v in the b-tile;
-// present for mirrored tiles and for pairs i < j)).  Fixed order.
-__global__ void __launch_bounds__(256) fx_reduce_vir_kernel(const double* __restrict__ vir_part,
-                                                            const int2* __restrict__ pairs,
-                                                            const int2* __restrict__ tiles, int64_t npairs,
-                                                            int ntiles, int nvir, double* acc_vir) {
-    const int v = blockIdx.x * 8 + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
-    if (v >= nvir) return;
-    const int tv = v / fx::BM, rv = v % fx::BM;
-    const int64_t nterm = npairs * ntiles;
+// present for mirrored tiles and for pairs i < j)), in two coalesced
+// fixed-order passes.  Pass 1: one block per (virtual
+// tile tv, chunk of pairs), one thread per virtual of the tile; for each pair
+// of the chunk in order it visits only the tile pairs that hold tv -- (tv, tb)
+// for the row part, (ta, tv) for the column part -- and reads their 128
+// partials as one 1 KB row.  Tile pairs are numbered ta-major with tb >= ta.
+// Pass 2 folds the chunks in order.
+__global__ void __launch_bounds__(128) fx_reduce_vir_part_kernel(const double* __restrict__ vir_part,
+                                                                 const int2* __restrict__ pairs, int64_t npairs,
+                                                                 int nT, int ntiles, int64_t pairs_per_chunk,
+                                                                 double* __restrict__ out) {
+    const int tv = blockIdx.x, rv = threadIdx.x;
+    const int64_t p0 = (int64_t)blockIdx.y * pairs_per_chunk;
+    const int64_t p1 = p0 + pairs_per_chunk < npairs ? p0 + pairs_per_chunk : npairs;
+    auto tidx = [&](int ta, int tb) { return ta * nT - ta * (ta - 1) / 2 + (tb - ta); };
     KSum s;
-    for (int64_t k = lane; k < nterm; k += 32) {
-        const int2 t = tiles[k % ntiles];
-        if (t.x == tv) s.add(vir_part[k * 2 * fx::BM + rv]);
-        if (t.y == tv) {
-            const int2 pr = pairs[k / ntiles];
-            if (t.x < t.y || pr.x != pr.y) s.add(vir_part[k * 2 * fx::BM + fx::BM + rv]);
-        }
+    for (int64_t p = p0; p < p1; ++p) {
+        const int2 pr = pairs[p];
+        const double* base = vir_part + p * ntiles * 2 * fx::BM;
+        for (int tb = tv; tb < nT; ++tb) s.add(base[(int64_t)tidx(tv, tb) * 2 * fx::BM + rv]);
+        for (int ta = 0; ta <= tv; ++ta)
+            if (ta < tv || pr.x != pr.y) s.add(base[(int64_t)tidx(ta, tv) * 2 * fx::BM + fx::BM + rv]);
     }
-    const double r = warp_sum(s.value());
-    if (lane == 0) acc_vir[v] += 2.0 * r;
+    out[((int64_t)blockIdx.y * nT + tv) * fx::BM + rv] = s.value();
+}
+
+__global__ void fx_reduce_vir_fold_kernel(const double* __restrict__ part, int nchunk, int nT, int nvir,
+                                          double* acc_vir) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= nvir) return;
+    KSum s;
+    for (int c = 0; c < nchunk; ++c) s.add(part[(int64_t)c * nT * fx::BM + v]);
+    acc_vir[v] += 2.0 * s.value();
 }
 
 // ------------------------------------------------------- batch kernels --
@@ -1453,7 +1491,13 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
     const int64_t mp_max = (cc * tp + 127) / 128 * 128;
     FC_TRY(ws_get(WS_T, cbytes * 8 + (size_t)mp_max * 8, &vT));
     FC_TRY(ws_get(WS_TS, (size_t)3 * mp_max * cc * tp, &vTs));
-    FC_TRY(ws_get(WS_PART, (size_t)max_items * (2 + 1 + 2 * fx::BM) * 8 + (size_t)(2 * ncp + nocc) * 8, &vpart));
+    int64_t max_np = 1;
+    for (const auto& x : cps) max_np = std::max(max_np, x.np);
+    const int vir_chunks = (int)std::min<int64_t>(max_np, std::max<int64_t>(1, 4 * c.sm_count / nTa));
+    FC_TRY(ws_get(WS_PART,
+                  (size_t)max_items * (2 + 1 + 2 * fx::BM) * 8 + (size_t)(2 * ncp + nocc) * 8 +
+                      (size_t)vir_chunks * nTa * fx::BM * 8,
+                  &vpart));
     float* T1 = (float*)vT;
     float* T2 = T1 + cbytes;
     double* ts = (double*)(T2 + cbytes);
@@ -1462,6 +1506,7 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
     double* vir_part = occ_part + max_items;
     double* e_cp = vir_part + 2 * fx::BM * max_items;  // [ncp][2]
     double* acc_occ = e_cp + 2 * ncp;                  // [nocc]
+    double* vir_fold = acc_occ + nocc;                 // [vir_chunks][nTa * 128]
     FC_CUDA(cudaMemcpyAsync(vtab, pairs.data(), pairs.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
     FC_CUDA(cudaMemsetAsync(de_dvir, 0, nvir * 8, st));
     FC_CUDA(cudaMemsetAsync(acc_occ, 0, nocc * 8, st));
@@ -1560,8 +1605,14 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
         fx_reduce_pairs_kernel<<<1, 1024, 0, st>>>(part, a.items, e_cp + 2 * x);
         fx_reduce_occ_kernel<<<(unsigned)(same ? cp.ni : cp.ni + cp.nj), 256, 0, st>>>(
             occ_part, dpairs + cp.p0, cp.np, ntiles, (int)cp.i0, (int)cp.ni, (int)cp.j0, acc_occ);
-        fx_reduce_vir_kernel<<<(unsigned)((nvir + 7) / 8), 256, 0, st>>>(vir_part, dpairs + cp.p0, dtiles, cp.np,
-                                                                          ntiles, (int)nvir, de_dvir);
+        {
+            const int nchunk = (int)std::min<int64_t>(vir_chunks, cp.np);
+            const int64_t ppc = (cp.np + nchunk - 1) / nchunk;
+            fx_reduce_vir_part_kernel<<<dim3((unsigned)nTa, (unsigned)nchunk), 128, 0, st>>>(
+                vir_part, dpairs + cp.p0, cp.np, nTa, ntiles, ppc, vir_fold);
+            fx_reduce_vir_fold_kernel<<<(unsigned)((nvir + 127) / 128), 128, 0, st>>>(vir_fold, nchunk, nTa,
+                                                                                       (int)nvir, de_dvir);
+        }
         FC_TRY(check_launch("gradient reductions"));
         FC_TRY(adjoint(T1, cp.i0, cp.ni, cp.j0, cp.nj));
         if (!same) FC_TRY(adjoint(T2, cp.j0, cp.nj, cp.i0, cp.ni));
