@@ -38,6 +38,11 @@ SIGNATURES = {
     "fc_rimp2_energy_dev": (_I32, [_P, _I64, _I64, _I64, _P, _P, _I32, _D, _I32, _DP, _DP, _P, _P]),
     "fc_rimp2_energy_grad": (_I32, [_P, _I64, _I64, _I64, _P, _P, _I32, _DP, _DP, _P, _P, _P, _P]),
     "fc_rimp2_energy_grad_dev": (_I32, [_P, _I64, _I64, _I64, _P, _P, _I32, _DP, _DP, _P, _P, _P, _P, _P]),
+    "fc_rimp2_energy_shard_dev": (_I32, [_P, _I64, _I64, _I64, _P, _P, _I32, _D, _I32, _I32, _I32, _DP, _DP, _P,
+                                         _P]),
+    "fc_rimp2_energy_grad_shard_dev": (_I32, [_P, _I64, _I64, _I64, _P, _P, _I32, _I32, _I32, _DP, _DP, _P, _P, _P,
+                                              _P, _P]),
+    "fc_rimp2_shard_pairs": (_I32, [_I64, _I64, _I32, _I32, _I32, _I32, _P, _I64, _c.POINTER(_I64)]),
     "fc_dfjk_create": (_I32, [_P, _I64, _I64, _I32, _I32, _c.POINTER(_P)]),
     "fc_dfjk_create_dev": (_I32, [_P, _I64, _I64, _I32, _I32, _P, _c.POINTER(_P)]),
     "fc_dfj_set_metric_chol": (_I32, [_P, _P]),

@@ -3,6 +3,7 @@
 // try_spin_components_on_device / spin_components_on_device
 // (ferric-mp2/src/rimp2_gpu.rs:105-471) and the host gradient intermediates
 // x_ov / P (ferric-mp2/src/zvector.rs:651-703, oo_rimp2.rs:1170-1300).
+#include <algorithm>
 #include "fc_internal.cuh"
 #include "rimp2.cuh"
 
@@ -80,6 +81,55 @@ fc_status grad_dispatch(const Rimp2Dev& d, int32_t precision, cudaStream_t st, d
 }  // namespace
 
 namespace fc {
+
+void shard_pair_range(int64_t nocc, int shard, int nshards, int64_t* lo, int64_t* hi) {
+    const int64_t np = nocc * (nocc + 1) / 2;
+    *lo = np * shard / nshards;
+    *hi = np * (shard + 1) / nshards;
+}
+
+std::vector<int> chunk_pair_owner(int64_t nocc, int64_t cc, int nshards) {
+    const int64_t nch = (nocc + cc - 1) / cc;
+    std::vector<int64_t> w;
+    for (int64_t I = 0; I < nch; ++I)
+        for (int64_t J = I; J < nch; ++J) {
+            const int64_t ni = std::min(cc, nocc - I * cc), nj = std::min(cc, nocc - J * cc);
+            w.push_back(I == J ? ni * (ni + 1) / 2 : ni * nj);
+        }
+    int64_t total = 0;
+    for (int64_t x : w) total += x;
+    std::vector<int> own(w.size());
+    int64_t pre = 0;
+    for (size_t x = 0; x < w.size(); ++x) {
+        // midpoint 2 pre + w of the chunk pair, on a scale of 2 total
+        const int64_t s = (int64_t)nshards * (2 * pre + w[x]) / (2 * total);
+        own[x] = (int)std::min<int64_t>(s, nshards - 1);
+        pre += w[x];
+    }
+    return own;
+}
+
+static int64_t shard_cap(int64_t nocc, int64_t cc, int nshards) {
+    if (nshards <= 1) return cc;
+    int64_t n = 1;
+    while (n * (n + 1) / 2 < 8 * (int64_t)nshards) ++n;  // chunks for >= 8 chunk pairs per shard
+    const int64_t cap = std::max<int64_t>(1, nocc / n);
+    return std::min(cc, cap);
+}
+
+int64_t grad_chunk_fx(int64_t nocc, int64_t nvir, int64_t budget, int nshards) {
+    const int64_t tp = (nvir + 15) / 16 * 16;
+    const int64_t per_c2 = tp * tp * (4 + 4 + 3) + 1024 * tp;  // two FP32 amplitude blocks, int8 slices
+    int64_t cc = 1;
+    while (cc < nocc && (cc + 1) * (cc + 1) * per_c2 <= budget) ++cc;
+    return shard_cap(nocc, cc, nshards);
+}
+
+int64_t grad_chunk_f64(int64_t nocc, int64_t nvir, int64_t budget, int nshards) {
+    int64_t cc = 1;
+    while (cc < nocc && 2 * (cc + 1) * nvir * (cc + 1) * nvir * 8 <= budget) ++cc;
+    return shard_cap(nocc, cc, nshards);
+}
 
 fc_status gamma_sink_block(const GammaSink* sink, const double* gamma, int64_t naux, int64_t nov, int64_t nvir,
                            int64_t r0, int64_t nr, cudaStream_t st) {
@@ -161,6 +211,91 @@ fc_status fc_rimp2_energy_grad_dev(const double* b_ov, int64_t naux, int64_t noc
     }
     Rimp2Dev d{b_ov, eps_occ, eps_vir, naux, nocc, nvir, 0, 0.0, chunk_budget()};
     return grad_dispatch(d, precision, st, e_os, e_ss, gamma, de_docc, de_dvir, stats);
+}
+
+fc_status fc_rimp2_energy_shard_dev(const double* b_ov, int64_t naux, int64_t nocc, int64_t nvir,
+                                    const double* eps_occ, const double* eps_vir, int32_t has_kappa,
+                                    double kappa, int32_t precision, int32_t shard, int32_t nshards,
+                                    double* e_os, double* e_ss, void* stream, fc_stats* stats) {
+    FC_TRY(check_shapes(b_ov, naux, nocc, nvir, eps_occ, eps_vir, precision, has_kappa, kappa, e_os, e_ss));
+    if (nshards < 1 || shard < 0 || shard >= nshards) return fail(FC_ERR_INVALID, "RI-MP2 shard: bad shard index");
+    FC_TRY(require_init());
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (stats) *stats = fc_stats{};
+    if (naux == 0 || nocc == 0 || nvir == 0) {
+        *e_os = 0.0;
+        *e_ss = 0.0;
+        return FC_OK;
+    }
+    Rimp2Dev d{b_ov, eps_occ, eps_vir, naux, nocc, nvir, has_kappa, kappa, chunk_budget(), shard, nshards};
+    return energy_dispatch(d, precision, pick_stream(stream), e_os, e_ss, stats);
+}
+
+fc_status fc_rimp2_energy_grad_shard_dev(const double* b_ov, int64_t naux, int64_t nocc, int64_t nvir,
+                                         const double* eps_occ, const double* eps_vir, int32_t precision,
+                                         int32_t shard, int32_t nshards, double* e_os, double* e_ss,
+                                         double* gamma, double* de_docc, double* de_dvir, void* stream,
+                                         fc_stats* stats) {
+    if (nshards < 1 || shard < 0 || shard >= nshards) return fail(FC_ERR_INVALID, "RI-MP2 shard: bad shard index");
+    if (precision != FC_PREC_F64 && precision != FC_PREC_MIXED)
+        return fail(FC_ERR_KERNEL, "RI-MP2 shard: the adjoint runs in FC_PREC_F64 or FC_PREC_MIXED");
+    FC_TRY(check_shapes(b_ov, naux, nocc, nvir, eps_occ, eps_vir, precision, 0, 0.0, e_os, e_ss));
+    if (naux && nocc && nvir && (!gamma || !de_docc || !de_dvir))
+        return fail(FC_ERR_INVALID, "RI-MP2 gradient: null output pointer");
+    FC_TRY(require_init());
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (stats) *stats = fc_stats{};
+    cudaStream_t st = pick_stream(stream);
+    if (naux == 0 || nocc == 0 || nvir == 0) {
+        *e_os = 0.0;
+        *e_ss = 0.0;
+        if (gamma && naux * nocc * nvir) FC_CUDA(cudaMemsetAsync(gamma, 0, naux * nocc * nvir * 8, st));
+        if (de_docc && nocc) FC_CUDA(cudaMemsetAsync(de_docc, 0, nocc * 8, st));
+        if (de_dvir && nvir) FC_CUDA(cudaMemsetAsync(de_dvir, 0, nvir * 8, st));
+        FC_CUDA(cudaStreamSynchronize(st));
+        return FC_OK;
+    }
+    Rimp2Dev d{b_ov, eps_occ, eps_vir, naux, nocc, nvir, 0, 0.0, chunk_budget(), shard, nshards};
+    return grad_dispatch(d, precision, st, e_os, e_ss, gamma, de_docc, de_dvir, stats);
+}
+
+fc_status fc_rimp2_shard_pairs(int64_t nocc, int64_t nvir, int32_t precision, int32_t grad, int32_t shard,
+                               int32_t nshards, int32_t* ij, int64_t cap, int64_t* npairs) {
+    if (nocc < 0 || nvir < 1 || nshards < 1 || shard < 0 || shard >= nshards || !npairs)
+        return fail(FC_ERR_INVALID, "fc_rimp2_shard_pairs: bad arguments");
+    if (precision != FC_PREC_F64 && precision != FC_PREC_MIXED && !(precision == FC_PREC_MIXED_FAST && !grad))
+        return fail(FC_ERR_INVALID, "fc_rimp2_shard_pairs: bad precision");
+    std::vector<std::pair<int32_t, int32_t>> out;
+    if (!grad) {
+        int64_t lo, hi;
+        shard_pair_range(nocc, shard, nshards, &lo, &hi);
+        for (int64_t i = 0, k = 0; i < nocc; ++i)
+            for (int64_t j = i; j < nocc; ++j, ++k)
+                if (k >= lo && k < hi) out.emplace_back((int32_t)i, (int32_t)j);
+    } else if (nocc > 0) {
+        const int64_t budget = chunk_budget();
+        const int64_t cc = precision == FC_PREC_F64 ? grad_chunk_f64(nocc, nvir, budget, nshards)
+                                                    : grad_chunk_fx(nocc, nvir, budget, nshards);
+        const std::vector<int> own = chunk_pair_owner(nocc, cc, nshards);
+        const int64_t nch = (nocc + cc - 1) / cc;
+        size_t x = 0;
+        for (int64_t I = 0; I < nch; ++I)
+            for (int64_t J = I; J < nch; ++J, ++x) {
+                if (own[x] != shard) continue;
+                for (int64_t i = I * cc; i < std::min(nocc, (I + 1) * cc); ++i)
+                    for (int64_t j = (I == J ? i : J * cc); j < std::min(nocc, (J + 1) * cc); ++j)
+                        out.emplace_back((int32_t)i, (int32_t)j);
+            }
+    }
+    *npairs = (int64_t)out.size();
+    if (ij) {
+        if (cap < (int64_t)out.size()) return fail(FC_ERR_LAYOUT, "fc_rimp2_shard_pairs: output too small");
+        for (size_t k = 0; k < out.size(); ++k) {
+            ij[2 * k] = out[k].first;
+            ij[2 * k + 1] = out[k].second;
+        }
+    }
+    return FC_OK;
 }
 
 fc_status fc_rimp2_energy_grad(const double* b_ov, int64_t naux, int64_t nocc, int64_t nvir,

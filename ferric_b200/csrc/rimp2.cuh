@@ -1,5 +1,6 @@
 // Internal interface of the RI-MP2 kernel sets (device pointers only).
 #pragma once
+#include <vector>
 #include "fc_internal.cuh"
 
 namespace fc {
@@ -12,7 +13,23 @@ struct Rimp2Dev {
     int has_kappa;
     double kappa;
     int64_t chunk_bytes;    // amplitude-chunk budget of the gradient
+    int shard = 0;          // this process's share of the occupied pairs (of nshards)
+    int nshards = 1;
 };
+
+// Occupied-pair sharding of one system over nshards processes (the same
+// partition in every process; the sum over shards of each call's E, Gamma
+// and dE/deps is the unsharded result).
+// Energy: pairs i <= j in i-major order, shard s computes [lo, hi).
+void shard_pair_range(int64_t nocc, int shard, int nshards, int64_t* lo, int64_t* hi);
+// Gradient: occupied chunks of size cc, chunk pairs (I <= J) in I-major
+// order; the owner of each is the shard whose share of the total pair count
+// holds the chunk pair's midpoint (contiguous, balanced ranges).
+std::vector<int> chunk_pair_owner(int64_t nocc, int64_t cc, int nshards);
+// Chunk sizes of the two gradient drivers for an amplitude budget, capped
+// with several shards so that there are at least 8 chunk pairs per shard.
+int64_t grad_chunk_fx(int64_t nocc, int64_t nvir, int64_t budget, int nshards);
+int64_t grad_chunk_f64(int64_t nocc, int64_t nvir, int64_t budget, int nshards);
 
 // Where the gradient's Gamma goes as its column blocks become final: a
 // pinned host array (naux x nov, row-major) and a copy stream; the block of

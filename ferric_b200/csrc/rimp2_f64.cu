@@ -323,17 +323,26 @@ fc_status rimp2_energy_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, dou
     const int64_t nocc = d.nocc, nvir = d.nvir;
     const int ntile = (int)((nvir + PR_T - 1) / PR_T);
     const int ntiles = ntile * (ntile + 1) / 2;  // tiles ta <= tb
-    const int64_t npairs = nocc * (nocc + 1) / 2;
+    int64_t plo, phi;  // this shard's pairs (all of them unsharded)
+    shard_pair_range(nocc, d.shard, d.nshards, &plo, &phi);
+    const int64_t npairs = phi - plo;
     const int64_t items = npairs * ntiles;
     if (items > INT32_MAX) return fail(FC_ERR_LAYOUT, "RI-MP2: too many pair tiles for one launch");
+    if (items == 0) {
+        *e_os = 0.0;
+        *e_ss = 0.0;
+        if (stats) stats->precision = FC_PREC_F64;
+        return FC_OK;
+    }
 
     void *vpairs, *vpart, *vout;
     FC_TRY(ws_get(WS_PAIRS, (npairs + ntiles) * sizeof(int2), &vpairs));
     FC_TRY(ws_get(WS_PART, items * 2 * sizeof(double), &vpart));
     FC_TRY(ws_get(WS_OUT, 64 * sizeof(double), &vout));
     std::vector<int2> hp;
-    for (int i = 0; i < nocc; ++i)
-        for (int j = i; j < nocc; ++j) hp.push_back(make_int2(i, j));
+    for (int64_t i = 0, k = 0; i < nocc; ++i)
+        for (int64_t j = i; j < nocc; ++j, ++k)
+            if (k >= plo && k < phi) hp.push_back(make_int2((int)i, (int)j));
     for (int ta = 0; ta < ntile; ++ta)
         for (int tb = ta; tb < ntile; ++tb) hp.push_back(make_int2(ta, tb));
     FC_CUDA(cudaMemcpyAsync(vpairs, hp.data(), hp.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
@@ -395,8 +404,7 @@ fc_status rimp2_grad_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, doubl
     // pair (i, j) is computed once and writes the amplitude rows of i (columns
     // of J) and of j (columns of I); both blocks (c nvir)^2 doubles fit the
     // chunk budget beside B and Gamma.
-    int64_t cc = 1;
-    while (cc < nocc && 2 * (cc + 1) * nvir * (cc + 1) * nvir * 8 <= (int64_t)d.chunk_bytes) ++cc;
+    const int64_t cc = grad_chunk_f64(nocc, nvir, d.chunk_bytes, d.nshards);
     const int64_t nch = (nocc + cc - 1) / cc;
     struct CP {
         int64_t i0, ni, j0, nj, p0, np;
@@ -420,6 +428,7 @@ fc_status rimp2_grad_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, doubl
     for (int ta = 0; ta < ntile; ++ta)
         for (int tb = 0; tb < ntile; ++tb) hp.push_back(make_int2(ta, tb));
     const int64_t ncp = (int64_t)cps.size();
+    const std::vector<int> owner = chunk_pair_owner(nocc, cc, d.nshards);
     int64_t max_items = 0;
     for (const auto& x : cps) max_items = std::max(max_items, x.np * ntile2);
     if (max_items > INT32_MAX) return fail(FC_ERR_LAYOUT, "RI-MP2 gradient: too many pair tiles per chunk pair");
@@ -440,6 +449,7 @@ fc_status rimp2_grad_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, doubl
     FC_CUDA(cudaMemcpyAsync(vpairs, hp.data(), hp.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
     FC_CUDA(cudaMemsetAsync(de_dvir, 0, nvir * sizeof(double), st));
     FC_CUDA(cudaMemsetAsync(acc_occ, 0, nocc * sizeof(double), st));
+    FC_CUDA(cudaMemsetAsync(e_cp, 0, 2 * ncp * sizeof(double), st));  // chunk pairs of other shards add nothing
     FC_CUDA(cudaMemsetAsync(gamma, 0, (size_t)naux * nov * sizeof(double), st));
     const int2* dpairs = (const int2*)vpairs;
 
@@ -460,6 +470,13 @@ fc_status rimp2_grad_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, doubl
     for (int64_t x = 0; x < ncp; ++x) {
         const CP& cp = cps[x];
         const bool same = cp.i0 == cp.j0;
+        if (owner[x] != d.shard) {
+            if (stats) {
+                FC_CUDA(cudaEventRecord(ev[2 * x], st));
+                FC_CUDA(cudaEventRecord(ev[2 * x + 1], st));
+            }
+            continue;
+        }
         PairArgs a{};
         a.B = d.b_ov;
         a.ldb = nov;

@@ -1357,10 +1357,19 @@ fc_status rimp2_energy_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, doub
     FC_TRY(fx_split_pairs(d, st, flags, &sp));
     const int nocc = (int)d.nocc;
     const int nT = (int)(sp.a_pad / fx::BM);
+    int64_t plo, phi;  // this shard's pairs (all of them unsharded)
+    shard_pair_range(nocc, d.shard, d.nshards, &plo, &phi);
     std::vector<int2> pairs;
-    for (int i = 0; i < nocc; ++i)
-        for (int j = i; j < nocc; ++j) pairs.push_back(make_int2(i, j));
+    for (int64_t i = 0, k = 0; i < nocc; ++i)
+        for (int64_t j = i; j < nocc; ++j, ++k)
+            if (k >= plo && k < phi) pairs.push_back(make_int2((int)i, (int)j));
     const size_t npairs = pairs.size();
+    if (npairs == 0) {
+        *e_os = 0.0;
+        *e_ss = 0.0;
+        if (stats) stats->precision = FC_PREC_MIXED;
+        return FC_OK;
+    }
     for (int ta = 0; ta < nT; ++ta)
         for (int tb = ta; tb < nT; ++tb) pairs.push_back(make_int2(ta, tb));
     void* vtab;
@@ -1453,9 +1462,7 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
     // occupied chunks: a chunk pair (I, J), I <= J, holds the amplitude rows of
     // I (columns of J) and of J (columns of I) in FP32, plus the slices of one
     // of them; each unordered pair (i, j) is computed once and feeds both.
-    const int64_t per_c2 = tp * tp * (4 + 4 + 3) + 1024 * tp;  // two FP32 amplitude blocks, int8 slices
-    int64_t cc = 1;
-    while (cc < nocc && (cc + 1) * (cc + 1) * per_c2 <= (int64_t)d.chunk_bytes) ++cc;
+    const int64_t cc = grad_chunk_fx(nocc, nvir, d.chunk_bytes, d.nshards);
     const int64_t nch = (nocc + cc - 1) / cc;
     struct CP {
         int64_t i0, ni, j0, nj, p0, np;
@@ -1479,6 +1486,7 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
     for (int ta = 0; ta < nTa; ++ta)
         for (int tb = ta; tb < nTa; ++tb) pairs.push_back(make_int2(ta, tb));
     const int64_t ncp = (int64_t)cps.size();
+    const std::vector<int> owner = chunk_pair_owner(nocc, cc, d.nshards);
     int64_t max_items = 0;
     for (const auto& x : cps) max_items = std::max(max_items, x.np * ntiles);
 
@@ -1510,6 +1518,7 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
     FC_CUDA(cudaMemcpyAsync(vtab, pairs.data(), pairs.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
     FC_CUDA(cudaMemsetAsync(de_dvir, 0, nvir * 8, st));
     FC_CUDA(cudaMemsetAsync(acc_occ, 0, nocc * 8, st));
+    FC_CUDA(cudaMemsetAsync(e_cp, 0, 2 * ncp * 8, st));  // chunk pairs of other shards add nothing
     FC_CUDA(cudaMemsetAsync(gamma, 0, (size_t)naux * nov * 8, st));
     // per-Q-row split of B_ov for the adjoint contraction
     FC_CUDA(cudaMemsetAsync(vbq, 0, (size_t)3 * q_rows * K2, st));
@@ -1570,6 +1579,13 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
     for (int64_t x = 0; x < ncp; ++x) {
         const CP& cp = cps[x];
         const bool same = cp.i0 == cp.j0;
+        if (owner[x] != d.shard) {
+            if (stats) {
+                FC_CUDA(cudaEventRecord(ev[2 * x], st));
+                FC_CUDA(cudaEventRecord(ev[2 * x + 1], st));
+            }
+            continue;
+        }
         PairFxArgs a{};
         a.eo = d.eps_occ;
         a.ev = d.eps_vir;

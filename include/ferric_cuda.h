@@ -127,6 +127,35 @@ fc_status fc_rimp2_energy_grad_dev(const double* b_ov, int64_t naux, int64_t noc
                                    double* de_docc, double* de_dvir, void* stream,
                                    fc_stats* stats);
 
+/* One system over nshards processes (one GPU each), partitioned by occupied
+ * pairs.  The reference's MPI RI-MP2 (ferric-mp2/src/mpi_rimp2.rs:16-43)
+ * cuts aux bands and all-reduces per-i intermediates; here every process
+ * holds all of B_ov and takes a balanced share of the pairs, so the only
+ * collectives are on the results.  Each call returns this shard's partial
+ * sums: e_os, e_ss, gamma (all naux x nocc*nvir entries, zero outside this
+ * shard's contributions), de_docc, de_dvir; their sum over the shards is the
+ * unsharded result (FP64: to summation order; FC_PREC_MIXED: the amplitude
+ * blocks are split at their own row scales, as with a smaller chunk budget).
+ * The caller adds them with its collectives (all-reduce of the scalars and
+ * dE/deps, reduce-scatter of gamma by aux rows).  No counterpart in the
+ * reference, which has no occupied-pair partition. */
+fc_status fc_rimp2_energy_shard_dev(const double* b_ov, int64_t naux, int64_t nocc, int64_t nvir,
+                                    const double* eps_occ, const double* eps_vir, int32_t has_kappa,
+                                    double kappa, int32_t precision, int32_t shard, int32_t nshards,
+                                    double* e_os, double* e_ss, void* stream, fc_stats* stats);
+fc_status fc_rimp2_energy_grad_shard_dev(const double* b_ov, int64_t naux, int64_t nocc, int64_t nvir,
+                                         const double* eps_occ, const double* eps_vir, int32_t precision,
+                                         int32_t shard, int32_t nshards, double* e_os, double* e_ss,
+                                         double* gamma, double* de_docc, double* de_dvir, void* stream,
+                                         fc_stats* stats);
+/* The occupied pairs (i <= j, as (i, j) int32 pairs into ij[2 * cap]) that
+ * shard `shard` of `nshards` computes in the energy (grad = 0) or energy +
+ * gradient (grad = 1) call under the current chunk budget.  Host only: needs
+ * no device and no fc_init.  *npairs receives the count (ij may be NULL to
+ * query it). */
+fc_status fc_rimp2_shard_pairs(int64_t nocc, int64_t nvir, int32_t precision, int32_t grad, int32_t shard,
+                               int32_t nshards, int32_t* ij, int64_t cap, int64_t* npairs);
+
 /* Unrestricted RI-MP2 energy components (alpha-alpha, beta-beta,
  * alpha-beta), the device part of u_ri_mp2: same_spin_block_energy and
  * opposite_spin_block_energy (ferric-mp2/src/u_rimp2.rs:693-753), with the

@@ -152,6 +152,40 @@ def energy_gamma_deps_small(b_ov, eps_occ, eps_vir):
     return e_os, e_ss, gamma, 2.0 * np.diag(p_oo).copy(), 2.0 * np.diag(p_vv).copy()
 
 
+def energy_gamma_deps_pairs(b_ov, eps_occ, eps_vir, pairs):
+    """The contributions of a set of unordered occupied pairs (i <= j) to E,
+    Gamma and dE/deps: each pair stands for its orderings (i, j) and (j, i),
+    computed with the per-ordered-pair terms of ``energy_gamma_deps``
+    (zvector.rs:651-703, oo_rimp2.rs:1170-1191).  The sums over a partition of
+    all pairs equal ``energy_gamma_deps``.  Small cases only.
+
+    Returns ``(e_os, e_ss, gamma, de_docc, de_dvir)``.
+    """
+    b_ov = np.ascontiguousarray(b_ov, dtype=np.float64)
+    eps_occ = np.asarray(eps_occ, dtype=np.float64)
+    eps_vir = np.asarray(eps_vir, dtype=np.float64)
+    naux = b_ov.shape[0]
+    nocc, nvir = len(eps_occ), len(eps_vir)
+    gamma = np.zeros((naux, nocc * nvir))
+    de_docc = np.zeros(nocc)
+    de_dvir = np.zeros(nvir)
+    e_os = e_ss = 0.0
+    for i0, j0 in pairs:
+        for i, j in ((i0, j0), (j0, i0)) if i0 != j0 else ((i0, j0),):
+            bi, bj = b_ov[:, i * nvir:(i + 1) * nvir], b_ov[:, j * nvir:(j + 1) * nvir]
+            g = bi.T @ bj                                          # (ia|jb)
+            denom = eps_occ[i] + eps_occ[j] - eps_vir[:, None] - eps_vir[None, :]
+            t = g / denom
+            tt = (2.0 * g - g.T) / denom
+            e_os += float(np.sum(g * t))
+            e_ss += float(np.sum(g * (g - g.T) / denom))
+            c = t * tt
+            de_docc[i] += -2.0 * float(np.sum(c))
+            de_dvir += 2.0 * np.sum(c, axis=1)
+            gamma[:, i * nvir:(i + 1) * nvir] += 4.0 * (bj @ tt.T)
+    return e_os, e_ss, gamma, de_docc, de_dvir
+
+
 def energy_gamma_deps(b_ov, eps_occ, eps_vir, occ=None):
     """E, Gamma = dE/dB and dE/deps without storing ``t2``.
 
