@@ -165,6 +165,23 @@ def test_adjoint_k_segments(fc, monkeypatch):
     assert np.abs(one[1] - seg[1]).max() <= 1e-13 * np.abs(one[1]).max()
 
 
+def test_mixed_refuses_naux_beyond_exact_int32(fc):
+    """The int8 pair kernel's level sums are exact while 3 * 127^2 * naux <
+    2^31: a larger aux basis is refused (FC_ERR_LAYOUT, nothing launched),
+    and FP64 takes it."""
+    import ferric_b200._lib as L
+    from ferric_b200 import rimp2
+    rng = np.random.default_rng(3)
+    b = rng.standard_normal((44383, 2)) * 1e-3
+    eo, ev = np.array([-1.0]), np.array([0.5, 0.9])
+    with pytest.raises(L.FcError) as ei:
+        rimp2.rimp2_energy(b, eo, ev, precision="mixed")
+    assert ei.value.name == "FC_ERR_LAYOUT"
+    e = rimp2.rimp2_energy(b, eo, ev, precision="f64")
+    ref = orc.spin_components(b, np.concatenate([eo, ev]), 1, 2)
+    assert abs(sum(e) - ref[2]) <= 1e-12 * abs(ref[2])
+
+
 def test_mixed_deterministic(fc):
     from ferric_b200 import rimp2
     b, eo, ev = synthetic.rimp2_inputs(200, 7, 65)
