@@ -63,7 +63,22 @@ constexpr int STAGES = 2;
 constexpr int XP = BM + 1;                       // pitch of the exchange rows (floats)
 constexpr int XBUF_BYTES = 32 * XP * 4;          // one lane quarter of a parked X tile
 constexpr int COL_BYTES = 3 * BN * 8;             // a tile's virtual energies and column scales
-constexpr int SMEM = STAGES * STAGE_BYTES + 1024 + 7168 + XBUF_BYTES + COL_BYTES;
+// Pair-kernel epilogue: EPI_WARPS warps, EPI_WARPS / 4 per TMEM lane quadrant;
+// each thread owns one row of the tile and HC of its columns.  The FP64
+// epilogue is latency-bound (few independent FP64 instructions in flight per
+// warp): 16 warps (4 per scheduler) at 32 columns each hide more of that
+// latency than 8 at 64, within the 96 registers a thread that 18 warps leave.
+constexpr int EPI_WARPS = 16;
+constexpr int NCG = EPI_WARPS / 4;                // column groups per row
+constexpr int HC = BN / NCG;                      // columns per thread
+constexpr int EPI_THREADS = 32 * EPI_WARPS;
+constexpr int PAIR_THREADS = 64 + EPI_THREADS;    // + TMA producer warp + MMA warp
+// epilogue scratch after the barriers (64 B): per-warp partials [2][EPI_WARPS][3],
+// row sums of column groups 1.. [NCG - 1][BM], column sums [4][NCG][HC] (doubles)
+constexpr int SCR_BYTES = 8192;
+static_assert(64 + 8 * (2 * EPI_WARPS * 3 + (NCG - 1) * BM + 4 * NCG * HC) <= SCR_BYTES, "pair scratch");
+static_assert(HC % 32 == 0 && 4 * NCG == EPI_WARPS, "pair epilogue layout");
+constexpr int SMEM = STAGES * STAGE_BYTES + 1024 + SCR_BYTES + XBUF_BYTES + COL_BYTES;
 constexpr uint32_t IDESC = tc::idesc_i8_s32(128, 128);
 constexpr double LW = 254.0, LW2INV = 1.0 / (254.0 * 254.0);
 
@@ -310,7 +325,7 @@ __device__ __forceinline__ ItemView item_view(const PairFxArgs& p, int64_t k) {
 }
 
 template <int GRAD, int BATCH = 0>
-__global__ void __launch_bounds__(320, 1)
+__global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
     pair_fx_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                    const PairFxArgs p) {
     using namespace fx;
@@ -327,11 +342,11 @@ __global__ void __launch_bounds__(320, 1)
     uint64_t* drain = bars + 2 * S + 2;   // [1]
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * S + 3);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
-    double* red = reinterpret_cast<double*>(bars + 2 * S + 4);  // [2][8][3]
-    double* rowsh = red + 48;                                    // [128] row sums of the upper column half
-    double* colsh = rowsh + 128;                                 // [4 quadrants][2 halves][64] column sums
-    float* xbuf = reinterpret_cast<float*>(base + S * STAGE_BYTES + 7168);  // [32][XP] exchange rows
-    double* colb = reinterpret_cast<double*>(base + S * STAGE_BYTES + 7168 + XBUF_BYTES);  // [3][BN]
+    double* red = reinterpret_cast<double*>(bars + 2 * S + 4);  // [2][EPI_WARPS][3]
+    double* rowsh = red + 2 * EPI_WARPS * 3;                     // [NCG - 1][BM] row sums of column groups 1..
+    double* colsh = rowsh + (NCG - 1) * BM;                      // [4 quadrants][NCG][HC] column sums
+    float* xbuf = reinterpret_cast<float*>(base + S * STAGE_BYTES + SCR_BYTES);  // [32][XP] exchange rows
+    double* colb = reinterpret_cast<double*>(base + S * STAGE_BYTES + SCR_BYTES + XBUF_BYTES);  // [3][BN]
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (tid == 0) {
@@ -340,7 +355,7 @@ __global__ void __launch_bounds__(320, 1)
             tc::mbar_init(&empty[s], 1);
         }
         tc::mbar_init(tfull, 1);
-        tc::mbar_init(tempty, 256);
+        tc::mbar_init(tempty, EPI_THREADS);
         tc::mbar_init(drain, 1);
         *abort_flag = 0;
         tc::fence_barrier_init();
@@ -427,13 +442,13 @@ __global__ void __launch_bounds__(320, 1)
         __syncwarp();
     } else {
         // ---------------------------------------------------------- epilogue
-        // 8 warps: lane quadrant q = warp % 4 (TMEM lanes 32q..32q+31), column
-        // half h = (warp - 2) / 4; each thread owns row `row`, columns [64h, 64h + 64).
-        constexpr int HC = BN / 2;
+        // EPI_WARPS warps: lane quadrant q = warp % 4 (TMEM lanes 32q..32q+31),
+        // column group h = (warp - 2) / 4; each thread owns row `row`, columns
+        // [HC h, HC h + HC).
         const int q = warp & 3;
         const int h = (warp - 2) >> 2;
         const int row = q * 32 + lane;  // a within the tile
-        const int et = tid - 64;        // 0..255
+        const int et = tid - 64;        // 0 .. EPI_THREADS - 1
         const uint32_t tl = tmem_base + ((uint32_t)(q * 32) << 16) + h * HC;
         uint32_t li = 0, pc = 0;
         for (int64_t k = blockIdx.x; k < p.items; k += gridDim.x, ++li) {
@@ -463,25 +478,25 @@ __global__ void __launch_bounds__(320, 1)
                 if (et < BN) {
                     colb[et] = cb < v.nvir ? v.ev[cb] : 0.0;
                     colb[BN + et] = v.scl[(int64_t)j * v.a_pad + cb];
-                } else {
+                } else if (et < 2 * BN) {
                     colb[2 * BN + (et - BN)] = v.scl[(int64_t)i * v.a_pad + cb];
                 }
             }
-            asm volatile("bar.sync 1, 256;" ::: "memory");
+            asm volatile("bar.sync 1, %0;" ::"n"(EPI_THREADS) : "memory");
             const double* evb = colb + h * HC;
             const double* sxb = colb + BN + h * HC;
             const double* syb = colb + 2 * BN + h * HC;
             const int bmax = v.nvir - b0;    // columns c < bmax are real virtuals
 
-            // X phase: park (ia|jb) of this half row in FP32 (round to nearest).
-            // One thread waits (bounded); the 256 epilogue threads leave together
+            // X phase: park (ia|jb) of this thread's columns in FP32 (round to nearest).
+            // One thread waits (bounded); the epilogue threads leave together
             // if it gave up, since named barriers follow.
-            if (!tc::bar_and<1, 256>(et != 0 || tc::mbar_wait(tfull, pc & 1, abort_flag, p.err))) break;
+            if (!tc::bar_and<1, EPI_THREADS>(et != 0 || tc::mbar_wait(tfull, pc & 1, abort_flag, p.err))) break;
             if (et != 0) tc::mbar_wait(tfull, pc & 1, abort_flag, p.err);  // phase complete: returns at once
             tc::fence_after_sync();
             const bool xt = v.xt;          // the same for every thread of the CTA
             const bool two = !diag && !xt;  // a Y phase follows in TMEM
-            // pk: this thread's 64 parked values -- X of a one-phase item, Y of a
+            // pk: this thread's HC parked values -- X of a one-phase item, Y of a
             // two-phase item (whose X waits in TMEM columns 3 BN + h HC .., beyond
             // the three levels the MMAs write) -- then its column terms.  Both
             // phases of a two-phase item are out of the level columns before the
@@ -509,8 +524,8 @@ __global__ void __launch_bounds__(320, 1)
             tc::mbar_arrive(tempty);
             ++pc;
             if (two) {
-                // Y phase: (ib|ja) = G_ji[a, b] of this half row, FP32 like X
-                if (!tc::bar_and<1, 256>(et != 0 || tc::mbar_wait(tfull, pc & 1, abort_flag, p.err))) break;
+                // Y phase: (ib|ja) = G_ji[a, b] of these columns, FP32 like X
+                if (!tc::bar_and<1, EPI_THREADS>(et != 0 || tc::mbar_wait(tfull, pc & 1, abort_flag, p.err))) break;
                 if (et != 0) tc::mbar_wait(tfull, pc & 1, abort_flag, p.err);
                 tc::fence_after_sync();
             }
@@ -530,7 +545,7 @@ __global__ void __launch_bounds__(320, 1)
                 tc::mbar_arrive(tempty);  // the level columns are free for the next item
                 ++pc;
             }
-            // plain FP64 sums over this thread's 64 terms (relative error <= 64 u);
+            // plain FP64 sums over this thread's HC terms (relative error <= HC u);
             // the tile partials are summed compensated
             double os = 0.0, ss = 0.0, oc = 0.0, rowc = 0.0;
             // the terms of this thread's columns c0 .. c0 + 7, given their Y values
@@ -656,59 +671,48 @@ __global__ void __launch_bounds__(320, 1)
                 }
                 if (!PARK && two) ++pc;
             } else {
-                // Y = X^T inside a diagonal tile: in round r the parked X of lane
-                // quarter r passes through shared memory, and the threads whose 64
-                // columns hold quarter r (half r / 2) take Y[a, b] = X[b, a] of those
-                // 32 columns from it.
+                // Y = X^T inside a diagonal tile: in round r the X values of lane
+                // quarter r (rows 32r .. 32r + 31) pass through shared memory, and
+                // the threads whose columns include 32r .. 32r + 31 take
+                // Y[a, b] = X[b, a] of those 32 columns from it.
 #pragma unroll
                 for (int r = 0; r < 4; ++r) {
                     if (q == r) {
 #pragma unroll
                         for (int c = 0; c < HC; ++c) xbuf[lane * XP + h * HC + c] = pk[c];
                     }
-                    asm volatile("bar.sync 1, 256;" ::: "memory");
-                    if (h == (r >> 1)) {
-                        if (r & 1) {
+                    asm volatile("bar.sync 1, %0;" ::"n"(EPI_THREADS) : "memory");
+#pragma unroll
+                    for (int sb = 0; sb < HC / 32; ++sb) {
+                        if (h * HC + sb * 32 == 32 * r) {
 #pragma unroll
                             for (int c0 = 0; c0 < 32; c0 += 8) {
                                 float xv[8];
                                 double yv[8];
 #pragma unroll
                                 for (int cc = 0; cc < 8; ++cc) {
-                                    xv[cc] = pk[32 + c0 + cc];
+                                    xv[cc] = pk[sb * 32 + c0 + cc];
                                     yv[cc] = (double)xbuf[(c0 + cc) * XP + row];
                                 }
-                                proc8(32 + c0, xv, yv);
-                            }
-                        } else {
-#pragma unroll
-                            for (int c0 = 0; c0 < 32; c0 += 8) {
-                                float xv[8];
-                                double yv[8];
-#pragma unroll
-                                for (int cc = 0; cc < 8; ++cc) {
-                                    xv[cc] = pk[c0 + cc];
-                                    yv[cc] = (double)xbuf[(c0 + cc) * XP + row];
-                                }
-                                proc8(c0, xv, yv);
+                                proc8(sb * 32 + c0, xv, yv);
                             }
                         }
                     }
-                    asm volatile("bar.sync 1, 256;" ::: "memory");
+                    asm volatile("bar.sync 1, %0;" ::"n"(EPI_THREADS) : "memory");
                 }
             }
             const double vo = warp_sum(os), vs = warp_sum(ss);
             const double vc = GRAD ? warp_sum(oc) : 0.0;
-            double* rb = red + (li & 1) * 24;
+            double* rb = red + (li & 1) * (EPI_WARPS * 3);
             if (lane == 0) {
                 rb[(warp - 2) * 3 + 0] = vo;
                 rb[(warp - 2) * 3 + 1] = vs;
                 rb[(warp - 2) * 3 + 2] = vc;
             }
-            if (GRAD && h == 1) rowsh[row] = rowc;
+            if (GRAD && h > 0) rowsh[(h - 1) * BM + row] = rowc;
             if ((mir || both) && !xt) {
                 // column sums of the mirrored terms over this warp's 32 rows: a
-                // reduce-scatter butterfly leaves columns 2*lane, 2*lane+1 in pk[0..1]
+                // reduce-scatter butterfly leaves columns (HC / 32) lane + u in pk[u]
 #pragma unroll
                 for (int half = HC / 2, off = 16; off > 0; half >>= 1, off >>= 1) {
                     const bool up = (lane & off) != 0;
@@ -719,22 +723,27 @@ __global__ void __launch_bounds__(320, 1)
                         pk[c] = (up ? pk[c + half] : pk[c]) + recv;
                     }
                 }
-                colsh[(q * 2 + h) * 64 + 2 * lane] = (double)pk[0];
-                colsh[(q * 2 + h) * 64 + 2 * lane + 1] = (double)pk[1];
+#pragma unroll
+                for (int u = 0; u < HC / 32; ++u) colsh[(q * NCG + h) * HC + (HC / 32) * lane + u] = (double)pk[u];
             }
-            asm volatile("bar.sync 1, 256;" ::: "memory");
-            if (GRAD && h == 0) p.vir_part[k * 2 * BM + row] = rowc + rowsh[row];
+            asm volatile("bar.sync 1, %0;" ::"n"(EPI_THREADS) : "memory");
+            if (GRAD && h == 0) {
+                double rs = rowc;
+#pragma unroll
+                for (int hh = 1; hh < NCG; ++hh) rs += rowsh[(hh - 1) * BM + row];
+                p.vir_part[k * 2 * BM + row] = rs;
+            }
             if ((mir || both) && et < BM) {  // an exchanged tile put its column terms on the rows
-                const int hh = et >> 6, c = et & 63;
+                const int hh = et / HC, c = et % HC;
                 double cs = 0.0;
 #pragma unroll
-                for (int qq = 0; qq < 4; ++qq) cs += colsh[(qq * 2 + hh) * 64 + c];
+                for (int qq = 0; qq < 4; ++qq) cs += colsh[(qq * NCG + hh) * HC + c];
                 p.vir_part[k * 2 * BM + BM + et] = xt ? 0.0 : cs;
             }
             if (et == 0) {
                 KSum so, sn, sc;
 #pragma unroll
-                for (int w = 0; w < 8; ++w) {
+                for (int w = 0; w < EPI_WARPS; ++w) {
                     so.add(rb[w * 3]);
                     sn.add(rb[w * 3 + 1]);
                     sc.add(rb[w * 3 + 2]);
@@ -744,7 +753,7 @@ __global__ void __launch_bounds__(320, 1)
                 if (GRAD) p.occ_part[k] = sc.value();
             }
             // rowsh is rewritten next item only after every thread passed the next barrier
-            asm volatile("bar.sync 1, 256;" ::: "memory");
+            asm volatile("bar.sync 1, %0;" ::"n"(EPI_THREADS) : "memory");
         }
     }
 
@@ -1402,7 +1411,7 @@ fc_status rimp2_energy_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, doub
         FC_TRY(timing_events(1, &ev));
         FC_CUDA(cudaEventRecord(ev[0], st));
     }
-    pair_fx_kernel<0><<<grid, 320, fx::SMEM, st>>>(sp.tmA, sp.tmB, a);
+    pair_fx_kernel<0><<<grid, fx::PAIR_THREADS, fx::SMEM, st>>>(sp.tmA, sp.tmB, a);
     FC_TRY(check_launch("pair_fx_kernel<energy>"));
     if (stats) FC_CUDA(cudaEventRecord(ev[1], st));
     fx_reduce_pairs_kernel<<<1, 1024, 0, st>>>((const double*)vpart, a.items, out);
@@ -1615,7 +1624,7 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
         a.vir_part = vir_part;
         const int grid = (int)(a.items < c.sm_count ? a.items : c.sm_count);
         if (stats) FC_CUDA(cudaEventRecord(ev[2 * x], st));
-        pair_fx_kernel<1><<<grid, 320, fx::SMEM, st>>>(sp.tmA, sp.tmB, a);
+        pair_fx_kernel<1><<<grid, fx::PAIR_THREADS, fx::SMEM, st>>>(sp.tmA, sp.tmB, a);
         FC_TRY(check_launch("pair_fx_kernel<grad>"));
         if (stats) FC_CUDA(cudaEventRecord(ev[2 * x + 1], st));
         fx_reduce_pairs_kernel<<<1, 1024, 0, st>>>(part, a.items, e_cp + 2 * x);
@@ -2067,7 +2076,7 @@ fc_status rimp2_batch_build_fx(fc_rimp2_batch* b, const std::vector<BatchMolIn>&
             a.items = items;
             a.part = (double*)vpart;
             const int grid = (int)std::min<int64_t>(items, c.sm_count);
-            pair_fx_kernel<0, 1><<<grid, 320, fx::SMEM, st>>>(tmA, tmB, a);
+            pair_fx_kernel<0, 1><<<grid, fx::PAIR_THREADS, fx::SMEM, st>>>(tmA, tmB, a);
             batch_energy_kernel<<<(unsigned)nmol, 256, 0, st>>>((const double*)vpart, (const int64_t*)vseg, 0,
                                                                   b->out);
             FC_TRY(check_launch("batched pair kernel"));
@@ -2082,7 +2091,7 @@ fc_status rimp2_batch_build_fx(fc_rimp2_batch* b, const std::vector<BatchMolIn>&
                 a.occ_part = (double*)vocc + g.i0;
                 a.vir_part = (double*)vvir;
                 const int grid = (int)std::min<int64_t>(gi, c.sm_count);
-                pair_fx_kernel<1, 1><<<grid, 320, fx::SMEM, st>>>(tmA, tmB, a);
+                pair_fx_kernel<1, 1><<<grid, fx::PAIR_THREADS, fx::SMEM, st>>>(tmA, tmB, a);
                 batch_energy_kernel<<<(unsigned)(g.m1 - g.m0), 256, 0, st>>>((const double*)vpart,
                                                                                (const int64_t*)vseg, g.m0, b->out);
                 batch_occ_kernel<<<(unsigned)(P(PRE_OCC, g.m1) - P(PRE_OCC, g.m0)), 256, 0, st>>>(
