@@ -671,10 +671,15 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
                 }
                 if (!PARK && two) ++pc;
             } else {
-                // Y = X^T inside a diagonal tile: in round r the X values of lane
-                // quarter r (rows 32r .. 32r + 31) pass through shared memory, and
-                // the threads whose columns include 32r .. 32r + 31 take
-                // Y[a, b] = X[b, a] of those 32 columns from it.
+                // Y = X^T inside a diagonal tile.  A one-phase item leaves the park
+                // columns free: in round r the X values of lane quarter r (rows
+                // 32r .. 32r + 31) pass through shared memory, and the threads
+                // whose columns include 32r .. 32r + 31 store Y[a, b] = X[b, a] of
+                // those 32 columns into their own lane of the park columns.  Then
+                // every thread runs its columns at once, X from registers and Y
+                // from TMEM (with only the threads of one column group busy in each
+                // round, exchanged tiles took about four times a two-phase tile's
+                // epilogue).
 #pragma unroll
                 for (int r = 0; r < 4; ++r) {
                     if (q == r) {
@@ -686,19 +691,29 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
                     for (int sb = 0; sb < HC / 32; ++sb) {
                         if (h * HC + sb * 32 == 32 * r) {
 #pragma unroll
-                            for (int c0 = 0; c0 < 32; c0 += 8) {
-                                float xv[8];
-                                double yv[8];
+                            for (int c0 = 0; c0 < 32; c0 += 16) {
+                                float yq[16];
 #pragma unroll
-                                for (int cc = 0; cc < 8; ++cc) {
-                                    xv[cc] = pk[sb * 32 + c0 + cc];
-                                    yv[cc] = (double)xbuf[(c0 + cc) * XP + row];
-                                }
-                                proc8(sb * 32 + c0, xv, yv);
+                                for (int cc = 0; cc < 16; ++cc) yq[cc] = xbuf[(c0 + cc) * XP + row];
+                                tc::tmem_st16(tpk + sb * 32 + c0, yq);
                             }
                         }
                     }
                     asm volatile("bar.sync 1, %0;" ::"n"(EPI_THREADS) : "memory");
+                }
+                tc::tmem_wait_st();
+#pragma unroll
+                for (int c0 = 0; c0 < HC; c0 += 8) {
+                    float xv[8], yf[8];
+                    double yv[8];
+                    tc::tmem_ld8(tpk + c0, yf);
+                    tc::tmem_wait_ld();
+#pragma unroll
+                    for (int cc = 0; cc < 8; ++cc) {
+                        xv[cc] = pk[c0 + cc];
+                        yv[cc] = (double)yf[cc];
+                    }
+                    proc8(c0, xv, yv);
                 }
             }
             const double vo = warp_sum(os), vs = warp_sum(ss);
