@@ -872,11 +872,14 @@ __device__ __forceinline__ GemmView gemm_view(const GemmFxArgs& p, const CUtenso
 constexpr int GF_STAGE = 3 * (16384 + 16384);  // 96 KiB
 constexpr int GF_STAGES = 2;
 constexpr int GF_SMEM = GF_STAGES * GF_STAGE + 1024 + 1024;
+// TMA warp, MMA warp and 8 epilogue warps (two per TMEM lane quadrant, 64
+// columns each: 64 FP64 values a thread, which 10 warps leave registers for)
+constexpr int GF_THREADS = 320;
 
 // out[Q, (i0 + il)*nvir + a] (+)= alpha * s_row s_Q (L0 + L1/254 + L2/254^2)
 // for amplitude rows m = il*tpad + a (a < nvir).
 template <int BATCH = 0>
-__global__ void __launch_bounds__(192, 1)
+__global__ void __launch_bounds__(GF_THREADS, 1)
     gemm_fx_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                    const GemmFxArgs p) {
     using namespace fx;
@@ -901,7 +904,7 @@ __global__ void __launch_bounds__(192, 1)
             tc::mbar_init(&empty[s], 1);
         }
         tc::mbar_init(tfull, 1);
-        tc::mbar_init(tempty, 128);
+        tc::mbar_init(tempty, GF_THREADS - 64);
         tc::mbar_init(drain, 1);
         *abort_flag = 0;
         tc::fence_barrier_init();
@@ -976,7 +979,14 @@ __global__ void __launch_bounds__(192, 1)
         }
         __syncwarp();
     } else {
+        // Epilogue: lane quadrant q = warp % 4, column half h; each thread owns
+        // amplitude row `row` of the tile and aux columns [64h, 64h + 64).  It
+        // combines its three level accumulators into FP64 registers and
+        // releases TMEM before touching Gamma, so the read-modify-write of
+        // Gamma runs under the next tile's MMAs (with one thread per row
+        // holding TMEM through it, the MMAs waited ~8% of the time).
         const int q = warp & 3;
+        const int h = (warp - 2) >> 2;
         const int row = q * 32 + lane;
         uint32_t li = 0;
         for (int64_t t = blockIdx.x; t < p.tiles; t += gridDim.x, ++li) {
@@ -988,37 +998,42 @@ __global__ void __launch_bounds__(192, 1)
             const bool vm = a < v.nvir && m < v.rows;
             const double sr = vm ? p.alpha * v.rs[m] : 0.0;
             double* orow = v.out + (int64_t)(v.i0 + il) * v.nvir + a;
-            const uint32_t tl = tmem_base + ((uint32_t)(q * 32) << 16);
-            // The 16 old Gamma values of a column chunk (nov apart) are loaded
-            // together before the TMEM wait: issued one by one between the
-            // stores, each was a DRAM round trip that the next tile's MMAs
-            // (single TMEM accumulator) waited for.
-#pragma unroll 1
-            for (int c0 = 0; c0 < 128; c0 += 16) {
+            const uint32_t tl = tmem_base + ((uint32_t)(q * 32) << 16) + h * 64;
+            const int q0 = v.tn * 128 + h * 64;     // first aux row Q of this thread's columns
+            double gv[64];
+#pragma unroll
+            for (int c0 = 0; c0 < 64; c0 += 16) {
                 float l0[16], l1[16], l2[16];
                 tc::tmem_ld16(tl + c0, l0);
                 tc::tmem_ld16(tl + 128 + c0, l1);
                 tc::tmem_ld16(tl + 256 + c0, l2);
-                double old[16];
+                tc::tmem_wait_ld();
 #pragma unroll
                 for (int cc = 0; cc < 16; ++cc) {
-                    const int Q = v.tn * 128 + c0 + cc;
-                    old[cc] = vm && p.accumulate && Q < v.naux ? orow[(int64_t)Q * v.nov] : 0.0;
-                }
-                tc::tmem_wait_ld();
-                if (vm) {
-#pragma unroll
-                    for (int cc = 0; cc < 16; ++cc) {
-                        const int Q = v.tn * 128 + c0 + cc;
-                        if (Q < v.naux) {
-                            const double g = level_value(l0[cc], l1[cc], l2[cc], sr * v.cs[Q]);
-                            orow[(int64_t)Q * v.nov] = p.accumulate ? old[cc] + g : g;
-                        }
-                    }
+                    const int Q = q0 + c0 + cc;
+                    gv[c0 + cc] = level_value(l0[cc], l1[cc], l2[cc], Q < v.naux ? sr * v.cs[Q] : 0.0);
                 }
             }
             tc::fence_before_sync();
             tc::mbar_arrive(tempty);
+            if (vm) {
+                // the 16 old Gamma values of a column chunk (nov apart) are
+                // loaded together, then updated
+#pragma unroll
+                for (int c0 = 0; c0 < 64; c0 += 16) {
+                    double old[16];
+#pragma unroll
+                    for (int cc = 0; cc < 16; ++cc) {
+                        const int Q = q0 + c0 + cc;
+                        old[cc] = p.accumulate && Q < v.naux ? orow[(int64_t)Q * v.nov] : 0.0;
+                    }
+#pragma unroll
+                    for (int cc = 0; cc < 16; ++cc) {
+                        const int Q = q0 + c0 + cc;
+                        if (Q < v.naux) orow[(int64_t)Q * v.nov] = p.accumulate ? old[cc] + gv[c0 + cc] : gv[c0 + cc];
+                    }
+                }
+            }
         }
     }
     tc::fence_before_sync();
@@ -1595,7 +1610,7 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
             g.aofs = (int)ks;
             g.kofs = (int)(k0 * tp + ks);
             g.nk = (int)((kl + fx::KT - 1) / fx::KT);
-            gemm_fx_kernel<0><<<g2, 192, GF_SMEM, st>>>(tmTs, tmBq, g);
+            gemm_fx_kernel<0><<<g2, GF_THREADS, GF_SMEM, st>>>(tmTs, tmBq, g);
             FC_TRY(check_launch("gemm_fx_kernel"));
         }
         return FC_OK;
@@ -2123,7 +2138,7 @@ fc_status rimp2_batch_build_fx(fc_rimp2_batch* b, const std::vector<BatchMolIn>&
                 ga.alpha = 4.0;
                 ga.err = b->flags + 1;
                 const int g2 = (int)std::min<int64_t>(ga.tiles, c.sm_count);
-                gemm_fx_kernel<1><<<g2, 192, GF_SMEM, st>>>(tmA, tmB, ga);
+                gemm_fx_kernel<1><<<g2, GF_THREADS, GF_SMEM, st>>>(tmA, tmB, ga);
                 FC_TRY(check_launch("batched adjoint contraction"));
                 launches += 6;
             }
