@@ -201,15 +201,19 @@ __global__ void __launch_bounds__(256) split_fx_rows_f32_kernel(const float* __r
 // A slice 0 has descriptor `da`; the three A slices are A_BYTES apart and the
 // B slices start BOFS bytes after A slice 0.  Offsets are compile-time: the
 // descriptor start-address field is linear in the address.
-template <int BOFS>
+// PART 0 issues all six; PART 1 the four products of slices 0 and 1, PART 2
+// the two with a slice 2 (their operands may arrive later).  The int32 sums
+// are exact, so the order of the products does not change the result.
+template <int BOFS, int PART = 0>
 __device__ __forceinline__ void issue_products(uint64_t da, uint32_t tmem_base, int kt) {
     using namespace fx;
-    constexpr int PA[6] = {0, 0, 1, 0, 1, 2};
-    constexpr int PB[6] = {0, 1, 0, 2, 1, 0};
+    constexpr int PA[6] = {0, 0, 1, 1, 0, 2};
+    constexpr int PB[6] = {0, 1, 0, 1, 2, 0};
     constexpr int PL[6] = {0, 1, 1, 2, 2, 2};
     constexpr int PF[6] = {1, 1, 0, 1, 0, 0};  // first product of its level
+    constexpr int P0 = PART == 2 ? 4 : 0, P1 = PART == 1 ? 4 : 6;
 #pragma unroll
-    for (int pr = 0; pr < 6; ++pr) {
+    for (int pr = P0; pr < P1; ++pr) {
 #pragma unroll
         for (int kk = 0; kk < KT / 32; ++kk)
             tc::umma_i8(tmem_base + PL[pr] * BN, da + (uint64_t)((PA[pr] * A_BYTES + kk * 32) >> 4),
@@ -896,11 +900,15 @@ __global__ void __launch_bounds__(GF_THREADS, 1)
     uint64_t* drain = bars + 2 * S + 2;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * S + 3);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    // a stage arrives in two parts: slices 0 and 1 of A and B (full), then
+    // slice 2 (full2); the four products of slices 0 and 1 start on the first
+    uint64_t* full2 = bars + 2 * S + 4;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (tid == 0) {
         for (int s = 0; s < S; ++s) {
             tc::mbar_init(&full[s], 1);
+            tc::mbar_init(&full2[s], 1);
             tc::mbar_init(&empty[s], 1);
         }
         tc::mbar_init(tfull, 1);
@@ -937,12 +945,14 @@ __global__ void __launch_bounds__(GF_THREADS, 1)
                     const int s = g % S;
                     const uint32_t u = g / S;
                     if (!tc::mbar_wait(&empty[s], (u & 1) ^ 1, abort_flag, p.err)) goto prod_done;
-                    tc::mbar_arrive_expect_tx(&full[s], GF_STAGE);
+                    tc::mbar_arrive_expect_tx(&full[s], GF_STAGE / 3 * 2);
+                    tc::mbar_arrive_expect_tx(&full2[s], GF_STAGE / 3);
 #pragma unroll
                     for (int sl = 0; sl < 3; ++sl) {
-                        tc::tma_load_2d(base + (sa(s, sl) - base_u32), v.tA, &full[s], p.aofs + kt * KT,
+                        uint64_t* bar = sl < 2 ? &full[s] : &full2[s];
+                        tc::tma_load_2d(base + (sa(s, sl) - base_u32), v.tA, bar, p.aofs + kt * KT,
                                         sl * v.M + v.tm * 128);
-                        tc::tma_load_2d(base + (sb(s, sl) - base_u32), v.tB, &full[s], p.kofs + kt * KT,
+                        tc::tma_load_2d(base + (sb(s, sl) - base_u32), v.tB, bar, p.kofs + kt * KT,
                                         sl * v.N + v.tn * 128);
                     }
                 }
@@ -952,6 +962,7 @@ __global__ void __launch_bounds__(GF_THREADS, 1)
                 const uint32_t gg = g - 1 - q;
                 int no_abort = 0;
                 tc::mbar_wait(&full[gg % S], (gg / S) & 1, &no_abort, p.err);
+                tc::mbar_wait(&full2[gg % S], (gg / S) & 1, &no_abort, p.err);
             }
         }
     } else if (warp == 1) {
@@ -967,7 +978,10 @@ __global__ void __launch_bounds__(GF_THREADS, 1)
                     const uint32_t u = g / S;
                     if (!tc::mbar_wait(&full[s], u & 1, abort_flag, p.err)) goto mma_done;
                     tc::fence_after_sync();
-                    issue_products<3 * 16384>(s ? da1 : da0, tmem_base, kt);
+                    issue_products<3 * 16384, 1>(s ? da1 : da0, tmem_base, kt);
+                    if (!tc::mbar_wait(&full2[s], u & 1, abort_flag, p.err)) goto mma_done;
+                    tc::fence_after_sync();
+                    issue_products<3 * 16384, 2>(s ? da1 : da0, tmem_base, kt);
                     tc::umma_commit(&empty[s]);
                 }
                 tc::umma_commit(tfull);
