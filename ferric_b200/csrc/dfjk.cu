@@ -335,11 +335,12 @@ __global__ void dfk_fold_kernel(const double* __restrict__ part, int nsplit, int
 }
 
 static fc_status dfjk_smem_once() {
-    static bool done = false;
-    if (done) return FC_OK;
+    static std::atomic<uint64_t> done{0};
+    uint64_t bit = 0;
+    if (!attrs_needed(done, &bit)) return FC_OK;
     FC_CUDA(cudaFuncSetAttribute(dgemm_tn_kernel<EpiScatterW>, cudaFuncAttributeMaxDynamicSharedMemorySize, DG_SMEM));
     FC_CUDA(cudaFuncSetAttribute(dgemm_tn_kernel<EpiSplit>, cudaFuncAttributeMaxDynamicSharedMemorySize, DG_SMEM));
-    done = true;
+    done.fetch_or(bit);
     return FC_OK;
 }
 

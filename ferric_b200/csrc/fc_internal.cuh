@@ -4,6 +4,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <mutex>
@@ -34,6 +35,17 @@ fc_status cuda_fail(cudaError_t e, const char* what);
 
 // A launch error is reported as FC_ERR_KERNEL (image missing / refused).
 fc_status check_launch(const char* what);
+
+// Kernel attributes (cudaFuncSetAttribute) belong to the device that is
+// current when they are set: a setter runs once per device, tracked in
+// `done` (one bit per device; devices past 63 set them on every call).
+inline bool attrs_needed(const std::atomic<uint64_t>& done, uint64_t* bit) {
+    int dev = 0;
+    *bit = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return true;
+    *bit = 1ull << dev;
+    return !(done.load() & *bit);
+}
 
 // ---------------------------------------------------------- the context --
 

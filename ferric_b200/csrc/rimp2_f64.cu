@@ -307,13 +307,14 @@ __global__ void __launch_bounds__(256) reduce_vir_kernel(const double* __restric
 }
 
 static fc_status set_smem_once() {
-    static bool done = false;
-    if (done) return FC_OK;
+    static std::atomic<uint64_t> done{0};
+    uint64_t bit = 0;
+    if (!attrs_needed(done, &bit)) return FC_OK;
     FC_CUDA(cudaFuncSetAttribute(pair_f64_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, PR_SMEM));
     FC_CUDA(cudaFuncSetAttribute(pair_f64_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, PR_SMEM));
     FC_CUDA(cudaFuncSetAttribute(pair_f64_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, PR_SMEM));
     FC_CUDA(cudaFuncSetAttribute(dgemm_tn_kernel<EpiStore>, cudaFuncAttributeMaxDynamicSharedMemorySize, DG_SMEM));
-    done = true;
+    done.fetch_or(bit);
     return FC_OK;
 }
 

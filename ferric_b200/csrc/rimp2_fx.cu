@@ -1369,15 +1369,16 @@ fc_status fx_split_pairs(const Rimp2Dev& d, cudaStream_t st, int* bad, FxSplit* 
 }
 
 fc_status fx_attrs() {
-    static bool done = false;
-    if (done) return FC_OK;
+    static std::atomic<uint64_t> done{0};
+    uint64_t bit = 0;
+    if (!attrs_needed(done, &bit)) return FC_OK;
     FC_CUDA(cudaFuncSetAttribute(pair_fx_kernel<0, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, fx::SMEM));
     FC_CUDA(cudaFuncSetAttribute(pair_fx_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, fx::SMEM));
     FC_CUDA(cudaFuncSetAttribute(pair_fx_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, fx::SMEM));
     FC_CUDA(cudaFuncSetAttribute(gemm_fx_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, GF_SMEM));
     FC_CUDA(cudaFuncSetAttribute(gemm_fx_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, GF_SMEM));
     FC_CUDA(cudaFuncSetAttribute(pair_fx_kernel<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, fx::SMEM));
-    done = true;
+    done.fetch_or(bit);
     return FC_OK;
 }
 
