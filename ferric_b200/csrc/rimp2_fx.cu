@@ -26,8 +26,9 @@
 // TMEM columns 384..511, the Y phase accumulates (ib|ja) = G_ji[a, b] into
 // the level columns, and the epilogue takes Y into registers (FP32) and hands
 // the level columns back before its FP64 work, which then runs under the
-// next item's X phase; each thread holds an element and its exchange partner.  Energy mode: unordered
-// pairs, E_OS += (X^2 + Y^2)/D, E_SS += (X - Y)^2/D (i == j: X phase only,
+// next item's X phase; 16 epilogue warps, each thread one row and 32 columns
+// of the tile, holding an element and its exchange partner.  Energy mode:
+// unordered pairs, E_OS += (X^2 + Y^2)/D, E_SS += (X - Y)^2/D (i == j: X phase only,
 // E_SS = 0), the reference pair loop of ferric-mp2/src/rimp2.rs:1399-1544
 // over both orderings.  Gradient mode: unordered pairs of an occupied chunk
 // pair (I, J); the item writes Tt_ij = (2X - Y)/D (FP32) into the rows of i
@@ -35,7 +36,7 @@
 // orderings; the adjoint contraction Gamma[:, I] += 4 Bq[:, J] Tt_IJ^T runs
 // in gemm_fx_kernel with the same exact-level scheme.  Diagonal tiles
 // (ta == tb, i != j) may run in one phase, Y = X^T passed through shared
-// memory (the exchange schedule).
+// memory into the free park columns (the exchange schedule).
 #include <algorithm>
 #include <cstdlib>
 
