@@ -47,6 +47,21 @@ fc_status copy_stream(cudaStream_t* s, cudaEvent_t* e) {
     return FC_OK;
 }
 
+// Stream and per-chunk events of the chunked upload of b_ov (host API).
+fc_status upload_stream(cudaStream_t* s, std::vector<cudaEvent_t>** evs, size_t n) {
+    static cudaStream_t us = nullptr;
+    static std::vector<cudaEvent_t> ev;
+    if (!us) FC_CUDA(cudaStreamCreateWithFlags(&us, cudaStreamNonBlocking));
+    while (ev.size() < n) {
+        cudaEvent_t e;
+        FC_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        ev.push_back(e);
+    }
+    *s = us;
+    *evs = &ev;
+    return FC_OK;
+}
+
 int64_t chunk_budget() {
     int64_t b = int64_t(8) << 30;
     if (const char* s = std::getenv("FERRIC_CUDA_CHUNK_BYTES")) {
@@ -323,11 +338,38 @@ fc_status fc_rimp2_energy_grad(const double* b_ov, int64_t naux, int64_t nocc, i
     FC_TRY(ws_get(WS_EPS, (nocc + nvir) * 8, &de));
     FC_TRY(ws_get(WS_GAMMA, nel * 8, &dg));
     FC_TRY(ws_get(WS_HOSTOUT, (nocc + nvir) * 8, &dd));
-    FC_CUDA(cudaMemcpyAsync(db, b_ov, nel * 8, cudaMemcpyHostToDevice, st));
-    FC_CUDA(cudaMemcpyAsync(de, eps_occ, nocc * 8, cudaMemcpyHostToDevice, st));
-    FC_CUDA(cudaMemcpyAsync((double*)de + nocc, eps_vir, nvir * 8, cudaMemcpyHostToDevice, st));
     Rimp2Dev d{(const double*)db, (const double*)de, (const double*)de + nocc, naux, nocc, nvir,
                0, 0.0, chunk_budget()};
+    // A pinned b_ov is uploaded in the gradient's occupied chunks on a copy
+    // stream: the mixed driver prepares each chunk once it has arrived, so all
+    // but the first chunk's copy overlap the first chunk pairs.  Otherwise one
+    // copy on the compute stream.
+    cudaPointerAttributes pb{};
+    const bool b_pinned = cudaPointerGetAttributes(&pb, b_ov) == cudaSuccess && pb.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    cudaStream_t us = nullptr;
+    if (b_pinned && precision == FC_PREC_MIXED) {
+        std::vector<cudaEvent_t>* evs = nullptr;
+        const int64_t cc = grad_chunk_fx(nocc, nvir, d.chunk_bytes, 1);
+        const int64_t nch = (nocc + cc - 1) / cc;
+        FC_TRY(upload_stream(&us, &evs, (size_t)nch));
+        // the upload may start once earlier work on the compute stream is done
+        FC_CUDA(cudaEventRecord((*evs)[0], st));
+        FC_CUDA(cudaStreamWaitEvent(us, (*evs)[0], 0));
+        const int64_t nov = nocc * nvir;
+        for (int64_t J = 0; J < nch; ++J) {
+            const int64_t o0 = J * cc, no = std::min(cc, nocc - o0);
+            FC_CUDA(cudaMemcpy2DAsync((double*)db + o0 * nvir, nov * 8, b_ov + o0 * nvir, nov * 8, no * nvir * 8,
+                                      naux, cudaMemcpyHostToDevice, us));
+            FC_CUDA(cudaEventRecord((*evs)[J], us));
+        }
+        d.arrive = evs->data();
+        d.arrive_cc = cc;
+    } else {
+        FC_CUDA(cudaMemcpyAsync(db, b_ov, nel * 8, cudaMemcpyHostToDevice, st));
+    }
+    FC_CUDA(cudaMemcpyAsync(de, eps_occ, nocc * 8, cudaMemcpyHostToDevice, st));
+    FC_CUDA(cudaMemcpyAsync((double*)de + nocc, eps_vir, nvir * 8, cudaMemcpyHostToDevice, st));
     // A pinned Gamma receives its column blocks while the gradient still runs
     // (a pageable one is copied at the end: an async copy from pageable memory
     // would hold the host thread that issues the kernels).
@@ -339,8 +381,11 @@ fc_status fc_rimp2_energy_grad(const double* b_ov, int64_t naux, int64_t nocc, i
     if (pinned && precision != FC_PREC_MIXED_FAST) {
         FC_TRY(copy_stream(&sink.stream, &sink.ready));
     }
-    FC_TRY(grad_dispatch(d, precision, st, e_os, e_ss, (double*)dg, (double*)dd, (double*)dd + nocc, stats,
-                         sink.stream ? &sink : nullptr));
+    const fc_status gs = grad_dispatch(d, precision, st, e_os, e_ss, (double*)dg, (double*)dd, (double*)dd + nocc,
+                                       stats, sink.stream ? &sink : nullptr);
+    // the caller may reuse b_ov once this returns, also after an error
+    if (us) FC_CUDA(cudaStreamSynchronize(us));
+    if (gs != FC_OK) return gs;
     if (!sink.stream) FC_CUDA(cudaMemcpyAsync(gamma, dg, nel * 8, cudaMemcpyDeviceToHost, st));
     FC_CUDA(cudaMemcpyAsync(de_docc, dd, nocc * 8, cudaMemcpyDeviceToHost, st));
     FC_CUDA(cudaMemcpyAsync(de_dvir, (double*)dd + nocc, nvir * 8, cudaMemcpyDeviceToHost, st));

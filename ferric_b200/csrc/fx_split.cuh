@@ -57,17 +57,19 @@ __device__ __forceinline__ void fx_slices(double x, double inv_s, typename SL::T
     c3 = SL::cast(c);
 }
 
-// Row q of B_ov -> Bq[s][q][j*tpad + b] (row pitch K) at the row's scale qs[q].
+// Row q of B_ov -> Bq[s][q][j*tpad + b] (row pitch K) at the row's scale qs[q],
+// over the columns k = j*nvir + b in [k0, k1) (k1 < 0: all).
 template <class SL = SliceBf16>
 __device__ __forceinline__ void split_fx_qrows_body(const double* __restrict__ B, int64_t nocc, int64_t nvir,
                                                     int64_t tpad, int64_t K, int64_t q_rows,
                                                     double* __restrict__ qs, typename SL::T* __restrict__ Bq,
-                                                    int64_t q) {
+                                                    int64_t q, int64_t k0 = 0, int64_t k1 = -1) {
     __shared__ double red[32];
     const int64_t nov = nocc * nvir;
+    const int64_t kend = k1 < 0 ? nov : k1;
     const double* row = B + q * nov;
     double m = 0.0;
-    for (int64_t k = threadIdx.x; k < nov; k += 256) m = fmax(m, fabs(row[k]));
+    for (int64_t k = k0 + threadIdx.x; k < kend; k += 256) m = fmax(m, fabs(row[k]));
     // block max (fixed order)
     for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
@@ -83,7 +85,7 @@ __device__ __forceinline__ void split_fx_qrows_body(const double* __restrict__ B
     const double inv = 1.0 / s;
     const int64_t ss = q_rows * K;
     typename SL::T* o0 = Bq + q * K;
-    for (int64_t k = threadIdx.x; k < nov; k += 256) {
+    for (int64_t k = k0 + threadIdx.x; k < kend; k += 256) {
         const int64_t j = k / nvir, b = k % nvir;
         typename SL::T c1, c2, c3;
         fx_slices<SL>(row[k], inv, c1, c2, c3);

@@ -15,6 +15,11 @@ struct Rimp2Dev {
     int64_t chunk_bytes;    // amplitude-chunk budget of the gradient
     int shard = 0;          // this process's share of the occupied pairs (of nshards)
     int nshards = 1;
+    // optional (mixed gradient): b_ov arrives in occupied chunks of arrive_cc
+    // orbitals, chunk J complete when arrive[J] has fired; the driver prepares
+    // a chunk after its event, so the upload overlaps the first chunk pairs
+    const cudaEvent_t* arrive = nullptr;
+    int64_t arrive_cc = 0;
 };
 
 // Occupied-pair sharding of one system over nshards processes (the same

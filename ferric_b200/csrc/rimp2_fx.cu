@@ -95,18 +95,20 @@ __device__ __forceinline__ double level_value(float w0, float w1, float w2, doub
 
 // ---------------------------------------------------------- split kernels --
 
-// cmax[c] = max over rows of |B[r, c]| (as ordered uint64 bits of a double).
+// cmax[c] = max over rows of |B[r, c]| (as ordered uint64 bits of a double),
+// for the columns c0 .. c0 + cols - 1 of rows of pitch ld (0: cols).
 __device__ __forceinline__ void colmax_body(const double* __restrict__ B, int64_t rows, int64_t cols,
                                             int64_t rows_per_split, unsigned long long* cmax, int* bad, int64_t bx,
-                                            int64_t by) {
-    const int64_t c = bx * 256 + threadIdx.x;
-    if (c >= cols) return;
+                                            int64_t by, int64_t ld = 0, int64_t c0 = 0) {
+    const int64_t c = c0 + bx * 256 + threadIdx.x;
+    if (c >= c0 + cols) return;
+    const int64_t pitch = ld ? ld : cols;
     const int64_t r0 = by * rows_per_split;
     const int64_t r1 = r0 + rows_per_split < rows ? r0 + rows_per_split : rows;
     double m = 0.0;
     bool nf = false;
     for (int64_t r = r0; r < r1; ++r) {
-        const double v = fabs(B[r * cols + c]);
+        const double v = fabs(B[r * pitch + c]);
         nf |= !(v <= 1.0e300);
         m = v > m ? v : m;
     }
@@ -115,39 +117,44 @@ __device__ __forceinline__ void colmax_body(const double* __restrict__ B, int64_
 }
 
 __global__ void __launch_bounds__(256) colmax_kernel(const double* __restrict__ B, int64_t rows, int64_t cols,
-                                                     int64_t rows_per_split, unsigned long long* cmax, int* bad) {
-    colmax_body(B, rows, cols, rows_per_split, cmax, bad, blockIdx.x, blockIdx.y);
+                                                     int64_t rows_per_split, unsigned long long* cmax, int* bad,
+                                                     int64_t ld = 0, int64_t c0 = 0) {
+    colmax_body(B, rows, cols, rows_per_split, cmax, bad, blockIdx.x, blockIdx.y, ld, c0);
 }
 
 
-// scl[i*a_pad + a] from the column maxima of B_ov (1 for padding rows).
+// scl[i*a_pad + a] from the column maxima of B_ov (1 for padding rows), for
+// the rows i*a_pad + a in [r0, r1) (r1 < 0: all).
 template <class SL>
 __global__ void row_scale_kernel(const unsigned long long* __restrict__ cmax, int64_t nocc, int64_t nvir,
-                                 int64_t a_pad, double* __restrict__ scl) {
-    const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= nocc * a_pad) return;
+                                 int64_t a_pad, double* __restrict__ scl, int64_t r0 = 0, int64_t r1 = -1) {
+    const int64_t r = r0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= (r1 < 0 ? nocc * a_pad : r1)) return;
     const int64_t i = r / a_pad, a = r % a_pad;
     scl[r] = a < nvir ? SL::scale(__longlong_as_double((long long)cmax[i * nvir + a])) : 1.0;
 }
 
 
-// B[q, ia] -> Bt[s][i][a][q] (q < q_pad) integer slices at scale scl[i*a_pad+a].
+// B[q, ia] -> Bt[s][i][a][q] (q < q_pad) integer slices at scale scl[i*a_pad+a],
+// for the columns ia in [c0, c1) (c1 < 0: all).
 template <class SL>
 __device__ __forceinline__ void split_fx_transpose_body(const double* __restrict__ B, int64_t naux, int64_t nocc,
                                                         int64_t nvir, int64_t a_pad, int64_t q_pad,
                                                         const double* __restrict__ scl,
-                                                        typename SL::T* __restrict__ Bt, int64_t bx, int64_t by) {
+                                                        typename SL::T* __restrict__ Bt, int64_t bx, int64_t by,
+                                                        int64_t c0 = 0, int64_t c1 = -1) {
     using E = typename SL::T;
     struct alignas(2 * sizeof(E)) P2 { E e[2]; };
     __shared__ double tile[64][65];
     const int64_t nov = nocc * nvir;
-    const int64_t q0 = by * 64, ia0 = bx * 64;
+    const int64_t cend = c1 < 0 ? nov : c1;
+    const int64_t q0 = by * 64, ia0 = c0 + bx * 64;
     const int tid = threadIdx.x;
 #pragma unroll
     for (int e = 0; e < 16; ++e) {
         const int idx = tid + 256 * e, r = idx >> 6, c = idx & 63;
         const int64_t q = q0 + r, ia = ia0 + c;
-        tile[r][c] = (q < naux && ia < nov) ? B[q * nov + ia] : 0.0;
+        tile[r][c] = (q < naux && ia < cend) ? B[q * nov + ia] : 0.0;
     }
     __syncthreads();
     const int64_t ss = nocc * a_pad * q_pad;
@@ -155,7 +162,7 @@ __device__ __forceinline__ void split_fx_transpose_body(const double* __restrict
     for (int e = 0; e < 8; ++e) {
         const int idx = tid + 256 * e, c = idx >> 5, qq = (idx & 31) * 2;
         const int64_t ia = ia0 + c;
-        if (ia >= nov) continue;
+        if (ia >= cend) continue;
         const int64_t i = ia / nvir, a = ia % nvir;
         const double inv = 1.0 / scl[i * a_pad + a];
         P2 pa, pb, pc;
@@ -172,8 +179,9 @@ template <class SL>
 __global__ void __launch_bounds__(256) split_fx_transpose_kernel(const double* __restrict__ B, int64_t naux,
                                                                  int64_t nocc, int64_t nvir, int64_t a_pad,
                                                                  int64_t q_pad, const double* __restrict__ scl,
-                                                                 typename SL::T* __restrict__ Bt) {
-    split_fx_transpose_body<SL>(B, naux, nocc, nvir, a_pad, q_pad, scl, Bt, blockIdx.x, blockIdx.y);
+                                                                 typename SL::T* __restrict__ Bt, int64_t c0 = 0,
+                                                                 int64_t c1 = -1) {
+    split_fx_transpose_body<SL>(B, naux, nocc, nvir, a_pad, q_pad, scl, Bt, blockIdx.x, blockIdx.y, c0, c1);
 }
 
 __global__ void fill_kernel(double* __restrict__ x, int64_t n, double v) {
@@ -187,8 +195,9 @@ __global__ void fill_kernel(double* __restrict__ x, int64_t n, double v) {
 __global__ void __launch_bounds__(256) split_fx_qrows_kernel(const double* __restrict__ B, int64_t nocc,
                                                              int64_t nvir, int64_t tpad, int64_t K,
                                                              int64_t q_rows, double* __restrict__ qs,
-                                                             int8_t* __restrict__ Bq) {
-    split_fx_qrows_body<SliceI8>(B, nocc, nvir, tpad, K, q_rows, qs, Bq, blockIdx.x);
+                                                             int8_t* __restrict__ Bq, int64_t k0 = 0,
+                                                             int64_t k1 = -1) {
+    split_fx_qrows_body<SliceI8>(B, nocc, nvir, tpad, K, q_rows, qs, Bq, blockIdx.x, k0, k1);
 }
 
 
@@ -1327,46 +1336,59 @@ constexpr int64_t PAIR_KMAX = 44382;
 struct FxSplit {
     int8_t* bt;
     double* scl;
+    unsigned long long* cmax;
     int64_t a_pad, q_pad;
     CUtensorMap tmA, tmB;
 };
 
-fc_status fx_split_pairs(const Rimp2Dev& d, cudaStream_t st, int* bad, FxSplit* o) {
+// The pair operands: buffers (zeroed: padding rows and columns stay 0) and
+// tensor maps; fx_split_range fills the slices of occupied orbitals [o0, o1).
+fc_status fx_split_alloc(const Rimp2Dev& d, cudaStream_t st, FxSplit* o) {
     const int64_t a_pad = (d.nvir + fx::BM - 1) / fx::BM * fx::BM;
     const int64_t q_pad = (d.naux + fx::KT - 1) / fx::KT * fx::KT;
     const int64_t nov = d.nocc * d.nvir;
     const int64_t rows = (int64_t)fx::NSL * d.nocc * a_pad;
     if (d.naux > PAIR_KMAX)
         return fail(FC_ERR_LAYOUT, "mixed RI-MP2: naux > 44382 exceeds the exact int32 level sums (use FP64)");
+    if ((d.naux + 63) / 64 > 65535) return fail(FC_ERR_LAYOUT, "split: naux too large");
+    if (rows > (int64_t)UINT32_MAX) return fail(FC_ERR_LAYOUT, "split: too many operand rows");
     void *vbt, *vscl;
     FC_TRY(ws_get(WS_SPLIT, (size_t)rows * q_pad, &vbt));
     FC_TRY(ws_get(WS_SCALE, (size_t)(nov + d.nocc * a_pad) * 8 + 256, &vscl));
-    unsigned long long* cmax = (unsigned long long*)vscl;
-    double* scl = (double*)vscl + nov;
-    FC_CUDA(cudaMemsetAsync(cmax, 0, nov * 8, st));
+    o->cmax = (unsigned long long*)vscl;
+    o->scl = (double*)vscl + nov;
+    FC_CUDA(cudaMemsetAsync(o->cmax, 0, nov * 8, st));
     FC_CUDA(cudaMemsetAsync(vbt, 0, (size_t)rows * q_pad, st));
-    {
-        const int64_t rps = 64;
-        dim3 g((unsigned)((nov + 255) / 256), (unsigned)((d.naux + rps - 1) / rps));
-        colmax_kernel<<<g, 256, 0, st>>>(d.b_ov, d.naux, nov, rps, cmax, bad);
-    }
-    row_scale_kernel<SliceI8><<<(unsigned)((d.nocc * a_pad + 255) / 256), 256, 0, st>>>(cmax, d.nocc, d.nvir,
-                                                                                        a_pad, scl);
-    {
-        dim3 g((unsigned)((nov + 63) / 64), (unsigned)((d.naux + 63) / 64));
-        if (g.y > 65535) return fail(FC_ERR_LAYOUT, "split: naux too large");
-        split_fx_transpose_kernel<SliceI8><<<g, 256, 0, st>>>(d.b_ov, d.naux, d.nocc, d.nvir, a_pad, q_pad, scl,
-                                                              (int8_t*)vbt);
-    }
-    FC_TRY(check_launch("fixed-point split kernels"));
-    if (rows > (int64_t)UINT32_MAX) return fail(FC_ERR_LAYOUT, "split: too many operand rows");
     FC_TRY(make_tmap_i8_2d(&o->tmA, vbt, q_pad, rows, q_pad, fx::KT, fx::BM));
     FC_TRY(make_tmap_i8_2d(&o->tmB, vbt, q_pad, rows, q_pad, fx::KT, fx::BN));
     o->bt = (int8_t*)vbt;
-    o->scl = scl;
     o->a_pad = a_pad;
     o->q_pad = q_pad;
     return FC_OK;
+}
+
+fc_status fx_split_range(const Rimp2Dev& d, cudaStream_t st, int* bad, const FxSplit& o, int64_t o0, int64_t o1) {
+    const int64_t nov = d.nocc * d.nvir;
+    const int64_t c0 = o0 * d.nvir, nc = (o1 - o0) * d.nvir;
+    {
+        const int64_t rps = 64;
+        dim3 g((unsigned)((nc + 255) / 256), (unsigned)((d.naux + rps - 1) / rps));
+        colmax_kernel<<<g, 256, 0, st>>>(d.b_ov, d.naux, nc, rps, o.cmax, bad, nov, c0);
+    }
+    const int64_t r0 = o0 * o.a_pad, r1 = o1 * o.a_pad;
+    row_scale_kernel<SliceI8><<<(unsigned)((r1 - r0 + 255) / 256), 256, 0, st>>>(o.cmax, d.nocc, d.nvir, o.a_pad,
+                                                                                 o.scl, r0, r1);
+    {
+        dim3 g((unsigned)((nc + 63) / 64), (unsigned)((d.naux + 63) / 64));
+        split_fx_transpose_kernel<SliceI8><<<g, 256, 0, st>>>(d.b_ov, d.naux, d.nocc, d.nvir, o.a_pad, o.q_pad,
+                                                              o.scl, o.bt, c0, c0 + nc);
+    }
+    return check_launch("fixed-point split kernels");
+}
+
+fc_status fx_split_pairs(const Rimp2Dev& d, cudaStream_t st, int* bad, FxSplit* o) {
+    FC_TRY(fx_split_alloc(d, st, o));
+    return fx_split_range(d, st, bad, *o, 0, d.nocc);
 }
 
 fc_status fx_attrs() {
@@ -1505,7 +1527,7 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
     int* flags = (int*)vout0;  // [0] range, [1] timeout
     FC_CUDA(cudaMemsetAsync(vout0, 0, 256, st));
     if (stats) FC_CUDA(cudaEventRecord(c.ev0, st));
-    FC_TRY(fx_split_pairs(d, st, flags, &sp));
+    FC_TRY(fx_split_alloc(d, st, &sp));
     const int64_t a_pad = sp.a_pad;
     const int64_t tp = (nvir + 15) / 16 * 16;  // amplitude pitch: rows (i, a) and columns (j, b), a, b < tp
                                                // (16: int8 slice columns of a chunk start 16-byte aligned)
@@ -1548,8 +1570,8 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
     void *vbq, *vtab, *vT, *vTs, *vpart;
     const size_t tab_bytes = ((pairs.size() * sizeof(int2) + 255) / 256) * 256;
     FC_TRY(ws_get(WS_SPLIT2, (size_t)3 * q_rows * K2, &vbq));
-    FC_TRY(ws_get(WS_PAIRS, tab_bytes + q_rows * 8, &vtab));
-    double* qs = (double*)((char*)vtab + tab_bytes);
+    FC_TRY(ws_get(WS_PAIRS, tab_bytes + (size_t)nch * q_rows * 8, &vtab));
+    double* qs = (double*)((char*)vtab + tab_bytes);  // [nch][q_rows] Q-row scales per occupied chunk
     const size_t cbytes = (size_t)cc * tp * cc * tp;  // elements of one amplitude block
     const int64_t mp_max = (cc * tp + 127) / 128 * 128;
     FC_TRY(ws_get(WS_T, cbytes * 8 + (size_t)mp_max * 8, &vT));
@@ -1575,11 +1597,29 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
     FC_CUDA(cudaMemsetAsync(acc_occ, 0, nocc * 8, st));
     FC_CUDA(cudaMemsetAsync(e_cp, 0, 2 * ncp * 8, st));  // chunk pairs of other shards add nothing
     FC_CUDA(cudaMemsetAsync(gamma, 0, (size_t)naux * nov * 8, st));
-    // per-Q-row split of B_ov for the adjoint contraction
+    // per-Q-row split of B_ov for the adjoint contraction, at one scale per
+    // (Q row, occupied chunk): a chunk's slices need only its own columns
     FC_CUDA(cudaMemsetAsync(vbq, 0, (size_t)3 * q_rows * K2, st));
-    fill_kernel<<<(unsigned)((q_rows + 255) / 256), 256, 0, st>>>(qs, q_rows, 1.0);
-    split_fx_qrows_kernel<<<(unsigned)naux, 256, 0, st>>>(d.b_ov, nocc, nvir, tp, K2, q_rows, qs, (int8_t*)vbq);
-    FC_TRY(check_launch("split_fx_qrows_kernel"));
+    fill_kernel<<<(unsigned)((nch * q_rows + 255) / 256), 256, 0, st>>>(qs, nch * q_rows, 1.0);
+    // Occupied chunk J's operands (pair slices and Q-row slices) are made the
+    // first time a chunk pair uses it -- after its columns of b_ov arrived,
+    // when the caller uploads them chunk by chunk (d.arrive)
+    const bool arrive_ok = d.arrive && d.arrive_cc == cc;
+    if (d.arrive && !arrive_ok)
+        for (int64_t J = 0; J < (nocc + d.arrive_cc - 1) / d.arrive_cc; ++J)
+            FC_CUDA(cudaStreamWaitEvent(st, d.arrive[J], 0));
+    std::vector<char> ready((size_t)nch, 0);
+    auto prep = [&](int64_t J) -> fc_status {
+        if (ready[(size_t)J]) return FC_OK;
+        if (arrive_ok) FC_CUDA(cudaStreamWaitEvent(st, d.arrive[J], 0));
+        const int64_t o0 = J * cc, o1 = std::min(nocc, o0 + cc);
+        FC_TRY(fx_split_range(d, st, flags, sp, o0, o1));
+        split_fx_qrows_kernel<<<(unsigned)naux, 256, 0, st>>>(d.b_ov, nocc, nvir, tp, K2, q_rows, qs + J * q_rows,
+                                                              (int8_t*)vbq, o0 * nvir, o1 * nvir);
+        FC_TRY(check_launch("split_fx_qrows_kernel"));
+        ready[(size_t)J] = 1;
+        return FC_OK;
+    };
     CUtensorMap tmBq;
     FC_TRY(make_tmap_i8_2d(&tmBq, vbq, K2, 3 * q_rows, K2, fx::KT, 128));
     const int2* dpairs = (const int2*)vtab;
@@ -1602,7 +1642,7 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
         FC_TRY(make_tmap_i8_2d(&tmTs, vTs, ldk, 3 * mp, ldk, fx::KT, 128));
         GemmFxArgs g{};
         g.rs = ts;
-        g.cs = qs;
+        g.cs = qs + (k0 / cc) * q_rows;  // the Q-row scales of the column chunk
         g.M = (int)mp;
         g.N = (int)q_rows;
         g.nTm = (int)(mp / 128);
@@ -1641,6 +1681,8 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
             }
             continue;
         }
+        FC_TRY(prep(cp.i0 / cc));
+        FC_TRY(prep(cp.j0 / cc));
         PairFxArgs a{};
         a.eo = d.eps_occ;
         a.ev = d.eps_vir;
