@@ -1600,7 +1600,9 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
     // per-Q-row split of B_ov for the adjoint contraction, at one scale per
     // (Q row, occupied chunk): a chunk's slices need only its own columns
     FC_CUDA(cudaMemsetAsync(vbq, 0, (size_t)3 * q_rows * K2, st));
+    int64_t nl = 0;  // kernels launched
     fill_kernel<<<(unsigned)((nch * q_rows + 255) / 256), 256, 0, st>>>(qs, nch * q_rows, 1.0);
+    ++nl;
     // Occupied chunk J's operands (pair slices and Q-row slices) are made the
     // first time a chunk pair uses it -- after its columns of b_ov arrived,
     // when the caller uploads them chunk by chunk (d.arrive)
@@ -1617,6 +1619,7 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
         split_fx_qrows_kernel<<<(unsigned)naux, 256, 0, st>>>(d.b_ov, nocc, nvir, tp, K2, q_rows, qs + J * q_rows,
                                                               (int8_t*)vbq, o0 * nvir, o1 * nvir);
         FC_TRY(check_launch("split_fx_qrows_kernel"));
+        nl += 4;  // column maxima, scales, pair slices, Q-row slices
         ready[(size_t)J] = 1;
         return FC_OK;
     };
@@ -1638,6 +1641,7 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
     auto adjoint = [&](float* T, int64_t r0, int64_t nr, int64_t k0, int64_t nk) -> fc_status {
         const int64_t ldk = nk * tp, rows = nr * tp, mp = (rows + 127) / 128 * 128;
         split_fx_rows_f32_kernel<<<(unsigned)rows, 256, 0, st>>>(T, ldk, mp, ts, (int8_t*)vTs);
+        ++nl;
         CUtensorMap tmTs;
         FC_TRY(make_tmap_i8_2d(&tmTs, vTs, ldk, 3 * mp, ldk, fx::KT, 128));
         GemmFxArgs g{};
@@ -1668,6 +1672,7 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
             g.nk = (int)((kl + fx::KT - 1) / fx::KT);
             gemm_fx_kernel<0><<<g2, GF_THREADS, GF_SMEM, st>>>(tmTs, tmBq, g);
             FC_TRY(check_launch("gemm_fx_kernel"));
+            ++nl;
         }
         return FC_OK;
     };
@@ -1727,12 +1732,14 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
                                                                                        (int)nvir, de_dvir);
         }
         FC_TRY(check_launch("gradient reductions"));
+        nl += 5;  // pair kernel and its four reductions
         FC_TRY(adjoint(T1, cp.i0, cp.ni, cp.j0, cp.nj));
         if (!same) FC_TRY(adjoint(T2, cp.j0, cp.nj, cp.i0, cp.ni));
         // row I of the chunk pairs is done: Gamma's columns of chunk I are final
         if (sink && cp.j0 + cp.nj == nocc) FC_TRY(gamma_sink_block(sink, gamma, naux, nov, nvir, cp.i0, cp.ni, st));
     }
     scale_copy_kernel<<<(unsigned)((nocc + 255) / 256), 256, 0, st>>>(acc_occ, nocc, -2.0, de_docc);
+    ++nl;
     FC_TRY(check_launch("scale_copy_kernel"));
     if (stats) FC_CUDA(cudaEventRecord(c.ev1, st));
     std::vector<double> h((size_t)(2 * ncp));
@@ -1761,7 +1768,7 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
         const double P = (double)nocc * (nocc + 1) / 2.0;
         stats->flops = 2.0 * naux * (double)nvir * nvir * P + 2.0 * naux * (double)nov * nov;
         stats->precision = FC_PREC_MIXED;
-        stats->launches += (int)(5 * ncp + 6 * (ncp - nch) + 6);
+        stats->launches += (int)nl;
         stats->tile_m = fx::BM;
         stats->tile_n = fx::BN;
         stats->main_launches = (int)ncp;
