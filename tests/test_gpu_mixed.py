@@ -152,6 +152,28 @@ def test_mixed_gradient_chunked(fc, monkeypatch):
     assert np.abs(many[3] - d_v).max() <= MIXED_D_REL * np.abs(d_v).max()
 
 
+def test_mixed_gradient_pinned_upload(fc, monkeypatch):
+    """A page-locked B_ov goes up chunk by chunk on a copy stream while the
+    gradient runs, each chunk's operands made after its arrival event: with
+    several chunks the host API's result is the device API's bit for bit,
+    and a pageable B_ov (one copy before the compute) gives the same."""
+    import torch
+    from ferric_b200 import rimp2
+    b, eo, ev = synthetic.rimp2_inputs(160, 9, 40)
+    monkeypatch.setenv("FERRIC_CUDA_CHUNK_BYTES", str(chunk_budget(40, 2)))  # chunks of 2
+    pinned = torch.empty(b.shape, dtype=torch.float64).pin_memory()
+    pinned.numpy()[:] = b
+    up = rimp2.rimp2_energy_grad(pinned.numpy(), eo, ev, precision="mixed")
+    dev = rimp2.rimp2_energy_grad(torch.from_numpy(b).cuda(), torch.from_numpy(eo).cuda(),
+                                  torch.from_numpy(ev).cuda(), precision="mixed")
+    paged = rimp2.rimp2_energy_grad(b, eo, ev, precision="mixed")
+    for other in (dev, paged):
+        assert (up[0].e_os, up[0].e_ss) == (other[0].e_os, other[0].e_ss)
+        for x, y in zip(up[1:], other[1:]):
+            y = y.cpu().numpy() if hasattr(y, "cpu") else y
+            assert np.array_equal(x, y)
+
+
 def test_adjoint_k_segments(fc, monkeypatch):
     """The adjoint contraction keeps its int32 level sums exact by running K
     in segments (32768 by default) that each add into Gamma; with 128-column
