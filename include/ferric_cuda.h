@@ -115,8 +115,12 @@ fc_status fc_rimp2_energy_dev(const double* b_ov, int64_t naux, int64_t nocc, in
  * de_docc[i] = dE/d eps_occ[i] and de_dvir[a] = dE/d eps_vir[a]
  * (= 2 diag(P_oo), 2 diag(P_vv) of ferric-mp2/src/oo_rimp2.rs:1170-1300).
  * E = E_os + E_ss.  No amplitudes are stored: occupied-pair blocks are
- * recomputed.  In the _dev form e_os/e_ss are host scalars and the call
- * synchronises its stream before returning. */
+ * recomputed.  In the host form, page-locked b_ov and gamma let the copies
+ * overlap the compute (b_ov goes up in occupied chunks as FC_PREC_MIXED
+ * needs them, gamma comes down in column blocks as they are final);
+ * pageable buffers are copied before and after.  In the _dev form
+ * e_os/e_ss are host scalars and the call synchronises its stream before
+ * returning. */
 fc_status fc_rimp2_energy_grad(const double* b_ov, int64_t naux, int64_t nocc, int64_t nvir,
                                const double* eps_occ, const double* eps_vir, int32_t precision,
                                double* e_os, double* e_ss, double* gamma,
