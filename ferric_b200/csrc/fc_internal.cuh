@@ -73,6 +73,7 @@ enum WsSlot {
     WS_SPLIT2,     // integer-slice adjoint operand (Q rows)
     WS_SCALE,      // column maxima + operand-row scales
     WS_MISC,       // DF-J weights / d_P, DF-K C^T
+    WS_PSCR,       // pair kernel: FP64 X / Y tiles of each CTA
     WS_COUNT
 };
 

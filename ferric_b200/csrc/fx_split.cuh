@@ -1,16 +1,19 @@
 // Exact integer-slice splits.  Every operand row r gets a power of two s_r
-// and three integer slices,
-//     x / s_r = c1 + c2 / W + c3 / W^2 + eps,   |eps| <= 1 / (2 W^2),
+// and three (or four) integer slices,
+//     x / s_r = c1 + c2 / W + c3 / W^2 [+ c4 / W^3] + eps,
+//     |eps| <= 1 / (2 W^2)  [1 / (2 W^3) with four slices],
 // so tensor-core sums of slice products are exact integers.  Two formats:
 //   SliceBf16  bf16 integers in [-128, 128], W = 256, max|x| / s in [64, 128);
 //              FP32 accumulation, exact while sums stay below 2^24 (the
 //              DF-K, dressing and Imat GEMMs, which drain to FP64 in panels);
 //   SliceI8    int8 integers in [-127, 127], W = 254, max|x| / s in (63.5, 127];
-//              int32 accumulation (tcgen05.mma kind::i8), exact for
-//              K <= 2^31 / (3 127^2) = 44382 (the RI-MP2 pair kernel and the
-//              adjoint contraction).
-// Both carry about 23 significant bits of each element relative to its row
-// maximum.
+//              int32 accumulation (tcgen05.mma kind::i8).  Three slices (the
+//              adjoint contraction, up to three products per level): exact for
+//              K <= (2^31 - 1) / (3 127^2) = 44381.  Four slices (the RI-MP2 pair
+//              kernel, up to four products per level): K <= (2^31 - 1) / (4 127^2)
+//              = 33286.
+// Three slices carry about 23 significant bits of each element relative to
+// its row maximum, four about 31.
 #pragma once
 #include <cuda_bf16.h>
 #include <cstdint>
@@ -55,6 +58,23 @@ __device__ __forceinline__ void fx_slices(double x, double inv_s, typename SL::T
     c1 = SL::cast(a);
     c2 = SL::cast(b);
     c3 = SL::cast(c);
+}
+
+// Four slices (the pair operands of the RI-MP2 pair kernel).
+template <class SL = SliceI8>
+__device__ __forceinline__ void fx_slices4(double x, double inv_s, typename SL::T& c1, typename SL::T& c2,
+                                           typename SL::T& c3, typename SL::T& c4) {
+    const double y = x * inv_s;
+    const double a = rint(y);
+    const double y2 = (y - a) * SL::W;
+    const double b = rint(y2);
+    const double y3 = (y2 - b) * SL::W;
+    const double c = rint(y3);
+    const double d = rint((y3 - c) * SL::W);
+    c1 = SL::cast(a);
+    c2 = SL::cast(b);
+    c3 = SL::cast(c);
+    c4 = SL::cast(d);
 }
 
 // Row q of B_ov -> Bq[s][q][j*tpad + b] (row pitch K) at the row's scale qs[q],

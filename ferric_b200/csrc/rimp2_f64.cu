@@ -675,6 +675,11 @@ extern "C" fc_status fc_rimp2_energy_noalloc(const double* b_ov, int64_t naux, i
     const int64_t npairs = nocc * (nocc + 1) / 2;
     const int64_t ntile = (nvir + PR_T - 1) / PR_T;
     const int64_t ntiles = ntile * (ntile + 1) / 2;
+    // the pair and tile tables alone must fit before their product is formed
+    // (npairs * ntiles can exceed int64 at the accepted dimension bounds)
+    if ((size_t)(npairs + ntiles) * sizeof(int2) > kNoallocScratchBytes)
+        return fail(FC_ERR_LAYOUT, "fc_rimp2_energy_noalloc: the pair and tile tables alone exceed the fixed scratch of " +
+                                       std::to_string(kNoallocScratchBytes) + " B; use fc_rimp2_energy_dev");
     const int64_t items = npairs * ntiles;
     const size_t pair_bytes = ((size_t)(npairs + ntiles) * sizeof(int2) + 255) / 256 * 256;
     const size_t part_bytes = ((size_t)items * 2 * sizeof(double) + 255) / 256 * 256;

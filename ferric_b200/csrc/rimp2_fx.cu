@@ -6,37 +6,43 @@
 // ~1e-5 relative in E (the effect the reference measured for its f32 path,
 // ferric-core/src/gpu/mixed.rs:18-21).  Here the operands are split into
 // integer slices and multiplied on tcgen05.mma kind::i8 with int32
-// accumulation, exact whatever the magnitudes (K <= 44382).  The int8 MMA
-// covers twice the K of a bf16 one per instruction and its operands are half
-// the bytes, so the six products cost what three bf16 products would.
+// accumulation, exact whatever the magnitudes.
 //
 // Split (SliceI8).  Each operand row r (an (i, a) column of B_ov over Q for
 // the pair products, a Q row over (j, b) for the adjoint contraction) gets a
-// power of two s_r with max|x| / s_r in (63.5, 127], and three int8 slices
-// holding integers in [-127, 127]:
-//     x / s_r = c1 + c2 / 254 + c3 / 254^2 + eps,   |eps| <= 2^-17.
-// Products.  Three levels, one TMEM accumulator each, exact in int32:
-//     L0 = c1 c1',  L1 = c1 c2' + c2 c1',  L2 = c1 c3' + c2 c2' + c3 c1'
-// (6 int8 tensor-core products), combined in FP64 in the epilogue:
-//     g = s_r s_r' ((L0 254 + L1) 254 + L2) / 254^2.
+// power of two s_r with max|x| / s_r in (63.5, 127], and int8 slices holding
+// integers in [-127, 127]:
+//     x / s_r = c1 + c2 / 254 + c3 / 254^2 [+ c4 / 254^3] + eps.
+// Pair kernel: four slices (|eps| <= 1/(2 254^3)) and the ten products of
+// level k + m <= 3 in four TMEM accumulators, exact in int32 while
+// 4 * 127^2 * naux < 2^31 (naux <= 33286):
+//     L0 = c1 c1',  L1 = c1 c2' + c2 c1',  L2 = c1 c3' + c2 c2' + c3 c1',
+//     L3 = c1 c4' + c2 c3' + c3 c2' + c4 c1',
+//     g = s_r s_r' (((L0 254 + L1) 254 + L2) 254 + L3) / 254^3   (exact FP64 integer).
+// The dropped level-4 products are 254^-4 of the row scales and of random
+// sign, except where a row meets itself: (ia|ia) in the i == j blocks, whose
+// c3 c3' term is one-signed; those values are taken exactly in FP64 from
+// sum_Q B_Q,ia^2 (colsq_kernel).  Emulated at the config-3 shapes (naux 4800,
+// nocc 120, nvir 1100, sampled pairs), E is within ~3e-8 Eh of FP64; three
+// slices were 5e-5 Eh off.
+// Adjoint contraction: three slices, six products in three accumulators
+// (L0, L1, L2 above), exact while 3 * 127^2 * K < 2^31 (K segments of 32768).
 //
 // Pair kernel (this file): item = (pair, a-tile 128, b-tile 128); the X phase
-// accumulates (ia|jb) into the three level accumulators (3 x 128 TMEM
-// columns), the epilogue parks it in FP32 (round to nearest) in the spare
-// TMEM columns 384..511, the Y phase accumulates (ib|ja) = G_ji[a, b] into
-// the level columns, and the epilogue takes Y into registers (FP32) and hands
-// the level columns back before its FP64 work, which then runs under the
-// next item's X phase; 16 epilogue warps, each thread one row and 32 columns
-// of the tile, holding an element and its exchange partner.  Energy mode:
-// unordered pairs, E_OS += (X^2 + Y^2)/D, E_SS += (X - Y)^2/D (i == j: X phase only,
-// E_SS = 0), the reference pair loop of ferric-mp2/src/rimp2.rs:1399-1544
-// over both orderings.  Gradient mode: unordered pairs of an occupied chunk
-// pair (I, J); the item writes Tt_ij = (2X - Y)/D (FP32) into the rows of i
-// and Tt_ji = Tt_ij^T into the rows of j, and the dE/deps partials of both
+// accumulates (ia|jb) into the four level accumulators (all 512 TMEM
+// columns); the epilogue drains them into the CTA's FP64 X tile in global
+// scratch (L2-resident) and hands TMEM back; the Y phase accumulates
+// (ib|ja) = G_ji[a, b] and is drained into the Y tile; the FP64 terms then
+// run from the tiles under the next item's X phase.  16 epilogue warps, each
+// thread one row and 32 columns of the tile.  Energy mode: unordered pairs,
+// E_OS += (X^2 + Y^2)/D, E_SS += (X - Y)^2/D (i == j: X phase only, E_SS = 0),
+// the reference pair loop of ferric-mp2/src/rimp2.rs:1399-1544 over both
+// orderings.  Gradient mode: unordered pairs of an occupied chunk pair
+// (I, J); the item writes Tt_ij = (2X - Y)/D (FP32) into the rows of i and
+// Tt_ji = Tt_ij^T into the rows of j, and the dE/deps partials of both
 // orderings; the adjoint contraction Gamma[:, I] += 4 Bq[:, J] Tt_IJ^T runs
-// in gemm_fx_kernel with the same exact-level scheme.  Diagonal tiles
-// (ta == tb, i != j) may run in one phase, Y = X^T passed through shared
-// memory into the free park columns (the exchange schedule).
+// in gemm_fx_kernel.  Diagonal tiles (ta == tb, i != j) run in one phase,
+// Y = X^T read back transposed from the X tile (the exchange schedule).
 #include <algorithm>
 #include <cstdlib>
 
@@ -53,35 +59,41 @@ namespace fc {
 namespace fx {
 
 constexpr int BM = 128, BN = 128;
-constexpr int KT = 128;       // int8 elements (128 B) of K per pipeline stage
+constexpr int KT = 128;       // int8 elements (128 B) of K per pipeline stage (adjoint contraction)
 constexpr int KT_BF16 = 64;   // bf16 elements per stage of the exact-slice xgemm (opposite-spin UMP2)
-constexpr int64_t KMAX = 32768;  // K per int32 accumulation (< 44382: 3 * 127^2 * K < 2^31)
+constexpr int64_t KMAX = 32768;  // K per int32 accumulation of the adjoint (3 * 127^2 * K < 2^31)
 constexpr int A_BYTES = BM * KT;  // 16 KiB of int8
 constexpr int B_BYTES = BN * KT;  // 16 KiB of int8
 constexpr int NSL = 3;
-constexpr int STAGE_BYTES = NSL * (A_BYTES + B_BYTES);  // 96 KiB
-constexpr int STAGES = 2;
-constexpr int XP = BM + 1;                       // pitch of the exchange rows (floats)
-constexpr int XBUF_BYTES = 32 * XP * 4;          // one lane quarter of a parked X tile
+// Pair kernel: four int8 slices per operand row, 64 B of K per stage (a
+// 64-byte-swizzled box), three stages; four level accumulators fill TMEM.
+constexpr int PKT = 64;
+constexpr int PSL = 4;
+constexpr int PA_BYTES = BM * PKT;                       // 8 KiB
+constexpr int PB_BYTES = BN * PKT;                       // 8 KiB
+constexpr int PSTAGE_BYTES = PSL * (PA_BYTES + PB_BYTES);  // 64 KiB
+constexpr int PSTAGES = 3;
 constexpr int COL_BYTES = 3 * BN * 8;             // a tile's virtual energies and column scales
 // Pair-kernel epilogue: EPI_WARPS warps, EPI_WARPS / 4 per TMEM lane quadrant;
 // each thread owns one row of the tile and HC of its columns.  The FP64
 // epilogue is latency-bound (few independent FP64 instructions in flight per
 // warp): 16 warps (4 per scheduler) at 32 columns each hide more of that
-// latency than 8 at 64, within the 96 registers a thread that 18 warps leave.
+// latency than 8 at 64.
 constexpr int EPI_WARPS = 16;
 constexpr int NCG = EPI_WARPS / 4;                // column groups per row
 constexpr int HC = BN / NCG;                      // columns per thread
 constexpr int EPI_THREADS = 32 * EPI_WARPS;
 constexpr int PAIR_THREADS = 64 + EPI_THREADS;    // + TMA producer warp + MMA warp
-// epilogue scratch after the barriers (64 B): per-warp partials [2][EPI_WARPS][3],
-// row sums of column groups 1.. [NCG - 1][BM], column sums [4][NCG][HC] (doubles)
+// epilogue scratch after the barriers ((2 PSTAGES + 4) x 8 B): per-warp partials
+// [2][EPI_WARPS][3], row sums of column groups 1.. [NCG - 1][BM], column sums
+// [4][NCG][HC] (doubles)
 constexpr int SCR_BYTES = 8192;
-static_assert(64 + 8 * (2 * EPI_WARPS * 3 + (NCG - 1) * BM + 4 * NCG * HC) <= SCR_BYTES, "pair scratch");
+static_assert((2 * PSTAGES + 4) * 8 + 8 * (2 * EPI_WARPS * 3 + (NCG - 1) * BM + 4 * NCG * HC) <= SCR_BYTES,
+              "pair scratch");
 static_assert(HC % 32 == 0 && 4 * NCG == EPI_WARPS, "pair epilogue layout");
-constexpr int SMEM = STAGES * STAGE_BYTES + 1024 + SCR_BYTES + XBUF_BYTES + COL_BYTES;
+constexpr int SMEM = PSTAGES * PSTAGE_BYTES + 1024 + SCR_BYTES + COL_BYTES;
 constexpr uint32_t IDESC = tc::idesc_i8_s32(128, 128);
-constexpr double LW = 254.0, LW2INV = 1.0 / (254.0 * 254.0);
+constexpr double LW = 254.0, LW2INV = 1.0 / (254.0 * 254.0), LW3INV = 1.0 / (254.0 * 254.0 * 254.0);
 
 // s (L0 + L1 / 254 + L2 / 254^2) from the three int32 TMEM words of a level
 // set: the integer combination (L0 254 + L1) 254 + L2 is exact in FP64.
@@ -90,6 +102,14 @@ __device__ __forceinline__ double level_value(float w0, float w1, float w2, doub
     return v * (s * LW2INV);
 }
 
+// s (L0 + L1 / 254 + L2 / 254^2 + L3 / 254^3) from the four int32 TMEM words
+// of the pair kernel's level set: ((L0 254 + L1) 254 + L2) 254 + L3 is an
+// integer below 2^53 while K <= 33286, so it is exact in FP64.
+__device__ __forceinline__ double level_value4(float w0, float w1, float w2, float w3, double s) {
+    const double v =
+        ((tc::i32_to_f64(w0) * LW + tc::i32_to_f64(w1)) * LW + tc::i32_to_f64(w2)) * LW + tc::i32_to_f64(w3);
+    return v * (s * LW3INV);
+}
 
 }  // namespace fx
 
@@ -184,6 +204,74 @@ __global__ void __launch_bounds__(256) split_fx_transpose_kernel(const double* _
     split_fx_transpose_body<SL>(B, naux, nocc, nvir, a_pad, q_pad, scl, Bt, blockIdx.x, blockIdx.y, c0, c1);
 }
 
+// The pair operands: B[q, ia] -> Bt[s][i][a][q] (q < q_pad), four int8 slices
+// at scale scl[i*a_pad+a], for the columns ia in [c0, c1) (c1 < 0: all).
+__device__ __forceinline__ void split_pair4_body(const double* __restrict__ B, int64_t naux, int64_t nocc,
+                                                 int64_t nvir, int64_t a_pad, int64_t q_pad,
+                                                 const double* __restrict__ scl, int8_t* __restrict__ Bt,
+                                                 int64_t bx, int64_t by, int64_t c0 = 0, int64_t c1 = -1) {
+    struct alignas(2) P2 { int8_t e[2]; };
+    __shared__ double tile[64][65];
+    const int64_t nov = nocc * nvir;
+    const int64_t cend = c1 < 0 ? nov : c1;
+    const int64_t q0 = by * 64, ia0 = c0 + bx * 64;
+    const int tid = threadIdx.x;
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+        const int idx = tid + 256 * e, r = idx >> 6, c = idx & 63;
+        const int64_t q = q0 + r, ia = ia0 + c;
+        tile[r][c] = (q < naux && ia < cend) ? B[q * nov + ia] : 0.0;
+    }
+    __syncthreads();
+    const int64_t ss = nocc * a_pad * q_pad;
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+        const int idx = tid + 256 * e, c = idx >> 5, qq = (idx & 31) * 2;
+        const int64_t ia = ia0 + c;
+        if (ia >= cend) continue;
+        const int64_t i = ia / nvir, a = ia % nvir;
+        const double inv = 1.0 / scl[i * a_pad + a];
+        P2 p[4];
+        fx_slices4<SliceI8>(tile[qq][c], inv, p[0].e[0], p[1].e[0], p[2].e[0], p[3].e[0]);
+        fx_slices4<SliceI8>(tile[qq + 1][c], inv, p[0].e[1], p[1].e[1], p[2].e[1], p[3].e[1]);
+        const int64_t off = (i * a_pad + a) * q_pad + q0 + qq;
+#pragma unroll
+        for (int s = 0; s < 4; ++s) *reinterpret_cast<P2*>(Bt + s * ss + off) = p[s];
+    }
+}
+
+__global__ void __launch_bounds__(256) split_pair4_kernel(const double* __restrict__ B, int64_t naux, int64_t nocc,
+                                                          int64_t nvir, int64_t a_pad, int64_t q_pad,
+                                                          const double* __restrict__ scl, int8_t* __restrict__ Bt,
+                                                          int64_t c0 = 0, int64_t c1 = -1) {
+    split_pair4_body(B, naux, nocc, nvir, a_pad, q_pad, scl, Bt, blockIdx.x, blockIdx.y, c0, c1);
+}
+
+// gd[i*a_pad + a] = sum_q B[q, ia]^2 in FP64 (fixed order), the exact
+// (ia|ia) of the pair kernel's i == j blocks, for the columns ia in [c0, c0+cols)
+// of B (row pitch ld).  One thread per column; rows in one pass.
+__device__ __forceinline__ void colsq_body(const double* __restrict__ B, int64_t rows, int64_t nvir, int64_t ld,
+                                           int64_t a_pad, int64_t c, double* __restrict__ gd) {
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    int64_t r = 0;
+    for (; r + 4 <= rows; r += 4) {
+        const double v0 = B[r * ld + c], v1 = B[(r + 1) * ld + c], v2 = B[(r + 2) * ld + c], v3 = B[(r + 3) * ld + c];
+        s0 = fma(v0, v0, s0);
+        s1 = fma(v1, v1, s1);
+        s2 = fma(v2, v2, s2);
+        s3 = fma(v3, v3, s3);
+    }
+    for (; r < rows; ++r) s0 = fma(B[r * ld + c], B[r * ld + c], s0);
+    gd[(c / nvir) * a_pad + c % nvir] = (s0 + s1) + (s2 + s3);
+}
+
+__global__ void __launch_bounds__(256) colsq_kernel(const double* __restrict__ B, int64_t rows, int64_t nvir,
+                                                    int64_t ld, int64_t a_pad, int64_t c0, int64_t c1,
+                                                    double* __restrict__ gd) {
+    const int64_t c = c0 + (int64_t)blockIdx.x * 256 + threadIdx.x;
+    if (c < c1) colsq_body(B, rows, nvir, ld, a_pad, c, gd);
+}
+
 __global__ void fill_kernel(double* __restrict__ x, int64_t n, double v) {
     const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k < n) x[k] = v;
@@ -234,12 +322,34 @@ __device__ __forceinline__ void issue_products(uint64_t da, uint32_t tmem_base, 
 
 // ------------------------------------------------------------ pair kernel --
 
-// One molecule of a batch (operand rows row0 .. row0 + 3*nocc*a_pad of the
+// The 10 products of one k-step of the pair kernel (2 MMAs of K = 32 each)
+// from the stage whose A slice 0 has descriptor `da`; the four A slices are
+// PA_BYTES apart and the B slices start BOFS bytes after A slice 0.  Level
+// l = k + m collects the products c_k c'_m of slices k and m, l <= 3.
+template <int BOFS>
+__device__ __forceinline__ void issue_products4(uint64_t da, uint32_t tmem_base, int kt) {
+    using namespace fx;
+    constexpr int PA[10] = {0, 0, 1, 0, 1, 2, 0, 1, 2, 3};
+    constexpr int PB[10] = {0, 1, 0, 2, 1, 0, 3, 2, 1, 0};
+    constexpr int PL[10] = {0, 1, 1, 2, 2, 2, 3, 3, 3, 3};
+    constexpr int PF[10] = {1, 1, 0, 1, 0, 0, 1, 0, 0, 0};  // first product of its level
+#pragma unroll
+    for (int pr = 0; pr < 10; ++pr) {
+#pragma unroll
+        for (int kk = 0; kk < PKT / 32; ++kk)
+            tc::umma_i8(tmem_base + PL[pr] * BN, da + (uint64_t)((PA[pr] * PA_BYTES + kk * 32) >> 4),
+                        da + (uint64_t)((BOFS + PB[pr] * PB_BYTES + kk * 32) >> 4), IDESC,
+                        (kt > 0 || kk > 0 || !PF[pr]) ? 1u : 0u);
+    }
+}
+
+// One molecule of a batch (operand rows row0 .. row0 + 4*nocc*a_pad of the
 // concatenated slice buffer, slice-major).
 struct BatchMol {
     const double* eo;
     const double* ev;
     const double* scl;
+    const double* gd;  // [nocc * a_pad] exact (ia|ia)
     int nocc, nvir, a_pad, nk;
     int row0, tpad;  // tpad: virtual pitch of the amplitude rows/columns (gradient)
     int xt, pad2_;   // exchange (one phase) on diagonal tiles
@@ -254,6 +364,7 @@ struct PairFxArgs {
     const double* eo;
     const double* ev;
     const double* scl;  // [nocc * a_pad] operand-row scales
+    const double* gd;   // [nocc * a_pad] exact (ia|ia) = sum_Q B_Q,ia^2
     const int2* pairs;  // pairs of the launch
     const int2* tiles;  // (a-tile, b-tile) of each item of a pair
     int ntiles;         // tiles per pair
@@ -263,6 +374,7 @@ struct PairFxArgs {
     int xt;        // exchange (one phase) on diagonal tiles
     int64_t items;
     double* part;  // [item][2]
+    double* scr;   // [grid][2][BM][BN] FP64 X and Y tiles of each CTA
     int* err;
     // gradient mode: pairs (i, j), i in chunk I (from i0), j in chunk J (from j0)
     float* T;        // amplitude rows of I: [|I| a_pad][ldt = |J| a_pad]
@@ -276,10 +388,11 @@ struct PairFxArgs {
 // Everything the roles need about item k.
 struct ItemView {
     int i, j, ta, tb, nk, a_pad, nvir, row0, slice_rows, tpad, i0, j0;
-    int xt;  // diagonal tile, i != j: Y = X^T exchanged in shared memory, no Y phase
+    int xt;  // diagonal tile, i != j: Y = X^T read back transposed, no Y phase
     const double* eo;
     const double* ev;
     const double* scl;
+    const double* gd;
     float* T;
     float* T2;
     int64_t ldt, ldt2;
@@ -303,6 +416,7 @@ __device__ __forceinline__ ItemView item_view(const PairFxArgs& p, int64_t k) {
         v.eo = m.eo;
         v.ev = m.ev;
         v.scl = m.scl;
+        v.gd = m.gd;
         v.tpad = m.tpad;
         v.xt = m.xt && v.ta == v.tb && v.i != v.j;
         v.i0 = 0;
@@ -326,6 +440,7 @@ __device__ __forceinline__ ItemView item_view(const PairFxArgs& p, int64_t k) {
         v.eo = p.eo;
         v.ev = p.ev;
         v.scl = p.scl;
+        v.gd = p.gd;
         v.tpad = p.tpad;
         v.xt = p.xt && v.ta == v.tb && v.i != v.j;
         v.i0 = p.i0;
@@ -338,17 +453,46 @@ __device__ __forceinline__ ItemView item_view(const PairFxArgs& p, int64_t k) {
     return v;
 }
 
+// This thread's HC columns of a phase's four level accumulators -> FP64
+// values s_r s_c (L0 + L1/254 + L2/254^2 + L3/254^3), stored at dst (its row
+// of the CTA's tile in global scratch, L2 only).  gdv >= 0 is the column (of
+// these HC) on the tile diagonal a == b of an i == j block: it takes the
+// exact (ia|ia) instead, whose dropped level-4 products (the slice c3 c3' of
+// a row with itself) are one-signed.
+__device__ __forceinline__ void drain_levels(uint32_t tl, double sr, const double* __restrict__ sc, double* dst,
+                                             int gdv, double gval) {
+    using namespace fx;
+#pragma unroll
+    for (int c0 = 0; c0 < HC; c0 += 8) {
+        float l0[8], l1[8], l2[8], l3[8];
+        tc::tmem_ld8(tl + c0, l0);
+        tc::tmem_ld8(tl + BN + c0, l1);
+        tc::tmem_ld8(tl + 2 * BN + c0, l2);
+        tc::tmem_ld8(tl + 3 * BN + c0, l3);
+        tc::tmem_wait_ld();
+        double x[8];
+#pragma unroll
+        for (int cc = 0; cc < 8; ++cc) {
+            x[cc] = level_value4(l0[cc], l1[cc], l2[cc], l3[cc], sr * sc[c0 + cc]);
+            if (c0 + cc == gdv) x[cc] = gval;
+        }
+        double2* d2 = reinterpret_cast<double2*>(dst + c0);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) __stcg(d2 + u, make_double2(x[2 * u], x[2 * u + 1]));
+    }
+}
+
 template <int GRAD, int BATCH = 0>
 __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
     pair_fx_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                    const PairFxArgs p) {
     using namespace fx;
-    constexpr int S = STAGES;
+    constexpr int S = PSTAGES;
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw_u32 = smem_u32(smem_raw);
     const uint32_t base_u32 = (raw_u32 + 1023u) & ~1023u;
     uint8_t* base = smem_raw + (base_u32 - raw_u32);
-    uint64_t* bars = reinterpret_cast<uint64_t*>(base + S * STAGE_BYTES);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(base + S * PSTAGE_BYTES);
     uint64_t* full = bars;                // [S]
     uint64_t* empty = bars + S;           // [S]
     uint64_t* tfull = bars + 2 * S;       // [1] a phase's levels are complete in TMEM
@@ -359,8 +503,7 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
     double* red = reinterpret_cast<double*>(bars + 2 * S + 4);  // [2][EPI_WARPS][3]
     double* rowsh = red + 2 * EPI_WARPS * 3;                     // [NCG - 1][BM] row sums of column groups 1..
     double* colsh = rowsh + (NCG - 1) * BM;                      // [4 quadrants][NCG][HC] column sums
-    float* xbuf = reinterpret_cast<float*>(base + S * STAGE_BYTES + SCR_BYTES);  // [32][XP] exchange rows
-    double* colb = reinterpret_cast<double*>(base + S * STAGE_BYTES + SCR_BYTES + XBUF_BYTES);  // [3][BN]
+    double* colb = reinterpret_cast<double*>(base + S * PSTAGE_BYTES + SCR_BYTES);  // [3][BN]
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (tid == 0) {
@@ -387,8 +530,8 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
     tc::fence_after_sync();
     const uint32_t tmem_base = *tmem_slot;
 
-    auto sa = [&](int s, int sl) { return base_u32 + s * STAGE_BYTES + sl * A_BYTES; };
-    auto sb = [&](int s, int sl) { return base_u32 + s * STAGE_BYTES + NSL * A_BYTES + sl * B_BYTES; };
+    auto sa = [&](int s, int sl) { return base_u32 + s * PSTAGE_BYTES + sl * PA_BYTES; };
+    auto sb = [&](int s, int sl) { return base_u32 + s * PSTAGE_BYTES + PSL * PA_BYTES + sl * PB_BYTES; };
     auto row_of = [&](const ItemView& v, int sl, int i, int r0) {
         return v.row0 + sl * v.slice_rows + i * v.a_pad + r0;
     };
@@ -406,12 +549,12 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
                         const int s = g % S;
                         const uint32_t u = g / S;
                         if (!tc::mbar_wait(&empty[s], (u & 1) ^ 1, abort_flag, p.err)) goto prod_done;
-                        tc::mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
+                        tc::mbar_arrive_expect_tx(&full[s], PSTAGE_BYTES);
 #pragma unroll
-                        for (int sl = 0; sl < NSL; ++sl) {
-                            tc::tma_load_2d(base + (sa(s, sl) - base_u32), &tmA, &full[s], kt * KT,
+                        for (int sl = 0; sl < PSL; ++sl) {
+                            tc::tma_load_2d(base + (sa(s, sl) - base_u32), &tmA, &full[s], kt * PKT,
                                             row_of(v, sl, ia, v.ta * BM));
-                            tc::tma_load_2d(base + (sb(s, sl) - base_u32), &tmB, &full[s], kt * KT,
+                            tc::tma_load_2d(base + (sb(s, sl) - base_u32), &tmB, &full[s], kt * PKT,
                                             row_of(v, sl, ib, v.tb * BN));
                         }
                     }
@@ -427,9 +570,11 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
     } else if (warp == 1) {
         // ------------------------------------------------------ UMMA issuer
         if (lane == 0) {
-            // the operand descriptors of both stages, computed once: rebuilding
+            // the operand descriptors of the stages, computed once: rebuilding
             // them every k-step delayed the MMA issue by ~9% (measured)
-            const uint64_t da0 = tc::sdesc_k128(sa(0, 0)), da1 = tc::sdesc_k128(sa(1, 0));
+            uint64_t da[S];
+#pragma unroll
+            for (int s = 0; s < S; ++s) da[s] = tc::sdesc_k64(sa(s, 0));
             uint32_t g = 0, pc = 0;  // pc: phases issued (TMEM hand-overs)
             for (int64_t k = blockIdx.x; k < p.items && !*abort_flag; k += gridDim.x) {
                 const ItemView v = item_view<BATCH>(p, k);
@@ -442,7 +587,11 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
                         const uint32_t u = g / S;
                         if (!tc::mbar_wait(&full[s], u & 1, abort_flag, p.err)) goto mma_done;
                         tc::fence_after_sync();
-                        issue_products<NSL * A_BYTES>(s ? da1 : da0, tmem_base, kt);
+                        uint64_t d = da[0];
+#pragma unroll
+                        for (int t = 1; t < S; ++t)
+                            if (s == t) d = da[t];
+                        issue_products4<PSL * PA_BYTES>(d, tmem_base, kt);
                         tc::umma_commit(&empty[s]);
                     }
                     tc::umma_commit(tfull);
@@ -458,12 +607,19 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
         // ---------------------------------------------------------- epilogue
         // EPI_WARPS warps: lane quadrant q = warp % 4 (TMEM lanes 32q..32q+31),
         // column group h = (warp - 2) / 4; each thread owns row `row`, columns
-        // [HC h, HC h + HC).
+        // [HC h, HC h + HC).  A phase's four level accumulators fill TMEM, so
+        // each phase is drained at once into the CTA's FP64 tiles in global
+        // scratch (X, then Y), which hands TMEM back to the MMA warp; the FP64
+        // terms then run from the tiles under the next item's X phase.
         const int q = warp & 3;
         const int h = (warp - 2) >> 2;
         const int row = q * 32 + lane;  // a within the tile
         const int et = tid - 64;        // 0 .. EPI_THREADS - 1
         const uint32_t tl = tmem_base + ((uint32_t)(q * 32) << 16) + h * HC;
+        double* const sxt = p.scr + (int64_t)blockIdx.x * (2 * BM * BN);  // X tile [row][col]
+        double* const syt = sxt + BM * BN;                                 // Y tile
+        double* const xrow = sxt + row * BN + h * HC;
+        double* const yrow = syt + row * BN + h * HC;
         uint32_t li = 0, pc = 0;
         for (int64_t k = blockIdx.x; k < p.items; k += gridDim.x, ++li) {
             const ItemView v = item_view<BATCH>(p, k);
@@ -501,73 +657,73 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
             const double* sxb = colb + BN + h * HC;
             const double* syb = colb + 2 * BN + h * HC;
             const int bmax = v.nvir - b0;    // columns c < bmax are real virtuals
+            const bool xt = v.xt;            // the same for every thread of the CTA
+            const bool two = !diag && !xt;   // a Y phase follows in TMEM
 
-            // X phase: park (ia|jb) of this thread's columns in FP32 (round to nearest).
-            // One thread waits (bounded); the epilogue threads leave together
-            // if it gave up, since named barriers follow.
+            // X phase -> X tile.  One thread waits (bounded); the epilogue
+            // threads leave together if it gave up, since named barriers follow.
             if (!tc::bar_and<1, EPI_THREADS>(et != 0 || tc::mbar_wait(tfull, pc & 1, abort_flag, p.err))) break;
             if (et != 0) tc::mbar_wait(tfull, pc & 1, abort_flag, p.err);  // phase complete: returns at once
             tc::fence_after_sync();
-            const bool xt = v.xt;          // the same for every thread of the CTA
-            const bool two = !diag && !xt;  // a Y phase follows in TMEM
-            // pk: this thread's HC parked values -- X of a one-phase item, Y of a
-            // two-phase item (whose X waits in TMEM columns 3 BN + h HC .., beyond
-            // the three levels the MMAs write) -- then its column terms.  Both
-            // phases of a two-phase item are out of the level columns before the
-            // heavy FP64 work below, which runs under the next item's X phase.
-            // Batched items (small molecules, phases of a few k-steps) are
-            // epilogue-bound: there X stays in registers and Y streams out of
-            // the level columns group by group (measured 8% faster for the
-            // 512-molecule batch), the same FP32 values either way.
-            constexpr bool PARK = !BATCH;
-            float pk[HC];
-            const uint32_t tpk = tmem_base + ((uint32_t)(q * 32) << 16) + 3 * BN + h * HC;
-#pragma unroll
-            for (int c0 = 0; c0 < HC; c0 += 16) {
-                float l0[16], l1[16], l2[16];
-                tc::tmem_ld16(tl + c0, l0);
-                tc::tmem_ld16(tl + BN + c0, l1);
-                tc::tmem_ld16(tl + 2 * BN + c0, l2);
-                tc::tmem_wait_ld();
-#pragma unroll
-                for (int cc = 0; cc < 16; ++cc) pk[c0 + cc] = (float)level_value(l0[cc], l1[cc], l2[cc], sxa * sxb[c0 + cc]);
-                if (PARK && two) tc::tmem_st16(tpk + c0, pk + c0);
+            {
+                // (ia|ia) on the diagonal of an i == j block's diagonal tile
+                const int gdv = (diag && ta == tb && va) ? row - h * HC : -1;
+                const double gval = gdv >= 0 ? v.gd[(int64_t)i * v.a_pad + a] : 0.0;
+                drain_levels(tl, sxa, sxb, xrow, (gdv >= 0 && gdv < HC) ? gdv : -1, gval);
             }
-            if (PARK && two) tc::tmem_wait_st();
             tc::fence_before_sync();
             tc::mbar_arrive(tempty);
             ++pc;
             if (two) {
-                // Y phase: (ib|ja) = G_ji[a, b] of these columns, FP32 like X
+                // Y phase: (ib|ja) = G_ji[a, b] -> Y tile
                 if (!tc::bar_and<1, EPI_THREADS>(et != 0 || tc::mbar_wait(tfull, pc & 1, abort_flag, p.err))) break;
                 if (et != 0) tc::mbar_wait(tfull, pc & 1, abort_flag, p.err);
                 tc::fence_after_sync();
-            }
-            if (PARK && two) {
-#pragma unroll
-                for (int c0 = 0; c0 < HC; c0 += 16) {
-                    float l0[16], l1[16], l2[16];
-                    tc::tmem_ld16(tl + c0, l0);
-                    tc::tmem_ld16(tl + BN + c0, l1);
-                    tc::tmem_ld16(tl + 2 * BN + c0, l2);
-                    tc::tmem_wait_ld();
-#pragma unroll
-                    for (int cc = 0; cc < 16; ++cc)
-                        pk[c0 + cc] = (float)level_value(l0[cc], l1[cc], l2[cc], sya * syb[c0 + cc]);
-                }
+                drain_levels(tl, sya, syb, yrow, -1, 0.0);
                 tc::fence_before_sync();
                 tc::mbar_arrive(tempty);  // the level columns are free for the next item
                 ++pc;
             }
+            // an exchanged tile reads other threads' rows of X
+            if (xt) asm volatile("bar.sync 1, %0;" ::"n"(EPI_THREADS) : "memory");
+
             // plain FP64 sums over this thread's HC terms (relative error <= HC u);
             // the tile partials are summed compensated
             double os = 0.0, ss = 0.0, oc = 0.0, rowc = 0.0;
-            // the terms of this thread's columns c0 .. c0 + 7, given their Y values
-            auto proc8 = [&](const int c0, const float (&xv)[8], const double (&yv)[8]) {
-                float tt8[8], mv8[8];
+            constexpr int CW = 4;  // columns per step of the FP64 terms
+            float ck[HC];  // column terms of this thread's columns (gradient)
 #pragma unroll
-                for (int cc = 0; cc < 8; ++cc) {
-                    const double x = (double)xv[cc];
+            for (int c0 = 0; c0 < HC; c0 += CW) {
+                double xv[CW], yv[CW];
+                {
+                    const double2* x2 = reinterpret_cast<const double2*>(xrow + c0);
+#pragma unroll
+                    for (int u = 0; u < CW / 2; ++u) {
+                        const double2 t = __ldcg(x2 + u);
+                        xv[2 * u] = t.x;
+                        xv[2 * u + 1] = t.y;
+                    }
+                }
+                if (two) {
+                    const double2* y2 = reinterpret_cast<const double2*>(yrow + c0);
+#pragma unroll
+                    for (int u = 0; u < CW / 2; ++u) {
+                        const double2 t = __ldcg(y2 + u);
+                        yv[2 * u] = t.x;
+                        yv[2 * u + 1] = t.y;
+                    }
+                } else if (xt) {
+                    // Y[a, b] = X[b, a]: lanes hold consecutive a, so each load is coalesced
+#pragma unroll
+                    for (int cc = 0; cc < CW; ++cc) yv[cc] = __ldcg(sxt + (h * HC + c0 + cc) * BN + row);
+                } else {
+#pragma unroll
+                    for (int cc = 0; cc < CW; ++cc) yv[cc] = xv[cc];  // i == j: Y = X
+                }
+                float tt8[CW], mv8[CW];
+#pragma unroll
+                for (int cc = 0; cc < CW; ++cc) {
+                    const double x = xv[cc];
                     const double y = yv[cc];
                     float tval = 0.f, mval = 0.f, colv = 0.f;
                     if (va && c0 + cc < bmax) {
@@ -605,7 +761,7 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
                     }
                     tt8[cc] = tval;
                     mv8[cc] = mval;
-                    if (GRAD && !xt) pk[c0 + cc] = colv;  // this column's value is consumed: keep cm there
+                    ck[c0 + cc] = colv;
                 }
                 if (GRAD && a < v.tpad) {
                     // amplitude rows (i, a) and columns (j, b) at pitch tpad (>= nvir);
@@ -615,119 +771,40 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
                     const int bw = v.tpad - (b0 + c0);  // columns of this group inside the pitch
                     float* trow = v.T + ((int64_t)(i - v.i0) * v.tpad) * v.ldt + (int64_t)(j - v.j0) * v.tpad;
                     float* d = trow + (int64_t)a * v.ldt + b0 + c0;
-                    if (bw >= 8) {
+                    if (bw >= CW) {
                         float4* dst = reinterpret_cast<float4*>(d);
-                        dst[0] = make_float4(tt8[0], tt8[1], tt8[2], tt8[3]);
-                        dst[1] = make_float4(tt8[4], tt8[5], tt8[6], tt8[7]);
+#pragma unroll
+                        for (int u = 0; u < CW / 4; ++u)
+                            dst[u] = make_float4(tt8[4 * u], tt8[4 * u + 1], tt8[4 * u + 2], tt8[4 * u + 3]);
                     } else {
 #pragma unroll
-                        for (int cc = 0; cc < 8; ++cc)
+                        for (int cc = 0; cc < CW; ++cc)
                             if (cc < bw) d[cc] = tt8[cc];
                     }
                     if (mir) {
 #pragma unroll
-                        for (int cc = 0; cc < 8; ++cc)  // lanes hold consecutive a: coalesced
+                        for (int cc = 0; cc < CW; ++cc)  // lanes hold consecutive a: coalesced
                             if (cc < bw) trow[(int64_t)(b0 + c0 + cc) * v.ldt + a] = mv8[cc];
                     }
                     if (both) {
                         float* t2 = v.T2 + ((int64_t)(j - v.j0) * v.tpad) * v.ldt2 + (int64_t)(i - v.i0) * v.tpad;
 #pragma unroll
-                        for (int cc = 0; cc < 8; ++cc)  // Tt_ji[b, a] = Tt_ij[a, b]
+                        for (int cc = 0; cc < CW; ++cc)  // Tt_ji[b, a] = Tt_ij[a, b]
                             if (cc < bw) t2[(int64_t)(b0 + c0 + cc) * v.ldt2 + a] = tt8[cc];
                         if (mir) {                      // Tt_ji[a, b] = Tt_ij[b, a]
                             float* d2 = t2 + (int64_t)a * v.ldt2 + b0 + c0;
-                            if (bw >= 8) {
+                            if (bw >= CW) {
                                 float4* dst = reinterpret_cast<float4*>(d2);
-                                dst[0] = make_float4(mv8[0], mv8[1], mv8[2], mv8[3]);
-                                dst[1] = make_float4(mv8[4], mv8[5], mv8[6], mv8[7]);
+#pragma unroll
+                                for (int u = 0; u < CW / 4; ++u)
+                                    dst[u] = make_float4(mv8[4 * u], mv8[4 * u + 1], mv8[4 * u + 2], mv8[4 * u + 3]);
                             } else {
 #pragma unroll
-                                for (int cc = 0; cc < 8; ++cc)
+                                for (int cc = 0; cc < CW; ++cc)
                                     if (cc < bw) d2[cc] = mv8[cc];
                             }
                         }
                     }
-                }
-            };
-            if (!xt) {
-#pragma unroll
-                for (int c0 = 0; c0 < HC; c0 += 8) {
-                    float xv[8];
-                    double yv[8];
-                    if (PARK && two) {
-                        tc::tmem_ld8(tpk + c0, xv);  // X back from its TMEM columns
-                        tc::tmem_wait_ld();
-#pragma unroll
-                        for (int cc = 0; cc < 8; ++cc) yv[cc] = (double)pk[c0 + cc];
-                    } else if (two) {
-                        float y0[8], y1[8], y2[8];
-                        tc::tmem_ld8(tl + c0, y0);
-                        tc::tmem_ld8(tl + BN + c0, y1);
-                        tc::tmem_ld8(tl + 2 * BN + c0, y2);
-                        tc::tmem_wait_ld();
-                        if (c0 + 8 == HC) {  // every level of this phase is read: release TMEM
-                            tc::fence_before_sync();
-                            tc::mbar_arrive(tempty);
-                        }
-#pragma unroll
-                        for (int cc = 0; cc < 8; ++cc) {
-                            xv[cc] = pk[c0 + cc];
-                            yv[cc] = (double)(float)level_value(y0[cc], y1[cc], y2[cc], sya * syb[c0 + cc]);
-                        }
-                    } else {
-#pragma unroll
-                        for (int cc = 0; cc < 8; ++cc) {
-                            xv[cc] = pk[c0 + cc];  // i == j: Y = X
-                            yv[cc] = (double)pk[c0 + cc];
-                        }
-                    }
-                    proc8(c0, xv, yv);
-                }
-                if (!PARK && two) ++pc;
-            } else {
-                // Y = X^T inside a diagonal tile.  A one-phase item leaves the park
-                // columns free: in round r the X values of lane quarter r (rows
-                // 32r .. 32r + 31) pass through shared memory, and the threads
-                // whose columns include 32r .. 32r + 31 store Y[a, b] = X[b, a] of
-                // those 32 columns into their own lane of the park columns.  Then
-                // every thread runs its columns at once, X from registers and Y
-                // from TMEM (with only the threads of one column group busy in each
-                // round, exchanged tiles took about four times a two-phase tile's
-                // epilogue).
-#pragma unroll
-                for (int r = 0; r < 4; ++r) {
-                    if (q == r) {
-#pragma unroll
-                        for (int c = 0; c < HC; ++c) xbuf[lane * XP + h * HC + c] = pk[c];
-                    }
-                    asm volatile("bar.sync 1, %0;" ::"n"(EPI_THREADS) : "memory");
-#pragma unroll
-                    for (int sb = 0; sb < HC / 32; ++sb) {
-                        if (h * HC + sb * 32 == 32 * r) {
-#pragma unroll
-                            for (int c0 = 0; c0 < 32; c0 += 16) {
-                                float yq[16];
-#pragma unroll
-                                for (int cc = 0; cc < 16; ++cc) yq[cc] = xbuf[(c0 + cc) * XP + row];
-                                tc::tmem_st16(tpk + sb * 32 + c0, yq);
-                            }
-                        }
-                    }
-                    asm volatile("bar.sync 1, %0;" ::"n"(EPI_THREADS) : "memory");
-                }
-                tc::tmem_wait_st();
-#pragma unroll
-                for (int c0 = 0; c0 < HC; c0 += 8) {
-                    float xv[8], yf[8];
-                    double yv[8];
-                    tc::tmem_ld8(tpk + c0, yf);
-                    tc::tmem_wait_ld();
-#pragma unroll
-                    for (int cc = 0; cc < 8; ++cc) {
-                        xv[cc] = pk[c0 + cc];
-                        yv[cc] = (double)yf[cc];
-                    }
-                    proc8(c0, xv, yv);
                 }
             }
             const double vo = warp_sum(os), vs = warp_sum(ss);
@@ -741,19 +818,19 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
             if (GRAD && h > 0) rowsh[(h - 1) * BM + row] = rowc;
             if ((mir || both) && !xt) {
                 // column sums of the mirrored terms over this warp's 32 rows: a
-                // reduce-scatter butterfly leaves columns (HC / 32) lane + u in pk[u]
+                // reduce-scatter butterfly leaves columns (HC / 32) lane + u in ck[u]
 #pragma unroll
                 for (int half = HC / 2, off = 16; off > 0; half >>= 1, off >>= 1) {
                     const bool up = (lane & off) != 0;
 #pragma unroll
                     for (int c = 0; c < half; ++c) {
-                        const float send = up ? pk[c] : pk[c + half];
+                        const float send = up ? ck[c] : ck[c + half];
                         const float recv = __shfl_xor_sync(0xffffffffu, send, off);
-                        pk[c] = (up ? pk[c + half] : pk[c]) + recv;
+                        ck[c] = (up ? ck[c + half] : ck[c]) + recv;
                     }
                 }
 #pragma unroll
-                for (int u = 0; u < HC / 32; ++u) colsh[(q * NCG + h) * HC + (HC / 32) * lane + u] = (double)pk[u];
+                for (int u = 0; u < HC / 32; ++u) colsh[(q * NCG + h) * HC + (HC / 32) * lane + u] = (double)ck[u];
             }
             asm volatile("bar.sync 1, %0;" ::"n"(EPI_THREADS) : "memory");
             if (GRAD && h == 0) {
@@ -781,7 +858,8 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
                 p.part[2 * k + 1] = wt * sn.value();
                 if (GRAD) p.occ_part[k] = sc.value();
             }
-            // rowsh is rewritten next item only after every thread passed the next barrier
+            // rowsh and the scratch tiles are rewritten next item only after every
+            // thread passed this barrier
             asm volatile("bar.sync 1, %0;" ::"n"(EPI_THREADS) : "memory");
         }
     }
@@ -1170,6 +1248,7 @@ struct BatchPrep {
     int64_t naux, nocc, nvir, a_pad, q_pad, tpad, ldt, q_rows, M;
     unsigned long long* cmax;  // [nocc*nvir]
     double* scl;               // [nocc*a_pad] pair-operand row scales
+    double* gd;                // [nocc*a_pad] exact (ia|ia)
     int8_t* bt;                // pair-operand slices (rows of this molecule)
     double* qs;                // [q_rows] Q-row scales (gradient)
     int8_t* bq;                // Q-row slices [3][q_rows][ldt]
@@ -1192,7 +1271,7 @@ __device__ __forceinline__ int seg_find(const int64_t* __restrict__ pre, int lo,
     return lo;
 }
 
-enum BatchPre { PRE_COLMAX, PRE_ROWSCALE, PRE_TRANSPOSE, PRE_QROWS, PRE_TROWS, PRE_OCC, PRE_VIR, PRE_COUNT };
+enum BatchPre { PRE_COLMAX, PRE_ROWSCALE, PRE_TRANSPOSE, PRE_QROWS, PRE_TROWS, PRE_OCC, PRE_VIR, PRE_COLSQ, PRE_COUNT };
 
 __global__ void __launch_bounds__(256) batch_colmax_kernel(const BatchPrep* __restrict__ mp,
                                                            const int64_t* __restrict__ pre, int nmol, int* bad) {
@@ -1219,8 +1298,16 @@ __global__ void __launch_bounds__(256) batch_transpose_kernel(const BatchPrep* _
     const int m = seg_find(pre, 0, nmol, x);
     const BatchPrep& d = mp[m];
     const int64_t nbx = (d.nocc * d.nvir + 63) / 64, loc = x - pre[m];
-    split_fx_transpose_body<SliceI8>(d.b, d.naux, d.nocc, d.nvir, d.a_pad, d.q_pad, d.scl, d.bt, loc % nbx,
-                                     loc / nbx);
+    split_pair4_body(d.b, d.naux, d.nocc, d.nvir, d.a_pad, d.q_pad, d.scl, d.bt, loc % nbx, loc / nbx);
+}
+
+__global__ void __launch_bounds__(256) batch_colsq_kernel(const BatchPrep* __restrict__ mp,
+                                                          const int64_t* __restrict__ pre, int nmol) {
+    const int64_t x = (int64_t)blockIdx.x * 256 + threadIdx.x;
+    if (x >= pre[nmol]) return;
+    const int m = seg_find(pre, 0, nmol, x);
+    const BatchPrep& d = mp[m];
+    colsq_body(d.b, d.naux, d.nvir, d.nocc * d.nvir, d.a_pad, x - pre[m], d.gd);
 }
 
 __global__ void __launch_bounds__(256) batch_qrows_kernel(const BatchPrep* __restrict__ mp,
@@ -1323,19 +1410,15 @@ __global__ void __launch_bounds__(256) batch_energy_kernel(const double* __restr
 
 namespace {
 
-// k-steps (of fx::KT) from which the exchange is the default: it pays when
-// a phase is long against the epilogue (energy items gain from K = 256 on;
-// gradient items, whose epilogue also writes amplitudes, from K ~ 2048)
-constexpr int XT_MIN_NK_ENERGY = 2;
-constexpr int XT_MIN_NK_GRAD = 16;
-
-// naux up to which the int32 level sums of the pair kernel are exact:
-// 3 * 127^2 * naux < 2^31.
-constexpr int64_t PAIR_KMAX = 44382;
+// naux up to which the int32 level sums of the pair kernel are exact: up to
+// four int8 products per level, 4 * 127^2 * naux <= 2^31 - 1 (and the FP64
+// combination of the four levels stays an integer below 2^53).
+constexpr int64_t PAIR_KMAX = 33286;
 
 struct FxSplit {
     int8_t* bt;
     double* scl;
+    double* gd;  // exact (ia|ia) per operand row
     unsigned long long* cmax;
     int64_t a_pad, q_pad;
     CUtensorMap tmA, tmB;
@@ -1345,22 +1428,23 @@ struct FxSplit {
 // tensor maps; fx_split_range fills the slices of occupied orbitals [o0, o1).
 fc_status fx_split_alloc(const Rimp2Dev& d, cudaStream_t st, FxSplit* o) {
     const int64_t a_pad = (d.nvir + fx::BM - 1) / fx::BM * fx::BM;
-    const int64_t q_pad = (d.naux + fx::KT - 1) / fx::KT * fx::KT;
+    const int64_t q_pad = (d.naux + fx::PKT - 1) / fx::PKT * fx::PKT;
     const int64_t nov = d.nocc * d.nvir;
-    const int64_t rows = (int64_t)fx::NSL * d.nocc * a_pad;
+    const int64_t rows = (int64_t)fx::PSL * d.nocc * a_pad;
     if (d.naux > PAIR_KMAX)
-        return fail(FC_ERR_LAYOUT, "mixed RI-MP2: naux > 44382 exceeds the exact int32 level sums (use FP64)");
+        return fail(FC_ERR_LAYOUT, "mixed RI-MP2: naux > 33286 exceeds the exact int32 level sums (use FP64)");
     if ((d.naux + 63) / 64 > 65535) return fail(FC_ERR_LAYOUT, "split: naux too large");
-    if (rows > (int64_t)UINT32_MAX) return fail(FC_ERR_LAYOUT, "split: too many operand rows");
+    if (rows > (int64_t)INT32_MAX) return fail(FC_ERR_LAYOUT, "split: too many operand rows");
     void *vbt, *vscl;
     FC_TRY(ws_get(WS_SPLIT, (size_t)rows * q_pad, &vbt));
-    FC_TRY(ws_get(WS_SCALE, (size_t)(nov + d.nocc * a_pad) * 8 + 256, &vscl));
+    FC_TRY(ws_get(WS_SCALE, (size_t)(nov + 2 * d.nocc * a_pad) * 8 + 256, &vscl));
     o->cmax = (unsigned long long*)vscl;
     o->scl = (double*)vscl + nov;
+    o->gd = o->scl + d.nocc * a_pad;
     FC_CUDA(cudaMemsetAsync(o->cmax, 0, nov * 8, st));
     FC_CUDA(cudaMemsetAsync(vbt, 0, (size_t)rows * q_pad, st));
-    FC_TRY(make_tmap_i8_2d(&o->tmA, vbt, q_pad, rows, q_pad, fx::KT, fx::BM));
-    FC_TRY(make_tmap_i8_2d(&o->tmB, vbt, q_pad, rows, q_pad, fx::KT, fx::BN));
+    FC_TRY(make_tmap_i8_2d_sw64(&o->tmA, vbt, q_pad, rows, q_pad, fx::BM));
+    FC_TRY(make_tmap_i8_2d_sw64(&o->tmB, vbt, q_pad, rows, q_pad, fx::BN));
     o->bt = (int8_t*)vbt;
     o->a_pad = a_pad;
     o->q_pad = q_pad;
@@ -1375,13 +1459,15 @@ fc_status fx_split_range(const Rimp2Dev& d, cudaStream_t st, int* bad, const FxS
         dim3 g((unsigned)((nc + 255) / 256), (unsigned)((d.naux + rps - 1) / rps));
         colmax_kernel<<<g, 256, 0, st>>>(d.b_ov, d.naux, nc, rps, o.cmax, bad, nov, c0);
     }
+    colsq_kernel<<<(unsigned)((nc + 255) / 256), 256, 0, st>>>(d.b_ov, d.naux, d.nvir, nov, o.a_pad, c0, c0 + nc,
+                                                               o.gd);
     const int64_t r0 = o0 * o.a_pad, r1 = o1 * o.a_pad;
     row_scale_kernel<SliceI8><<<(unsigned)((r1 - r0 + 255) / 256), 256, 0, st>>>(o.cmax, d.nocc, d.nvir, o.a_pad,
                                                                                  o.scl, r0, r1);
     {
         dim3 g((unsigned)((nc + 63) / 64), (unsigned)((d.naux + 63) / 64));
-        split_fx_transpose_kernel<SliceI8><<<g, 256, 0, st>>>(d.b_ov, d.naux, d.nocc, d.nvir, o.a_pad, o.q_pad,
-                                                              o.scl, o.bt, c0, c0 + nc);
+        split_pair4_kernel<<<g, 256, 0, st>>>(d.b_ov, d.naux, d.nocc, d.nvir, o.a_pad, o.q_pad, o.scl, o.bt, c0,
+                                              c0 + nc);
     }
     return check_launch("fixed-point split kernels");
 }
@@ -1408,16 +1494,25 @@ fc_status fx_attrs() {
 }  // namespace
 
 // Diagonal tiles (ta == tb, i != j) in one tensor-core phase with the
-// transpose exchanged in shared memory (1), or in two phases (0).  The
-// exchange saves a phase of MMAs and costs the epilogue two passes over
-// shared memory with half the threads busy in each: it pays when the phase
-// is long (many k-steps).  FERRIC_CUDA_XT=0/1 forces it.
-int fx_ksteps(int64_t naux) { return (int)((naux + fx::KT - 1) / fx::KT); }
+// transpose read back from the CTA's X tile (1), or in two phases (0).  The
+// exchange saves a phase of MMAs for the price of strided (coalesced) reads
+// of the X tile, so it is the default; FERRIC_CUDA_XT=0/1 forces it.
+int fx_ksteps(int64_t naux) { return (int)((naux + fx::PKT - 1) / fx::PKT); }
 
 int fx_exchange_choice(int nk, int grad) {
+    (void)nk;
+    (void)grad;
     const char* e = std::getenv("FERRIC_CUDA_XT");
     if (e && (e[0] == '0' || e[0] == '1')) return e[0] == '1';
-    return nk >= (grad ? XT_MIN_NK_GRAD : XT_MIN_NK_ENERGY);
+    return 1;
+}
+
+// FP64 X / Y tiles of the pair kernel's CTAs (global scratch, L2-resident).
+fc_status pair_scratch(int grid, double** out) {
+    void* v;
+    FC_TRY(ws_get(WS_PSCR, (size_t)grid * 2 * fx::BM * fx::BN * sizeof(double), &v));
+    *out = (double*)v;
+    return FC_OK;
 }
 
 fc_status rimp2_energy_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double* e_ss, fc_stats* stats) {
@@ -1465,15 +1560,17 @@ fc_status rimp2_energy_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, doub
     a.a_pad = (int)sp.a_pad;
     a.nTa = (int)(sp.a_pad / fx::BM);
     a.nTb = (int)(sp.a_pad / fx::BN);
-    a.nk = (int)(sp.q_pad / fx::KT);
+    a.nk = (int)(sp.q_pad / fx::PKT);
     a.tpad = a.a_pad;
     a.xt = fx_exchange_choice(a.nk, 0);
     a.items = (int64_t)a.npairs * a.ntiles;
+    a.gd = sp.gd;
     void* vpart;
     FC_TRY(ws_get(WS_PART, a.items * 2 * sizeof(double), &vpart));
     a.part = (double*)vpart;
     a.err = flags + 1;
     const int grid = (int)(a.items < c.sm_count ? a.items : c.sm_count);
+    FC_TRY(pair_scratch(grid, &a.scr));
     cudaEvent_t* ev = nullptr;
     if (stats) {
         FC_TRY(timing_events(1, &ev));
@@ -1508,7 +1605,7 @@ fc_status rimp2_energy_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, doub
         stats->main_launches = 1;
         FC_TRY(timing_sum(1, &stats->main_ms));
         stats->main_flops = stats->flops;
-        stats->main_bytes = 6.0 * (double)d.naux * (double)(d.nocc * d.nvir);
+        stats->main_bytes = 8.0 * (double)d.naux * (double)(d.nocc * d.nvir);
         stats->h2d_bytes += pairs.size() * sizeof(int2);
         stats->d2h_bytes += sizeof(h) + sizeof(hf);
     }
@@ -1701,10 +1798,11 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
         a.a_pad = (int)a_pad;
         a.nTa = nTa;
         a.nTb = nTa;
-        a.nk = (int)(sp.q_pad / fx::KT);
+        a.nk = (int)(sp.q_pad / fx::PKT);
         a.tpad = (int)tp;
         a.xt = fx_exchange_choice(a.nk, 1);
         a.items = cp.np * ntiles;
+        a.gd = sp.gd;
         a.part = part;
         a.err = flags + 1;
         a.T = T1;
@@ -1716,6 +1814,7 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
         a.occ_part = occ_part;
         a.vir_part = vir_part;
         const int grid = (int)(a.items < c.sm_count ? a.items : c.sm_count);
+        FC_TRY(pair_scratch(grid, &a.scr));
         if (stats) FC_CUDA(cudaEventRecord(ev[2 * x], st));
         pair_fx_kernel<1><<<grid, fx::PAIR_THREADS, fx::SMEM, st>>>(sp.tmA, sp.tmB, a);
         FC_TRY(check_launch("pair_fx_kernel<grad>"));
@@ -1780,7 +1879,7 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
         }
         stats->main_ms = tsum;
         stats->main_flops = 2.0 * naux * (double)nvir * nvir * P;  // G_ij over unordered pairs
-        stats->main_bytes = 6.0 * naux * (double)nov * (double)nch;
+        stats->main_bytes = 8.0 * naux * (double)nov * (double)nch;
         stats->h2d_bytes += pairs.size() * sizeof(int2);
         stats->d2h_bytes += h.size() * 8 + sizeof(hf);
     }
@@ -1951,8 +2050,8 @@ fc_status rimp2_batch_build_fx(fc_rimp2_batch* b, const std::vector<BatchMolIn>&
     const int nmol = (int)mols.size();
     const bool grad = b->grad != 0;
     Context& c = ctx();
-    int64_t q_pad = fx::KT;
-    for (const auto& d : mols) q_pad = std::max(q_pad, rup(d.naux, fx::KT));
+    int64_t q_pad = fx::PKT;
+    for (const auto& d : mols) q_pad = std::max(q_pad, rup(d.naux, fx::PKT));
     const int NP = nmol + 1;
     std::vector<BatchPrep> hp(nmol);
     std::vector<BatchMol> hm(nmol);
@@ -1987,7 +2086,7 @@ fc_status rimp2_batch_build_fx(fc_rimp2_batch* b, const std::vector<BatchMolIn>&
         cmax_off[m] = ncmax;
         ncmax += nov;
         hm[m].row0 = (int)rows;
-        rows += 3 * d.nocc * x.a_pad;
+        rows += fx::PSL * d.nocc * x.a_pad;
         qs_off[m] = nqs;
         nqs += x.q_rows;
         bq_off[m] = nbq;
@@ -1999,6 +2098,7 @@ fc_status rimp2_batch_build_fx(fc_rimp2_batch* b, const std::vector<BatchMolIn>&
         P(PRE_TROWS, m + 1) = P(PRE_TROWS, m) + x.ldt;
         P(PRE_OCC, m + 1) = P(PRE_OCC, m) + d.nocc;
         P(PRE_VIR, m + 1) = P(PRE_VIR, m) + d.nvir;
+        P(PRE_COLSQ, m + 1) = P(PRE_COLSQ, m) + nov;
         const double P2 = (double)d.nocc * (d.nocc + 1) / 2.0;
         b->flops += 2.0 * (double)d.naux * (double)d.nvir * (double)d.nvir * P2;
         if (grad) b->flops += 2.0 * (double)d.naux * (double)nov * (double)nov;
@@ -2039,9 +2139,10 @@ fc_status rimp2_batch_build_fx(fc_rimp2_batch* b, const std::vector<BatchMolIn>&
     }
 
     // ---- device buffers
-    void *vbt, *vscl, *vcmax, *vmols, *vprep, *vpre, *vseg, *vitems, *vpart;
+    void *vbt, *vscl, *vgd, *vcmax, *vmols, *vprep, *vpre, *vseg, *vitems, *vpart, *vscr;
     FC_TRY(batch_alloc(b, (size_t)rows * q_pad, &vbt));
     FC_TRY(batch_alloc(b, (size_t)nscl * 8, &vscl));
+    FC_TRY(batch_alloc(b, (size_t)nscl * 8, &vgd));
     FC_TRY(batch_alloc(b, (size_t)ncmax * 8, &vcmax));
     FC_TRY(batch_alloc(b, (size_t)nmol * sizeof(BatchMol), &vmols));
     FC_TRY(batch_alloc(b, (size_t)nmol * sizeof(BatchPrep), &vprep));
@@ -2049,6 +2150,8 @@ fc_status rimp2_batch_build_fx(fc_rimp2_batch* b, const std::vector<BatchMolIn>&
     FC_TRY(batch_alloc(b, seg.size() * 8, &vseg));
     FC_TRY(batch_alloc(b, (size_t)items * sizeof(int4), &vitems));
     FC_TRY(batch_alloc(b, (size_t)items * 16, &vpart));
+    const int pgrid = (int)std::min<int64_t>(std::max<int64_t>(items, 1), c.sm_count);
+    FC_TRY(batch_alloc(b, (size_t)pgrid * 2 * fx::BM * fx::BN * sizeof(double), &vscr));
     FC_CUDA(cudaMemset(vbt, 0, (size_t)rows * q_pad));
     void *vocc = nullptr, *vvir = nullptr, *vqs = nullptr, *vbq = nullptr, *vgws = nullptr;
     void *vgm = nullptr, *vmaps = nullptr, *vgit = nullptr;
@@ -2070,14 +2173,16 @@ fc_status rimp2_batch_build_fx(fc_rimp2_batch* b, const std::vector<BatchMolIn>&
         BatchPrep& x = hp[m];
         x.cmax = (unsigned long long*)vcmax + cmax_off[m];
         x.scl = (double*)vscl + scl_off[m];
+        x.gd = (double*)vgd + scl_off[m];
         x.bt = (int8_t*)vbt + (int64_t)hm[m].row0 * q_pad;
         hm[m].eo = mols[m].eps_occ;
         hm[m].ev = mols[m].eps_vir;
         hm[m].scl = x.scl;
+        hm[m].gd = x.gd;
         hm[m].nocc = (int)x.nocc;
         hm[m].nvir = (int)x.nvir;
         hm[m].a_pad = (int)x.a_pad;
-        hm[m].nk = (int)(rup(x.naux, fx::KT) / fx::KT);
+        hm[m].nk = (int)(rup(x.naux, fx::PKT) / fx::PKT);
         hm[m].tpad = (int)x.tpad;
         hm[m].xt = plan ? plan[m] : fx_exchange_choice(hm[m].nk, grad);
         hm[m].T = nullptr;
@@ -2139,8 +2244,8 @@ fc_status rimp2_batch_build_fx(fc_rimp2_batch* b, const std::vector<BatchMolIn>&
     FC_CUDA(cudaMemcpy(vseg, seg.data(), seg.size() * 8, cudaMemcpyHostToDevice));
     FC_CUDA(cudaMemcpy(vitems, hi.data(), hi.size() * sizeof(int4), cudaMemcpyHostToDevice));
     CUtensorMap tmA, tmB;
-    FC_TRY(make_tmap_i8_2d(&tmA, vbt, q_pad, rows, q_pad, fx::KT, fx::BM));
-    FC_TRY(make_tmap_i8_2d(&tmB, vbt, q_pad, rows, q_pad, fx::KT, fx::BN));
+    FC_TRY(make_tmap_i8_2d_sw64(&tmA, vbt, q_pad, rows, q_pad, fx::BM));
+    FC_TRY(make_tmap_i8_2d_sw64(&tmB, vbt, q_pad, rows, q_pad, fx::BN));
     FC_CUDA(cudaDeviceSynchronize());
 
     // ---- the recorded sequence
@@ -2157,7 +2262,8 @@ fc_status rimp2_batch_build_fx(fc_rimp2_batch* b, const std::vector<BatchMolIn>&
         batch_row_scale_kernel<<<(unsigned)((P(PRE_ROWSCALE, nmol) + 255) / 256), 256, 0, st>>>(
             dp, PD(PRE_ROWSCALE), nmol);
         batch_transpose_kernel<<<(unsigned)P(PRE_TRANSPOSE, nmol), 256, 0, st>>>(dp, PD(PRE_TRANSPOSE), nmol);
-        launches += 3;
+        batch_colsq_kernel<<<(unsigned)((P(PRE_COLSQ, nmol) + 255) / 256), 256, 0, st>>>(dp, PD(PRE_COLSQ), nmol);
+        launches += 4;
         if (grad) {
             batch_qrows_kernel<<<(unsigned)P(PRE_QROWS, nmol), 256, 0, st>>>(dp, PD(PRE_QROWS), nmol);
             ++launches;
@@ -2167,6 +2273,7 @@ fc_status rimp2_batch_build_fx(fc_rimp2_batch* b, const std::vector<BatchMolIn>&
         a.bitems = (const int4*)vitems;
         a.bmols = (const BatchMol*)vmols;
         a.err = b->flags + 1;
+        a.scr = (double*)vscr;
         if (!grad) {
             a.items = items;
             a.part = (double*)vpart;

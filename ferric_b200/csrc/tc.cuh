@@ -202,6 +202,19 @@ __device__ __forceinline__ uint64_t sdesc_k128(uint32_t smem_addr) {
     return d;
 }
 
+// The same for a K-major tile with 64-byte swizzle: rows of 64 B, 8-row atoms
+// 512 B apart; the tile base must be 512-byte aligned.  Advancing K by 32
+// int8 elements adds 32 B to the address.
+__device__ __forceinline__ uint64_t sdesc_k64(uint32_t smem_addr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((smem_addr >> 4) & 0x3FFF);          // start address
+    d |= (uint64_t)1 << 16;                               // leading byte offset (unused, 1)
+    d |= (uint64_t)(512 >> 4) << 32;                      // stride byte offset: 8 rows x 64 B
+    d |= (uint64_t)1 << 46;                               // descriptor version (sm_100)
+    d |= (uint64_t)4 << 61;                               // SWIZZLE_64B
+    return d;
+}
+
 // Instruction descriptor: BF16 x BF16 -> F32, both operands K-major.
 __host__ __device__ constexpr uint32_t idesc_bf16_f32(int m, int n) {
     return (1u << 4)                       // D format F32

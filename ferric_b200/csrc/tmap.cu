@@ -8,7 +8,8 @@
 namespace fc {
 
 static fc_status make_tmap_2d(CUtensorMap* map, CUtensorMapDataType type, const void* base, uint64_t inner,
-                              uint64_t outer, uint64_t row_bytes, uint32_t box_inner, uint32_t box_outer) {
+                              uint64_t outer, uint64_t row_bytes, uint32_t box_inner, uint32_t box_outer,
+                              CUtensorMapSwizzle swz = CU_TENSOR_MAP_SWIZZLE_128B) {
     static PFN_cuTensorMapEncodeTiled_v12000 enc = nullptr;
     if (!enc) {
         void* fn = nullptr;
@@ -25,7 +26,7 @@ static fc_status make_tmap_2d(CUtensorMap* map, CUtensorMapDataType type, const 
     cuuint32_t box[2] = {box_inner, box_outer};
     cuuint32_t estr[2] = {1, 1};
     CUresult r = enc(map, type, 2, const_cast<void*>(base), dims, strides, box, estr,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, swz,
                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS)
         return fail(FC_ERR_LAYOUT, "cuTensorMapEncodeTiled failed with CUresult " + std::to_string((int)r));
@@ -40,6 +41,12 @@ fc_status make_tmap_bf16_2d(CUtensorMap* map, const void* base, uint64_t inner, 
 fc_status make_tmap_i8_2d(CUtensorMap* map, const void* base, uint64_t inner, uint64_t outer, uint64_t row_bytes,
                           uint32_t box_inner, uint32_t box_outer) {
     return make_tmap_2d(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, base, inner, outer, row_bytes, box_inner, box_outer);
+}
+
+fc_status make_tmap_i8_2d_sw64(CUtensorMap* map, const void* base, uint64_t inner, uint64_t outer,
+                               uint64_t row_bytes, uint32_t box_outer) {
+    return make_tmap_2d(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, base, inner, outer, row_bytes, 64, box_outer,
+                        CU_TENSOR_MAP_SWIZZLE_64B);
 }
 
 }  // namespace fc

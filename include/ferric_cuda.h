@@ -207,9 +207,12 @@ fc_status fc_rimp2_imat_dev(const double* x_ov, const double* b_full, int64_t na
  * address and sets the kernel's shared-memory limit; make that first call
  * before any stream capture.  All calls on a device share the one array
  * (each call writes every byte it later reads, so earlier contents do not
- * matter): calls that overlap on the GPU, e.g. from two streams or two
- * threads' streams, race.  Calls within one process are serialised on the
- * host. */
+ * matter), so two calls that overlapped on the GPU would race on it.  The
+ * function rules that out within a process: it holds one process-wide lock
+ * from its first launch until its stream has finished, so calls from
+ * different threads or streams run one after another, and calls on
+ * different devices also queue behind each other.  Separate processes each
+ * have their own copy of the array. */
 fc_status fc_rimp2_energy_noalloc(const double* b_ov, int64_t naux, int64_t nocc, int64_t nvir,
                                   const double* eps_occ, const double* eps_vir,
                                   int32_t has_kappa, double kappa,

@@ -2,8 +2,9 @@
 
 Reads the reference's bundled MolSSI-BSE JSON files
 (ferric-core/src/basis/bundled/*.json) at run time; nothing is copied into
-this repository.  The directory is taken from ``FERRIC_BASIS_DIR`` or the
-reference mount.
+this repository.  The directory is taken from ``FERRIC_BASIS_DIR``, else
+from the reference checkout named by ``FERRIC_REFERENCE_ROOT``; with neither
+set, ``available()`` is False and the callers skip.
 """
 from __future__ import annotations
 
@@ -16,15 +17,24 @@ BOHR_PER_ANGSTROM = 1.0 / 0.52917721092   # the conversion the reference's JSONs
 SYMBOLS = {"H": 1, "He": 2, "C": 6, "N": 7, "O": 8, "F": 9}
 
 
+def reference_root():
+    """The reference checkout (``FERRIC_REFERENCE_ROOT``), or None."""
+    return os.environ.get("FERRIC_REFERENCE_ROOT") or None
+
+
 def basis_dir():
     d = os.environ.get("FERRIC_BASIS_DIR")
     if d:
         return d
-    return os.path.join("/root/reference", "crates", "ferric-core", "src", "basis", "bundled")
+    root = reference_root()
+    if root is None:
+        return None
+    return os.path.join(root, "crates", "ferric-core", "src", "basis", "bundled")
 
 
 def available():
-    return os.path.isdir(basis_dir())
+    d = basis_dir()
+    return d is not None and os.path.isdir(d)
 
 
 def load(name):

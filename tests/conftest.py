@@ -8,8 +8,17 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 
+def pytest_addoption(parser):
+    parser.addoption("--reference-root", default=os.environ.get("FERRIC_REFERENCE_ROOT"),
+                     help="reference checkout whose basis JSONs the oracle pipeline tests read "
+                          "(default: $FERRIC_REFERENCE_ROOT; those tests skip without it)")
+
+
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a B200 (sm_100a) device")
+    root = config.getoption("--reference-root")
+    if root:
+        os.environ["FERRIC_REFERENCE_ROOT"] = root
 
 
 def gpu_available():

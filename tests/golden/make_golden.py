@@ -6,9 +6,10 @@ inputs (dressed B_ov, orbital energies) and the reference's golden energies
 (PySCF 2.13.1 numbers from the reference's testdata/reference/validation JSONs)
 into ``<name>.npz``.  The device tests read only these fixtures.
 
-    python tests/golden/make_golden.py [name ...]
+    FERRIC_REFERENCE_ROOT=<reference checkout> python tests/golden/make_golden.py [name ...]
 
-Needs the reference mount for the basis JSONs and golden JSONs.
+Reads the basis JSONs and golden JSONs from the reference checkout named by
+``FERRIC_REFERENCE_ROOT``.
 """
 from __future__ import annotations
 
@@ -26,7 +27,13 @@ sys.path.insert(0, ROOT)
 from oracle import basis, integrals, scf  # noqa: E402
 from oracle import rimp2 as orc  # noqa: E402
 
-REF = "/root/reference/testdata/reference/validation"
+
+def validation_dir():
+    root = basis.reference_root()
+    if root is None:
+        sys.exit("set FERRIC_REFERENCE_ROOT to the reference checkout")
+    return os.path.join(root, "testdata", "reference", "validation")
+
 SYSTEMS = {
     # name: (golden json, basis, aux basis, kappa json or None, JK-fit basis for the DF-JK SCF or None)
     "h2o_ccpvdz": ("sos_mp2/h2o_cc-pvdz.json", "cc-pvdz", "cc-pvdz-ri", "kappa_mp2/h2o_cc-pvdz.json", "cc-pvtz-jkfit"),
@@ -37,6 +44,7 @@ SYSTEMS = {
 
 def build(name):
     gfile, bas, aux, kfile, jkfit = SYSTEMS[name]
+    REF = validation_dir()
     g = json.load(open(os.path.join(REF, gfile)))
     atoms = [(s, (x, y, z)) for s, x, y, z in g["provenance"]["geometry_bohr"]]
     zs = [basis.SYMBOLS[s] for s, _ in atoms]
@@ -84,7 +92,7 @@ U_SYSTEMS = {
 
 
 def build_u(name):
-    g = json.load(open(os.path.join(REF, U_SYSTEMS[name])))
+    g = json.load(open(os.path.join(validation_dir(), U_SYSTEMS[name])))
     atoms = [(s, (x, y, z)) for s, x, y, z in g["provenance"]["geometry_bohr"]]
     zs = [basis.SYMBOLS[s] for s, _ in atoms]
     rs = [c for _, c in atoms]

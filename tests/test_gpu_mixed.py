@@ -1,11 +1,12 @@
 """Exact integer-slice RI-MP2 kernels (tcgen05 kind::i8) against the FP64
 oracle and against an exact NumPy emulation of the split algorithm.
 
-FC_PREC_MIXED slices every operand row into three int8 integers at a power-of-
-two scale; the tensor cores sum the integer products exactly in int32, so the
+FC_PREC_MIXED splits every pair-operand row into four int8 integers at a
+power-of-two scale and sums the ten slice products of level <= 3 exactly in
+int32 (the adjoint contraction keeps three slices and six products); the
 device energy must equal the emulation (slices in NumPy, integer products
-summed exactly) to FP64 rounding, and the FP64 oracle to the slice truncation
-error (~1e-9 relative measured on B200).
+summed exactly, (ia|ia) of the i == j blocks in FP64) to FP64 rounding, and
+the FP64 oracle to the slice truncation error.
 """
 import numpy as np
 import pytest
@@ -15,17 +16,19 @@ from oracle import synthetic
 
 pytestmark = pytest.mark.gpu
 
-# Energy bound of the split: each element of G carries 23-24 bits relative
-# to its row maximum, so for small systems, where a few elements dominate E,
-# E's relative error reaches ~2.6e-7 (largest of 120 seeded random systems
-# of 2-4 occupied orbitals; either integer-slice format, emulated exactly);
-# large systems sit near 1e-10.
-MIXED_E_REL = 3e-7
-# Gamma (max-normalised) and dE/deps bounds (measured max x 5)
+# Energy bound of the split: four int8 slices carry ~31 bits of each element
+# relative to its row maximum.  For small systems, where a few elements
+# dominate E, the relative energy error reaches ~5e-10 (largest over the
+# shapes below and 120 seeded random systems of 2-4 occupied orbitals,
+# emulated exactly on the CPU); large systems sit near 1e-12 (config 3:
+# ~5e-8 Eh of 1.9e5 Eh, emulated on sampled pairs).
+MIXED_E_REL = 2e-9
+# Gamma (max-normalised) and dE/deps bounds: the adjoint contraction's three
+# slices (measured max x 5)
 MIXED_G_REL = 1e-5
 MIXED_D_REL = 1e-6
-# absolute floor (Eh) for tiny systems, where one product carries the full 2^-23 slice error
-MIXED_E_ABS = 1e-12
+# absolute floor (Eh) for tiny systems
+MIXED_E_ABS = 1e-13
 FAST_E_REL = 2e-4     # hi+lo, FP32 accumulation (accumulation-bound)
 
 
@@ -37,57 +40,52 @@ def chunk_budget(nvir, chunk):
     return (chunk + 1) ** 2 * (tp * tp * 11 + 1024 * tp) - 1
 
 
-def emulate_fixed_slices(b):
+def pair_slices(b):
     """The FC_PREC_MIXED split of every column of b (power-of-two scale with
-    max|x|/s in (63.5, 127], three int8 slices at weights 1/254) and the exact
-    level sums, combined as the device does: s_r s_r' ((L0 254 + L1) 254 + L2)
-    / 254^2."""
+    max|x|/s in (63.5, 127], four int8 slices at weights 1/254^k)."""
     mx = np.abs(b).max(axis=0)
     k = np.frexp(np.where(mx > 0, mx, 1.0))[1]
     s = np.ldexp(1.0, k - 7)
     s = np.where(mx > 127.0 * s, 2.0 * s, s)
     s = np.where(mx > 0, s, 1.0)
-    y = b / s[None, :]
-    c1 = np.rint(y)
-    y2 = (y - c1) * 254.0
-    c2 = np.rint(y2)
-    c3 = np.rint((y2 - c2) * 254.0)
-    assert np.abs(c1).max() <= 127 and np.abs(c2).max() <= 127 and np.abs(c3).max() <= 127
-    l0 = c1.T @ c1
-    l1 = c1.T @ c2 + c2.T @ c1
-    l2 = c1.T @ c3 + c2.T @ c2 + c3.T @ c1
-    v = (l0 * 254.0 + l1) * 254.0 + l2
-    return (np.outer(s, s) * (1.0 / 64516.0)) * v
+    r = b / s[None, :]
+    cs = []
+    for _ in range(4):
+        c = np.rint(r)
+        assert np.abs(c).max() <= 127
+        cs.append(c)
+        r = (r - c) * 254.0
+    return s, cs
 
 
-def energy_from_g(g, eo, ev, tile=128, xt=False):
-    """The device's energy from the exact level sums.  Per pair i <= j the
-    device visits 128 x 128 tiles (ta, tb) with ta <= tb (weight 2 off the tile
-    diagonal: the summands are symmetric under a <-> b); in each the X element
-    (ia|jb) and the Y element (ib|ja) are held in FP32 (round to nearest)
-    between the tensor-core phases and the FP64 epilogue; i == j uses X only.
-    With the exchange (xt) a diagonal tile's Y is the parked X transposed, the
-    same FP32 values."""
+def emulate_fixed_slices(b):
+    """G = B^T B as the pair kernel forms it: the exact level sums of the ten
+    products of level <= 3, combined as s_r s_r' (((L0 254 + L1) 254 + L2) 254
+    + L3) / 254^3."""
+    s, c = pair_slices(b)
+    lev = [sum(c[k].T @ c[l - k] for k in range(l + 1)) for l in range(4)]
+    v = ((lev[0] * 254.0 + lev[1]) * 254.0 + lev[2]) * 254.0 + lev[3]
+    return (np.outer(s, s) * (1.0 / 254.0 ** 3)) * v
+
+
+def energy_from_g(g, eo, ev, b=None):
+    """The device's energy from the emulated G: per pair i <= j the X element
+    (ia|jb) and the Y element (ib|ja) in FP64; i == j uses X only, with the
+    exact (ia|ia) = sum_Q B_Q,ia^2 on its diagonal (when b is given)."""
     nocc, nvir = len(eo), len(ev)
-    nt = (nvir + tile - 1) // tile
     e_os = e_ss = 0.0
     for i in range(nocc):
         for j in range(i, nocc):
-            gx = g[i * nvir:(i + 1) * nvir, j * nvir:(j + 1) * nvir]
-            gy = g[j * nvir:(j + 1) * nvir, i * nvir:(i + 1) * nvir]   # G_ji[a, b] = (ib|ja)
-            for ta in range(nt):
-                for tb in range(ta, nt):
-                    sa = slice(ta * tile, min(nvir, (ta + 1) * tile))
-                    sb = slice(tb * tile, min(nvir, (tb + 1) * tile))
-                    w = 2.0 if ta < tb else 1.0
-                    x = gx[sa, sb].astype(np.float32).astype(np.float64)
-                    d = eo[i] + eo[j] - ev[sa, None] - ev[None, sb]
-                    if i == j:
-                        e_os += w * np.sum(x * x / d)
-                    else:
-                        y = gy[sa, sb].astype(np.float32).astype(np.float64)
-                        e_os += w * np.sum((x * x + y * y) / d)
-                        e_ss += w * np.sum((x - y) ** 2 / d)
+            x = g[i * nvir:(i + 1) * nvir, j * nvir:(j + 1) * nvir].copy()
+            d = eo[i] + eo[j] - ev[:, None] - ev[None, :]
+            if i == j:
+                if b is not None:
+                    x[np.diag_indices(nvir)] = (b[:, i * nvir:(i + 1) * nvir] ** 2).sum(axis=0)
+                e_os += np.sum(x * x / d)
+            else:
+                y = g[j * nvir:(j + 1) * nvir, i * nvir:(i + 1) * nvir]   # G_ji[a, b] = (ib|ja)
+                e_os += 2.0 * np.sum(x * x / d)
+                e_ss += 2.0 * np.sum(x * (x - y) / d)
     return e_os, e_ss
 
 
@@ -97,7 +95,7 @@ SHAPES = [(96, 5, 23), (84, 5, 19), (200, 7, 65), (300, 4, 130), (130, 3, 128), 
 @pytest.mark.parametrize("xt", ["0", "1"])
 @pytest.mark.parametrize("naux,nocc,nvir", SHAPES)
 def test_mixed_energy_matches_oracle_and_emulation(fc, monkeypatch, naux, nocc, nvir, xt):
-    """xt = 1: diagonal tiles in one phase, Y = X^T exchanged in shared memory."""
+    """xt = 1: diagonal tiles in one phase, Y = X^T read back from the X tile."""
     from ferric_b200 import rimp2
     monkeypatch.setenv("FERRIC_CUDA_XT", xt)
     b, eo, ev = synthetic.rimp2_inputs(naux, nocc, nvir)
@@ -106,8 +104,8 @@ def test_mixed_energy_matches_oracle_and_emulation(fc, monkeypatch, naux, nocc, 
     e_os, e_ss = rimp2.rimp2_energy(b, eo, ev, precision="mixed", stats=st)
     assert st["precision"] == 1 and st["launches"] > 0
     assert abs(e_os + e_ss - ref[2]) <= MIXED_E_REL * abs(ref[2]) + MIXED_E_ABS
-    em = energy_from_g(emulate_fixed_slices(b), eo, ev, xt=xt == "1")
-    # exact accumulation: device == emulation (incl. the FP32 parking of X) to summation rounding
+    em = energy_from_g(emulate_fixed_slices(b), eo, ev, b)
+    # exact accumulation: device == emulation to summation rounding
     assert abs(e_os - em[0]) <= 1e-12 * abs(em[0]) + 1e-15
     assert abs(e_ss - em[1]) <= 1e-12 * abs(em[0]) + 1e-15
 
@@ -124,10 +122,10 @@ def test_mixed_gradient_matches_oracle(fc, monkeypatch, naux, nocc, nvir, xt):
     assert np.abs(g - gamma).max() <= MIXED_G_REL * np.abs(gamma).max()
     assert np.abs(go - d_o).max() <= MIXED_D_REL * np.abs(d_o).max()
     assert np.abs(gv - d_v).max() <= MIXED_D_REL * np.abs(d_v).max()
-    # the gradient call's energy is the energy call's energy, up to which
-    # element of each pair was parked in FP32 (2^-24 relative, random)
+    # the gradient call's energy is the energy call's energy (the same FP64
+    # terms), up to the order of the partial sums
     e2 = rimp2.rimp2_energy(b, eo, ev, precision="mixed")
-    assert abs(sum(e2) - sc.e_total) <= 1e-9 * abs(sc.e_total)
+    assert abs(sum(e2) - sc.e_total) <= 1e-13 * abs(sc.e_total)
 
 
 def test_mixed_gradient_chunked(fc, monkeypatch):
@@ -188,13 +186,28 @@ def test_adjoint_k_segments(fc, monkeypatch):
 
 
 def test_mixed_refuses_naux_beyond_exact_int32(fc):
-    """The int8 pair kernel's level sums are exact while 3 * 127^2 * naux <
-    2^31: a larger aux basis is refused (FC_ERR_LAYOUT, nothing launched),
-    and FP64 takes it."""
+    """The pair kernel's level sums are exact while 4 * 127^2 * naux <= 2^31 - 1
+    (naux <= 33286): at naux = 33286 a constant B whose four slices all sit at
+    +-127 (x / s = 127 - 127/254 + 127/254^2 - 127/254^3, so level 3 sums
+    -4 * 127^2 per aux function, 2147479576 in magnitude) still equals the
+    exact emulation -- an int32 wrap would be off by 2^32 -- and FP64 to the
+    dropped level-4 products (3 127^2 / 254^4 of each term here, where the
+    two occupied rows are equal); naux = 33287 is refused (FC_ERR_LAYOUT,
+    nothing launched), and FP64 takes it."""
     import ferric_b200._lib as L
     from ferric_b200 import rimp2
+    c = 127.0 - 127.0 / 254 + 127.0 / 254 ** 2 - 127.0 / 254 ** 3
+    _, sl = pair_slices(np.full((4, 1), c))
+    assert [int(x[0, 0]) for x in sl] == [127, -127, 127, -127]
+    eo, ev = np.array([-1.0, -0.8]), np.array([0.5])
+    b = np.full((33286, 2), c)
+    e = rimp2.rimp2_energy(b, eo, ev, precision="mixed")
+    em = energy_from_g(emulate_fixed_slices(b), eo, ev, b)
+    assert abs(e[0] - em[0]) <= 1e-12 * abs(em[0]) and abs(e[1] - em[1]) <= 1e-12 * abs(em[0])
+    ref = orc.spin_components(b, np.concatenate([eo, ev]), 2, 1)
+    assert abs(sum(e) - ref[2]) <= 2.0 * 3.0 * 127 ** 2 / 254.0 ** 4 / 127 ** 2 * abs(ref[2])
     rng = np.random.default_rng(3)
-    b = rng.standard_normal((44383, 2)) * 1e-3
+    b = rng.standard_normal((33287, 2)) * 1e-3
     eo, ev = np.array([-1.0]), np.array([0.5, 0.9])
     with pytest.raises(L.FcError) as ei:
         rimp2.rimp2_energy(b, eo, ev, precision="mixed")
@@ -246,19 +259,21 @@ def test_mixed_fast_has_no_adjoint(fc):
 
 
 def test_exchange_matches_two_phases(fc, monkeypatch):
-    """The diagonal-tile exchange changes only which Y values are parked in
-    FP32 (those of diagonal tiles): energy to ~1e-9, Gamma to the FP32 rounding
-    of the amplitudes."""
+    """The diagonal-tile exchange reads Y = X^T back from the FP64 X tile; the
+    two-phase schedule computes Y with the operands swapped, whose level sums
+    are the same integers (the kept products are symmetric in the two
+    operands), so both give the same energy, Gamma and dE/deps_occ bits."""
     from ferric_b200 import rimp2
     b, eo, ev = synthetic.rimp2_inputs(520, 7, 300)
     out = {}
     for xt in ("0", "1"):
         monkeypatch.setenv("FERRIC_CUDA_XT", xt)
         out[xt] = rimp2.rimp2_energy_grad(b, eo, ev, precision="mixed")
-    e0, e1 = out["0"][0].e_total, out["1"][0].e_total
-    assert abs(e0 - e1) <= 1e-9 * abs(e0)
-    for k in (1, 2, 3):
-        assert np.abs(out["0"][k] - out["1"][k]).max() <= 1e-6 * np.abs(out["0"][k]).max()
+    assert out["0"][0].e_os == out["1"][0].e_os and out["0"][0].e_ss == out["1"][0].e_ss
+    assert np.array_equal(out["0"][1], out["1"][1]) and np.array_equal(out["0"][2], out["1"][2])
+    # dE/deps_vir: a two-phase tile sums its column terms in FP32 over a warp's
+    # rows, the exchanged tile adds them to its rows in FP64
+    assert np.abs(out["0"][3] - out["1"][3]).max() <= 1e-7 * np.abs(out["0"][3]).max()
 
 
 EDGE = [

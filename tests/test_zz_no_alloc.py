@@ -2,15 +2,16 @@
 cudaMalloc (their device memory belongs to another allocator, or an inner loop
 must not take cudaMalloc's device synchronisation).  Its scratch is a fixed
 array inside the library.  The test calls it through the C ABI twice in a row
-and checks both results against the workspace entry point fc_rimp2_energy_dev,
-and that the library's workspace pool and the device's free memory do not
-change across the calls.  Collected last so a failure here leaves every other
-test already run."""
+and checks both results against the workspace entry point fc_rimp2_energy_dev
+and against the FP64 oracle, and that the library's workspace pool and the
+device's free memory do not change across the calls.  Collected last so a
+failure here leaves every other test already run."""
 import ctypes
 
 import numpy as np
 import pytest
 
+from oracle import rimp2 as orc
 from oracle import synthetic
 
 pytestmark = pytest.mark.gpu
@@ -40,6 +41,7 @@ def test_noalloc_matches_workspace_entry_point(fc, naux, nocc, nvir, kappa):
     tb, to, tv = (torch.from_numpy(x).cuda() for x in (b, eo, ev))
     stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
     ref = _reference(L, tb, to, tv, stream, kappa)
+    o_os, o_ss, _ = orc.spin_components(b, np.concatenate([eo, ev]), nocc, nvir, kappa=kappa)
     torch.cuda.synchronize()
     pool0 = L.lib.fc_pool_used()
     free0 = torch.cuda.mem_get_info()[0]
@@ -49,6 +51,9 @@ def test_noalloc_matches_workspace_entry_point(fc, naux, nocc, nvir, kappa):
         # same kernel and reduction order as the workspace path: FP64 tolerance of the plain set
         assert abs(e_os - ref[0]) <= 1e-12 * abs(ref[0]) + 1e-15
         assert abs(e_ss - ref[1]) <= 1e-12 * abs(ref[0]) + 1e-15
+        # and the FP64 oracle to the plain set's parity bar
+        assert abs(e_os - o_os) <= 1e-10 + 1e-13 * abs(o_os)
+        assert abs(e_ss - o_ss) <= 1e-10 + 1e-13 * abs(o_os)
     torch.cuda.synchronize()
     assert L.lib.fc_pool_used() == pool0
     assert free0 - torch.cuda.mem_get_info()[0] < (1 << 20)
