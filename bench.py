@@ -11,9 +11,18 @@ The metric is algorithmic TFLOP/s of the step:
 ``e2e``    : the same step through the host-array C ABI (fc_rimp2_energy_grad,
              fc_dfj_build, fc_dfk_build_occ) from pinned host buffers, copies
              inside the timed region.
-``--impl reference`` times the CPU restatement of the reference algorithms
-(the oracle port, NumPy/OpenBLAS on every host core) on a bounded sample of
-the same step.
+``--impl reference`` and ``cpu_baseline`` time the C++ restatement of the
+reference's host algorithms (oracle/cpu_ref.cpp: OpenMP over work units,
+OpenBLAS at one thread per unit, on every physical host core) on a bounded
+sample of the same step: RI-MP2 units (i, j-block) spread over the whole
+occupied range, scaled to the full step, plus one whole DF-J and DF-K build.
+``roofline`` is the dominant kernel of the step (by device time, CUDA events
+in this run), ``roofline_kernels`` both RI-MP2 kernels: achieved = executed
+tensor-core work per launch in BF16-equivalent flops (an int8 MMA of K = 32
+takes the time of a bf16 one of K = 16) / mean launch time, against the
+measured sustained BF16 peak (MEASURED_PEAKS.json); ``traffic`` is the DRAM
+bytes per launch of an ncu capture committed in profiles/traffic.txt, with
+the commit it was captured at.
 
 Under torchrun each rank runs its own replica of the step (independent
 systems, no data-path collective): weak scaling.
@@ -39,15 +48,19 @@ PREC_NAMES = {"f64": 0, "mixed": 1, "mixed_fast": 2}
 # tensor-core products per algorithmic product of the pair kernel: four int8
 # slices, the ten products of level <= 3 (mixed); hi+lo bf16 (mixed_fast)
 EXECUTED_PRODUCTS = {"f64": 1, "mixed": 10, "mixed_fast": 3}
+# the adjoint contraction: three int8 slices, six products (mixed)
+ADJOINT_PRODUCTS = {"f64": 1, "mixed": 6, "mixed_fast": 6}
 
 
-def step_flops():
-    naux, nocc, nvir = RIMP2["naux"], RIMP2["nocc"], RIMP2["nvir"]
+def step_flops(rim=None, jkc=None):
+    rim = rim or RIMP2
+    jkc = jkc or DFJK
+    naux, nocc, nvir = rim["naux"], rim["nocc"], rim["nvir"]
     nov = nocc * nvir
     P = nocc * (nocc + 1) / 2
     f_e = 2.0 * naux * nvir * nvir * P
     f_g = 2.0 * naux * nov * nov
-    n, na, no = DFJK["n"], DFJK["naux"], DFJK["nocc"]
+    n, na, no = jkc["n"], jkc["naux"], jkc["nocc"]
     f_j = 4.0 * na * n * (n + 1) / 2
     f_k = 4.0 * na * n * n * no
     return dict(rimp2_e=f_e, rimp2_grad=f_g, dfj=f_j, dfk=f_k, total=f_e + f_g + f_j + f_k)
@@ -115,12 +128,14 @@ class ClockSampler:
 
 # ------------------------------------------------------------ workloads --
 
-def make_inputs(torch, dev):
+def make_inputs(torch, dev, rim=None, jkc=None):
     """Seeded synthetic tensors of both workloads, generated on the device."""
     import numpy as np
+    rim = rim or RIMP2
+    jkc = jkc or DFJK
     g = torch.Generator(device=dev)
     g.manual_seed(3)
-    naux, nocc, nvir = RIMP2["naux"], RIMP2["nocc"], RIMP2["nvir"]
+    naux, nocc, nvir = rim["naux"], rim["nocc"], rim["nvir"]
     b_ov = torch.randn((naux, nocc * nvir), generator=g, device=dev, dtype=torch.float64)
     decay = 3000.0 * naux / 4800.0
     b_ov *= 0.02 * torch.exp(-torch.arange(naux, device=dev, dtype=torch.float64) / decay)[:, None]
@@ -128,7 +143,7 @@ def make_inputs(torch, dev):
     eo = torch.from_numpy(np.sort(r2.uniform(-20.0, -0.3, nocc))).to(dev)
     ev = torch.from_numpy(np.sort(r2.uniform(0.05, 6.0, nvir))).to(dev)
 
-    n, na, no = DFJK["n"], DFJK["naux"], DFJK["nocc"]
+    n, na, no = jkc["n"], jkc["naux"], jkc["nocc"]
     g.manual_seed(2)
     idx = torch.arange(n, device=dev, dtype=torch.float64)
     env = 0.05 * torch.exp(-(idx[:, None] - idx[None, :]).abs() / 50.0)
@@ -194,76 +209,74 @@ def measure_dgemm_tflops(torch, dev):
 
 
 def read_traffic(kernel):
-    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, if any."""
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary
+    (profiles/traffic.txt: `<key> <bytes> <commit> <capture>`), with the
+    commit and capture it came from; (None, None) if there is none."""
     path = os.path.join(ROOT, "profiles", "traffic.txt")
     try:
         for line in open(path):
-            parts = line.split()
+            parts = line.split(None, 3)
             if len(parts) >= 2 and parts[0] == kernel:
-                return float(parts[1])
+                src = (f"ncu dram__bytes_read.sum + dram__bytes_write.sum at commit {parts[2]}: {parts[3].strip()}"
+                       if len(parts) == 4 else "ncu (profiles/traffic.txt)")
+                return float(parts[1]), src
     except OSError:
         pass
-    return None
+    return None, None
 
 
 # --------------------------------------------------------------- CPU arm --
 
-def cpu_sample(inputs_host, occ_sample=(0, 1), k_rows=240):
-    """Oracle port on the host cores: a bounded sample of one step.
-
-    RI-MP2: the recompute-per-i energy + adjoint for occupied rows
-    ``occ_sample``; DF-J: both passes in full; DF-K: the occupied path over
-    the first ``k_rows`` aux rows.  Returns (tflops, seconds, description).
-    """
-    import numpy as np
-    from oracle import dfjk as odfjk
-    from oracle import rimp2 as ormp2
-    b, eo, ev, bp, bsq_rows, c, d = (inputs_host[k] for k in ("b_ov", "eo", "ev", "bp", "bsq_rows", "c", "d"))
-    naux, nocc, nvir = RIMP2["naux"], RIMP2["nocc"], RIMP2["nvir"]
-    nov = nocc * nvir
-    n = DFJK["n"]
-    t0 = time.perf_counter()
-    ormp2.energy_gamma_deps(b, eo, ev, occ=occ_sample)
-    t1 = time.perf_counter()
-    w = odfjk.packed_density_weights(d)
-    dp = bp @ w
-    _ = bp.T @ dp
-    t2 = time.perf_counter()
-    odfjk.df_k_occ(bsq_rows, c)
-    t3 = time.perf_counter()
-    f_rimp2 = len(occ_sample) * (2.0 * naux * nvir * nov * 2)   # G_i and x_i per sampled i
-    f_j = 4.0 * bp.shape[0] * bp.shape[1]
-    f_k = 4.0 * bsq_rows.shape[0] * n * n * c.shape[1]
-    secs = t3 - t0
-    desc = (f"RI-MP2 E+grad for {len(occ_sample)} of {nocc} occupied rows ({t1 - t0:.2f} s), "
-            f"DF-J full ({t2 - t1:.2f} s), DF-K over {bsq_rows.shape[0]} of {DFJK['naux']} aux rows "
-            f"({t3 - t2:.2f} s)")
-    return (f_rimp2 + f_j + f_k) / secs / 1e12, secs, desc
+def rimp2_cpu_units(nocc, cores, width=4, offset=0):
+    """A bounded sample of RI-MP2 units (i, j0, j0 + width): one per core,
+    i spread over the whole occupied range (the work of a unit does not
+    depend on i) and the j-blocks over the whole range too."""
+    nblk = -(-nocc // width)
+    units = []
+    for k in range(cores):
+        i = (k * nocc // cores + offset) % nocc
+        jb = (k * 7 + 3 * offset) % nblk
+        units.append((i, jb * width, min(nocc, (jb + 1) * width)))
+    return units, nocc * nblk
 
 
-def host_threads():
-    try:
-        from threadpoolctl import threadpool_info
-        n = [i.get("num_threads", 0) for i in threadpool_info() if i.get("internal_api") == "openblas"]
-        if n:
-            return max(n)
-    except Exception:  # noqa: BLE001
-        pass
-    return os.cpu_count()
+def cpu_sample(inputs_host, offset=0):
+    """The C++ restatement of the reference's host algorithms on every
+    physical core: a sample of RI-MP2 units (one per core, scaled to the full
+    step), one whole DF-J and one whole DF-K build.  Returns (tflops of the
+    whole step, extrapolated step seconds, cores, description)."""
+    from oracle import cpu_ref
+    cores = cpu_ref.physical_cores()
+    b, eo, ev, bp, w, bsq, c = (inputs_host[k] for k in ("b_ov", "eo", "ev", "bp", "w", "bsq", "c"))
+    nocc = len(eo)
+    units, total_units = rimp2_cpu_units(nocc, cores, offset=offset)
+    t_r, _, _ = cpu_ref.rimp2_units(b, eo, ev, units, cores)
+    t_j, _ = cpu_ref.dfj(bp, w, cores)
+    t_k, _ = cpu_ref.dfk(bsq, c, cores)
+    t_rimp2 = t_r * total_units / len(units)
+    secs = t_rimp2 + t_j + t_k
+    desc = (f"C++ port (OpenMP over units, OpenBLAS 1 thread each) on {cores} physical cores: "
+            f"RI-MP2 E+grad {len(units)} of {total_units} units (i, 4-orbital j-block) spread over the "
+            f"occupied range in {t_r:.2f} s, scaled to {t_rimp2:.1f} s; DF-J full {t_j:.2f} s; "
+            f"DF-K full {t_k:.2f} s")
+    return step_flops()["total"] / secs / 1e12, secs, cores, desc
 
 
 def host_inputs_from(torch, inp):
+    """Host copies of the step's inputs for the CPU arm: B_ov, the DF-JK
+    tensor square (DF-K) and as packed lower rows (DF-J), the packed density
+    weights, C_occ."""
     import numpy as np
     from oracle import dfjk as odfjk
-    k_rows = 240
-    bsq_rows = inp["bjk"][:k_rows].cpu().numpy()
     n = DFJK["n"]
     il, jl = np.tril_indices(n)
     il_t = torch.from_numpy(il).to(inp["bjk"].device)
     jl_t = torch.from_numpy(jl).to(inp["bjk"].device)
     bp = inp["bjk"][:, il_t, jl_t].cpu().numpy()
+    d = inp["d"].cpu().numpy()
     return dict(b_ov=inp["b_ov"].cpu().numpy(), eo=inp["eo"].cpu().numpy(), ev=inp["ev"].cpu().numpy(),
-                bp=bp, bsq_rows=bsq_rows, c=inp["c"].cpu().numpy(), d=inp["d"].cpu().numpy()), odfjk
+                bp=bp, w=odfjk.packed_density_weights(d), bsq=inp["bjk"].cpu().numpy(),
+                c=inp["c"].cpu().numpy(), d=d)
 
 
 # ------------------------------------------------------------------ main --
@@ -365,6 +378,68 @@ def dress_leg(torch, dev, naux=2150, n=872, nocc=81):
     return out
 
 
+C5_RIMP2 = dict(naux=2150, nocc=81, nvir=791)
+C5_DFJK = dict(n=872, naux=2256, nocc=81)
+
+
+def c5_leg(torch, dev, prec, steps=3):
+    """Config 5 at the shapes of all-trans C20H42 in def2-TZVP (RI-MP2: naux
+    2150 def2-TZVP-RIFIT, nocc 81, nvir 791; DF-JK: n 872, naux 2256
+    def2-universal-jkfit, nocc 81), synthetic tensors with the config-3 /
+    config-2 distributions: the mixed step (median of `steps` after a
+    warm-up) and one FP64-plain step, the speed-up, the mixed errors against
+    FP64, and the pair kernel's and the adjoint's device time."""
+    from ferric_b200 import rimp2
+    from ferric_b200.dfjk import DfJK
+    inp = make_inputs(torch, dev, C5_RIMP2, C5_DFJK)
+    fl = step_flops(C5_RIMP2, C5_DFJK)
+    stream = torch.cuda.current_stream(dev)
+    out = {"rimp2": C5_RIMP2, "dfjk": C5_DFJK, "flops": fl["total"],
+           "data": "synthetic (seeded, generated on device) at the C20H42 def2-TZVP shapes"}
+    res = {}
+    for p in (prec, "f64"):
+        jk = DfJK(inp["bjk"], layout="square", precision=p)
+        gamma, d_o, d_v = torch.empty_like(inp["b_ov"]), torch.empty_like(inp["eo"]), torch.empty_like(inp["ev"])
+
+        def one():
+            st = ({}, {}, {})
+            sc, *_ = rimp2.rimp2_energy_grad(inp["b_ov"], inp["eo"], inp["ev"], precision=p, stats=st[0],
+                                             out=(gamma, d_o, d_v))
+            j = jk.j(inp["d"], stats=st[1])
+            k = jk.k_from_occ(inp["c"], stats=st[2])
+            return sc, st, j, k
+        one()
+        ms = []
+        for _ in range(steps if p == prec else 1):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            sc, st, j, k = one()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        t = statistics.median(ms)
+        r = st[0]
+        res[p] = dict(sc=sc, gamma=gamma.clone(), j=j, k=k)
+        out[p] = {"ms_per_step": t, "tflops": fl["total"] / (t * 1e-3) / 1e12,
+                  "components_ms": {"rimp2_e_grad": r["kernel_ms"], "dfj": st[1]["kernel_ms"],
+                                    "dfk": st[2]["kernel_ms"]},
+                  "pair_kernel_ms": r["main_ms"], "pair_launches": r["main_launches"],
+                  "adjoint_ms": r["aux_ms"], "adjoint_launches": r["aux_launches"]}
+        jk.close()
+        del gamma
+    m, f = res[prec], res["f64"]
+    out["speedup_mixed_vs_plain"] = out["f64"]["ms_per_step"] / out[prec]["ms_per_step"]
+    out["mixed_error"] = {"e_total_abs": m["sc"].e_total - f["sc"].e_total,
+                          "e_total_rel": (m["sc"].e_total - f["sc"].e_total) / abs(f["sc"].e_total),
+                          "gamma_max_rel": float((m["gamma"] - f["gamma"]).abs().max() / f["gamma"].abs().max()),
+                          "j_max_abs": float((m["j"] - f["j"]).abs().max()),
+                          "k_max_abs": float((m["k"] - f["k"]).abs().max())}
+    del inp, res, m, f
+    torch.cuda.empty_cache()
+    return out
+
+
 def max_over_ranks(torch, ms, world, dev):
     """The slowest rank's device time: every rank takes part in one MAX all-reduce."""
     if world <= 1:
@@ -392,6 +467,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched config-4 leg")
     ap.add_argument("--batch-mols", type=int, default=512)
     ap.add_argument("--no-dress", action="store_true", help="skip the MO-dressing leg")
+    ap.add_argument("--no-c5", action="store_true", help="skip the config-5 leg")
     ap.add_argument("--size", choices=["full", "small", "c5"], default="full",
                     help="small: naux 2400, nocc 60, nvir 550 + n 300, naux 1200, nocc 30 "
                          "(the profiling case; inputs still larger than L2); c5: the shapes of "
@@ -424,21 +500,22 @@ def main():
         import numpy as np
         dev = torch.device("cuda", local) if torch.cuda.is_available() else torch.device("cpu")
         inp = make_inputs(torch, dev)
-        host, _ = host_inputs_from(torch, inp)
+        host = host_inputs_from(torch, inp)
         del inp
+        torch.cuda.empty_cache()
         vals = []
         for s in range(args.warmup + args.steps):
-            v, secs, desc = cpu_sample(host, occ_sample=(s % RIMP2["nocc"],))
+            v, secs, cores, desc = cpu_sample(host, offset=s)
             if s >= args.warmup:
                 vals.append(v)
-        value = statistics.median(vals)
+        value = max(vals)   # the fastest of the timed samples (min time)
         ms = flops["total"] / (value * 1e12) * 1e3
         out = {"impl": "reference", "metric": "RI-MP2 E+grad & DF-JK step throughput (algorithmic TFLOP/s)",
                "value": value, "unit": "TFLOP/s", "n_gpus": args.gpus, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "config": config,
-               "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": host_threads(), "kind": "port",
-                                "sample": "per step: " + desc},
+               "cpu_baseline": {"value": value, "unit": "TFLOP/s", "cores": cores, "kind": "port",
+                                "sample": f"per step (best of {args.steps}, after {args.warmup} warm-up): " + desc},
                "e2e": {"value": value, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(out))
         return
@@ -507,6 +584,8 @@ def main():
     launches = 0
     main_ms = main_flops = 0.0
     main_launch = 0
+    aux_ms = aux_flops = 0.0
+    aux_launch = 0
     with ClockSampler(local) as clk:
         torch.cuda.synchronize()
         barrier()
@@ -518,6 +597,9 @@ def main():
             main_ms += last["rimp2"]["main_ms"]
             main_flops += last["rimp2"]["main_flops"]
             main_launch += last["rimp2"]["main_launches"]
+            aux_ms += last["rimp2"]["aux_ms"]
+            aux_flops += last["rimp2"]["aux_flops"]
+            aux_launch += last["rimp2"]["aux_launches"]
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
@@ -526,30 +608,48 @@ def main():
     value = replica_throughput(world, flops["total"], ms_step)
     sc = last["energy"]
 
-    # ---- roofline of the dominant kernel (the fused RI-MP2 pair kernel)
+    # ---- rooflines of the two RI-MP2 kernels; `roofline` is the one with
+    # more device time in the timed steps
     peaks, peak_src = measured_peaks()
-    avg_launch_ms = main_ms / max(1, main_launch)
-    flops_per_launch = main_flops / max(1, main_launch)
-    executed = EXECUTED_PRODUCTS[prec]
-    if prec == "f64":
-        peak = measure_dgemm_tflops(torch, dev)
-        peak_note = "measured in this run: cuBLAS DGEMM 8192^3 (FP64 tensor path)"
-        achieved = flops_per_launch / (avg_launch_ms * 1e-3) / 1e12
-    elif prec == "mixed":
-        peak = measure_i8_tops(torch, dev)
-        peak_note = ("measured in this run: cuBLAS int8 GEMM 8192^3 sustained (torch._int_mm); "
-                     f"executed = {executed} x algorithmic int8 ops")
-        achieved = executed * flops_per_launch / (avg_launch_ms * 1e-3) / 1e12
-    else:
-        peak = peaks.get("bf16_tflops_sustained", peaks["bf16_tflops"])
-        peak_note = f"{peak_src} bf16 dense (sustained), executed = {executed} x algorithmic flops"
-        achieved = executed * flops_per_launch / (avg_launch_ms * 1e-3) / 1e12
-    roofline = {"bound": "tensor", "kernel": "rimp2 pair kernel (fused G_ij + denominator epilogue)",
-                "achieved": achieved, "peak": peak, "unit": "TOP/s" if prec == "mixed" else "TFLOP/s",
-                "frac": achieved / peak,
-                "peak_source": peak_note, "flops_per_launch": flops_per_launch,
-                "avg_launch_ms": avg_launch_ms,
-                "traffic": read_traffic(f"rimp2_pair_{prec}")}
+    bf16_peak = peaks.get("bf16_tflops_sustained", peaks["bf16_tflops"])
+    i8_peak = measure_i8_tops(torch, dev) if prec == "mixed" else None
+    f64_peak = measure_dgemm_tflops(torch, dev) if prec == "f64" else None
+    kern = {"pair": dict(ms=main_ms, flops=main_flops, launches=main_launch, products=EXECUTED_PRODUCTS[prec],
+                         name="pair kernel: G_ij tiles + denominator / energy / amplitude epilogue",
+                         traffic_key=f"rimp2_pair_{prec}"),
+            "adjoint": dict(ms=aux_ms, flops=aux_flops, launches=aux_launch, products=ADJOINT_PRODUCTS[prec],
+                            name="adjoint contraction Gamma += 4 B Tt^T",
+                            traffic_key=f"rimp2_adjoint_{prec}")}
+    rooflines = {}
+    for key, k in kern.items():
+        if k["launches"] == 0 or k["ms"] <= 0.0:
+            continue
+        avg_ms = k["ms"] / k["launches"]
+        alg = k["flops"] / k["launches"]                        # algorithmic flops per launch
+        alg_tf = alg / (avg_ms * 1e-3) / 1e12
+        traffic, tsrc = read_traffic(k["traffic_key"])
+        r = {"bound": "tensor", "kernel": k["name"], "launches_per_step": k["launches"] // args.steps,
+             "avg_launch_ms": avg_ms, "algorithmic_flops_per_launch": alg, "algorithmic_tflops": alg_tf,
+             "traffic": traffic, "traffic_source": tsrc}
+        if prec == "f64":
+            r.update(achieved=alg_tf, peak=f64_peak, unit="TFLOP/s", frac=alg_tf / f64_peak,
+                     peak_source="cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor path)")
+        else:
+            # int8 (kind::i8): an MMA of K = 32 takes the time of a bf16 MMA of K = 16
+            per_bf16 = 0.5 if prec == "mixed" else 1.0
+            ex = k["products"] * per_bf16 * alg_tf
+            r.update(achieved=ex, peak=bf16_peak, unit="TFLOP/s", frac=ex / bf16_peak,
+                     peak_source=f"{peak_src} bf16_tflops_sustained (MEASURED_PEAKS.json)",
+                     achieved_note=(f"BF16-equivalent executed: {k['products']} tensor-core products per "
+                                    f"algorithmic product" + (" at int8 (half a bf16 MMA each)"
+                                                              if prec == "mixed" else "")))
+            if i8_peak:
+                r["int8_tops"] = k["products"] * alg_tf
+                r["int8_peak_measured"] = i8_peak
+                r["int8_frac"] = r["int8_tops"] / i8_peak
+        rooflines[key] = r
+    dom = max(rooflines, key=lambda x: kern[x]["ms"])
+    roofline = dict(rooflines[dom], which=dom)
     dfj = last["dfj"]
     roof_dfj = {"bound": "hbm", "achieved": dfj["main_bytes"] / (dfj["main_ms"] * 1e-3) / 1e9,
                 "peak": peaks["hbm_gbs"], "unit": "GB/s"}
@@ -569,8 +669,11 @@ def main():
         p1.record(stream)
         torch.cuda.synchronize()
         pms = p0.elapsed_time(p1)
+        cm = {"rimp2_e_grad": last["rimp2"]["kernel_ms"], "dfjk": last["dfj"]["kernel_ms"] + last["dfk"]["kernel_ms"]}
         plain = {"ms_per_step": pms, "value": flops["total"] / (pms * 1e-3) / 1e12, "unit": "TFLOP/s",
                  "speedup_mixed_vs_plain": pms / ms_step,
+                 "speedup_rimp2_e_grad": sp_r["kernel_ms"] / cm["rimp2_e_grad"],
+                 "speedup_dfjk": (sp_j["kernel_ms"] + sp_k["kernel_ms"]) / cm["dfjk"],
                  "components_ms": {"rimp2_e_grad": sp_r["kernel_ms"], "dfj": sp_j["kernel_ms"],
                                    "dfk": sp_k["kernel_ms"]},
                  "mixed_error": {"e_total_abs": (sc.e_os + sc.e_ss) - sc64.e_total,
@@ -631,16 +734,23 @@ def main():
     # ---- CPU baseline (rank 0, N = 1)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        host, _ = host_inputs_from(torch, inp)
-        v, secs, desc = cpu_sample(host)
-        cpu = {"value": v, "unit": "TFLOP/s", "cores": host_threads(), "kind": "port",
-               "sample": desc, "seconds": secs}
+        host = host_inputs_from(torch, inp)
+        v, secs, cores, desc = cpu_sample(host)
+        cpu = {"value": v, "unit": "TFLOP/s", "cores": cores, "kind": "port",
+               "sample": desc, "seconds_per_step": secs}
+        del host
+
+    jk.close()
+    del gamma, inp
+    torch.cuda.empty_cache()
+    # ---- config 5: C20H42 def2-TZVP shapes, mixed vs FP64 plain
+    c5 = None
+    if prec == "mixed" and args.size == "full" and not args.no_c5:
+        c5 = c5_leg(torch, dev, prec)
 
     # ---- config 4: batched RI-MP2 E+grad over 512 molecules of uneven size
     batch = None
     if prec == "mixed" and not args.no_batch:
-        del gamma, inp
-        torch.cuda.empty_cache()
         batch = batch_leg(torch, dev, args.batch_mols)
 
     # ---- the step before the path: MO transform + metric dressing, config-5 shapes
@@ -654,19 +764,19 @@ def main():
             "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": {"f64": "f64",
-                      "mixed": "int8 x3 integer slices, 6 products, exact int32 accumulation, f64 epilogue"}[prec],
+                      "mixed": ("int8 integer slices, exact int32 accumulation, f64 epilogue (pair kernel: 4 slices, "
+                                "10 products; adjoint: 3 slices, 6 products)")}[prec],
             "precision": prec, "dfj_precision": dfj_prec, "dfk_precision": dfk_prec,
             "data": "synthetic (seeded, generated on device)", "config": config,
             "components_ms": {"rimp2_e_grad": last["rimp2"]["kernel_ms"], "dfj": last["dfj"]["kernel_ms"],
                               "dfk": last["dfk"]["kernel_ms"]},
             "flops": flops, "energy": {"e_os": sc.e_os, "e_ss": sc.e_ss},
-            "roofline": roofline, "roofline_dfj": roof_dfj,
+            "roofline": roofline, "roofline_kernels": rooflines, "roofline_dfj": roof_dfj,
             "plain_f64": plain,
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
-            "config4_batch": batch, "mo_dressing": dress,
+            "config4_batch": batch, "config5": c5, "mo_dressing": dress,
         }
         print(json.dumps(out))
-    jk.close()
     if world > 1:
         torch.distributed.destroy_process_group()
 

@@ -102,6 +102,8 @@ class FcStats(ctypes.Structure):
         ("k_panel", ctypes.c_int32), ("main_launches", ctypes.c_int32),
         ("main_ms", ctypes.c_double), ("main_flops", ctypes.c_double),
         ("main_bytes", ctypes.c_double),
+        ("aux_launches", ctypes.c_int32), ("reserved_", ctypes.c_int32),
+        ("aux_ms", ctypes.c_double), ("aux_flops", ctypes.c_double), ("aux_bytes", ctypes.c_double),
     ]
 
     def as_dict(self):

@@ -111,6 +111,30 @@ fc_status timing_sum(int n, double* ms) {
     return FC_OK;
 }
 
+fc_status timing_events2(int n, cudaEvent_t** out) {
+    Context& c = ctx();
+    while ((int)c.evs2.size() < 2 * n) {
+        cudaEvent_t e;
+        FC_CUDA(cudaEventCreate(&e));
+        c.evs2.push_back(e);
+    }
+    *out = c.evs2.data();
+    return FC_OK;
+}
+
+fc_status timing_sum2(int n, double* ms) {
+    Context& c = ctx();
+    double t = 0.0;
+    if (n > 0) FC_CUDA(cudaEventSynchronize(c.evs2[2 * n - 1]));
+    for (int k = 0; k < n; ++k) {
+        float x = 0.f;
+        FC_CUDA(cudaEventElapsedTime(&x, c.evs2[2 * k], c.evs2[2 * k + 1]));
+        t += x;
+    }
+    *ms = t;
+    return FC_OK;
+}
+
 cudaStream_t pick_stream(void* s) { return s ? static_cast<cudaStream_t>(s) : ctx().stream; }
 
 bool mul_ok(int64_t a, int64_t b, int64_t* out) {

@@ -86,7 +86,8 @@ struct Context {
     std::mutex mu;
     Workspace ws[WS_COUNT];
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    std::vector<cudaEvent_t> evs;  // per-launch timing pairs of the dominant kernel
+    std::vector<cudaEvent_t> evs;   // per-launch timing pairs of the dominant kernel
+    std::vector<cudaEvent_t> evs2;  // per-launch timing pairs of the second kernel
 };
 
 Context& ctx();
@@ -101,6 +102,9 @@ cudaStream_t pick_stream(void* s);
 fc_status timing_events(int n, cudaEvent_t** out);
 // Sum of elapsed times of the n event pairs (waits for the last one).
 fc_status timing_sum(int n, double* ms);
+// The same pool for a call's second timed kernel.
+fc_status timing_events2(int n, cudaEvent_t** out);
+fc_status timing_sum2(int n, double* ms);
 
 // Overflow-checked size products.
 bool mul_ok(int64_t a, int64_t b, int64_t* out);

@@ -456,7 +456,11 @@ fc_status rimp2_grad_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, doubl
 
     Context& c = ctx();
     cudaEvent_t* ev = nullptr;
+    cudaEvent_t* ev2 = nullptr;
+    int nadj = 0;
+    double adj_flops = 0.0, adj_bytes = 0.0;
     if (stats) FC_TRY(timing_events((int)ncp, &ev));
+    if (stats) FC_TRY(timing_events2((int)(2 * ncp), &ev2));
     if (stats) FC_CUDA(cudaEventRecord(c.ev0, st));
     // Gamma[:, rows of R] += 4 B_ov[:, columns of K] . T^T
     auto adjoint = [&](const double* T, int64_t r0, int64_t nr, int64_t k0, int64_t nk) -> fc_status {
@@ -464,8 +468,13 @@ fc_status rimp2_grad_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, doubl
         dim3 grid((N + DG_BN - 1) / DG_BN, (unsigned)((naux + DG_BM - 1) / DG_BM), 1);
         EpiStore epi{gamma + r0 * nvir, nov, 4.0, 1};
         const int64_t K = nk * nvir;
+        if (stats) FC_CUDA(cudaEventRecord(ev2[2 * nadj], st));
         dgemm_tn_kernel<EpiStore><<<grid, 256, DG_SMEM, st>>>(d.b_ov + k0 * nvir, nov, T, K, (int)naux, N, K, K, 0,
                                                                epi);
+        if (stats) FC_CUDA(cudaEventRecord(ev2[2 * nadj + 1], st));
+        ++nadj;
+        adj_flops += 2.0 * (double)naux * (double)N * (double)K;
+        adj_bytes += 8.0 * (double)naux * (double)K + 8.0 * (double)N * (double)K + 16.0 * (double)naux * (double)N;
         return check_launch("dgemm_tn_kernel<gamma>");
     };
     for (int64_t x = 0; x < ncp; ++x) {
@@ -549,6 +558,10 @@ fc_status rimp2_grad_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, doubl
         FC_TRY(timing_sum((int)ncp, &stats->main_ms));
         stats->main_flops = 4.0 * naux * (double)nvir * nvir * P;
         stats->main_bytes = 8.0 * naux * (double)nov * (double)nch + 8.0 * (double)nov * nov;
+        stats->aux_launches = nadj;
+        FC_TRY(timing_sum2(nadj, &stats->aux_ms));
+        stats->aux_flops = adj_flops;
+        stats->aux_bytes = adj_bytes;
     }
     return FC_OK;
 }

@@ -1734,6 +1734,12 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
         const long long v = std::atoll(e);
         if (v > 0 && v % fx::KT == 0 && v <= fx::KMAX) kseg = v;
     }
+    // timing of the adjoint launches: at most two blocks per chunk pair, each
+    // in ceil(K / kseg) segments
+    cudaEvent_t* ev2 = nullptr;
+    int nadj = 0;
+    double adj_flops = 0.0, adj_bytes = 0.0;
+    if (stats) FC_TRY(timing_events2((int)(2 * ncp * ((cc * tp + kseg - 1) / kseg)), &ev2));
     // Gamma[:, rows] += 4 Bq[:, cols] T^T for one amplitude block
     auto adjoint = [&](float* T, int64_t r0, int64_t nr, int64_t k0, int64_t nk) -> fc_status {
         const int64_t ldk = nk * tp, rows = nr * tp, mp = (rows + 127) / 128 * 128;
@@ -1767,10 +1773,18 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
             g.aofs = (int)ks;
             g.kofs = (int)(k0 * tp + ks);
             g.nk = (int)((kl + fx::KT - 1) / fx::KT);
+            if (stats) FC_CUDA(cudaEventRecord(ev2[2 * nadj], st));
             gemm_fx_kernel<0><<<g2, GF_THREADS, GF_SMEM, st>>>(tmTs, tmBq, g);
             FC_TRY(check_launch("gemm_fx_kernel"));
+            if (stats) FC_CUDA(cudaEventRecord(ev2[2 * nadj + 1], st));
+            ++nadj;
             ++nl;
         }
+        // algorithmic: Gamma[:, rows] += 4 B[:, cols] T^T, and the bytes of
+        // the three Q-row and amplitude slices plus Gamma's read-modify-write
+        adj_flops += 2.0 * (double)naux * (double)(nr * nvir) * (double)(nk * nvir);
+        adj_bytes += 3.0 * (double)naux * (double)(nk * nvir) + 3.0 * (double)(nr * nvir) * (double)(nk * nvir) +
+                     16.0 * (double)naux * (double)(nr * nvir);
         return FC_OK;
     };
     for (int64_t x = 0; x < ncp; ++x) {
@@ -1880,6 +1894,10 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
         stats->main_ms = tsum;
         stats->main_flops = 2.0 * naux * (double)nvir * nvir * P;  // G_ij over unordered pairs
         stats->main_bytes = 8.0 * naux * (double)nov * (double)nch;
+        stats->aux_launches = nadj;
+        FC_TRY(timing_sum2(nadj, &stats->aux_ms));
+        stats->aux_flops = adj_flops;
+        stats->aux_bytes = adj_bytes;
         stats->h2d_bytes += pairs.size() * sizeof(int2);
         stats->d2h_bytes += h.size() * 8 + sizeof(hf);
     }

@@ -41,12 +41,14 @@ typedef int32_t fc_status;
 /* Arithmetic of the contraction kernels. */
 #define FC_PREC_F64        0  /* all-FP64 "plain" kernels: the drop-in             */
 #define FC_PREC_MIXED      1  /* exact integer slices: each operand row scaled by  */
-                              /* a power of two and split into 3 integer slices;   */
-                              /* 6 tensor-core products into 3 accumulators that   */
-                              /* never round.  RI-MP2 pair/adjoint kernels: int8   */
-                              /* slices, int32 sums (tcgen05 kind::i8); DF-K,      */
-                              /* dressing, Imat: bf16 slices, FP32 sums drained    */
-                              /* to FP64 before they could round                   */
+                              /* a power of two and split into integer slices      */
+                              /* whose tensor-core products sum in accumulators    */
+                              /* that never round.  RI-MP2 pair kernel: 4 int8     */
+                              /* slices, the 10 products of level <= 3 in 4 int32  */
+                              /* sums (tcgen05 kind::i8), (ia|ia) of the i == j    */
+                              /* blocks in FP64; adjoint: 3 int8 slices, 6         */
+                              /* products; DF-K, dressing, Imat: 3 bf16 slices,    */
+                              /* FP32 sums drained to FP64 before they could round */
 #define FC_PREC_MIXED_FAST 2  /* split-BF16 hi+lo, 3 products, FP32 accumulation   */
                               /* (energy only; ~1e-5 relative, accumulation-bound) */
 
@@ -73,6 +75,11 @@ typedef struct fc_stats {
     double   main_ms;      /* device time of the dominant kernel, all its launches */
     double   main_flops;   /* algorithmic flops done by the dominant kernel        */
     double   main_bytes;   /* algorithmic bytes moved by the dominant kernel       */
+    int32_t  aux_launches; /* launches of the second kernel (RI-MP2 gradient: the  */
+    int32_t  reserved_;    /* adjoint contraction Gamma += 4 B Tt^T), 0 if none    */
+    double   aux_ms;       /* its device time, all its launches (CUDA events)      */
+    double   aux_flops;    /* its algorithmic flops                                */
+    double   aux_bytes;    /* its algorithmic bytes                                */
 } fc_stats;
 
 /* ---- library ------------------------------------------------------------ */

@@ -74,3 +74,134 @@ def test_dfjk_config2_identities(fc):
         ref = float((dp * dp).sum())
         assert abs(tr - ref) <= (1e-12 if prec == "f64" else 1e-6) * ref
         jk.close()
+
+
+# ---- oracle parity at the benchmark shapes ----------------------------------
+#
+# Config 3 is split into occupied-pair shards (fc_rimp2_energy_grad_shard_dev):
+# with 400 shards the chunks hold one orbital, and shard 0 computes the pairs
+# (0, 0), (0, 1), ..., (0, 17) at the full naux 4800 and nvir 1100.  The
+# oracle restates the reference's per-pair terms for exactly those pairs
+# (rimp2.rs:1399-1441, zvector.rs:651-703) on the orbitals they touch.
+
+NSH = 400
+
+
+def _shard0(torch, precision):
+    from ferric_b200 import sharded
+    b, eo, ev = _rimp2_inputs(torch)
+    pairs = sharded.shard_pairs(120, 1100, 0, NSH, precision=precision, grad=True)
+    return b, eo, ev, pairs
+
+
+def _oracle_subset(b, eo, ev, pairs):
+    """The oracle's (E_os, E_ss, Gamma, dE/deps_occ, dE/deps_vir) of `pairs`,
+    restricted to the occupied orbitals they touch (columns of those
+    orbitals of Gamma; everything else is zero)."""
+    from oracle import rimp2 as orc
+    nvir = ev.numel()
+    occ = sorted(set(int(x) for x in pairs.reshape(-1)))
+    loc = {o: k for k, o in enumerate(occ)}
+    cols = np.concatenate([np.arange(o * nvir, (o + 1) * nvir) for o in occ])
+    bsub = b[:, torch_index(cols, b)].cpu().numpy()
+    lp = [(loc[int(i)], loc[int(j)]) for i, j in pairs]
+    r = orc.energy_gamma_deps_pairs(bsub, eo.cpu().numpy()[occ], ev.cpu().numpy(), lp)
+    return occ, cols, r
+
+
+def torch_index(cols, like):
+    import torch
+    return torch.from_numpy(cols).to(like.device)
+
+
+def test_rimp2_config3_shard_matches_oracle(fc):
+    """FP64 plain on the pairs of one shard at the config-3 shape: E to 1e-10 Eh,
+    Gamma and dE/deps to 1e-12 of their maxima; the mixed form's energy error on
+    the same pairs is inside this shard's share of the 1 uEh budget."""
+    import torch
+    from ferric_b200 import sharded
+    b, eo, ev, pairs = _shard0(torch, "f64")
+    assert len(pairs) == 18 and tuple(pairs[0]) == (0, 0)
+    occ, cols, (r_os, r_ss, r_g, r_do, r_dv) = _oracle_subset(b, eo, ev, pairs)
+    e_os, e_ss, g, d_o, d_v = sharded.rimp2_energy_grad_shard(b, eo, ev, 0, NSH, precision="f64")
+    torch.cuda.synchronize()
+    assert abs(e_os - r_os) <= 1e-10 and abs(e_ss - r_ss) <= 1e-10
+    gs = g[:, torch_index(cols, g)].cpu().numpy()
+    assert np.abs(gs - r_g).max() <= 1e-12 * np.abs(r_g).max()
+    mask = torch.ones(g.shape[1], dtype=torch.bool, device=g.device)
+    mask[torch_index(cols, g)] = False
+    assert float(g[:, mask].abs().max()) == 0.0            # no other orbital is touched
+    do = d_o.cpu().numpy()
+    assert np.abs(do[occ] - r_do).max() <= 1e-12 * np.abs(r_do).max()
+    assert not np.delete(do, occ).any()
+    assert np.abs(d_v.cpu().numpy() - r_dv).max() <= 1e-12 * np.abs(r_dv).max()
+    # the mixed form on the same pairs (the same 18 with one-orbital chunks)
+    assert np.array_equal(pairs, sharded.shard_pairs(120, 1100, 0, NSH, precision="mixed", grad=True))
+    m_os, m_ss, mg, m_do, m_dv = sharded.rimp2_energy_grad_shard(b, eo, ev, 0, NSH, precision="mixed")
+    err = (m_os + m_ss) - (r_os + r_ss)
+    print(f"config-3 shard 0 (18 pairs): mixed E error {err:.3e} Eh of {r_os + r_ss:.6f}")
+    # random per-pair errors add in quadrature: 1 uEh over 7260 pairs is 5e-8 Eh over 18
+    assert abs(err) <= 1e-6 * np.sqrt(18 / 7260)
+    mgs = mg[:, torch_index(cols, mg)].cpu().numpy()
+    assert np.abs(mgs - r_g).max() <= 1e-5 * np.abs(r_g).max()
+
+
+def test_rimp2_config3_shard_finite_differences(fc):
+    """Central finite differences at h = 1e-5 of the shard's FP64 energy on 64
+    seeded entries of B_ov (aux row, column of an orbital of the shard) equal
+    the shard's Gamma: Gamma = dE/dB at the config-3 shape."""
+    import torch
+    from ferric_b200 import sharded
+    b, eo, ev, pairs = _shard0(torch, "f64")
+    _, _, g, _, _ = sharded.rimp2_energy_grad_shard(b, eo, ev, 0, NSH, precision="f64")
+    occ = sorted(set(int(x) for x in pairs.reshape(-1)))
+    rng = np.random.default_rng(31)
+    ps = rng.integers(0, 4800, 64)
+    cs = np.array(occ)[rng.integers(0, len(occ), 64)] * 1100 + rng.integers(0, 1100, 64)
+    h = 1e-5
+    fd = np.empty(64)
+    for k, (p, c) in enumerate(zip(ps.tolist(), cs.tolist())):
+        e = []
+        for s in (h, -2.0 * h):
+            b[p, c] += s
+            r = sharded.rimp2_energy_grad_shard(b, eo, ev, 0, NSH, precision="f64")
+            e.append(r[0] + r[1])
+        b[p, c] += h
+        fd[k] = (e[0] - e[1]) / (2.0 * h)
+    an = g[torch.from_numpy(ps).cuda(), torch.from_numpy(cs).cuda()].cpu().numpy()
+    scale = float(g.abs().max())
+    assert np.abs(fd - an).max() <= 1e-6 * scale, (np.abs(fd - an).max(), scale)
+
+
+def test_dfjk_config2_matches_oracle(fc):
+    """DF-J and DF-K at n 600, naux 2400, nocc 60 against the oracle
+    (df_j.rs:1199-1245 two-pass J, df_k.rs:1575-1660 occupied-path K): FP64
+    plain within 1e-10 max|dJ|, max|dK|; the mixed builds within their bars."""
+    import torch
+    from ferric_b200.dfjk import DfJK
+    from oracle import dfjk as odfjk
+    n, naux, nocc = 600, 2400, 60
+    g = torch.Generator(device="cuda")
+    g.manual_seed(2)
+    idx = torch.arange(n, device="cuda", dtype=torch.float64)
+    env = 0.05 * torch.exp(-(idx[:, None] - idx[None, :]).abs() / 50.0)
+    bjk = torch.empty((naux, n, n), device="cuda", dtype=torch.float64)
+    for q0 in range(0, naux, 256):
+        x = torch.randn((min(256, naux - q0), n, n), generator=g, device="cuda", dtype=torch.float64) * env
+        bjk[q0:q0 + x.shape[0]] = (x + x.transpose(1, 2)) / (2.0 ** 0.5)
+    c, _ = np.linalg.qr(np.random.default_rng(20).standard_normal((n, nocc)))
+    c = np.ascontiguousarray(c)
+    d = c @ c.T
+    bh = bjk.cpu().numpy()
+    j_ref = odfjk.df_j_square(bh, d)
+    k_ref = odfjk.df_k_occ(bh, c)
+    del bh
+    ct, dt = torch.from_numpy(c).cuda(), torch.from_numpy(d).cuda()
+    for prec, jb, kb in (("f64", 1e-10, 1e-10), ("mixed", 1e-6 * np.abs(j_ref).max(), 1e-6 * np.abs(k_ref).max())):
+        jk = DfJK(bjk, layout="square", precision=prec)
+        dj = np.abs(jk.j(dt).cpu().numpy() - j_ref).max()
+        dk = np.abs(jk.k_from_occ(ct).cpu().numpy() - k_ref).max()
+        jk.close()
+        print(f"config 2 {prec}: max|dJ| {dj:.3e} (|J| {np.abs(j_ref).max():.3f}), "
+              f"max|dK| {dk:.3e} (|K| {np.abs(k_ref).max():.3f})")
+        assert dj <= jb and dk <= kb
