@@ -2,15 +2,17 @@
 
 One step = one RI-MP2 energy + adjoint (Gamma = dE/dB, dE/deps) on the
 synthetic RI-MP2 workload (naux 4800, nocc 120, nvir 1100) plus one DF-JK
-build (J and K) on the synthetic DF-JK workload (n 600, naux 2400, nocc 60).
+build (J and K of C_occ in one fc_dfjk_build_occ call: J's first pass read
+off K's stage-1 product) on the synthetic DF-JK workload (n 600, naux 2400,
+nocc 60); the FP64 plain step uses the same calls.
 The metric is algorithmic TFLOP/s of the step:
     F = 2 naux nvir^2 P + 2 naux nov^2   (energy + adjoint, P = nocc(nocc+1)/2)
       + 4 naux n(n+1)/2 + 4 naux n^2 nocc   (J two passes, K occupied path)
 
 ``value``  : device-resident inputs, CUDA events on the launching stream.
 ``e2e``    : the same step through the host-array C ABI (fc_rimp2_energy_grad,
-             fc_dfj_build, fc_dfk_build_occ) from pinned host buffers, copies
-             inside the timed region.
+             fc_dfjk_build_occ) from pinned host buffers, copies inside the
+             timed region.
 ``--impl reference`` and ``cpu_baseline`` time the C++ restatement of the
 reference's host algorithms (oracle/cpu_ref.cpp: OpenMP over work units,
 OpenBLAS at one thread per unit, on every physical host core) on a bounded
@@ -286,25 +288,40 @@ def alkane_shape(n):
     return 84 * n + 28, 4 * n + 1, 20 * n + 9
 
 
+ALKANES = os.path.join(ROOT, "tests", "golden", "_cache", "alkanes_c1_c8.npz")
+
+
 def batch_leg(torch, dev, nmol):
-    """Config 4: nmol alkanes C1..C8 (n ~ U{1..8}, seed 4), synthetic B of their
-    exact shapes (the config-3 distributions), one batched E+grad replay
-    timed; the diagonal-tile schedule of each size bucket autotuned; errors
-    against FP64 on one molecule of every size."""
+    """Config 4: nmol alkanes C1..C8 (n ~ U{1..8}, seed 4), one batched E+grad
+    replay timed; the diagonal-tile schedule of each size bucket autotuned;
+    errors against FP64 on one molecule of every size.  Inputs: B_ov and
+    orbital energies of the oracle's RHF for all-trans C_nH_2n+2 in cc-pVDZ /
+    cc-pVDZ-RI (tests/golden/make_alkanes.py), one device copy per molecule,
+    with the oracle's FP64 energies; synthetic B of the exact shapes (the
+    config-3 distributions) when that file is absent."""
     import numpy as np
     from ferric_b200 import rimp2
     from ferric_b200.batch import Rimp2Batch
     os.environ.setdefault("FERRIC_CUDA_AUTOTUNE", "1")
     ns = np.random.default_rng(4).integers(1, 9, nmol)
+    real = os.path.exists(ALKANES)
+    src = np.load(ALKANES) if real else None
     g = torch.Generator(device=dev)
     g.manual_seed(4)
     mols = []
     for n in ns:
         naux, nocc, nvir = alkane_shape(int(n))
-        b = torch.randn((naux, nocc * nvir), generator=g, device=dev, dtype=torch.float64)
-        b *= 0.02 * torch.exp(-torch.arange(naux, device=dev, dtype=torch.float64) / (3000.0 * naux / 4800.0))[:, None]
-        eo = torch.sort(torch.rand(nocc, generator=g, device=dev, dtype=torch.float64) * 19.7 - 20.0).values
-        ev = torch.sort(torch.rand(nvir, generator=g, device=dev, dtype=torch.float64) * 5.95 + 0.05).values
+        if real:
+            b = torch.from_numpy(src[f"c{n}_b_ov"]).to(dev)
+            eo = torch.from_numpy(src[f"c{n}_eps_occ"]).to(dev)
+            ev = torch.from_numpy(src[f"c{n}_eps_vir"]).to(dev)
+            assert tuple(b.shape) == (naux, nocc * nvir)
+        else:
+            b = torch.randn((naux, nocc * nvir), generator=g, device=dev, dtype=torch.float64)
+            b *= 0.02 * torch.exp(-torch.arange(naux, device=dev, dtype=torch.float64)
+                                  / (3000.0 * naux / 4800.0))[:, None]
+            eo = torch.sort(torch.rand(nocc, generator=g, device=dev, dtype=torch.float64) * 19.7 - 20.0).values
+            ev = torch.sort(torch.rand(nvir, generator=g, device=dev, dtype=torch.float64) * 5.95 + 0.05).values
         mols.append((b, eo, ev))
     t0 = time.time()
     bt = Rimp2Batch(mols, grad=True)
@@ -324,12 +341,17 @@ def batch_leg(torch, dev, nmol):
         seen.add(int(n))
         b, eo, ev = mols[m]
         sc, g64, _, _ = rimp2.rimp2_energy_grad(b, eo, ev, precision="f64")
-        errs.append({"n": int(n), "e_abs": float(e_os[m] + e_ss[m] - sc.e_total),
-                     "e_rel": float((e_os[m] + e_ss[m] - sc.e_total) / abs(sc.e_total)),
-                     "gamma_max_rel": float((bt.gamma[m] - g64).abs().max() / g64.abs().max())})
+        e = {"n": int(n), "e_mp2": sc.e_total, "e_abs": float(e_os[m] + e_ss[m] - sc.e_total),
+             "e_rel": float((e_os[m] + e_ss[m] - sc.e_total) / abs(sc.e_total)),
+             "gamma_max_rel": float((bt.gamma[m] - g64).abs().max() / g64.abs().max())}
+        if real:  # the FP64 device energy against the oracle's
+            e["f64_vs_oracle_abs"] = sc.e_total - float(src[f"c{n}_e_os"] + src[f"c{n}_e_ss"])
+        errs.append(e)
     t_ms = statistics.median(ms)
     out = {"molecules": int(nmol), "sizes": {str(k): int((ns == k).sum()) for k in range(1, 9)},
-           "data": "synthetic B of the alkane shapes (naux 84n+28, nocc 4n+1, nvir 20n+9), seeded",
+           "data": ("oracle RHF tensors of all-trans C_nH_2n+2 (cc-pVDZ / cc-pVDZ-RI), one copy per molecule"
+                    if real else "synthetic B of the alkane shapes (naux 84n+28, nocc 4n+1, nvir 20n+9), seeded; "
+                                 "the oracle's alkane tensors were not found"),
            "ms_e_grad": t_ms, "tflops": info["flops"] / (t_ms * 1e-3) / 1e12, "flops": info["flops"],
            "graph_launches": info["launches"], "pair_launches": info["pair_launches"], "groups": info["groups"],
            "create_s": create_s, "plan": bt.plan(), "error_vs_f64": errs}
@@ -405,8 +427,7 @@ def c5_leg(torch, dev, prec, steps=3):
             st = ({}, {}, {})
             sc, *_ = rimp2.rimp2_energy_grad(inp["b_ov"], inp["eo"], inp["ev"], precision=p, stats=st[0],
                                              out=(gamma, d_o, d_v))
-            j = jk.j(inp["d"], stats=st[1])
-            k = jk.k_from_occ(inp["c"], stats=st[2])
+            j, k = jk.jk_from_occ(inp["c"], stats=st[1])
             return sc, st, j, k
         one()
         ms = []
@@ -422,8 +443,8 @@ def c5_leg(torch, dev, prec, steps=3):
         r = st[0]
         res[p] = dict(sc=sc, gamma=gamma.clone(), j=j, k=k)
         out[p] = {"ms_per_step": t, "tflops": fl["total"] / (t * 1e-3) / 1e12,
-                  "components_ms": {"rimp2_e_grad": r["kernel_ms"], "dfj": st[1]["kernel_ms"],
-                                    "dfk": st[2]["kernel_ms"]},
+                  "components_ms": {"rimp2_e_grad": r["kernel_ms"], "dfjk": st[1]["kernel_ms"],
+                                    "dfk_stages": st[1]["main_ms"], "dfj_pass2": st[1]["aux_ms"]},
                   "pair_kernel_ms": r["main_ms"], "pair_launches": r["main_launches"],
                   "adjoint_ms": r["aux_ms"], "adjoint_launches": r["aux_launches"]}
         jk.close()
@@ -571,11 +592,9 @@ def main():
         st_r, st_j, st_k = {}, {}, {}
         sc, *_ = rimp2.rimp2_energy_grad(inp["b_ov"], inp["eo"], inp["ev"], precision=prec, stats=st_r,
                                          out=(gamma, d_o, d_v))
-        jk.set_precision(dfj_prec)
-        jk.j(inp["d"], out=jbuf, stats=st_j)
         jk.set_precision(dfk_prec)
-        jk.k_from_occ(inp["c"], out=kbuf, stats=st_k)
-        last.update(rimp2=st_r, dfj=st_j, dfk=st_k, energy=sc)
+        jk.jk_from_occ(inp["c"], out=(jbuf, kbuf), stats=st_j)
+        last.update(rimp2=st_r, dfjk=st_j, energy=sc)
 
     for _ in range(args.warmup):
         step()
@@ -593,7 +612,7 @@ def main():
         e0.record(stream)
         for _ in range(args.steps):
             step()
-            launches += sum(last[k]["launches"] for k in ("rimp2", "dfj", "dfk"))
+            launches += sum(last[k]["launches"] for k in ("rimp2", "dfjk"))
             main_ms += last["rimp2"]["main_ms"]
             main_flops += last["rimp2"]["main_flops"]
             main_launch += last["rimp2"]["main_launches"]
@@ -650,10 +669,16 @@ def main():
         rooflines[key] = r
     dom = max(rooflines, key=lambda x: kern[x]["ms"])
     roofline = dict(rooflines[dom], which=dom)
-    dfj = last["dfj"]
-    roof_dfj = {"bound": "hbm", "achieved": dfj["main_bytes"] / (dfj["main_ms"] * 1e-3) / 1e9,
-                "peak": peaks["hbm_gbs"], "unit": "GB/s"}
+    # DF-JK: J's second pass (GEMV over the packed rows) and K's stages
+    # (stage 1 reads the B slices once), both HBM rooflines
+    djk = last["dfjk"]
+    roof_dfj = {"bound": "hbm", "kernel": "DF-J second pass", "ms": djk["aux_ms"],
+                "achieved": djk["aux_bytes"] / (djk["aux_ms"] * 1e-3) / 1e9, "peak": peaks["hbm_gbs"], "unit": "GB/s"}
     roof_dfj["frac"] = roof_dfj["achieved"] / roof_dfj["peak"]
+    roof_dfk = {"bound": "hbm", "kernel": "DF-K stages (stage 1 reads B once)", "ms": djk["main_ms"],
+                "achieved": djk["main_bytes"] / (djk["main_ms"] * 1e-3) / 1e9, "peak": peaks["hbm_gbs"],
+                "unit": "GB/s"}
+    roof_dfk["frac"] = roof_dfk["achieved"] / roof_dfk["peak"]
 
     # ---- one FP64-plain step on the same inputs (the "mixed vs FP64 plain" ratio)
     plain = None
@@ -664,18 +689,17 @@ def main():
         p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         p0.record(stream)
         sc64, g64, _, _ = rimp2.rimp2_energy_grad(inp["b_ov"], inp["eo"], inp["ev"], precision="f64", stats=sp_r)
-        j64 = jk64.j(inp["d"], stats=sp_j)
-        k64 = jk64.k_from_occ(inp["c"], stats=sp_k)
+        j64, k64 = jk64.jk_from_occ(inp["c"], stats=sp_j)
         p1.record(stream)
         torch.cuda.synchronize()
         pms = p0.elapsed_time(p1)
-        cm = {"rimp2_e_grad": last["rimp2"]["kernel_ms"], "dfjk": last["dfj"]["kernel_ms"] + last["dfk"]["kernel_ms"]}
+        cm = {"rimp2_e_grad": last["rimp2"]["kernel_ms"], "dfjk": last["dfjk"]["kernel_ms"]}
         plain = {"ms_per_step": pms, "value": flops["total"] / (pms * 1e-3) / 1e12, "unit": "TFLOP/s",
                  "speedup_mixed_vs_plain": pms / ms_step,
                  "speedup_rimp2_e_grad": sp_r["kernel_ms"] / cm["rimp2_e_grad"],
-                 "speedup_dfjk": (sp_j["kernel_ms"] + sp_k["kernel_ms"]) / cm["dfjk"],
-                 "components_ms": {"rimp2_e_grad": sp_r["kernel_ms"], "dfj": sp_j["kernel_ms"],
-                                   "dfk": sp_k["kernel_ms"]},
+                 "speedup_dfjk": sp_j["kernel_ms"] / cm["dfjk"],
+                 "components_ms": {"rimp2_e_grad": sp_r["kernel_ms"], "dfjk": sp_j["kernel_ms"],
+                                   "dfk_stages": sp_j["main_ms"], "dfj_pass2": sp_j["aux_ms"]},
                  "mixed_error": {"e_total_abs": (sc.e_os + sc.e_ss) - sc64.e_total,
                                  "e_total_rel": ((sc.e_os + sc.e_ss) - sc64.e_total) / abs(sc64.e_total),
                                  "gamma_max_rel": float((gamma - g64).abs().max() / g64.abs().max()),
@@ -708,12 +732,10 @@ def main():
             check(_lib.lib.fc_rimp2_energy_grad(ptr(hb), naux, nocc, nvir, ptr(heo), ptr(hev), pr,
                                                 ctypes.byref(eo_), ctypes.byref(es_), ptr(hg), ptr(ddo),
                                                 ptr(ddv), ctypes.byref(s)))
-            s2, s3 = FcStats(), FcStats()
-            jk.set_precision(dfj_prec)
-            check(_lib.lib.fc_dfj_build(jk._h, ptr(hd), ptr(hj), ctypes.byref(s2)))
+            s2 = FcStats()
             jk.set_precision(dfk_prec)
-            check(_lib.lib.fc_dfk_build_occ(jk._h, ptr(hc), DFJK["nocc"], ptr(hk), ctypes.byref(s3)))
-            return s.h2d_bytes + s2.h2d_bytes + s3.h2d_bytes, s.d2h_bytes + s2.d2h_bytes + s3.d2h_bytes
+            check(_lib.lib.fc_dfjk_build_occ(jk._h, ptr(hc), DFJK["nocc"], ptr(hj), ptr(hk), ctypes.byref(s2)))
+            return s.h2d_bytes + s2.h2d_bytes, s.d2h_bytes + s2.d2h_bytes
 
         e2e_step()
         torch.cuda.synchronize()
@@ -768,10 +790,10 @@ def main():
                                 "10 products; adjoint: 3 slices, 6 products)")}[prec],
             "precision": prec, "dfj_precision": dfj_prec, "dfk_precision": dfk_prec,
             "data": "synthetic (seeded, generated on device)", "config": config,
-            "components_ms": {"rimp2_e_grad": last["rimp2"]["kernel_ms"], "dfj": last["dfj"]["kernel_ms"],
-                              "dfk": last["dfk"]["kernel_ms"]},
+            "components_ms": {"rimp2_e_grad": last["rimp2"]["kernel_ms"], "dfjk": last["dfjk"]["kernel_ms"],
+                              "dfk_stages": last["dfjk"]["main_ms"], "dfj_pass2": last["dfjk"]["aux_ms"]},
             "flops": flops, "energy": {"e_os": sc.e_os, "e_ss": sc.e_ss},
-            "roofline": roofline, "roofline_kernels": rooflines, "roofline_dfj": roof_dfj,
+            "roofline": roofline, "roofline_kernels": rooflines, "roofline_dfj": roof_dfj, "roofline_dfk": roof_dfk,
             "plain_f64": plain,
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
             "config4_batch": batch, "config5": c5, "mo_dressing": dress,

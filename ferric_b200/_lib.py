@@ -50,6 +50,8 @@ SIGNATURES = {
     "fc_dfj_build_dev": (_I32, [_P, _P, _P, _P, _P]),
     "fc_dfk_build_occ": (_I32, [_P, _P, _I64, _P, _P]),
     "fc_dfk_build_occ_dev": (_I32, [_P, _P, _I64, _P, _P, _P]),
+    "fc_dfjk_build_occ": (_I32, [_P, _P, _I64, _P, _P, _P]),
+    "fc_dfjk_build_occ_dev": (_I32, [_P, _P, _I64, _P, _P, _P, _P]),
     "fc_dfjk_set_precision": (_I32, [_P, _I32]),
     "fc_dfjk_destroy": (_I32, [_P]),
     "fc_rimp2_energy_noalloc": (_I32, [_P, _I64, _I64, _I64, _P, _P, _I32, _D, _DP, _DP, _P]),

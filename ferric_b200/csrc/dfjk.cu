@@ -344,6 +344,30 @@ static fc_status dfjk_smem_once() {
     return FC_OK;
 }
 
+// c = V^-1 d in place (when a metric is set), pass 2 J_k = sum_P Bp[P, k] c_P
+// in nsplit row splits (part: nsplit x ld doubles), fixed-order fold and unpack.
+template <typename TB>
+static fc_status dfj_solve_pass2(fc_dfjk* h, const TB* bp, double* dp, double* part, int nsplit, double* j,
+                                 cudaStream_t st) {
+    const int64_t naux = h->naux, n = h->n, pair = h->pair;
+    constexpr bool F32 = sizeof(TB) == 4;
+    const int64_t ld = F32 ? h->ld32 : pair;
+    if (h->l_chol) chol_solve_kernel<<<1, 1024, 0, st>>>(h->l_chol, naux, dp);
+    const int64_t rps = (naux + nsplit - 1) / nsplit;
+    if constexpr (F32) {
+        dim3 g2((unsigned)((ld / 4 + 255) / 256), nsplit);
+        if (h->pk32_subnormal)
+            dfj_pass2_f32v_kernel<true><<<g2, 256, 0, st>>>((const float*)bp, naux, ld, dp, rps, part);
+        else
+            dfj_pass2_f32v_kernel<false><<<g2, 256, 0, st>>>((const float*)bp, naux, ld, dp, rps, part);
+    } else {
+        dim3 g2((unsigned)((pair + 255) / 256), nsplit);
+        dfj_pass2_kernel<TB><<<g2, 256, 0, st>>>(bp, naux, pair, dp, rps, part);
+    }
+    dfj_unpack_kernel<<<(unsigned)((n * n + 255) / 256), 256, 0, st>>>(part, nsplit, ld, n, j);
+    return check_launch("DF-J pass 2");
+}
+
 template <typename TB>
 static fc_status dfj_build_t(fc_dfjk* h, const TB* bp, int prec, const double* d, double* j, cudaStream_t st,
                              fc_stats* stats) {
@@ -373,19 +397,7 @@ static fc_status dfj_build_t(fc_dfjk* h, const TB* bp, int prec, const double* d
         dfj_pass1_kernel<TB><<<dim3((unsigned)naux, (unsigned)nseg), 256, 0, st>>>(bp, pair, seg, w, segp);
     }
     dfj_seg_sum_kernel<<<(unsigned)((naux + 255) / 256), 256, 0, st>>>(segp, (int)nseg, naux, dp);
-    if (h->l_chol) chol_solve_kernel<<<1, 1024, 0, st>>>(h->l_chol, naux, dp);
-    const int64_t rps = (naux + nsplit - 1) / nsplit;
-    if constexpr (F32) {
-        dim3 g2((unsigned)((ld / 4 + 255) / 256), nsplit);
-        if (h->pk32_subnormal)
-            dfj_pass2_f32v_kernel<true><<<g2, 256, 0, st>>>((const float*)bp, naux, ld, dp, rps, (double*)vpart);
-        else
-            dfj_pass2_f32v_kernel<false><<<g2, 256, 0, st>>>((const float*)bp, naux, ld, dp, rps, (double*)vpart);
-    } else {
-        dim3 g2((unsigned)((pair + 255) / 256), nsplit);
-        dfj_pass2_kernel<TB><<<g2, 256, 0, st>>>(bp, naux, pair, dp, rps, (double*)vpart);
-    }
-    dfj_unpack_kernel<<<(unsigned)((n * n + 255) / 256), 256, 0, st>>>((const double*)vpart, nsplit, ld, n, j);
+    FC_TRY(dfj_solve_pass2<TB>(h, bp, dp, (double*)vpart, nsplit, j, st));
     FC_TRY(check_launch("DF-J kernels"));
     if (stats) {
         FC_CUDA(cudaEventRecord(c.ev1, st));
@@ -445,7 +457,7 @@ void dfjk_free_mixed(fc_dfjk* h) {
 }
 
 fc_status dfk_build_f64(fc_dfjk* h, const double* c_occ, int64_t nocc, double* k, cudaStream_t st,
-                        fc_stats* stats) {
+                        fc_stats* stats, double* d_out) {
     FC_TRY(dfjk_smem_once());
     const int64_t naux = h->naux, n = h->n;
     const int64_t M1 = naux * n;
@@ -476,6 +488,9 @@ fc_status dfk_build_f64(fc_dfjk* h, const double* c_occ, int64_t nocc, double* k
         dgemm_tn_kernel<EpiScatterW><<<g, 256, DG_SMEM, st>>>(h->b_sq, n, (const double*)vct, n, (int)M1,
                                                                (int)nocc, n, n, 0, epi);
     }
+    if (d_out)  // the J pass-1 vector from W = B C
+        dfj_d_from_w_kernel<double><<<(unsigned)naux, 256, 0, st>>>((const double*)vw, kdim, nocc, n, nocc, c_occ,
+                                                                    d_out);
     {
         dim3 g(tn, tm, nsplit);
         EpiSplit epi{(double*)vpart, n * n, (int)n};
@@ -499,6 +514,48 @@ fc_status dfk_build_f64(fc_dfjk* h, const double* c_occ, int64_t nocc, double* k
         stats->main_bytes = 8.0 * (double)naux * (double)n * (double)n;
         stats->tile_m = DG_BM;
         stats->tile_n = DG_BN;
+    }
+    return FC_OK;
+}
+
+// J and K of one occupied-orbital matrix: K as dfk_build_*, J = J(C C^T) from
+// the pass-1 vector d_P = <B_P, C C^T> that the K stage's W = B C already
+// holds (one kernel over W instead of a pass over B), then the metric solve
+// and J's second pass over the packed rows (FP64, or the FP32 copy in mixed).
+static fc_status dfjk_build_occ(fc_dfjk* h, const double* c_occ, int64_t nocc, double* j, double* k,
+                                cudaStream_t st, fc_stats* stats) {
+    const bool mixed = h->active != FC_PREC_F64;
+    const int nsplit = 4;
+    const int64_t ld = mixed ? h->ld32 : h->pair;
+    void* vd;
+    FC_TRY(ws_get(WS_JD, (size_t)(h->naux + 64 + (int64_t)nsplit * ld) * 8, &vd));
+    double* dp = (double*)vd;
+    double* part = dp + h->naux + 64;
+    Context& c = ctx();
+    fc_stats sk{};
+    if (mixed) FC_TRY(dfk_build_mixed(h, c_occ, nocc, k, st, stats ? &sk : nullptr, dp));
+    else FC_TRY(dfk_build_f64(h, c_occ, nocc, k, st, stats ? &sk : nullptr, dp));
+    cudaEvent_t* ev = nullptr;
+    if (stats) {
+        FC_TRY(timing_events2(1, &ev));
+        FC_CUDA(cudaEventRecord(ev[0], st));
+    }
+    if (mixed) FC_TRY(dfj_solve_pass2<float>(h, h->pk32, dp, part, nsplit, j, st));
+    else FC_TRY(dfj_solve_pass2<double>(h, h->b_pk, dp, part, nsplit, j, st));
+    if (stats) {
+        FC_CUDA(cudaEventRecord(ev[1], st));
+        FC_CUDA(cudaEventSynchronize(ev[1]));
+        float jms = 0.f;
+        FC_CUDA(cudaEventElapsedTime(&jms, ev[0], ev[1]));
+        *stats = sk;
+        stats->kernel_ms = sk.kernel_ms + jms;
+        stats->flops = sk.flops + 2.0 * (double)h->naux * (double)h->pair;  // + J pass 2
+        stats->launches = sk.launches + 3 + (h->l_chol ? 1 : 0);
+        stats->aux_launches = 1;
+        stats->aux_ms = jms;
+        stats->aux_flops = 2.0 * (double)h->naux * (double)h->pair;
+        stats->aux_bytes = (mixed ? 4.0 : 8.0) * (double)h->naux * (double)h->pair;
+        (void)c;
     }
     return FC_OK;
 }
@@ -678,6 +735,53 @@ fc_status fc_dfk_build_occ(fc_dfjk* h, const double* c_occ, int64_t nocc, double
     if (stats) {
         stats->h2d_bytes += nc;
         stats->d2h_bytes += nn;
+    }
+    return FC_OK;
+}
+
+fc_status fc_dfjk_build_occ_dev(fc_dfjk* h, const double* c_occ, int64_t nocc, double* j, double* k, void* stream,
+                               fc_stats* stats) {
+    if (!h || !j || !k || (nocc > 0 && !c_occ)) return fail(FC_ERR_INVALID, "fc_dfjk_build_occ: null argument");
+    if (nocc < 0) return fail(FC_ERR_LAYOUT, "fc_dfjk_build_occ: nocc < 0");
+    if (!h->b_sq) return fail(FC_ERR_LAYOUT, "fc_dfjk_build_occ: needs an FC_LAYOUT_SQUARE handle");
+    FC_TRY(require_init());
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (stats) *stats = fc_stats{};
+    cudaStream_t st = pick_stream(stream);
+    if (nocc == 0) {  // empty channel: D = 0, J = K = 0
+        FC_CUDA(cudaMemsetAsync(j, 0, h->n * h->n * 8, st));
+        FC_CUDA(cudaMemsetAsync(k, 0, h->n * h->n * 8, st));
+        return FC_OK;
+    }
+    return dfjk_build_occ(h, c_occ, nocc, j, k, st, stats);
+}
+
+fc_status fc_dfjk_build_occ(fc_dfjk* h, const double* c_occ, int64_t nocc, double* j, double* k, fc_stats* stats) {
+    if (!h || !j || !k || (nocc > 0 && !c_occ)) return fail(FC_ERR_INVALID, "fc_dfjk_build_occ: null argument");
+    if (nocc < 0) return fail(FC_ERR_LAYOUT, "fc_dfjk_build_occ: nocc < 0");
+    if (!h->b_sq) return fail(FC_ERR_LAYOUT, "fc_dfjk_build_occ: needs an FC_LAYOUT_SQUARE handle");
+    FC_TRY(require_init());
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (stats) *stats = fc_stats{};
+    const size_t nn = (size_t)h->n * h->n * 8, nc = (size_t)h->n * nocc * 8;
+    if (nocc == 0) {
+        for (size_t q = 0; q < (size_t)h->n * h->n; ++q) j[q] = k[q] = 0.0;
+        return FC_OK;
+    }
+    cudaStream_t st = ctx().stream;
+    void* buf;
+    FC_TRY(ws_get(WS_B, 2 * nn + nc, &buf));
+    double* dj = (double*)buf;
+    double* dk = dj + h->n * h->n;
+    double* dc = dk + h->n * h->n;
+    FC_CUDA(cudaMemcpyAsync(dc, c_occ, nc, cudaMemcpyHostToDevice, st));
+    FC_TRY(dfjk_build_occ(h, dc, nocc, dj, dk, st, stats));
+    FC_CUDA(cudaMemcpyAsync(j, dj, nn, cudaMemcpyDeviceToHost, st));
+    FC_CUDA(cudaMemcpyAsync(k, dk, nn, cudaMemcpyDeviceToHost, st));
+    FC_CUDA(cudaStreamSynchronize(st));
+    if (stats) {
+        stats->h2d_bytes += nc;
+        stats->d2h_bytes += 2 * nn;
     }
     return FC_OK;
 }

@@ -1,14 +1,16 @@
-// Split-BF16 DF-K (FC_PREC_MIXED) on the exact-slice tcgen05 GEMM.
+// Exact-slice DF-K (FC_PREC_MIXED) on the tcgen05 GEMM.
 //
 // K = sum_Q (B_Q C)(B_Q C)^T for C = C_occ (n x nocc), no occupation factor
 // (KBuilder::build_from_occ, ferric-scf/src/fock.rs:22-52; the occupied
 // path of ferric-scf/src/df_k.rs:1409-1520, 1575-1660):
-//   once per handle  B rows (Q, mu) split into three bf16 integer slices at a
-//                    power-of-two scale per row (fx_split.cuh)
+//   once per handle  B rows (Q, mu) split into three int8 integer slices at a
+//                    power-of-two scale per row (fx_split.cuh): 3 bytes per
+//                    element, the bytes of the HBM-bound stage 1
 //   per build        C^T rows (one per occupied orbital) split the same way
-//   stage 1          W[mu, (Q, i)] = sum_nu B[Q, mu, nu] C[nu, i]: exact-slice
-//                    GEMM, 128 x 64 tiles over the naux*n rows of B (each B
-//                    slice read once: the stage is HBM-bound), FP32 W
+//   stage 1          W[mu, (Q, i)] = sum_nu B[Q, mu, nu] C[nu, i]: int8
+//                    exact-slice GEMM (kind::i8, exact int32 levels),
+//                    128 x 64 tiles over the naux*n rows of B (each B slice
+//                    read once), FP32 W
 //   split            rows mu of W, three slices at a scale per row
 //   stage 2          K = W W^T: upper 128 x 128 tiles, split over (Q, i) into
 //                    about one item per SM, k-panel flush into FP64 registers
@@ -31,17 +33,17 @@ namespace {
 
 int64_t rup(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
-// Row r = (Q, mu) of the square tensor -> slices [3][rows][ldk], scale s[r].
+// Row r = (Q, mu) of the square tensor -> int8 slices [3][rows][ldk], scale s[r].
 __global__ void __launch_bounds__(256) dfk_split_b_kernel(const double* __restrict__ b, int64_t n, int64_t ldk,
                                                           int64_t rows, double* __restrict__ s,
-                                                          __nv_bfloat16* __restrict__ bs) {
-    split_fx_qrows_body(b, 1, n, ldk, ldk, rows, s, bs, blockIdx.x);
+                                                          int8_t* __restrict__ bs) {
+    split_fx_qrows_body<SliceI8>(b, 1, n, ldk, ldk, rows, s, bs, blockIdx.x);
 }
 
-// Column i of C (n x nocc) -> row i of the C^T slices [3][npad][ldk], scale sc[i].
+// Column i of C (n x nocc) -> row i of the int8 C^T slices [3][npad][ldk], scale sc[i].
 __global__ void __launch_bounds__(256) dfk_split_c_kernel(const double* __restrict__ c, int64_t n, int64_t nocc,
                                                           int64_t ldk, int64_t npad, double* __restrict__ sc,
-                                                          __nv_bfloat16* __restrict__ cs, int* bad) {
+                                                          int8_t* __restrict__ cs, int* bad) {
     __shared__ double red[32];
     const int64_t i = blockIdx.x;
     double m = 0.0;
@@ -61,13 +63,13 @@ __global__ void __launch_bounds__(256) dfk_split_c_kernel(const double* __restri
         if (threadIdx.x == 0) red[0] = t;
     }
     __syncthreads();
-    const double s = pow2_scale(red[0]);
+    const double s = SliceI8::scale(red[0]);
     if (threadIdx.x == 0) sc[i] = s;
     const double inv = 1.0 / s;
     const int64_t ss = npad * ldk;
     for (int64_t nu = threadIdx.x; nu < n; nu += 256) {
-        __nv_bfloat16 c1, c2, c3;
-        fx_slices(c[nu * nocc + i], inv, c1, c2, c3);
+        int8_t c1, c2, c3;
+        fx_slices<SliceI8>(c[nu * nocc + i], inv, c1, c2, c3);
         cs[i * ldk + nu] = c1;
         cs[ss + i * ldk + nu] = c2;
         cs[2 * ss + i * ldk + nu] = c3;
@@ -147,8 +149,8 @@ bool g_attr_done = false;
 
 fc_status xg_attrs() {
     if (g_attr_done) return FC_OK;
-    FC_CUDA(cudaFuncSetAttribute(xgemm_kernel<64, EpiW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 xg::Cfg<64>::SMEM));
+    FC_CUDA(cudaFuncSetAttribute(xgemm_kernel<64, EpiW, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 xg::Cfg<64, true>::SMEM));
     FC_CUDA(cudaFuncSetAttribute(xgemm_kernel<128, EpiPart>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  xg::Cfg<128>::SMEM));
     g_attr_done = true;
@@ -159,8 +161,8 @@ fc_status xg_attrs() {
 
 // Split of the square tensor for the tensor-core stages (mixed square handles).
 fc_status dfk_prepare_split(fc_dfjk* h, cudaStream_t st) {
-    const int64_t rows = h->naux * h->n, ldk = rup(h->n, 8);
-    const size_t sbytes = (size_t)3 * rows * ldk * 2, scl = (size_t)rows * 8;
+    const int64_t rows = h->naux * h->n, ldk = rup(h->n, 16);  // 16-byte int8 rows for TMA
+    const size_t sbytes = (size_t)3 * rows * ldk, scl = (size_t)rows * 8;
     const size_t bytes = rup((int64_t)sbytes, 256) + scl;
     FC_TRY(pool_reserve(bytes));
     FC_CUDA(cudaMalloc(&h->sq_split, bytes));
@@ -169,24 +171,24 @@ fc_status dfk_prepare_split(fc_dfjk* h, cudaStream_t st) {
     if (ldk != h->n) FC_CUDA(cudaMemsetAsync(h->sq_split, 0, sbytes, st));
     if (rows > INT32_MAX) return fail(FC_ERR_LAYOUT, "DF-K: naux*n too large");
     dfk_split_b_kernel<<<(unsigned)rows, 256, 0, st>>>(h->b_sq, h->n, ldk, rows, h->sq_scale,
-                                                       (__nv_bfloat16*)h->sq_split);
+                                                       (int8_t*)h->sq_split);
     return check_launch("dfk_split_b_kernel");
 }
 
 fc_status dfk_build_mixed(fc_dfjk* h, const double* c_occ, int64_t nocc, double* kout, cudaStream_t st,
-                          fc_stats* stats) {
+                          fc_stats* stats, double* d_out) {
     if (!h->sq_split)
         return fail(FC_ERR_KERNEL, "DF-K: handle has no split-BF16 copy (created with FC_PREC_F64)");
     FC_TRY(xg_attrs());
     Context& cx = ctx();
-    const int64_t n = h->n, naux = h->naux, ldk = rup(n, 8);
+    const int64_t n = h->n, naux = h->naux, ldk = rup(n, 16);
     const int64_t rows = naux * n;
     const int64_t nocc_p = rup(nocc, 8), npad = rup(nocc, 64), ldw = naux * nocc_p, mp = rup(n, 128);
     if (rows > INT32_MAX || 3 * rows > (int64_t)UINT32_MAX || mp > 65536 || ldw > INT32_MAX)
         return fail(FC_ERR_LAYOUT, "DF-K mixed: shape too large");
     // stage-1 and stage-2 work items
     std::vector<int4> items;
-    const int ntm1 = (int)((rows + 127) / 128), ntn1 = (int)(npad / 64), nks1 = (int)((n + 63) / 64);
+    const int ntm1 = (int)((rows + 127) / 128), ntn1 = (int)(npad / 64), nks1 = (int)((n + 127) / 128);
     for (int tm = 0; tm < ntm1; ++tm)
         for (int tn = 0; tn < ntn1; ++tn) items.push_back(make_int4(tm, tn, 0, nks1));
     const int64_t n1 = (int64_t)items.size();
@@ -209,7 +211,7 @@ fc_status dfk_build_mixed(fc_dfjk* h, const double* c_occ, int64_t nocc, double*
     const int64_t n2 = (int64_t)items.size() - n1;
 
     void *vc, *vout, *vw, *vws, *vsw, *vpart, *vtab;
-    const size_t cs_bytes = (size_t)3 * npad * ldk * 2;
+    const size_t cs_bytes = (size_t)3 * npad * ldk;
     FC_TRY(ws_get(WS_MISC, rup((int64_t)cs_bytes, 256) + npad * 8, &vc));
     FC_TRY(ws_get(WS_OUT, 256, &vout));
     FC_TRY(ws_get(WS_T, (size_t)n * ldw * 4, &vw));
@@ -226,12 +228,12 @@ fc_status dfk_build_mixed(fc_dfjk* h, const double* c_occ, int64_t nocc, double*
     FC_CUDA(cudaMemsetAsync(vc, 0, cs_bytes, st));
 
     CUtensorMap tb, tcm, tw;
-    FC_TRY(make_tmap_bf16_2d(&tb, h->sq_split, n, 3 * rows, ldk * 2, 64, 128));
-    FC_TRY(make_tmap_bf16_2d(&tcm, vc, n, 3 * npad, ldk * 2, 64, 64));
+    FC_TRY(make_tmap_i8_2d(&tb, h->sq_split, n, 3 * rows, ldk, 128, 128));
+    FC_TRY(make_tmap_i8_2d(&tcm, vc, n, 3 * npad, ldk, 128, 64));
     FC_TRY(make_tmap_bf16_2d(&tw, vws, ldw, 3 * mp, ldw * 2, 64, 128));
 
     if (stats) FC_CUDA(cudaEventRecord(cx.ev0, st));
-    dfk_split_c_kernel<<<(unsigned)nocc, 256, 0, st>>>(c_occ, n, nocc, ldk, npad, sc, (__nv_bfloat16*)vc, flags);
+    dfk_split_c_kernel<<<(unsigned)nocc, 256, 0, st>>>(c_occ, n, nocc, ldk, npad, sc, (int8_t*)vc, flags);
     cudaEvent_t* ev = nullptr;
     if (stats) {
         FC_TRY(timing_events(2, &ev));
@@ -241,9 +243,13 @@ fc_status dfk_build_mixed(fc_dfjk* h, const double* c_occ, int64_t nocc, double*
         XArgs a{(const int4*)vtab, n1, (int)rows, (int)npad, flags + 1};
         EpiW epi{h->sq_scale, sc, (float*)vw, ldw, rows, (int)n, (int)nocc, (int)nocc_p};
         const int grid = (int)std::min<int64_t>(n1, cx.sm_count);
-        xgemm_kernel<64, EpiW><<<grid, xg::Cfg<64>::THREADS, xg::Cfg<64>::SMEM, st>>>(tb, tcm, a, epi);
+        xgemm_kernel<64, EpiW, true><<<grid, xg::Cfg<64, true>::THREADS, xg::Cfg<64, true>::SMEM, st>>>(tb, tcm, a,
+                                                                                                         epi);
     }
     if (stats) FC_CUDA(cudaEventRecord(ev[1], st));
+    if (d_out)  // the J pass-1 vector from the FP32 W (each element rounded once)
+        dfj_d_from_w_kernel<float><<<(unsigned)naux, 256, 0, st>>>((const float*)vw, ldw, nocc_p, n, nocc, c_occ,
+                                                                   d_out);
     dfk_split_w_kernel<<<(unsigned)n, 256, 0, st>>>((const float*)vw, ldw, mp, (double*)vsw, (__nv_bfloat16*)vws);
     if (stats) FC_CUDA(cudaEventRecord(ev[2], st));
     {
@@ -277,7 +283,7 @@ fc_status dfk_build_mixed(fc_dfjk* h, const double* c_occ, int64_t nocc, double*
         stats->main_launches = 2;
         stats->main_ms = (double)m1 + (double)m2;
         stats->main_flops = stats->flops;
-        stats->main_bytes = 6.0 * (double)rows * (double)n;  // the B slices, read once
+        stats->main_bytes = 3.0 * (double)rows * (double)n;  // the int8 B slices, read once
         stats->h2d_bytes += items.size() * sizeof(int4) + tix.size() * sizeof(int);
         stats->d2h_bytes += sizeof(hf);
     }

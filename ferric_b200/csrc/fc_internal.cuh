@@ -74,6 +74,7 @@ enum WsSlot {
     WS_SCALE,      // column maxima + operand-row scales
     WS_MISC,       // DF-J weights / d_P, DF-K C^T
     WS_PSCR,       // pair kernel: FP64 X / Y tiles of each CTA
+    WS_JD,         // fused DF-JK: d_P and J's pass-2 partials
     WS_COUNT
 };
 

@@ -1,7 +1,10 @@
 // Generic exact-slice GEMM on tcgen05 with a k-panel flush:
 //     C[m, n] = sum_k A[m, k] B[n, k]
-// for A, B given as three bf16 integer slices each (the exact split of
-// fx_split.cuh; row scales are applied by the epilogue functor).
+// for A, B given as three integer slices each (the exact split of
+// fx_split.cuh; row scales are applied by the epilogue functor): bf16 slices
+// (weights 1/256, tcgen05.mma kind::f16, FP32 accumulators) or, with I8,
+// int8 slices (weights 1/254, kind::i8, int32 accumulators).  A k-step is
+// 128 bytes of each operand row either way (64 bf16 or 128 int8 elements).
 //
 // Each work item is (m-tile of 128 rows, n-tile of BN rows, first k-step,
 // k-steps); a persistent CTA takes items round-robin.  The MMA warp
@@ -13,7 +16,9 @@
 //     acc += L0 + L1 / 256 + L2 / 65536     (exact in FP64),
 // so the result is exact up to the slicing itself for any K -- the
 // k-panelled FP64 flush of the reference's mixed GEMM
-// (ferric-core/src/gpu/mixed.rs:122-192), here inside one kernel.
+// (ferric-core/src/gpu/mixed.rs:122-192), here inside one kernel.  The
+// int8 form's panels (1024 of K) are far inside its int32 range
+// (3 * 127^2 * 1024 < 2^26) and combine as L0 + L1 / 254 + L2 / 254^2.
 //
 // Roles: warp 0 TMA producer, warp 1 UMMA issuer, warps 2 .. 2 + BN/8 - 1
 // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (its rows) and
@@ -32,6 +37,7 @@ namespace xg {
 
 constexpr int BM = 128, KT = 64, KP = 8;
 constexpr double L1W = 1.0 / 256.0, L2W = 1.0 / 65536.0;
+constexpr double I8L1W = 1.0 / 254.0, I8L2W = 1.0 / (254.0 * 254.0);
 
 // products: (A slice, B slice, level)
 static __constant__ int8_t kPA[6] = {0, 0, 1, 0, 1, 2};
@@ -39,9 +45,10 @@ static __constant__ int8_t kPB[6] = {0, 1, 0, 2, 1, 0};
 static __constant__ int8_t kPL[6] = {0, 1, 1, 2, 2, 2};
 static __constant__ int8_t kPFirst[6] = {1, 1, 0, 1, 0, 0};
 
-template <int BN>
+template <int BN, bool I8 = false>
 struct Cfg {
     static_assert(BN == 64 || BN == 128, "BN is 64 or 128");
+    static constexpr int KTE = I8 ? 2 * KT : KT;   // elements of K per k-step (128 bytes)
     static constexpr int A_BYTES = BM * KT * 2;
     static constexpr int B_BYTES = BN * KT * 2;
     static constexpr int STAGE = 3 * (A_BYTES + B_BYTES);
@@ -51,7 +58,7 @@ struct Cfg {
     static constexpr int NSET = BN == 64 ? 2 : 1;  // TMEM accumulator sets
     static constexpr int TCOLS = NSET * 3 * BN <= 256 ? 256 : 512;
     static constexpr int SMEM = STAGES * STAGE + 1024 + 256;
-    static constexpr uint32_t IDESC = tc::idesc_bf16_f32(128, BN);
+    static constexpr uint32_t IDESC = I8 ? tc::idesc_i8_s32(128, BN) : tc::idesc_bf16_f32(128, BN);
 };
 
 }  // namespace xg
@@ -65,11 +72,11 @@ struct XArgs {
 
 // Epi: __device__ void operator()(int64_t item, int4 it, int row, int col0,
 //                                 const double (&acc)[32]) const
-template <int BN, class Epi>
-__global__ void __launch_bounds__(xg::Cfg<BN>::THREADS, 1)
+template <int BN, class Epi, bool I8 = false>
+__global__ void __launch_bounds__(xg::Cfg<BN, I8>::THREADS, 1)
     xgemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const XArgs p,
                  const Epi epi) {
-    using C = xg::Cfg<BN>;
+    using C = xg::Cfg<BN, I8>;
     using namespace xg;
     constexpr int S = C::STAGES, NS = C::NSET;
     extern __shared__ uint8_t smem_raw[];
@@ -126,9 +133,9 @@ __global__ void __launch_bounds__(xg::Cfg<BN>::THREADS, 1)
                     tc::mbar_arrive_expect_tx(&full[s], C::STAGE);
 #pragma unroll
                     for (int sl = 0; sl < 3; ++sl) {
-                        tc::tma_load_2d(base + (sa(s, sl) - base_u32), &tmA, &full[s], kt * KT,
+                        tc::tma_load_2d(base + (sa(s, sl) - base_u32), &tmA, &full[s], kt * C::KTE,
                                         sl * p.Ma + it.x * BM);
-                        tc::tma_load_2d(base + (sb(s, sl) - base_u32), &tmB, &full[s], kt * KT,
+                        tc::tma_load_2d(base + (sb(s, sl) - base_u32), &tmB, &full[s], kt * C::KTE,
                                         sl * p.Nb + it.y * BN);
                     }
                 }
@@ -162,9 +169,15 @@ __global__ void __launch_bounds__(xg::Cfg<BN>::THREADS, 1)
                             const uint32_t a0 = sa(s, kPA[pr]), b0 = sb(s, kPB[pr]);
                             const uint32_t dcol = dset + kPL[pr] * BN;
 #pragma unroll
-                            for (int kk = 0; kk < KT / 16; ++kk)
-                                tc::umma_bf16(dcol, tc::sdesc_k128(a0 + kk * 32), tc::sdesc_k128(b0 + kk * 32),
-                                              C::IDESC, (kq > k0 || kk > 0 || !kPFirst[pr]) ? 1u : 0u);
+                            for (int kk = 0; kk < 4; ++kk) {  // 32 bytes of K per MMA
+                                const uint32_t acc = (kq > k0 || kk > 0 || !kPFirst[pr]) ? 1u : 0u;
+                                if constexpr (I8)
+                                    tc::umma_i8(dcol, tc::sdesc_k128(a0 + kk * 32), tc::sdesc_k128(b0 + kk * 32),
+                                                C::IDESC, acc);
+                                else
+                                    tc::umma_bf16(dcol, tc::sdesc_k128(a0 + kk * 32), tc::sdesc_k128(b0 + kk * 32),
+                                                  C::IDESC, acc);
+                            }
                         }
                         tc::umma_commit(&empty[s]);
                     }
@@ -206,8 +219,13 @@ __global__ void __launch_bounds__(xg::Cfg<BN>::THREADS, 1)
                     tc::tmem_ld8(ts + 2 * BN + c0, l2);
                     tc::tmem_wait_ld();
 #pragma unroll
-                    for (int cc = 0; cc < 8; ++cc)
-                        acc[c0 + cc] += (double)l0[cc] + (double)l1[cc] * L1W + (double)l2[cc] * L2W;
+                    for (int cc = 0; cc < 8; ++cc) {
+                        if constexpr (I8)
+                            acc[c0 + cc] += tc::i32_to_f64(l0[cc]) + tc::i32_to_f64(l1[cc]) * I8L1W +
+                                            tc::i32_to_f64(l2[cc]) * I8L2W;
+                        else
+                            acc[c0 + cc] += (double)l0[cc] + (double)l1[cc] * L1W + (double)l2[cc] * L2W;
+                    }
                 }
                 tc::fence_before_sync();
                 tc::mbar_arrive(&tempty[b]);

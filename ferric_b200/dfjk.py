@@ -115,6 +115,31 @@ class DfJK:
         return out
 
 
+    def jk_from_occ(self, c_occ, out=None, stats=None):
+        """``(J, K)`` of one occupied-orbital matrix in one call
+        (``fc_dfjk_build_occ``): K as ``k_from_occ`` and J = J(C C^T), J's
+        first pass taken from K's stage-1 product.  ``out``: optional (J, K)
+        buffers."""
+        st = FcStats()
+        nocc = int(c_occ.shape[1])
+        if hasattr(c_occ, "is_cuda") and c_occ.is_cuda:
+            import torch
+            cc = c_occ.contiguous()
+            if out is None:
+                out = tuple(torch.empty((self.n, self.n), dtype=torch.float64, device=cc.device) for _ in range(2))
+            check(_lib.lib.fc_dfjk_build_occ_dev(self._h, ptr(cc), nocc, ptr(out[0]), ptr(out[1]),
+                                                 ctypes.c_void_p(torch.cuda.current_stream(cc.device).cuda_stream),
+                                                 ctypes.byref(st)))
+        else:
+            cc = np.ascontiguousarray(c_occ, dtype=np.float64)
+            if out is None:
+                out = (np.empty((self.n, self.n)), np.empty((self.n, self.n)))
+            check(_lib.lib.fc_dfjk_build_occ(self._h, ptr(cc), nocc, ptr(out[0]), ptr(out[1]), ctypes.byref(st)))
+        if stats is not None:
+            stats.update(st.as_dict())
+        return out
+
+
 class DfJ:
     """``JBuilder`` over a device-resident tensor (``DfJ``, ferric-scf/src/df_j.rs:127)."""
 

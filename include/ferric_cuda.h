@@ -335,6 +335,21 @@ fc_status fc_dfk_build_occ(fc_dfjk* h, const double* c_occ, int64_t nocc, double
                            fc_stats* stats);
 fc_status fc_dfk_build_occ_dev(fc_dfjk* h, const double* c_occ, int64_t nocc, double* k,
                                void* stream, fc_stats* stats);
+/* J and K of one occupied-orbital matrix in one call (square handles):
+ * K exactly as fc_dfk_build_occ, and j = J(C_occ C_occ^T), the density of
+ * build_from_occ with no occupation factor.  J's first pass d_P =
+ * <B_P, C C^T> = sum_mu (B_P C)[mu, :] . C[mu, :] is read off the K stage's
+ * W = B C, so B is read once for K's stage 1 and once for J's second pass
+ * (instead of two passes for J); the metric solve (fc_dfj_set_metric_chol)
+ * applies as in fc_dfj_build.  No counterpart in the reference, whose RHF
+ * calls JBuilder::build(D) and KBuilder::build_from_occ(C_occ) with
+ * D = 2 C_occ C_occ^T (ferric-scf/src/rhf.rs:3164-3178): J(D) = 2 j here.
+ * stats: kernel_ms/flops of the whole call, main_* of the K stages, aux_*
+ * of J's second pass. */
+fc_status fc_dfjk_build_occ(fc_dfjk* h, const double* c_occ, int64_t nocc, double* j, double* k,
+                            fc_stats* stats);
+fc_status fc_dfjk_build_occ_dev(fc_dfjk* h, const double* c_occ, int64_t nocc, double* j, double* k,
+                                void* stream, fc_stats* stats);
 /* Precision of the handle's next builds: FC_PREC_F64 always works (the FP64
  * tensor stays resident beside the mixed copy); the handle's creation
  * precision switches back.  This is how the SCF precision ladder

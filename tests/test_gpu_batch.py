@@ -235,3 +235,28 @@ def test_batch_single_and_degenerate_molecules(fc):
             assert np.abs(bt.gamma[m].cpu().numpy() - gamma).max() <= MIXED_G_REL * np.abs(gamma).max()
             assert np.abs(bt.de_docc[m].cpu().numpy() - d_o).max() <= MIXED_D_REL * np.abs(d_o).max()
         bt.close()
+
+
+def test_batch_on_oracle_alkane_tensors(fc):
+    """Real SCF tensors: the oracle's RHF B_ov and orbital energies of
+    all-trans CH4, C2H6 and C3H8 in cc-pVDZ / cc-pVDZ-RI (committed fixture,
+    tests/golden/make_alkanes.py), several copies each in one batch: every
+    molecule's mixed energy within the bar of the oracle's FP64 RI-MP2
+    energy, and the FP64 device path within 1e-10 Eh of it."""
+    import torch
+    from ferric_b200 import rimp2
+    from ferric_b200.batch import Rimp2Batch
+    d = dict(np.load(os.path.join(HERE, "golden", "alkanes_c1_c3.npz")))
+    ns = [3, 1, 2, 2, 3, 1]
+    mols = [(d[f"c{n}_b_ov"], d[f"c{n}_eps_occ"], d[f"c{n}_eps_vir"]) for n in ns]
+    bt = Rimp2Batch(_to_dev(mols), grad=True)
+    bt.run()
+    e_os, e_ss = bt.energies()
+    for m, n in enumerate(ns):
+        ref = float(d[f"c{n}_e_os"] + d[f"c{n}_e_ss"])
+        assert abs(e_os[m] + e_ss[m] - ref) <= MIXED_E_REL * abs(ref) + MIXED_E_ABS
+        b, eo, ev = mols[m]
+        sc, g, _, _ = rimp2.rimp2_energy_grad(b, eo, ev, precision="f64")
+        assert abs(sc.e_total - ref) <= 1e-10
+        assert np.abs(bt.gamma[m].cpu().numpy() - g).max() <= MIXED_G_REL * np.abs(g).max()
+    bt.close()

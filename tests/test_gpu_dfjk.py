@@ -139,10 +139,11 @@ def test_set_precision_refuses_missing_copy(fc):
 
 @pytest.mark.parametrize("n,naux,nocc", [(30, 50, 6), (65, 130, 9), (130, 260, 17), (200, 300, 70), (1, 3, 1)])
 def test_mixed_dfk_exact_slices(fc, n, naux, nocc):
-    """Split-BF16 DF-K (tcgen05 exact-slice stages, k-panel FP64 flush):
-    |dK| within the slicing error -- B, C and W rows carry about 24
-    significant bits and W is rounded to FP32 once -- and K exactly
-    symmetric and bit-identical on rebuild."""
+    """Exact-slice DF-K (tcgen05: stage 1 on int8 slices with exact int32
+    levels, stage 2 on bf16 slices with a k-panel FP64 flush): |dK| within
+    the slicing error -- B, C and W rows carry about 24 significant bits and
+    W is rounded to FP32 once -- and K exactly symmetric and bit-identical on
+    rebuild."""
     from ferric_b200.dfjk import DfJK
     b, c, d = synthetic.dfjk_inputs(n, naux, nocc)
     ref = orc.df_k_occ(b, c)
@@ -171,3 +172,59 @@ def test_mixed_dfk_refuses_nonfinite_c(fc):
         jk.k_from_occ(c)
     assert ei.value.name == "FC_ERR_RANGE"
     jk.close()
+
+
+@pytest.mark.parametrize("n,naux,nocc", [(30, 50, 6), (65, 130, 9), (130, 260, 17), (200, 300, 70), (1, 3, 1)])
+def test_fused_jk_from_occ(fc, n, naux, nocc):
+    """fc_dfjk_build_occ: K as fc_dfk_build_occ (the same bits) and
+    J = J(C C^T) with J's first pass read off K's stage-1 product W = B C:
+    FP64 within 1e-10 of the oracle; mixed within the FP32-storage bound of
+    J's second pass plus the slicing and FP32 rounding of W in d."""
+    from ferric_b200.dfjk import DfJK
+    b, c, d = synthetic.dfjk_inputs(n, naux, nocc)
+    j_ref, k_ref = orc.df_j_square(b, d), orc.df_k_occ(b, c)
+    for prec in ("f64", "mixed"):
+        jk = DfJK(b, precision=prec)
+        st = {}
+        j, k = jk.jk_from_occ(c, stats=st)
+        assert st["aux_launches"] == 1 and st["aux_ms"] > 0
+        assert np.array_equal(k, jk.k_from_occ(c))
+        assert np.array_equal(j, j.T)
+        if prec == "f64":
+            assert np.abs(j - j_ref).max() < F_TOL and np.abs(k - k_ref).max() < F_TOL
+            assert np.abs(j - jk.j(d)).max() <= 1e-12 * max(1.0, np.abs(j_ref).max())
+        else:
+            # pass 2 on FP32-stored B, plus d's error: W = B C from slices
+            # carrying ~24 bits of each row of B and of C, rounded to FP32
+            dp = np.einsum("qmn,mn->q", b, d)
+            cc = np.abs(c) @ np.abs(c).T
+            bound = 2.0 ** -23 * np.einsum("qmn,q->mn", np.abs(b), np.abs(dp)) \
+                + 2.0 ** -20 * np.einsum("qmn,q->mn", np.abs(b), np.einsum("qmn,mn->q", np.abs(b), cc))
+            assert np.all(np.abs(j - j_ref) <= bound + 1e-300)
+        jk.close()
+
+
+def test_fused_jk_device_api_and_metric(fc):
+    """The device form on torch tensors equals the host form, and a metric
+    set on the handle enters J as in fc_dfj_build (c = V^-1 d)."""
+    import torch
+    from ferric_b200.dfjk import DfJK
+    rng = np.random.default_rng(7)
+    b, c, d = synthetic.dfjk_inputs(48, 90, 7)
+    a = rng.standard_normal((90, 90))
+    l = orc.cholesky_lower(a @ a.T + 90 * np.eye(90))
+    jk = DfJK(b, precision="f64", metric_chol=l)
+    jh, kh = jk.jk_from_occ(c)
+    jd, kd = jk.jk_from_occ(torch.from_numpy(c).cuda())
+    assert np.array_equal(jh, jd.cpu().numpy()) and np.array_equal(kh, kd.cpu().numpy())
+    assert np.abs(jh - orc.df_j_square(b, d, metric_chol=l)).max() < F_TOL
+    assert np.abs(jh - jk.j(d)).max() <= 1e-12 * np.abs(jh).max()
+    jk.close()
+
+
+def test_fused_jk_empty_channel(fc):
+    from ferric_b200.dfjk import DfJK
+    b, c, d = synthetic.dfjk_inputs(20, 30, 3)
+    jk = DfJK(b)
+    j, k = jk.jk_from_occ(np.zeros((20, 0)))
+    assert not j.any() and not k.any()
