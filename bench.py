@@ -342,6 +342,7 @@ def batch_leg(torch, dev, nmol):
         b, eo, ev = mols[m]
         sc, g64, _, _ = rimp2.rimp2_energy_grad(b, eo, ev, precision="f64")
         e = {"n": int(n), "e_mp2": sc.e_total, "e_abs": float(e_os[m] + e_ss[m] - sc.e_total),
+             "e_os_abs": float(e_os[m] - sc.e_os), "e_ss_abs": float(e_ss[m] - sc.e_ss),
              "e_rel": float((e_os[m] + e_ss[m] - sc.e_total) / abs(sc.e_total)),
              "gamma_max_rel": float((bt.gamma[m] - g64).abs().max() / g64.abs().max())}
         if real:  # the FP64 device energy against the oracle's
@@ -452,6 +453,8 @@ def c5_leg(torch, dev, prec, steps=3):
     m, f = res[prec], res["f64"]
     out["speedup_mixed_vs_plain"] = out["f64"]["ms_per_step"] / out[prec]["ms_per_step"]
     out["mixed_error"] = {"e_total_abs": m["sc"].e_total - f["sc"].e_total,
+                          "e_os_abs": m["sc"].e_os - f["sc"].e_os, "e_ss_abs": m["sc"].e_ss - f["sc"].e_ss,
+                          "e_corr_f64": f["sc"].e_total,
                           "e_total_rel": (m["sc"].e_total - f["sc"].e_total) / abs(f["sc"].e_total),
                           "gamma_max_rel": float((m["gamma"] - f["gamma"]).abs().max() / f["gamma"].abs().max()),
                           "j_max_abs": float((m["j"] - f["j"]).abs().max()),
@@ -701,6 +704,8 @@ def main():
                  "components_ms": {"rimp2_e_grad": sp_r["kernel_ms"], "dfjk": sp_j["kernel_ms"],
                                    "dfk_stages": sp_j["main_ms"], "dfj_pass2": sp_j["aux_ms"]},
                  "mixed_error": {"e_total_abs": (sc.e_os + sc.e_ss) - sc64.e_total,
+                                 "e_os_abs": sc.e_os - sc64.e_os, "e_ss_abs": sc.e_ss - sc64.e_ss,
+                                 "e_corr_f64": sc64.e_total,
                                  "e_total_rel": ((sc.e_os + sc.e_ss) - sc64.e_total) / abs(sc64.e_total),
                                  "gamma_max_rel": float((gamma - g64).abs().max() / g64.abs().max()),
                                  "j_max_abs": float((jbuf - j64).abs().max()),

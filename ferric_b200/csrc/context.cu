@@ -171,6 +171,9 @@ fc_status fc_init(int32_t device, uint64_t pool_bytes) {
     if (c.device >= 0) return fail(FC_ERR_INVALID, "libferric_cuda is already bound to another device");
     FC_CUDA(cudaSetDevice(device));
     FC_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+    FC_CUDA(cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking));
+    FC_CUDA(cudaEventCreateWithFlags(&c.fork, cudaEventDisableTiming));
+    FC_CUDA(cudaEventCreateWithFlags(&c.join, cudaEventDisableTiming));
     FC_CUDA(cudaEventCreate(&c.ev0));
     FC_CUDA(cudaEventCreate(&c.ev1));
     c.sm_count = p.multiProcessorCount;

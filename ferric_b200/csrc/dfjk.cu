@@ -457,7 +457,7 @@ void dfjk_free_mixed(fc_dfjk* h) {
 }
 
 fc_status dfk_build_f64(fc_dfjk* h, const double* c_occ, int64_t nocc, double* k, cudaStream_t st,
-                        fc_stats* stats, double* d_out) {
+                        fc_stats* stats, const JFork* jf) {
     FC_TRY(dfjk_smem_once());
     const int64_t naux = h->naux, n = h->n;
     const int64_t M1 = naux * n;
@@ -488,9 +488,20 @@ fc_status dfk_build_f64(fc_dfjk* h, const double* c_occ, int64_t nocc, double* k
         dgemm_tn_kernel<EpiScatterW><<<g, 256, DG_SMEM, st>>>(h->b_sq, n, (const double*)vct, n, (int)M1,
                                                                (int)nocc, n, n, 0, epi);
     }
-    if (d_out)  // the J pass-1 vector from W = B C
-        dfj_d_from_w_kernel<double><<<(unsigned)naux, 256, 0, st>>>((const double*)vw, kdim, nocc, n, nocc, c_occ,
-                                                                    d_out);
+    if (jf) {  // J: pass-1 vector from W = B C, second pass forked off
+        // W rows of nocc doubles: 16-byte vectors when nocc is even (and W's base is)
+        if (nocc % 2 == 0) {
+            const int64_t dq = dfj_d_rows(nocc, 2);
+            dfj_d_from_w_kernel<double, 2><<<dim3((unsigned)((naux + dq - 1) / dq), DFJ_DY), 256, 0, st>>>(
+                (const double*)vw, kdim, nocc, n, nocc, naux, dq, c_occ, jf->dpart);
+        } else {
+            const int64_t dq = dfj_d_rows(nocc, 1);
+            dfj_d_from_w_kernel<double, 1><<<dim3((unsigned)((naux + dq - 1) / dq), DFJ_DY), 256, 0, st>>>(
+                (const double*)vw, kdim, nocc, n, nocc, naux, dq, c_occ, jf->dpart);
+        }
+        dfj_d_sum_kernel<<<(unsigned)((naux + 255) / 256), 256, 0, st>>>(jf->dpart, naux, jf->dp);
+        FC_TRY(dfj_fork_pass2(h, *jf, st));
+    }
     {
         dim3 g(tn, tm, nsplit);
         EpiSplit epi{(double*)vpart, n * n, (int)n};
@@ -499,6 +510,10 @@ fc_status dfk_build_f64(fc_dfjk* h, const double* c_occ, int64_t nocc, double* k
     }
     dfk_fold_kernel<<<(unsigned)((n * n + 255) / 256), 256, 0, st>>>((const double*)vpart, nsplit, n, k);
     FC_TRY(check_launch("DF-K kernels"));
+    if (jf) {  // join J's second pass
+        FC_CUDA(cudaEventRecord(c.join, c.side));
+        FC_CUDA(cudaStreamWaitEvent(st, c.join, 0));
+    }
     if (stats) {
         FC_CUDA(cudaEventRecord(c.ev1, st));
         FC_CUDA(cudaEventSynchronize(c.ev1));
@@ -518,44 +533,55 @@ fc_status dfk_build_f64(fc_dfjk* h, const double* c_occ, int64_t nocc, double* k
     return FC_OK;
 }
 
+// J's second pass on the side stream, after everything `st` holds so far.
+fc_status dfj_fork_pass2(fc_dfjk* h, const JFork& f, cudaStream_t st) {
+    Context& c = ctx();
+    FC_CUDA(cudaEventRecord(c.fork, st));
+    FC_CUDA(cudaStreamWaitEvent(c.side, c.fork, 0));
+    if (f.ev[0]) FC_CUDA(cudaEventRecord(f.ev[0], c.side));
+    if (h->active != FC_PREC_F64) FC_TRY(dfj_solve_pass2<float>(h, h->pk32, f.dp, f.part, f.nsplit, f.j, c.side));
+    else FC_TRY(dfj_solve_pass2<double>(h, h->b_pk, f.dp, f.part, f.nsplit, f.j, c.side));
+    if (f.ev[1]) FC_CUDA(cudaEventRecord(f.ev[1], c.side));
+    return FC_OK;
+}
+
 // J and K of one occupied-orbital matrix: K as dfk_build_*, J = J(C C^T) from
 // the pass-1 vector d_P = <B_P, C C^T> that the K stage's W = B C already
 // holds (one kernel over W instead of a pass over B), then the metric solve
-// and J's second pass over the packed rows (FP64, or the FP32 copy in mixed).
+// and J's second pass over the packed rows (FP64, or the FP32 copy in mixed)
+// on the side stream, where it overlaps the rest of DF-K (W's split and the
+// tensor-core W W^T).
 static fc_status dfjk_build_occ(fc_dfjk* h, const double* c_occ, int64_t nocc, double* j, double* k,
                                 cudaStream_t st, fc_stats* stats) {
     const bool mixed = h->active != FC_PREC_F64;
     const int nsplit = 4;
     const int64_t ld = mixed ? h->ld32 : h->pair;
+    // d, then the pass-2 partials at a 256-byte aligned offset (the FP32
+    // pass stores them as double2)
+    const int64_t dlen = (h->naux + 31) / 32 * 32;
     void* vd;
-    FC_TRY(ws_get(WS_JD, (size_t)(h->naux + 64 + (int64_t)nsplit * ld) * 8, &vd));
-    double* dp = (double*)vd;
-    double* part = dp + h->naux + 64;
-    Context& c = ctx();
-    fc_stats sk{};
-    if (mixed) FC_TRY(dfk_build_mixed(h, c_occ, nocc, k, st, stats ? &sk : nullptr, dp));
-    else FC_TRY(dfk_build_f64(h, c_occ, nocc, k, st, stats ? &sk : nullptr, dp));
+    FC_TRY(ws_get(WS_JD, (size_t)((1 + DFJ_DY) * dlen + (int64_t)nsplit * ld) * 8, &vd));
+    JFork jf{(double*)vd, (double*)vd + dlen, (double*)vd + (1 + DFJ_DY) * dlen, nsplit, j, {nullptr, nullptr}};
     cudaEvent_t* ev = nullptr;
     if (stats) {
         FC_TRY(timing_events2(1, &ev));
-        FC_CUDA(cudaEventRecord(ev[0], st));
+        jf.ev[0] = ev[0];
+        jf.ev[1] = ev[1];
     }
-    if (mixed) FC_TRY(dfj_solve_pass2<float>(h, h->pk32, dp, part, nsplit, j, st));
-    else FC_TRY(dfj_solve_pass2<double>(h, h->b_pk, dp, part, nsplit, j, st));
+    fc_stats sk{};
+    if (mixed) FC_TRY(dfk_build_mixed(h, c_occ, nocc, k, st, stats ? &sk : nullptr, &jf));
+    else FC_TRY(dfk_build_f64(h, c_occ, nocc, k, st, stats ? &sk : nullptr, &jf));
     if (stats) {
-        FC_CUDA(cudaEventRecord(ev[1], st));
-        FC_CUDA(cudaEventSynchronize(ev[1]));
         float jms = 0.f;
+        FC_CUDA(cudaEventSynchronize(ev[1]));
         FC_CUDA(cudaEventElapsedTime(&jms, ev[0], ev[1]));
-        *stats = sk;
-        stats->kernel_ms = sk.kernel_ms + jms;
+        *stats = sk;  // kernel_ms spans the whole call (the join comes before its last event)
         stats->flops = sk.flops + 2.0 * (double)h->naux * (double)h->pair;  // + J pass 2
         stats->launches = sk.launches + 3 + (h->l_chol ? 1 : 0);
         stats->aux_launches = 1;
         stats->aux_ms = jms;
         stats->aux_flops = 2.0 * (double)h->naux * (double)h->pair;
         stats->aux_bytes = (mixed ? 4.0 : 8.0) * (double)h->naux * (double)h->pair;
-        (void)c;
     }
     return FC_OK;
 }

@@ -76,18 +76,45 @@ __global__ void __launch_bounds__(256) dfk_split_c_kernel(const double* __restri
     }
 }
 
+// Row mu of the FP32 W -> int8 slices [3][mp][ldw] at the row scale sw[mu],
+// from the row maximum the stage-1 epilogue gathered, so W is read once.
+// blockIdx.y cuts the row into gridDim.y column ranges (more CTAs in flight).
 __global__ void __launch_bounds__(256) dfk_split_w_kernel(const float* __restrict__ w, int64_t ldw, int64_t mp,
-                                                          double* __restrict__ sw, __nv_bfloat16* __restrict__ ws) {
-    split_fx_rows_f32_body(w, ldw, ldw, mp, sw, ws, blockIdx.x);
+                                                          double* __restrict__ sw, int8_t* __restrict__ ws,
+                                                          const unsigned* __restrict__ wmax) {
+    const int64_t mu = blockIdx.x;
+    const double s = SliceI8::scale((double)__uint_as_float(wmax[mu]));
+    if (blockIdx.y == 0 && threadIdx.x == 0) sw[mu] = s;
+    const double inv = 1.0 / s;
+    const int64_t k4 = ldw / 4, per = (k4 + gridDim.y - 1) / gridDim.y;
+    const int64_t k0 = blockIdx.y * per, k1 = k0 + per < k4 ? k0 + per : k4;
+    const float4* row = reinterpret_cast<const float4*>(w + mu * ldw);
+    const int64_t ss = mp * ldw;
+    int8_t* o0 = ws + mu * ldw;
+    struct alignas(4) Q4 { int8_t e[4]; };
+    for (int64_t k = k0 + threadIdx.x; k < k1; k += 256) {
+        const float4 v = row[k];
+        Q4 pa, pb, pc;
+        fx_slices<SliceI8>(v.x, inv, pa.e[0], pb.e[0], pc.e[0]);
+        fx_slices<SliceI8>(v.y, inv, pa.e[1], pb.e[1], pc.e[1]);
+        fx_slices<SliceI8>(v.z, inv, pa.e[2], pb.e[2], pc.e[2]);
+        fx_slices<SliceI8>(v.w, inv, pa.e[3], pb.e[3], pc.e[3]);
+        reinterpret_cast<Q4*>(o0)[k] = pa;
+        reinterpret_cast<Q4*>(o0 + ss)[k] = pb;
+        reinterpret_cast<Q4*>(o0 + 2 * ss)[k] = pc;
+    }
 }
 
 // Stage 1 store: row r = (Q, mu) of B, column i: W[mu * ldw + Q * nocc_p + i].
+// Also, per thread, the max |W| of its values (atomicMax into wmax[mu]: the
+// order-free maximum of non-negative FP32 bits), so W's split reads W once.
 struct EpiW {
     const double* sa;  // [naux*n] B row scales
     const double* sc;  // [npad] C^T row scales
     float* w;
     int64_t ldw, rows;
     int n, nocc, nocc_p;
+    unsigned* wmax;     // [n]
     __device__ void operator()(int64_t, int4 it, int row, int col0, const double (&acc)[32]) const {
         const int64_t r = (int64_t)it.x * xg::BM + row;
         if (r >= rows) return;
@@ -96,17 +123,20 @@ struct EpiW {
         if (i0 >= nocc_p) return;
         const double s = sa[r];
         float* dst = w + mu * ldw + q * nocc_p + i0;
+        float m = 0.f;
 #pragma unroll
         for (int c4 = 0; c4 < 32; c4 += 4) {
-            if (i0 + c4 >= nocc_p) break;  // nocc_p is a multiple of 8
+            if (i0 + c4 >= nocc_p) break;  // nocc_p is a multiple of 16
             float v[4];
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
                 const int i = i0 + c4 + e;
                 v[e] = i < nocc ? (float)(s * sc[i] * acc[c4 + e]) : 0.f;
+                m = fmaxf(m, fabsf(v[e]));
             }
             *reinterpret_cast<float4*>(dst + c4) = make_float4(v[0], v[1], v[2], v[3]);
         }
+        atomicMax(wmax + mu, __float_as_uint(m));
     }
 };
 
@@ -151,8 +181,8 @@ fc_status xg_attrs() {
     if (g_attr_done) return FC_OK;
     FC_CUDA(cudaFuncSetAttribute(xgemm_kernel<64, EpiW, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  xg::Cfg<64, true>::SMEM));
-    FC_CUDA(cudaFuncSetAttribute(xgemm_kernel<128, EpiPart>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 xg::Cfg<128>::SMEM));
+    FC_CUDA(cudaFuncSetAttribute(xgemm_kernel<128, EpiPart, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 xg::Cfg<128, true>::SMEM));
     g_attr_done = true;
     return FC_OK;
 }
@@ -176,14 +206,16 @@ fc_status dfk_prepare_split(fc_dfjk* h, cudaStream_t st) {
 }
 
 fc_status dfk_build_mixed(fc_dfjk* h, const double* c_occ, int64_t nocc, double* kout, cudaStream_t st,
-                          fc_stats* stats, double* d_out) {
+                          fc_stats* stats, const JFork* jf) {
     if (!h->sq_split)
         return fail(FC_ERR_KERNEL, "DF-K: handle has no split-BF16 copy (created with FC_PREC_F64)");
     FC_TRY(xg_attrs());
     Context& cx = ctx();
     const int64_t n = h->n, naux = h->naux, ldk = rup(n, 16);
     const int64_t rows = naux * n;
-    const int64_t nocc_p = rup(nocc, 8), npad = rup(nocc, 64), ldw = naux * nocc_p, mp = rup(n, 128);
+    // nocc_p a multiple of 16: W's rows (ldw = naux nocc_p bytes as int8 slices) stay 16-byte aligned
+    const int64_t nocc_p = rup(nocc, 16), npad = rup(nocc, 64), ldw = naux * nocc_p, mp = rup(n, 128);
+
     if (rows > INT32_MAX || 3 * rows > (int64_t)UINT32_MAX || mp > 65536 || ldw > INT32_MAX)
         return fail(FC_ERR_LAYOUT, "DF-K mixed: shape too large");
     // stage-1 and stage-2 work items
@@ -194,7 +226,7 @@ fc_status dfk_build_mixed(fc_dfjk* h, const double* c_occ, int64_t nocc, double*
     const int64_t n1 = (int64_t)items.size();
     const int nt = (int)(mp / 128);
     const int ntile = nt * (nt + 1) / 2;
-    const int nks2 = (int)((ldw + 63) / 64);
+    const int nks2 = (int)((ldw + 127) / 128);  // k-steps of 128 int8
     int want = std::max(1, cx.sm_count / ntile);
     const int kps = (nks2 + want - 1) / want;
     const int nsplit = (nks2 + kps - 1) / kps;
@@ -215,8 +247,10 @@ fc_status dfk_build_mixed(fc_dfjk* h, const double* c_occ, int64_t nocc, double*
     FC_TRY(ws_get(WS_MISC, rup((int64_t)cs_bytes, 256) + npad * 8, &vc));
     FC_TRY(ws_get(WS_OUT, 256, &vout));
     FC_TRY(ws_get(WS_T, (size_t)n * ldw * 4, &vw));
-    FC_TRY(ws_get(WS_TS, (size_t)3 * mp * ldw * 2, &vws));
-    FC_TRY(ws_get(WS_SCALE, (size_t)mp * 8, &vsw));
+    FC_TRY(ws_get(WS_TS, (size_t)3 * mp * ldw, &vws));
+    FC_TRY(ws_get(WS_SCALE, (size_t)mp * 8 + (size_t)rup(n, 64) * 4, &vsw));
+    unsigned* wmax = (unsigned*)((double*)vsw + mp);  // [n] row maxima of |W| (FP32 bits)
+
     FC_TRY(ws_get(WS_PART, (size_t)n2 * 128 * 128 * 8, &vpart));
     FC_TRY(ws_get(WS_PAIRS, items.size() * sizeof(int4) + tix.size() * sizeof(int), &vtab));
     int* flags = (int*)vout;  // [0] range, [1] timeout
@@ -230,9 +264,10 @@ fc_status dfk_build_mixed(fc_dfjk* h, const double* c_occ, int64_t nocc, double*
     CUtensorMap tb, tcm, tw;
     FC_TRY(make_tmap_i8_2d(&tb, h->sq_split, n, 3 * rows, ldk, 128, 128));
     FC_TRY(make_tmap_i8_2d(&tcm, vc, n, 3 * npad, ldk, 128, 64));
-    FC_TRY(make_tmap_bf16_2d(&tw, vws, ldw, 3 * mp, ldw * 2, 64, 128));
+    FC_TRY(make_tmap_i8_2d(&tw, vws, ldw, 3 * mp, ldw, 128, 128));
 
     if (stats) FC_CUDA(cudaEventRecord(cx.ev0, st));
+    FC_CUDA(cudaMemsetAsync(wmax, 0, (size_t)n * 4, st));
     dfk_split_c_kernel<<<(unsigned)nocc, 256, 0, st>>>(c_occ, n, nocc, ldk, npad, sc, (int8_t*)vc, flags);
     cudaEvent_t* ev = nullptr;
     if (stats) {
@@ -241,27 +276,37 @@ fc_status dfk_build_mixed(fc_dfjk* h, const double* c_occ, int64_t nocc, double*
     }
     {
         XArgs a{(const int4*)vtab, n1, (int)rows, (int)npad, flags + 1};
-        EpiW epi{h->sq_scale, sc, (float*)vw, ldw, rows, (int)n, (int)nocc, (int)nocc_p};
+        EpiW epi{h->sq_scale, sc, (float*)vw, ldw, rows, (int)n, (int)nocc, (int)nocc_p, wmax};
         const int grid = (int)std::min<int64_t>(n1, cx.sm_count);
         xgemm_kernel<64, EpiW, true><<<grid, xg::Cfg<64, true>::THREADS, xg::Cfg<64, true>::SMEM, st>>>(tb, tcm, a,
                                                                                                          epi);
     }
     if (stats) FC_CUDA(cudaEventRecord(ev[1], st));
-    if (d_out)  // the J pass-1 vector from the FP32 W (each element rounded once)
-        dfj_d_from_w_kernel<float><<<(unsigned)naux, 256, 0, st>>>((const float*)vw, ldw, nocc_p, n, nocc, c_occ,
-                                                                   d_out);
-    dfk_split_w_kernel<<<(unsigned)n, 256, 0, st>>>((const float*)vw, ldw, mp, (double*)vsw, (__nv_bfloat16*)vws);
+    if (jf) {  // J: pass-1 vector from the FP32 W (each element rounded once), second pass forked off
+        const int64_t dq = dfj_d_rows(nocc, 4);  // nocc_p: a multiple of 16 floats
+        dfj_d_from_w_kernel<float, 4><<<dim3((unsigned)((naux + dq - 1) / dq), DFJ_DY), 256, 0, st>>>(
+            (const float*)vw, ldw, nocc_p, n, nocc, naux, dq, c_occ, jf->dpart);
+        dfj_d_sum_kernel<<<(unsigned)((naux + 255) / 256), 256, 0, st>>>(jf->dpart, naux, jf->dp);
+        FC_TRY(dfj_fork_pass2(h, *jf, st));
+    }
+    dfk_split_w_kernel<<<dim3((unsigned)n, 4), 256, 0, st>>>((const float*)vw, ldw, mp, (double*)vsw, (int8_t*)vws,
+                                                              wmax);
     if (stats) FC_CUDA(cudaEventRecord(ev[2], st));
     {
         XArgs a{(const int4*)vtab + n1, n2, (int)mp, (int)mp, flags + 1};
         EpiPart epi{(const double*)vsw, (double*)vpart, (int)n};
         const int grid = (int)std::min<int64_t>(n2, cx.sm_count);
-        xgemm_kernel<128, EpiPart><<<grid, xg::Cfg<128>::THREADS, xg::Cfg<128>::SMEM, st>>>(tw, tw, a, epi);
+        xgemm_kernel<128, EpiPart, true><<<grid, xg::Cfg<128, true>::THREADS, xg::Cfg<128, true>::SMEM, st>>>(
+            tw, tw, a, epi);
     }
     if (stats) FC_CUDA(cudaEventRecord(ev[3], st));
     dfk_fold_fx_kernel<<<(unsigned)((n * n + 255) / 256), 256, 0, st>>>((const double*)vpart, dtix, nsplit, nt, n,
                                                                          kout);
-    FC_TRY(check_launch("split-BF16 DF-K kernels"));
+    FC_TRY(check_launch("exact-slice DF-K kernels"));
+    if (jf) {  // join J's second pass
+        FC_CUDA(cudaEventRecord(cx.join, cx.side));
+        FC_CUDA(cudaStreamWaitEvent(st, cx.join, 0));
+    }
     if (stats) FC_CUDA(cudaEventRecord(cx.ev1, st));
     int hf[2];
     FC_CUDA(cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, st));

@@ -83,6 +83,8 @@ struct Context {
     uint64_t pool_cap = 0;
     uint64_t handle_bytes = 0;  // held by DF-JK handles
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;   // a call's second stream (work that overlaps its main stream)
+    cudaEvent_t fork = nullptr, join = nullptr;
     int sm_count = 0;
     std::mutex mu;
     Workspace ws[WS_COUNT];

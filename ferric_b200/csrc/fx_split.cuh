@@ -118,27 +118,33 @@ __device__ __forceinline__ void split_fx_qrows_body(const double* __restrict__ B
 
 // Per-row split of the FP32 amplitude chunk T[rows][pitch] (first Kv columns)
 // -> Ts[s][rows][pitch], ts[row].  One CTA per row; the row is read twice
-// (max, then slices).  Kv and pitch are multiples of 4.
+// (max, then slices), or once when its max |T| is given (rmax: bits of the
+// non-negative FP32 maximum per row).  Kv and pitch are multiples of 4.
 template <class SL = SliceBf16>
 __device__ __forceinline__ void split_fx_rows_f32_body(const float* __restrict__ T, int64_t Kv, int64_t K,
                                                        int64_t slice_rows, double* __restrict__ ts,
-                                                       typename SL::T* __restrict__ Ts, int64_t r) {
+                                                       typename SL::T* __restrict__ Ts, int64_t r,
+                                                       const unsigned* __restrict__ rmax = nullptr) {
     using E = typename SL::T;
     __shared__ double red[32];
     const float4* row = reinterpret_cast<const float4*>(T + r * K);
     const int64_t K4 = Kv / 4;
-    float m = 0.f;
-    for (int64_t k = threadIdx.x; k < K4; k += 256) {
-        const float4 v = row[k];
-        m = fmaxf(m, fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w))));
-    }
-    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        double t = threadIdx.x < 8 ? red[threadIdx.x] : 0.0;
-        for (int o = 16; o > 0; o >>= 1) t = fmax(t, __shfl_xor_sync(0xffffffffu, t, o));
-        if (threadIdx.x == 0) red[0] = t;
+    if (rmax) {
+        if (threadIdx.x == 0) red[0] = (double)__uint_as_float(rmax[r]);
+    } else {
+        float m = 0.f;
+        for (int64_t k = threadIdx.x; k < K4; k += 256) {
+            const float4 v = row[k];
+            m = fmaxf(m, fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w))));
+        }
+        for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            double t = threadIdx.x < 8 ? red[threadIdx.x] : 0.0;
+            for (int o = 16; o > 0; o >>= 1) t = fmax(t, __shfl_xor_sync(0xffffffffu, t, o));
+            if (threadIdx.x == 0) red[0] = t;
+        }
     }
     __syncthreads();
     const double s = SL::scale(red[0]);

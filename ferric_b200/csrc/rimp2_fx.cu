@@ -376,6 +376,11 @@ struct PairFxArgs {
     double* part;  // [item][2]
     double* scr;   // [grid][2][BM][BN] FP64 X and Y tiles of each CTA
     int* err;
+    // failure-path test hook: the MMA warp's waits for operand stages give up
+    // after wait_ns; with drop_load, CTA 0's producer issues no load for its
+    // first stage, so that wait runs out with nothing in flight
+    uint64_t wait_ns;
+    int drop_load;
     // gradient mode: pairs (i, j), i in chunk I (from i0), j in chunk J (from j0)
     float* T;        // amplitude rows of I: [|I| a_pad][ldt = |J| a_pad]
     float* T2;       // amplitude rows of J: [|J| a_pad][ldt2 = |I| a_pad] (T when I == J)
@@ -540,6 +545,7 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
         // ------------------------------------------------------ TMA producer
         if (lane == 0) {
             uint32_t g = 0;
+            const bool drop = p.drop_load && blockIdx.x == 0;  // stage g == 0 gets no load
             for (int64_t k = blockIdx.x; k < p.items && !*abort_flag; k += gridDim.x) {
                 const ItemView v = item_view<BATCH>(p, k);
                 const int nph = (v.i == v.j || v.xt) ? 1 : 2;
@@ -549,6 +555,7 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
                         const int s = g % S;
                         const uint32_t u = g / S;
                         if (!tc::mbar_wait(&empty[s], (u & 1) ^ 1, abort_flag, p.err)) goto prod_done;
+                        if (drop && g == 0) continue;
                         tc::mbar_arrive_expect_tx(&full[s], PSTAGE_BYTES);
 #pragma unroll
                         for (int sl = 0; sl < PSL; ++sl) {
@@ -561,8 +568,10 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
                 }
             }
         prod_done:
+            // every load issued lands before the CTA leaves (a dropped stage has none)
             for (uint32_t q = 0; q < (uint32_t)S && q < g; ++q) {
                 const uint32_t gg = g - 1 - q;
+                if (drop && gg == 0) continue;
                 int no_abort = 0;
                 tc::mbar_wait(&full[gg % S], (gg / S) & 1, &no_abort, p.err);
             }
@@ -585,7 +594,9 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
                     for (int kt = 0; kt < v.nk; ++kt, ++g) {
                         const int s = g % S;
                         const uint32_t u = g / S;
-                        if (!tc::mbar_wait(&full[s], u & 1, abort_flag, p.err)) goto mma_done;
+                        if (!tc::mbar_wait(&full[s], u & 1, abort_flag, p.err,
+                                           p.wait_ns ? p.wait_ns : tc::WAIT_LIMIT_NS))
+                            goto mma_done;
                         tc::fence_after_sync();
                         uint64_t d = da[0];
 #pragma unroll
@@ -1507,6 +1518,21 @@ int fx_exchange_choice(int nk, int grad) {
     return 1;
 }
 
+// Failure-path test hook of the pair kernel.  FERRIC_CUDA_WAIT_MS bounds the
+// MMA warp's waits for operand stages (default 4 s); with
+// FERRIC_CUDA_TEST_DROP_LOAD=1 CTA 0's producer issues no load for its first
+// stage, so that bounded wait runs out (nothing in flight, FC_ERR_TIMEOUT)
+// while every other wait of the kernel keeps its 4 s limit.
+static void fx_test_hooks(PairFxArgs* a) {
+    a->wait_ns = tc::WAIT_LIMIT_NS;
+    if (const char* e = std::getenv("FERRIC_CUDA_WAIT_MS")) {
+        const long long v = std::atoll(e);
+        if (v > 0 && v <= 60000) a->wait_ns = (uint64_t)v * 1000000ull;
+    }
+    const char* d = std::getenv("FERRIC_CUDA_TEST_DROP_LOAD");
+    a->drop_load = (d && d[0] == '1') ? 1 : 0;
+}
+
 // FP64 X / Y tiles of the pair kernel's CTAs (global scratch, L2-resident).
 fc_status pair_scratch(int grid, double** out) {
     void* v;
@@ -1548,6 +1574,7 @@ fc_status rimp2_energy_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, doub
     FC_TRY(ws_get(WS_PAIRS, pairs.size() * sizeof(int2), &vtab));
     FC_CUDA(cudaMemcpyAsync(vtab, pairs.data(), pairs.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
     PairFxArgs a{};
+    fx_test_hooks(&a);
     a.eo = d.eps_occ;
     a.ev = d.eps_vir;
     a.scl = sp.scl;
@@ -1800,6 +1827,7 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
         FC_TRY(prep(cp.i0 / cc));
         FC_TRY(prep(cp.j0 / cc));
         PairFxArgs a{};
+        fx_test_hooks(&a);
         a.eo = d.eps_occ;
         a.ev = d.eps_vir;
         a.scl = sp.scl;
@@ -2288,6 +2316,7 @@ fc_status rimp2_batch_build_fx(fc_rimp2_batch* b, const std::vector<BatchMolIn>&
         }
         FC_TRY(check_launch("batch split kernels"));
         PairFxArgs a{};
+        a.wait_ns = tc::WAIT_LIMIT_NS;
         a.bitems = (const int4*)vitems;
         a.bmols = (const BatchMol*)vmols;
         a.err = b->flags + 1;

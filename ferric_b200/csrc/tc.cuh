@@ -57,17 +57,17 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // Wait for the phase of parity `parity` to complete.  Returns false (after
-// raising the error word and abort flag) when the time limit runs out or
-// another role already aborted.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
-                                          int* err) {
+// raising the error word and abort flag) when `limit_ns` runs out or another
+// role already aborted.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int* err,
+                                          uint64_t limit_ns = WAIT_LIMIT_NS) {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = globaltimer();
     for (uint32_t it = 1;; ++it) {
         if (mbar_try_wait(bar, parity)) return true;
         if ((it & 63) == 0) {
             if (*abort_flag) return false;
-            if (globaltimer() - t0 > WAIT_LIMIT_NS) {
+            if (globaltimer() - t0 > limit_ns) {
                 *abort_flag = 1;
                 atomicExch(err, ERR_TIMEOUT);
                 return false;

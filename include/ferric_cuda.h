@@ -341,7 +341,9 @@ fc_status fc_dfk_build_occ_dev(fc_dfjk* h, const double* c_occ, int64_t nocc, do
  * <B_P, C C^T> = sum_mu (B_P C)[mu, :] . C[mu, :] is read off the K stage's
  * W = B C, so B is read once for K's stage 1 and once for J's second pass
  * (instead of two passes for J); the metric solve (fc_dfj_set_metric_chol)
- * applies as in fc_dfj_build.  No counterpart in the reference, whose RHF
+ * applies as in fc_dfj_build; J's second pass runs on the library's side
+ * stream, overlapping the rest of DF-K, and the call's stream waits for it
+ * before the call returns.  No counterpart in the reference, whose RHF
  * calls JBuilder::build(D) and KBuilder::build_from_occ(C_occ) with
  * D = 2 C_occ C_occ^T (ferric-scf/src/rhf.rs:3164-3178): J(D) = 2 j here.
  * stats: kernel_ms/flops of the whole call, main_* of the K stages, aux_*

@@ -174,7 +174,10 @@ def test_mixed_dfk_refuses_nonfinite_c(fc):
     jk.close()
 
 
-@pytest.mark.parametrize("n,naux,nocc", [(30, 50, 6), (65, 130, 9), (130, 260, 17), (200, 300, 70), (1, 3, 1)])
+# (320, 40, 301) and (1040, 12, 1030): more than 256 vectors per aux row in
+# J's first pass (FP64 odd nocc, one double per vector; mixed, four floats)
+@pytest.mark.parametrize("n,naux,nocc", [(30, 50, 6), (65, 130, 9), (130, 260, 17), (200, 300, 70), (1, 3, 1),
+                                         (320, 40, 301), (1040, 12, 1030)])
 def test_fused_jk_from_occ(fc, n, naux, nocc):
     """fc_dfjk_build_occ: K as fc_dfk_build_occ (the same bits) and
     J = J(C C^T) with J's first pass read off K's stage-1 product W = B C:
