@@ -38,6 +38,9 @@ SIGNATURES = {
     "fc_rimp2_energy_dev": (_I32, [_P, _I64, _I64, _I64, _P, _P, _I32, _D, _I32, _DP, _DP, _P, _P]),
     "fc_rimp2_energy_grad": (_I32, [_P, _I64, _I64, _I64, _P, _P, _I32, _DP, _DP, _P, _P, _P, _P]),
     "fc_rimp2_energy_grad_dev": (_I32, [_P, _I64, _I64, _I64, _P, _P, _I32, _DP, _DP, _P, _P, _P, _P, _P]),
+    "fc_rimp2_energy_grad_dens": (_I32, [_P, _I64, _I64, _I64, _P, _P, _I32, _DP, _DP, _P, _P, _P, _P, _P, _P]),
+    "fc_rimp2_energy_grad_dens_dev": (_I32, [_P, _I64, _I64, _I64, _P, _P, _I32, _DP, _DP, _P, _P, _P, _P, _P, _P,
+                                             _P]),
     "fc_rimp2_energy_shard_dev": (_I32, [_P, _I64, _I64, _I64, _P, _P, _I32, _D, _I32, _I32, _I32, _DP, _DP, _P,
                                          _P]),
     "fc_rimp2_energy_grad_shard_dev": (_I32, [_P, _I64, _I64, _I64, _P, _P, _I32, _I32, _I32, _DP, _DP, _P, _P, _P,

@@ -85,11 +85,11 @@ fc_status energy_dispatch(const Rimp2Dev& d, int32_t precision, cudaStream_t st,
 
 fc_status grad_dispatch(const Rimp2Dev& d, int32_t precision, cudaStream_t st, double* e_os,
                         double* e_ss, double* gamma, double* de_docc, double* de_dvir,
-                        fc_stats* stats, const GammaSink* sink = nullptr) {
+                        fc_stats* stats, const GammaSink* sink = nullptr, const DensOut* dens = nullptr) {
     if (precision == FC_PREC_F64)
-        return rimp2_grad_f64(d, st, e_os, e_ss, gamma, de_docc, de_dvir, stats, sink);
+        return rimp2_grad_f64(d, st, e_os, e_ss, gamma, de_docc, de_dvir, stats, sink, dens);
     if (precision == FC_PREC_MIXED)
-        return rimp2_grad_fx(d, st, e_os, e_ss, gamma, de_docc, de_dvir, stats, sink);
+        return rimp2_grad_fx(d, st, e_os, e_ss, gamma, de_docc, de_dvir, stats, sink, dens);
     return fail(FC_ERR_KERNEL, "FC_PREC_MIXED_FAST has no adjoint kernel; use FC_PREC_MIXED");
 }
 
@@ -204,13 +204,15 @@ fc_status fc_rimp2_energy(const double* b_ov, int64_t naux, int64_t nocc, int64_
     return FC_OK;
 }
 
-fc_status fc_rimp2_energy_grad_dev(const double* b_ov, int64_t naux, int64_t nocc, int64_t nvir,
-                                   const double* eps_occ, const double* eps_vir, int32_t precision,
-                                   double* e_os, double* e_ss, double* gamma, double* de_docc,
-                                   double* de_dvir, void* stream, fc_stats* stats) {
+static fc_status grad_dev_impl(const double* b_ov, int64_t naux, int64_t nocc, int64_t nvir,
+                               const double* eps_occ, const double* eps_vir, int32_t precision, double* e_os,
+                               double* e_ss, double* gamma, double* de_docc, double* de_dvir, double* p_oo,
+                               double* p_vv, bool dens, void* stream, fc_stats* stats) {
     FC_TRY(check_shapes(b_ov, naux, nocc, nvir, eps_occ, eps_vir, precision, 0, 0.0, e_os, e_ss));
     if (naux && nocc && nvir && (!gamma || !de_docc || !de_dvir))
         return fail(FC_ERR_INVALID, "RI-MP2 gradient: null output pointer");
+    if (dens && ((nocc && !p_oo) || (nvir && !p_vv)))
+        return fail(FC_ERR_INVALID, "RI-MP2 densities: null output pointer");
     FC_TRY(require_init());
     std::lock_guard<std::mutex> lk(ctx().mu);
     if (stats) *stats = fc_stats{};
@@ -221,11 +223,32 @@ fc_status fc_rimp2_energy_grad_dev(const double* b_ov, int64_t naux, int64_t noc
         if (gamma && naux * nocc * nvir) FC_CUDA(cudaMemsetAsync(gamma, 0, naux * nocc * nvir * 8, st));
         if (de_docc && nocc) FC_CUDA(cudaMemsetAsync(de_docc, 0, nocc * 8, st));
         if (de_dvir && nvir) FC_CUDA(cudaMemsetAsync(de_dvir, 0, nvir * 8, st));
+        if (dens && nocc) FC_CUDA(cudaMemsetAsync(p_oo, 0, nocc * nocc * 8, st));
+        if (dens && nvir) FC_CUDA(cudaMemsetAsync(p_vv, 0, nvir * nvir * 8, st));
         FC_CUDA(cudaStreamSynchronize(st));
         return FC_OK;
     }
     Rimp2Dev d{b_ov, eps_occ, eps_vir, naux, nocc, nvir, 0, 0.0, chunk_budget()};
-    return grad_dispatch(d, precision, st, e_os, e_ss, gamma, de_docc, de_dvir, stats);
+    const DensOut dn{p_oo, p_vv};
+    return grad_dispatch(d, precision, st, e_os, e_ss, gamma, de_docc, de_dvir, stats, nullptr,
+                         dens ? &dn : nullptr);
+}
+
+fc_status fc_rimp2_energy_grad_dev(const double* b_ov, int64_t naux, int64_t nocc, int64_t nvir,
+                                   const double* eps_occ, const double* eps_vir, int32_t precision,
+                                   double* e_os, double* e_ss, double* gamma, double* de_docc,
+                                   double* de_dvir, void* stream, fc_stats* stats) {
+    return grad_dev_impl(b_ov, naux, nocc, nvir, eps_occ, eps_vir, precision, e_os, e_ss, gamma, de_docc, de_dvir,
+                         nullptr, nullptr, false, stream, stats);
+}
+
+fc_status fc_rimp2_energy_grad_dens_dev(const double* b_ov, int64_t naux, int64_t nocc, int64_t nvir,
+                                        const double* eps_occ, const double* eps_vir, int32_t precision,
+                                        double* e_os, double* e_ss, double* gamma, double* de_docc,
+                                        double* de_dvir, double* p_oo, double* p_vv, void* stream,
+                                        fc_stats* stats) {
+    return grad_dev_impl(b_ov, naux, nocc, nvir, eps_occ, eps_vir, precision, e_os, e_ss, gamma, de_docc, de_dvir,
+                         p_oo, p_vv, true, stream, stats);
 }
 
 fc_status fc_rimp2_energy_shard_dev(const double* b_ov, int64_t naux, int64_t nocc, int64_t nvir,
@@ -313,13 +336,15 @@ fc_status fc_rimp2_shard_pairs(int64_t nocc, int64_t nvir, int32_t precision, in
     return FC_OK;
 }
 
-fc_status fc_rimp2_energy_grad(const double* b_ov, int64_t naux, int64_t nocc, int64_t nvir,
-                               const double* eps_occ, const double* eps_vir, int32_t precision,
-                               double* e_os, double* e_ss, double* gamma, double* de_docc,
-                               double* de_dvir, fc_stats* stats) {
+static fc_status grad_host_impl(const double* b_ov, int64_t naux, int64_t nocc, int64_t nvir,
+                                const double* eps_occ, const double* eps_vir, int32_t precision, double* e_os,
+                                double* e_ss, double* gamma, double* de_docc, double* de_dvir, double* p_oo,
+                                double* p_vv, bool dens, fc_stats* stats) {
     FC_TRY(check_shapes(b_ov, naux, nocc, nvir, eps_occ, eps_vir, precision, 0, 0.0, e_os, e_ss));
     if (naux && nocc && nvir && (!gamma || !de_docc || !de_dvir))
         return fail(FC_ERR_INVALID, "RI-MP2 gradient: null output pointer");
+    if (dens && ((nocc && !p_oo) || (nvir && !p_vv)))
+        return fail(FC_ERR_INVALID, "RI-MP2 densities: null output pointer");
     FC_TRY(require_init());
     std::lock_guard<std::mutex> lk(ctx().mu);
     if (stats) *stats = fc_stats{};
@@ -330,6 +355,8 @@ fc_status fc_rimp2_energy_grad(const double* b_ov, int64_t naux, int64_t nocc, i
         for (size_t k = 0; gamma && k < nel; ++k) gamma[k] = 0.0;
         for (int64_t k = 0; de_docc && k < nocc; ++k) de_docc[k] = 0.0;
         for (int64_t k = 0; de_dvir && k < nvir; ++k) de_dvir[k] = 0.0;
+        for (int64_t k = 0; dens && k < nocc * nocc; ++k) p_oo[k] = 0.0;
+        for (int64_t k = 0; dens && k < nvir * nvir; ++k) p_vv[k] = 0.0;
         return FC_OK;
     }
     cudaStream_t st = ctx().stream;
@@ -337,7 +364,8 @@ fc_status fc_rimp2_energy_grad(const double* b_ov, int64_t naux, int64_t nocc, i
     FC_TRY(ws_get(WS_B, nel * 8, &db));
     FC_TRY(ws_get(WS_EPS, (nocc + nvir) * 8, &de));
     FC_TRY(ws_get(WS_GAMMA, nel * 8, &dg));
-    FC_TRY(ws_get(WS_HOSTOUT, (nocc + nvir) * 8, &dd));
+    const size_t np2 = dens ? (size_t)(nocc * nocc + nvir * nvir) : 0;  // P_oo, P_vv after dE/deps
+    FC_TRY(ws_get(WS_HOSTOUT, ((nocc + nvir) + np2) * 8, &dd));
     Rimp2Dev d{(const double*)db, (const double*)de, (const double*)de + nocc, naux, nocc, nvir,
                0, 0.0, chunk_budget()};
     // A pinned b_ov is uploaded in the gradient's occupied chunks on a copy
@@ -381,22 +409,44 @@ fc_status fc_rimp2_energy_grad(const double* b_ov, int64_t naux, int64_t nocc, i
     if (pinned && precision != FC_PREC_MIXED_FAST) {
         FC_TRY(copy_stream(&sink.stream, &sink.ready));
     }
+    double* dp = (double*)dd + nocc + nvir;
+    const DensOut dn{dp, dp + nocc * nocc};
     const fc_status gs = grad_dispatch(d, precision, st, e_os, e_ss, (double*)dg, (double*)dd, (double*)dd + nocc,
-                                       stats, sink.stream ? &sink : nullptr);
+                                       stats, sink.stream ? &sink : nullptr, dens ? &dn : nullptr);
     // the caller may reuse b_ov once this returns, also after an error
     if (us) FC_CUDA(cudaStreamSynchronize(us));
     if (gs != FC_OK) return gs;
     if (!sink.stream) FC_CUDA(cudaMemcpyAsync(gamma, dg, nel * 8, cudaMemcpyDeviceToHost, st));
     FC_CUDA(cudaMemcpyAsync(de_docc, dd, nocc * 8, cudaMemcpyDeviceToHost, st));
     FC_CUDA(cudaMemcpyAsync(de_dvir, (double*)dd + nocc, nvir * 8, cudaMemcpyDeviceToHost, st));
+    if (dens) {
+        FC_CUDA(cudaMemcpyAsync(p_oo, dn.p_oo, nocc * nocc * 8, cudaMemcpyDeviceToHost, st));
+        FC_CUDA(cudaMemcpyAsync(p_vv, dn.p_vv, nvir * nvir * 8, cudaMemcpyDeviceToHost, st));
+    }
     FC_CUDA(cudaStreamSynchronize(st));
     if (sink.stream) FC_CUDA(cudaStreamSynchronize(sink.stream));
     (void)c;
     if (stats) {
         stats->h2d_bytes += nel * 8 + (nocc + nvir) * 8;
-        stats->d2h_bytes += nel * 8 + (nocc + nvir) * 8;
+        stats->d2h_bytes += nel * 8 + (nocc + nvir + np2) * 8;
     }
     return FC_OK;
+}
+
+fc_status fc_rimp2_energy_grad(const double* b_ov, int64_t naux, int64_t nocc, int64_t nvir,
+                               const double* eps_occ, const double* eps_vir, int32_t precision,
+                               double* e_os, double* e_ss, double* gamma, double* de_docc,
+                               double* de_dvir, fc_stats* stats) {
+    return grad_host_impl(b_ov, naux, nocc, nvir, eps_occ, eps_vir, precision, e_os, e_ss, gamma, de_docc, de_dvir,
+                          nullptr, nullptr, false, stats);
+}
+
+fc_status fc_rimp2_energy_grad_dens(const double* b_ov, int64_t naux, int64_t nocc, int64_t nvir,
+                                    const double* eps_occ, const double* eps_vir, int32_t precision,
+                                    double* e_os, double* e_ss, double* gamma, double* de_docc,
+                                    double* de_dvir, double* p_oo, double* p_vv, fc_stats* stats) {
+    return grad_host_impl(b_ov, naux, nocc, nvir, eps_occ, eps_vir, precision, e_os, e_ss, gamma, de_docc, de_dvir,
+                          p_oo, p_vv, true, stats);
 }
 
 }  // extern "C"

@@ -75,6 +75,8 @@ enum WsSlot {
     WS_MISC,       // DF-J weights / d_P, DF-K C^T
     WS_PSCR,       // pair kernel: FP64 X / Y tiles of each CTA
     WS_JD,         // fused DF-JK: d_P and J's pass-2 partials
+    WS_DSLAB,      // MP2 densities: amplitude slabs (t and Tt)
+    WS_DPART,      // MP2 densities: row scales, partial tiles, work items
     WS_COUNT
 };
 

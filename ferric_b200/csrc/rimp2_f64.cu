@@ -396,8 +396,9 @@ fc_status rimp2_energy_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, dou
 
 fc_status rimp2_grad_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, double* e_ss,
                          double* gamma, double* de_docc, double* de_dvir, fc_stats* stats,
-                         const GammaSink* sink) {
+                         const GammaSink* sink, const DensOut* dens) {
     FC_TRY(set_smem_once());
+    if (dens && d.nshards != 1) return fail(FC_ERR_INVALID, "RI-MP2 densities: no sharded form");
     const int64_t nocc = d.nocc, nvir = d.nvir, naux = d.naux, nov = nocc * nvir;
     const int ntile = (int)((nvir + PR_T - 1) / PR_T);
     const int ntile2 = ntile * ntile;  // every tile (ta, tb) of a pair, ta-major
@@ -405,15 +406,21 @@ fc_status rimp2_grad_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, doubl
     // pair (i, j) is computed once and writes the amplitude rows of i (columns
     // of J) and of j (columns of I); both blocks (c nvir)^2 doubles fit the
     // chunk budget beside B and Gamma.
-    const int64_t cc = grad_chunk_f64(nocc, nvir, d.chunk_bytes, d.nshards);
+    // with densities the chunk is also bounded by the FP64 slabs (four chunk
+    // budgets: the slabs are the densities' whole working set)
+    const int64_t cc = dens ? dens_chunk_f64(nocc, nvir, grad_chunk_f64(nocc, nvir, d.chunk_bytes, 1),
+                                             4 * d.chunk_bytes)
+                            : grad_chunk_f64(nocc, nvir, d.chunk_bytes, d.nshards);
     const int64_t nch = (nocc + cc - 1) / cc;
     struct CP {
         int64_t i0, ni, j0, nj, p0, np;
     };
     std::vector<CP> cps;
     std::vector<int2> hp;
+    std::vector<int64_t> cp_index((size_t)(nch * nch), -1);  // [I][J], I <= J
     for (int64_t I = 0; I < nch; ++I)
         for (int64_t J = I; J < nch; ++J) {
+            cp_index[(size_t)(I * nch + J)] = (int64_t)cps.size();
             CP x;
             x.i0 = I * cc;
             x.ni = std::min(cc, nocc - x.i0);
@@ -433,6 +440,26 @@ fc_status rimp2_grad_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, doubl
     int64_t max_items = 0;
     for (const auto& x : cps) max_items = std::max(max_items, x.np * ntile2);
     if (max_items > INT32_MAX) return fail(FC_ERR_LAYOUT, "RI-MP2 gradient: too many pair tiles per chunk pair");
+    // The run order: each chunk pair once (gradient), or by column chunk K
+    // with the block (I, K) of every I (densities; as in the mixed driver):
+    // the pair kernel then writes that block straight into the slab.
+    struct Step {
+        int64_t x;
+        int blk;    // 0: T, 1: T2, 2: both
+        bool sums;  // take the chunk pair's energy and dE/deps terms
+        bool last;  // last block of the column chunk
+    };
+    std::vector<Step> steps;
+    if (!dens) {
+        for (int64_t x = 0; x < ncp; ++x) steps.push_back({x, 2, true, false});
+    } else {
+        for (int64_t K = 0; K < nch; ++K)
+            for (int64_t I = 0; I < nch; ++I)
+                steps.push_back({cp_index[(size_t)(std::min(I, K) * nch + std::max(I, K))], I <= K ? 0 : 1, I <= K,
+                                 I == nch - 1});
+    }
+    const int64_t nsteps = (int64_t)steps.size();
+    DensF64 dx{};
 
     void *vpairs, *vpart, *vT, *vout;
     const size_t blk = (size_t)cc * nvir * cc * nvir;  // doubles of one amplitude block
@@ -459,9 +486,11 @@ fc_status rimp2_grad_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, doubl
     cudaEvent_t* ev2 = nullptr;
     int nadj = 0;
     double adj_flops = 0.0, adj_bytes = 0.0;
-    if (stats) FC_TRY(timing_events((int)ncp, &ev));
-    if (stats) FC_TRY(timing_events2((int)(2 * ncp), &ev2));
+    if (stats) FC_TRY(timing_events((int)nsteps, &ev));
+    if (stats) FC_TRY(timing_events2((int)(2 * nsteps), &ev2));
     if (stats) FC_CUDA(cudaEventRecord(c.ev0, st));
+    if (dens) FC_TRY(dens_f64_alloc(nocc, nvir, cc, st, &dx));
+    int64_t nl = 0, npair_launch = 0;
     // Gamma[:, rows of R] += 4 B_ov[:, columns of K] . T^T
     auto adjoint = [&](const double* T, int64_t r0, int64_t nr, int64_t k0, int64_t nk) -> fc_status {
         const int N = (int)(nr * nvir);
@@ -477,13 +506,15 @@ fc_status rimp2_grad_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, doubl
         adj_bytes += 8.0 * (double)naux * (double)K + 8.0 * (double)N * (double)K + 16.0 * (double)naux * (double)N;
         return check_launch("dgemm_tn_kernel<gamma>");
     };
-    for (int64_t x = 0; x < ncp; ++x) {
+    for (int64_t sx = 0; sx < nsteps; ++sx) {
+        const Step& step = steps[(size_t)sx];
+        const int64_t x = step.x;
         const CP& cp = cps[x];
         const bool same = cp.i0 == cp.j0;
         if (owner[x] != d.shard) {
             if (stats) {
-                FC_CUDA(cudaEventRecord(ev[2 * x], st));
-                FC_CUDA(cudaEventRecord(ev[2 * x + 1], st));
+                FC_CUDA(cudaEventRecord(ev[2 * sx], st));
+                FC_CUDA(cudaEventRecord(ev[2 * sx + 1], st));
             }
             continue;
         }
@@ -506,20 +537,48 @@ fc_status rimp2_grad_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, doubl
         a.j0 = (int)cp.j0;
         a.occ_part = occ;
         a.vir_part = vir;
+        double* tb1 = T1;
+        double* tb2 = same ? T1 : T2;
+        if (dens) {  // the column chunk's block goes straight into the slab
+            if (step.blk == 0) {
+                tb1 = dx.ts + cp.i0 * nvir * a.ldt;
+                if (same) tb2 = tb1;
+            } else {
+                tb2 = dx.ts + cp.j0 * nvir * a.ldt2;
+            }
+        }
+        a.T = tb1;
+        a.T2 = tb2;
         const int64_t nit = cp.np * ntile2;
-        if (stats) FC_CUDA(cudaEventRecord(ev[2 * x], st));
+        if (stats) FC_CUDA(cudaEventRecord(ev[2 * sx], st));
         pair_f64_kernel<1><<<(unsigned)nit, 256, PR_SMEM, st>>>(a);
         FC_TRY(check_launch("pair_f64_kernel<grad>"));
-        if (stats) FC_CUDA(cudaEventRecord(ev[2 * x + 1], st));
-        reduce_pairs_kernel<<<1, 1024, 0, st>>>(part, nit, e_cp + 2 * x);
-        reduce_occ_kernel<<<(unsigned)(same ? cp.ni : cp.ni + cp.nj), 256, 0, st>>>(
-            occ, dpairs + cp.p0, cp.np, ntile2, (int)cp.i0, (int)cp.ni, (int)cp.j0, acc_occ);
-        reduce_vir_kernel<<<(unsigned)((nvir + 7) / 8), 256, 0, st>>>(vir, cp.np, ntile, (int)nvir, de_dvir);
-        FC_TRY(check_launch("rimp2 gradient reductions"));
-        FC_TRY(adjoint(T1, cp.i0, cp.ni, cp.j0, cp.nj));
-        if (!same) FC_TRY(adjoint(T2, cp.j0, cp.nj, cp.i0, cp.ni));
+        if (stats) FC_CUDA(cudaEventRecord(ev[2 * sx + 1], st));
+        ++npair_launch;
+        if (step.sums) {
+            reduce_pairs_kernel<<<1, 1024, 0, st>>>(part, nit, e_cp + 2 * x);
+            reduce_occ_kernel<<<(unsigned)(same ? cp.ni : cp.ni + cp.nj), 256, 0, st>>>(
+                occ, dpairs + cp.p0, cp.np, ntile2, (int)cp.i0, (int)cp.ni, (int)cp.j0, acc_occ);
+            reduce_vir_kernel<<<(unsigned)((nvir + 7) / 8), 256, 0, st>>>(vir, cp.np, ntile, (int)nvir, de_dvir);
+            FC_TRY(check_launch("rimp2 gradient reductions"));
+            nl += 3;
+        }
+        ++nl;
+        if (step.blk != 1) FC_TRY(adjoint(tb1, cp.i0, cp.ni, cp.j0, cp.nj));
+        if (step.blk != 0 && !same) FC_TRY(adjoint(tb2, cp.j0, cp.nj, cp.i0, cp.ni));
+        if (dens) {
+            const bool t2 = step.blk == 1;
+            const int64_t r0 = t2 ? cp.j0 : cp.i0, nr = t2 ? cp.nj : cp.ni, nk = t2 ? cp.ni : cp.nj;
+            FC_TRY(dens_f64_block(dx, r0 * nvir, nr, nk, st, &nl));
+            if (step.last) FC_TRY(dens_f64_slab(dx, nk, st, &nl));
+        }
         // row I of the chunk pairs is done: Gamma's columns of chunk I are final
-        if (sink && cp.j0 + cp.nj == nocc) FC_TRY(gamma_sink_block(sink, gamma, naux, nov, nvir, cp.i0, cp.ni, st));
+        if (!dens && sink && cp.j0 + cp.nj == nocc)
+            FC_TRY(gamma_sink_block(sink, gamma, naux, nov, nvir, cp.i0, cp.ni, st));
+    }
+    if (dens) {
+        FC_TRY(dens_f64_finish(dx, *dens, st, &nl));
+        if (sink) FC_TRY(gamma_sink_block(sink, gamma, naux, nov, nvir, 0, nocc, st));
     }
     scale_copy_f64_kernel<<<(unsigned)((nocc + 255) / 256), 256, 0, st>>>(acc_occ, nocc, -2.0, de_docc);
     FC_TRY(check_launch("scale_copy_f64_kernel"));
@@ -546,7 +605,7 @@ fc_status rimp2_grad_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, doubl
         const double P = (double)nocc * (nocc + 1) / 2.0;
         stats->flops = 2.0 * naux * (double)nvir * nvir * P + 2.0 * naux * (double)nov * nov;
         stats->precision = FC_PREC_F64;
-        stats->launches += (int)(5 * ncp + (ncp - nch) + 5);
+        stats->launches += (int)(nl + nadj + 1);
         stats->tile_m = PR_T;
         stats->tile_n = PR_T;
         stats->k_panel = 0;
@@ -554,10 +613,11 @@ fc_status rimp2_grad_f64(const Rimp2Dev& d, cudaStream_t st, double* e_os, doubl
         stats->h2d_bytes += hp.size() * sizeof(int2);
         // dominant kernel: the fused pair kernel, one launch per chunk pair,
         // forming G_ij and G_ji of every unordered pair
-        stats->main_launches = (int)ncp;
-        FC_TRY(timing_sum((int)ncp, &stats->main_ms));
-        stats->main_flops = 4.0 * naux * (double)nvir * nvir * P;
-        stats->main_bytes = 8.0 * naux * (double)nov * (double)nch + 8.0 * (double)nov * nov;
+        stats->main_launches = (int)npair_launch;
+        FC_TRY(timing_sum((int)nsteps, &stats->main_ms));
+        const double rep = dens ? (double)nsteps / ncp : 1.0;  // densities: chunk pairs run per column
+        stats->main_flops = 4.0 * naux * (double)nvir * nvir * P * rep;
+        stats->main_bytes = (8.0 * naux * (double)nov * (double)nch + 8.0 * (double)nov * nov) * rep;
         stats->aux_launches = nadj;
         FC_TRY(timing_sum2(nadj, &stats->aux_ms));
         stats->aux_flops = adj_flops;

@@ -1640,9 +1640,11 @@ fc_status rimp2_energy_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, doub
 }
 
 fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double* e_ss, double* gamma,
-                        double* de_docc, double* de_dvir, fc_stats* stats, const GammaSink* sink) {
+                        double* de_docc, double* de_dvir, fc_stats* stats, const GammaSink* sink,
+                        const DensOut* dens) {
     FC_TRY(fx_attrs());
     if (d.nocc > (1 << 15)) return fail(FC_ERR_LAYOUT, "mixed RI-MP2: nocc too large");
+    if (dens && d.nshards != 1) return fail(FC_ERR_INVALID, "RI-MP2 densities: no sharded form");
     const int64_t nocc = d.nocc, nvir = d.nvir, naux = d.naux, nov = nocc * nvir;
     Context& c = ctx();
     FxSplit sp;
@@ -1663,15 +1665,21 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
     // occupied chunks: a chunk pair (I, J), I <= J, holds the amplitude rows of
     // I (columns of J) and of J (columns of I) in FP32, plus the slices of one
     // of them; each unordered pair (i, j) is computed once and feeds both.
-    const int64_t cc = grad_chunk_fx(nocc, nvir, d.chunk_bytes, d.nshards);
+    // with densities the chunk is also bounded by the slab budget (four
+    // chunk budgets: the slabs are the densities' whole working set)
+    const int64_t cc = dens ? dens_chunk_fx(nocc, nvir, grad_chunk_fx(nocc, nvir, d.chunk_bytes, 1),
+                                            4 * d.chunk_bytes)
+                            : grad_chunk_fx(nocc, nvir, d.chunk_bytes, d.nshards);
     const int64_t nch = (nocc + cc - 1) / cc;
     struct CP {
         int64_t i0, ni, j0, nj, p0, np;
     };
     std::vector<CP> cps;
     std::vector<int2> pairs;
+    std::vector<int64_t> cp_index((size_t)(nch * nch), -1);  // [I][J], I <= J
     for (int64_t I = 0; I < nch; ++I)
         for (int64_t J = I; J < nch; ++J) {
+            cp_index[(size_t)(I * nch + J)] = (int64_t)cps.size();
             CP x;
             x.i0 = I * cc;
             x.ni = std::min(cc, nocc - x.i0);
@@ -1690,6 +1698,28 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
     const std::vector<int> owner = chunk_pair_owner(nocc, cc, d.nshards);
     int64_t max_items = 0;
     for (const auto& x : cps) max_items = std::max(max_items, x.np * ntiles);
+    // The run order.  Gradient: each chunk pair once, both of its amplitude
+    // blocks.  Densities: by column chunk K, the block (I, K) of every I from
+    // chunk pair (min, max) -- T (rows of its first chunk) when I <= K, T2
+    // otherwise; the energy and dE/deps terms of a chunk pair are taken at
+    // its I <= K visit.  The slab of K is complete after its last step.
+    struct Step {
+        int64_t x;
+        int blk;    // 0: T, 1: T2, 2: both
+        bool sums;  // take the chunk pair's energy and dE/deps terms
+        bool last;  // last block of the column chunk
+    };
+    std::vector<Step> steps;
+    if (!dens) {
+        for (int64_t x = 0; x < ncp; ++x) steps.push_back({x, 2, true, false});
+    } else {
+        for (int64_t K = 0; K < nch; ++K)
+            for (int64_t I = 0; I < nch; ++I)
+                steps.push_back({cp_index[(size_t)(std::min(I, K) * nch + std::max(I, K))], I <= K ? 0 : 1, I <= K,
+                                 I == nch - 1});
+    }
+    DensFx dx{};
+    if (dens) FC_TRY(dens_fx_alloc(nocc, nvir, tp, cc, st, &dx));
 
     void *vbq, *vtab, *vT, *vTs, *vpart;
     const size_t tab_bytes = ((pairs.size() * sizeof(int2) + 255) / 256) * 256;
@@ -1753,7 +1783,10 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
     const int2* dtiles = dpairs + npairs_all;
 
     cudaEvent_t* ev = nullptr;
-    if (stats) FC_TRY(timing_events((int)ncp, &ev));
+    const int64_t nsteps = (int64_t)steps.size();
+    int64_t npair_launch = 0;
+    double pair_flops = 0.0;
+    if (stats) FC_TRY(timing_events((int)nsteps, &ev));
     // K segment of the adjoint contraction: fx::KMAX, or FERRIC_CUDA_KSEG (a
     // positive multiple of fx::KT up to fx::KMAX; tests use short segments)
     int64_t kseg = fx::KMAX;
@@ -1766,18 +1799,23 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
     cudaEvent_t* ev2 = nullptr;
     int nadj = 0;
     double adj_flops = 0.0, adj_bytes = 0.0;
-    if (stats) FC_TRY(timing_events2((int)(2 * ncp * ((cc * tp + kseg - 1) / kseg)), &ev2));
+    if (stats) FC_TRY(timing_events2((int)(2 * nsteps * ((cc * tp + kseg - 1) / kseg)), &ev2));
     // Gamma[:, rows] += 4 Bq[:, cols] T^T for one amplitude block
+    // (with densities the slices go to the block's rows of the column chunk's
+    // slab, slices nocc tp rows apart, and stay there for the density terms)
     auto adjoint = [&](float* T, int64_t r0, int64_t nr, int64_t k0, int64_t nk) -> fc_status {
         const int64_t ldk = nk * tp, rows = nr * tp, mp = (rows + 127) / 128 * 128;
-        split_fx_rows_f32_kernel<<<(unsigned)rows, 256, 0, st>>>(T, ldk, mp, ts, (int8_t*)vTs);
+        const int64_t sstride = dens ? dx.rows : mp;  // rows between slices
+        int8_t* sl = dens ? dx.ts + r0 * tp * ldk : (int8_t*)vTs;
+        double* rsc = dens ? dx.tsc + r0 * tp : ts;
+        split_fx_rows_f32_kernel<<<(unsigned)rows, 256, 0, st>>>(T, ldk, sstride, rsc, sl);
         ++nl;
         CUtensorMap tmTs;
-        FC_TRY(make_tmap_i8_2d(&tmTs, vTs, ldk, 3 * mp, ldk, fx::KT, 128));
+        FC_TRY(make_tmap_i8_2d(&tmTs, sl, ldk, 3 * sstride - (dens ? r0 * tp : 0), ldk, fx::KT, 128));
         GemmFxArgs g{};
-        g.rs = ts;
+        g.rs = rsc;
         g.cs = qs + (k0 / cc) * q_rows;  // the Q-row scales of the column chunk
-        g.M = (int)mp;
+        g.M = (int)sstride;
         g.N = (int)q_rows;
         g.nTm = (int)(mp / 128);
         g.rows = (int)rows;
@@ -1814,13 +1852,15 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
                      16.0 * (double)naux * (double)(nr * nvir);
         return FC_OK;
     };
-    for (int64_t x = 0; x < ncp; ++x) {
+    for (size_t sx = 0; sx < steps.size(); ++sx) {
+        const Step& step = steps[sx];
+        const int64_t x = step.x;
         const CP& cp = cps[x];
         const bool same = cp.i0 == cp.j0;
         if (owner[x] != d.shard) {
             if (stats) {
-                FC_CUDA(cudaEventRecord(ev[2 * x], st));
-                FC_CUDA(cudaEventRecord(ev[2 * x + 1], st));
+                FC_CUDA(cudaEventRecord(ev[2 * sx], st));
+                FC_CUDA(cudaEventRecord(ev[2 * sx + 1], st));
             }
             continue;
         }
@@ -1857,27 +1897,45 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
         a.vir_part = vir_part;
         const int grid = (int)(a.items < c.sm_count ? a.items : c.sm_count);
         FC_TRY(pair_scratch(grid, &a.scr));
-        if (stats) FC_CUDA(cudaEventRecord(ev[2 * x], st));
+        if (stats) FC_CUDA(cudaEventRecord(ev[2 * sx], st));
         pair_fx_kernel<1><<<grid, fx::PAIR_THREADS, fx::SMEM, st>>>(sp.tmA, sp.tmB, a);
         FC_TRY(check_launch("pair_fx_kernel<grad>"));
-        if (stats) FC_CUDA(cudaEventRecord(ev[2 * x + 1], st));
-        fx_reduce_pairs_kernel<<<1, 1024, 0, st>>>(part, a.items, e_cp + 2 * x);
-        fx_reduce_occ_kernel<<<(unsigned)(same ? cp.ni : cp.ni + cp.nj), 256, 0, st>>>(
-            occ_part, dpairs + cp.p0, cp.np, ntiles, (int)cp.i0, (int)cp.ni, (int)cp.j0, acc_occ);
-        {
-            const int nchunk = (int)std::min<int64_t>(vir_chunks, cp.np);
-            const int64_t ppc = (cp.np + nchunk - 1) / nchunk;
-            fx_reduce_vir_part_kernel<<<dim3((unsigned)nTa, (unsigned)nchunk), 128, 0, st>>>(
-                vir_part, dpairs + cp.p0, cp.np, nTa, ntiles, ppc, vir_fold);
-            fx_reduce_vir_fold_kernel<<<(unsigned)((nvir + 127) / 128), 128, 0, st>>>(vir_fold, nchunk, nTa,
-                                                                                       (int)nvir, de_dvir);
+        if (stats) FC_CUDA(cudaEventRecord(ev[2 * sx + 1], st));
+        ++npair_launch;
+        pair_flops += 2.0 * naux * (double)nvir * nvir * (double)cp.np;
+        if (step.sums) {
+            fx_reduce_pairs_kernel<<<1, 1024, 0, st>>>(part, a.items, e_cp + 2 * x);
+            fx_reduce_occ_kernel<<<(unsigned)(same ? cp.ni : cp.ni + cp.nj), 256, 0, st>>>(
+                occ_part, dpairs + cp.p0, cp.np, ntiles, (int)cp.i0, (int)cp.ni, (int)cp.j0, acc_occ);
+            {
+                const int nchunk = (int)std::min<int64_t>(vir_chunks, cp.np);
+                const int64_t ppc = (cp.np + nchunk - 1) / nchunk;
+                fx_reduce_vir_part_kernel<<<dim3((unsigned)nTa, (unsigned)nchunk), 128, 0, st>>>(
+                    vir_part, dpairs + cp.p0, cp.np, nTa, ntiles, ppc, vir_fold);
+                fx_reduce_vir_fold_kernel<<<(unsigned)((nvir + 127) / 128), 128, 0, st>>>(vir_fold, nchunk, nTa,
+                                                                                           (int)nvir, de_dvir);
+            }
+            FC_TRY(check_launch("gradient reductions"));
+            nl += 4;  // the four reductions
         }
-        FC_TRY(check_launch("gradient reductions"));
-        nl += 5;  // pair kernel and its four reductions
-        FC_TRY(adjoint(T1, cp.i0, cp.ni, cp.j0, cp.nj));
-        if (!same) FC_TRY(adjoint(T2, cp.j0, cp.nj, cp.i0, cp.ni));
+        ++nl;  // the pair kernel
+        if (step.blk != 1) FC_TRY(adjoint(T1, cp.i0, cp.ni, cp.j0, cp.nj));
+        if (step.blk != 0 && !same) FC_TRY(adjoint(T2, cp.j0, cp.nj, cp.i0, cp.ni));
+        if (dens) {
+            // the block (I, K) of the column chunk K: t and its slices, and
+            // the slab's density terms once the column is complete
+            const bool t2 = step.blk == 1;
+            const int64_t r0 = t2 ? cp.j0 : cp.i0, nr = t2 ? cp.nj : cp.ni, nk = t2 ? cp.ni : cp.nj;
+            FC_TRY(dens_fx_block(dx, t2 ? T2 : T1, r0 * tp, nr, nk, st, &nl));
+            if (step.last) FC_TRY(dens_fx_slab(dx, nk, st, flags + 1, &nl));
+        }
         // row I of the chunk pairs is done: Gamma's columns of chunk I are final
-        if (sink && cp.j0 + cp.nj == nocc) FC_TRY(gamma_sink_block(sink, gamma, naux, nov, nvir, cp.i0, cp.ni, st));
+        if (!dens && sink && cp.j0 + cp.nj == nocc)
+            FC_TRY(gamma_sink_block(sink, gamma, naux, nov, nvir, cp.i0, cp.ni, st));
+    }
+    if (dens) {
+        FC_TRY(dens_fx_finish(dx, *dens, st, &nl));
+        if (sink) FC_TRY(gamma_sink_block(sink, gamma, naux, nov, nvir, 0, nocc, st));
     }
     scale_copy_kernel<<<(unsigned)((nocc + 255) / 256), 256, 0, st>>>(acc_occ, nocc, -2.0, de_docc);
     ++nl;
@@ -1912,16 +1970,18 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
         stats->launches += (int)nl;
         stats->tile_m = fx::BM;
         stats->tile_n = fx::BN;
-        stats->main_launches = (int)ncp;
+        stats->main_launches = (int)npair_launch;
         double tsum = 0.0;
-        for (int64_t x = 0; x < ncp; ++x) {
+        for (int64_t x = 0; x < nsteps; ++x) {
             float t = 0.f;
             FC_CUDA(cudaEventElapsedTime(&t, ev[2 * x], ev[2 * x + 1]));
             tsum += t;
         }
         stats->main_ms = tsum;
-        stats->main_flops = 2.0 * naux * (double)nvir * nvir * P;  // G_ij over unordered pairs
-        stats->main_bytes = 8.0 * naux * (double)nov * (double)nch;
+        // G_ij over unordered pairs (with densities: over the pairs launched,
+        // off-diagonal chunk pairs twice)
+        stats->main_flops = dens ? pair_flops : 2.0 * naux * (double)nvir * nvir * P;
+        stats->main_bytes = 8.0 * naux * (double)nov * (double)nch * (dens ? (double)nsteps / ncp : 1.0);
         stats->aux_launches = nadj;
         FC_TRY(timing_sum2(nadj, &stats->aux_ms));
         stats->aux_flops = adj_flops;

@@ -20,6 +20,14 @@
 // int8 form's panels (1024 of K) are far inside its int32 range
 // (3 * 127^2 * 1024 < 2^26) and combine as L0 + L1 / 254 + L2 / 254^2.
 //
+// Where an item's rows are is the loader policy's (Ld): LdTiles takes the
+// m-tile / n-tile of a 2-D map per slice; LdRows takes first rows it.x / it.y
+// directly (tiles at any row); LdPlanes takes one row (it.z) of each of 128
+// planes of a 3-D map (rows strided by a plane: the occupied index of an
+// amplitude slab at fixed virtual).  LdRows and LdPlanes are int8 only and
+// let a panel run 256 k-steps: 3 * 127^2 * 32768 < 2^31 keeps every int32
+// level sum exact, so one drain per item suffices for K <= 32768.
+//
 // Roles: warp 0 TMA producer, warp 1 UMMA issuer, warps 2 .. 2 + BN/8 - 1
 // epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (its rows) and
 // columns 32 ((w - 2) / 4) .. + 31 of each level.  With BN = 64 two
@@ -64,21 +72,55 @@ struct Cfg {
 }  // namespace xg
 
 struct XArgs {
-    const int4* items;  // (m-tile, n-tile, first k-step, k-steps)
+    const int4* items;  // (m-tile, n-tile, first k-step, k-steps) for LdTiles
     int64_t nitems;
-    int Ma, Nb;  // rows between the slices of the A and B tensor maps
+    int Ma, Nb;  // rows (LdPlanes: planes) between the slices of the A and B tensor maps
     int* err;
+};
+
+struct LdTiles {
+    static constexpr int KP = xg::KP;
+    __device__ static int k0(int4 it) { return it.z; }
+    template <int BN, int KTE>
+    __device__ static void load(void* da, void* db, const CUtensorMap* ta, const CUtensorMap* tb, uint64_t* bar,
+                                const XArgs& p, int4 it, int kt, int sl) {
+        tc::tma_load_2d(da, ta, bar, kt * KTE, sl * p.Ma + it.x * xg::BM);
+        tc::tma_load_2d(db, tb, bar, kt * KTE, sl * p.Nb + it.y * BN);
+    }
+};
+
+struct LdRows {  // item (A row, B row, first k-step, k-steps)
+    static constexpr int KP = 256;
+    __device__ static int k0(int4 it) { return it.z; }
+    template <int BN, int KTE>
+    __device__ static void load(void* da, void* db, const CUtensorMap* ta, const CUtensorMap* tb, uint64_t* bar,
+                                const XArgs& p, int4 it, int kt, int sl) {
+        tc::tma_load_2d(da, ta, bar, kt * KTE, sl * p.Ma + it.x);
+        tc::tma_load_2d(db, tb, bar, kt * KTE, sl * p.Nb + it.y);
+    }
+};
+
+struct LdPlanes {  // item (A plane tile, B plane tile, row in every plane, k-steps from 0)
+    static constexpr int KP = 256;
+    __device__ static int k0(int4) { return 0; }
+    template <int BN, int KTE>
+    __device__ static void load(void* da, void* db, const CUtensorMap* ta, const CUtensorMap* tb, uint64_t* bar,
+                                const XArgs& p, int4 it, int kt, int sl) {
+        tc::tma_load_3d(da, ta, bar, kt * KTE, it.z, sl * p.Ma + it.x * xg::BM);
+        tc::tma_load_3d(db, tb, bar, kt * KTE, it.z, sl * p.Nb + it.y * BN);
+    }
 };
 
 // Epi: __device__ void operator()(int64_t item, int4 it, int row, int col0,
 //                                 const double (&acc)[32]) const
-template <int BN, class Epi, bool I8 = false>
+template <int BN, class Epi, bool I8 = false, class Ld = LdTiles>
 __global__ void __launch_bounds__(xg::Cfg<BN, I8>::THREADS, 1)
     xgemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const XArgs p,
                  const Epi epi) {
     using C = xg::Cfg<BN, I8>;
     using namespace xg;
-    constexpr int S = C::STAGES, NS = C::NSET;
+    constexpr int S = C::STAGES, NS = C::NSET, KP = Ld::KP;
+    static_assert(I8 || KP == xg::KP, "FP32 level sums are exact over 8 k-steps only");
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw_u32 = smem_u32(smem_raw);
     const uint32_t base_u32 = (raw_u32 + 1023u) & ~1023u;
@@ -126,18 +168,16 @@ __global__ void __launch_bounds__(xg::Cfg<BN, I8>::THREADS, 1)
             uint32_t g = 0;
             for (int64_t t = blockIdx.x; t < p.nitems && !*abort_flag; t += gridDim.x) {
                 const int4 it = p.items[t];
-                for (int kt = it.z; kt < it.z + it.w; ++kt, ++g) {
+                const int kb = Ld::k0(it);
+                for (int kt = kb; kt < kb + it.w; ++kt, ++g) {
                     const int s = g % S;
                     const uint32_t u = g / S;
                     if (!tc::mbar_wait(&empty[s], (u & 1) ^ 1, abort_flag, p.err)) goto prod_done;
                     tc::mbar_arrive_expect_tx(&full[s], C::STAGE);
 #pragma unroll
-                    for (int sl = 0; sl < 3; ++sl) {
-                        tc::tma_load_2d(base + (sa(s, sl) - base_u32), &tmA, &full[s], kt * C::KTE,
-                                        sl * p.Ma + it.x * BM);
-                        tc::tma_load_2d(base + (sb(s, sl) - base_u32), &tmB, &full[s], kt * C::KTE,
-                                        sl * p.Nb + it.y * BN);
-                    }
+                    for (int sl = 0; sl < 3; ++sl)
+                        Ld::template load<BN, C::KTE>(base + (sa(s, sl) - base_u32), base + (sb(s, sl) - base_u32),
+                                                      &tmA, &tmB, &full[s], p, it, kt, sl);
                 }
             }
         prod_done:

@@ -11,7 +11,10 @@ Mirrors, with the same argument meaning:
   the plain form raises :class:`FcError`.
 * ``Mp2Intermediates::from_ri_densities`` inputs (rimp2.rs:1841-1883):
   :func:`rimp2_energy_grad` returns ``Gamma = dE/dB = 4 x_ov`` and
-  ``dE/d eps`` (``2 diag(P_oo)``, ``2 diag(P_vv)``) without storing amplitudes.
+  ``dE/d eps`` (``2 diag(P_oo)``, ``2 diag(P_vv)``) without storing amplitudes;
+  :func:`rimp2_energy_grad_dens` adds the full unrelaxed ``P_oo`` / ``P_vv``
+  of ``build_mp2_density`` (ferric-mp2/src/oo_rimp2.rs:1170-1300), and
+  :func:`ri_densities` returns exactly ``(x_ov, p_oo, p_vv, e_corr)``.
 
 Inputs may be NumPy arrays (host API: the library copies) or CUDA torch
 tensors (device API on torch's current stream).
@@ -174,12 +177,49 @@ def rimp2_energy_grad(b_ov, eps_occ, eps_vir, precision="f64", stats=None, out=N
     return SpinComponents(eo.value, es.value, eo.value + es.value), gamma, d_o, d_v
 
 
+def rimp2_energy_grad_dens(b_ov, eps_occ, eps_vir, precision="f64", stats=None):
+    """``(SpinComponents, gamma, de_docc, de_dvir, p_oo, p_vv)``: as
+    :func:`rimp2_energy_grad` plus the unrelaxed MP2 densities
+    ``p_oo[i, j] = -sum_kab t_ik^ab (2 t_jk^ab - t_jk^ba)`` and
+    ``p_vv[a, b] = sum_ijc t_ij^ac (2 t_ij^bc - t_ij^cb)``
+    (build_mp2_density, ferric-mp2/src/oo_rimp2.rs:1170-1300)."""
+    _lib.ensure_init()
+    nocc, nvir = int(eps_occ.shape[0]), int(eps_vir.shape[0])
+    naux = int(b_ov.shape[0])
+    if b_ov.shape[1] != nocc * nvir:
+        raise ValueError(f"b_ov has {b_ov.shape[1]} columns, expected nocc*nvir = {nocc * nvir}")
+    eo, es = ctypes.c_double(), ctypes.c_double()
+    st = FcStats()
+    prec = _precision(precision)
+    if _is_torch_cuda(b_ov):
+        import torch
+        b, o, v = (t.contiguous() for t in (b_ov, eps_occ, eps_vir))
+        gamma, d_o, d_v = torch.empty_like(b), torch.empty_like(o), torch.empty_like(v)
+        p_oo = torch.empty((nocc, nocc), dtype=torch.float64, device=b.device)
+        p_vv = torch.empty((nvir, nvir), dtype=torch.float64, device=b.device)
+        check(_lib.lib.fc_rimp2_energy_grad_dens_dev(
+            ptr(b), naux, nocc, nvir, ptr(o), ptr(v), prec, ctypes.byref(eo), ctypes.byref(es),
+            ptr(gamma), ptr(d_o), ptr(d_v), ptr(p_oo), ptr(p_vv), _stream_of(b), ctypes.byref(st)))
+    else:
+        b = np.ascontiguousarray(b_ov, dtype=np.float64)
+        o = np.ascontiguousarray(eps_occ, dtype=np.float64)
+        v = np.ascontiguousarray(eps_vir, dtype=np.float64)
+        gamma, d_o, d_v = np.empty_like(b), np.empty(nocc), np.empty(nvir)
+        p_oo, p_vv = np.empty((nocc, nocc)), np.empty((nvir, nvir))
+        check(_lib.lib.fc_rimp2_energy_grad_dens(
+            ptr(b), naux, nocc, nvir, ptr(o), ptr(v), prec, ctypes.byref(eo), ctypes.byref(es),
+            ptr(gamma), ptr(d_o), ptr(d_v), ptr(p_oo), ptr(p_vv), ctypes.byref(st)))
+    if stats is not None:
+        stats.update(st.as_dict())
+    return SpinComponents(eo.value, es.value, eo.value + es.value), gamma, d_o, d_v, p_oo, p_vv
+
+
 def ri_densities(b_ov, eps_occ, eps_vir, precision="f64"):
-    """``(x_ov, de_docc, de_dvir, e_corr)``: the inputs
-    ``Mp2Intermediates::from_ri_densities`` takes (rimp2.rs:1841-1883), with
-    ``x_ov = Gamma / 4``; the P diagonals enter as ``dE/deps / 2``."""
-    sc, gamma, d_o, d_v = rimp2_energy_grad(b_ov, eps_occ, eps_vir, precision)
-    return gamma / 4.0, d_o, d_v, sc.e_total
+    """``(x_ov, p_oo, p_vv, e_corr)``: the arguments
+    ``Mp2Intermediates::from_ri_densities`` takes after ``rpa``
+    (rimp2.rs:1841-1883), with ``x_ov = Gamma / 4``."""
+    sc, gamma, _, _, p_oo, p_vv = rimp2_energy_grad_dens(b_ov, eps_occ, eps_vir, precision)
+    return gamma / 4.0, p_oo, p_vv, sc.e_total
 
 
 def ump2_energy(b_a, eps_occ_a, eps_vir_a, b_b, eps_occ_b, eps_vir_b, precision="f64", stats=None):

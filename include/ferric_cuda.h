@@ -138,6 +138,28 @@ fc_status fc_rimp2_energy_grad_dev(const double* b_ov, int64_t naux, int64_t noc
                                    double* de_docc, double* de_dvir, void* stream,
                                    fc_stats* stats);
 
+/* The gradient call plus the full unrelaxed MP2 densities the reference's
+ * gradient chain takes (build_mp2_density, ferric-mp2/src/oo_rimp2.rs:
+ * 1170-1300; Mp2Intermediates::from_ri_densities, ferric-mp2/src/rimp2.rs:
+ * 1841-1883, with x_ov = gamma / 4):
+ *   p_oo[i*nocc + j] = -sum_kab t_ik^ab (2 t_jk^ab - t_jk^ba)   (nocc x nocc)
+ *   p_vv[a*nvir + b] =  sum_ijc t_ij^ac (2 t_ij^bc - t_ij^cb)   (nvir x nvir)
+ * row-major and symmetric.  Amplitudes are still not stored: occupied-pair
+ * blocks are recomputed per column chunk (the chunk pairs off the diagonal
+ * twice) and each column's blocks are held as one slab (FC_PREC_MIXED: int8
+ * slices of t and 2t - t^T, 6 B per element; FC_PREC_F64: 16 B per
+ * element), at most four chunk budgets.  Otherwise as fc_rimp2_energy_grad /
+ * _dev (gamma, de_docc, de_dvir as there). */
+fc_status fc_rimp2_energy_grad_dens(const double* b_ov, int64_t naux, int64_t nocc, int64_t nvir,
+                                    const double* eps_occ, const double* eps_vir, int32_t precision,
+                                    double* e_os, double* e_ss, double* gamma, double* de_docc,
+                                    double* de_dvir, double* p_oo, double* p_vv, fc_stats* stats);
+fc_status fc_rimp2_energy_grad_dens_dev(const double* b_ov, int64_t naux, int64_t nocc, int64_t nvir,
+                                        const double* eps_occ, const double* eps_vir, int32_t precision,
+                                        double* e_os, double* e_ss, double* gamma, double* de_docc,
+                                        double* de_dvir, double* p_oo, double* p_vv, void* stream,
+                                        fc_stats* stats);
+
 /* One system over nshards processes (one GPU each), partitioned by occupied
  * pairs.  The reference's MPI RI-MP2 (ferric-mp2/src/mpi_rimp2.rs:16-43)
  * cuts aux bands and all-reduces per-i intermediates; here every process
