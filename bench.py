@@ -464,6 +464,45 @@ def c5_leg(torch, dev, prec, steps=3):
     return out
 
 
+def dens_leg(torch, dev, prec):
+    """The gradient call with the full unrelaxed densities P_oo / P_vv at the
+    config-3 RI-MP2 shapes: device time against the gradient call alone (one
+    warm-up, then one timed call of each), and the densities' own checks at
+    full size (2 diag P against the pair kernel's dE/deps, symmetry)."""
+    from ferric_b200 import rimp2
+    inp = make_inputs(torch, dev, RIMP2, None)
+    stream = torch.cuda.current_stream(dev)
+    out = {"rimp2": RIMP2, "precision": prec}
+    for name in ("grad", "grad_dens", "grad_dens_timed", "grad_timed"):
+        dens = "dens" in name
+        st = {}
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        if dens:
+            sc, g, d_o, d_v, p_oo, p_vv = rimp2.rimp2_energy_grad_dens(inp["b_ov"], inp["eo"], inp["ev"],
+                                                                       precision=prec, stats=st)
+        else:
+            sc, g, d_o, d_v = rimp2.rimp2_energy_grad(inp["b_ov"], inp["eo"], inp["ev"], precision=prec, stats=st)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if name.endswith("timed"):
+            key = "grad_dens" if dens else "grad"
+            out[key] = {"ms": e0.elapsed_time(e1), "kernel_ms": st["kernel_ms"], "pair_launches": st["main_launches"],
+                        "pair_kernel_ms": st["main_ms"], "adjoint_ms": st["aux_ms"]}
+            if dens:
+                out["checks"] = {
+                    "diag_oo_vs_de_docc_rel": float((2.0 * torch.diagonal(p_oo) - d_o).abs().max() / d_o.abs().max()),
+                    "diag_vv_vs_de_dvir_rel": float((2.0 * torch.diagonal(p_vv) - d_v).abs().max() / d_v.abs().max()),
+                    "symmetric": bool(torch.equal(p_oo, p_oo.T) and torch.equal(p_vv, p_vv.T)),
+                    "e_total": sc.e_total}
+        del g
+    out["overhead_vs_grad"] = out["grad_dens"]["ms"] / out["grad"]["ms"]
+    del inp
+    torch.cuda.empty_cache()
+    return out
+
+
 def max_over_ranks(torch, ms, world, dev):
     """The slowest rank's device time: every rank takes part in one MAX all-reduce."""
     if world <= 1:
@@ -492,6 +531,7 @@ def main():
     ap.add_argument("--batch-mols", type=int, default=512)
     ap.add_argument("--no-dress", action="store_true", help="skip the MO-dressing leg")
     ap.add_argument("--no-c5", action="store_true", help="skip the config-5 leg")
+    ap.add_argument("--no-dens", action="store_true", help="skip the densities leg")
     ap.add_argument("--size", choices=["full", "small", "c5"], default="full",
                     help="small: naux 2400, nocc 60, nvir 550 + n 300, naux 1200, nocc 30 "
                          "(the profiling case; inputs still larger than L2); c5: the shapes of "
@@ -775,6 +815,11 @@ def main():
     if prec == "mixed" and args.size == "full" and not args.no_c5:
         c5 = c5_leg(torch, dev, prec)
 
+    # ---- the gradient with the full densities, config-3 RI-MP2 shapes
+    dens = None
+    if prec == "mixed" and args.size == "full" and not args.no_dens:
+        dens = dens_leg(torch, dev, prec)
+
     # ---- config 4: batched RI-MP2 E+grad over 512 molecules of uneven size
     batch = None
     if prec == "mixed" and not args.no_batch:
@@ -801,7 +846,7 @@ def main():
             "roofline": roofline, "roofline_kernels": rooflines, "roofline_dfj": roof_dfj, "roofline_dfk": roof_dfk,
             "plain_f64": plain,
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
-            "config4_batch": batch, "config5": c5, "mo_dressing": dress,
+            "config4_batch": batch, "config5": c5, "mo_dressing": dress, "densities": dens,
         }
         print(json.dumps(out))
     if world > 1:

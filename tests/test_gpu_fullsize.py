@@ -205,3 +205,29 @@ def test_dfjk_config2_matches_oracle(fc):
         print(f"config 2 {prec}: max|dJ| {dj:.3e} (|J| {np.abs(j_ref).max():.3f}), "
               f"max|dK| {dk:.3e} (|K| {np.abs(k_ref).max():.3f})")
         assert dj <= jb and dk <= kb
+
+
+def test_rimp2_config3_densities(fc):
+    """P_oo / P_vv at config 3: mixed against the FP64 plain densities (both
+    from the column-chunk schedule), and for each 2 diag P against the pair
+    kernel's own dE/deps (oo_rimp2.rs:1170-1191), symmetric by construction;
+    Gamma and E are the gradient call's."""
+    import torch
+    from ferric_b200 import rimp2
+    b, eo, ev = _rimp2_inputs(torch)
+    res = {}
+    for prec in ("mixed", "f64"):
+        sc, g, d_o, d_v, p_oo, p_vv = rimp2.rimp2_energy_grad_dens(b, eo, ev, precision=prec)
+        assert torch.equal(p_oo, p_oo.T) and torch.equal(p_vv, p_vv.T)
+        tol = 1e-12 if prec == "f64" else 1e-6
+        assert float((2.0 * torch.diagonal(p_oo) - d_o).abs().max()) <= tol * float(d_o.abs().max())
+        assert float((2.0 * torch.diagonal(p_vv) - d_v).abs().max()) <= tol * float(d_v.abs().max())
+        res[prec] = (sc, p_oo.cpu().numpy(), p_vv.cpu().numpy())
+        del g
+    (sm, mo, mv), (sf, fo, fv) = res["mixed"], res["f64"]
+    eo_rel = np.abs(mo - fo).max() / np.abs(fo).max()
+    ev_rel = np.abs(mv - fv).max() / np.abs(fv).max()
+    print(f"config-3 densities: mixed vs FP64 max rel P_oo {eo_rel:.3e} P_vv {ev_rel:.3e}; "
+          f"E {sm.e_total - sf.e_total:.3e}")
+    assert eo_rel <= 1e-6 and ev_rel <= 1e-6
+    assert abs(sm.e_total - sf.e_total) <= 1e-6
