@@ -38,6 +38,10 @@ SIGNATURES = {
     "fc_rimp2_energy_dev": (_I32, [_P, _I64, _I64, _I64, _P, _P, _I32, _D, _I32, _DP, _DP, _P, _P]),
     "fc_rimp2_energy_grad": (_I32, [_P, _I64, _I64, _I64, _P, _P, _I32, _DP, _DP, _P, _P, _P, _P]),
     "fc_rimp2_energy_grad_dev": (_I32, [_P, _I64, _I64, _I64, _P, _P, _I32, _DP, _DP, _P, _P, _P, _P, _P]),
+    "fc_rimp2_response_2c": (_I32, [_P, _P, _P, _I64, _I64, _D, _P, _P, _P]),
+    "fc_rimp2_response_2c_dev": (_I32, [_P, _P, _P, _I64, _I64, _D, _P, _P, _P, _P]),
+    "fc_rimp2_response_3c": (_I32, [_P, _P, _P, _I64, _I64, _I64, _I64, _I64, _I64, _D, _P, _P]),
+    "fc_rimp2_response_3c_dev": (_I32, [_P, _P, _P, _I64, _I64, _I64, _I64, _I64, _I64, _D, _P, _P, _P]),
     "fc_rimp2_energy_grad_dens": (_I32, [_P, _I64, _I64, _I64, _P, _P, _I32, _DP, _DP, _P, _P, _P, _P, _P, _P]),
     "fc_rimp2_energy_grad_dens_dev": (_I32, [_P, _I64, _I64, _I64, _P, _P, _I32, _DP, _DP, _P, _P, _P, _P, _P, _P,
                                              _P]),

@@ -1,8 +1,10 @@
-// All-FP64 "TN" tile GEMM on the DMMA tensor path:
-//     value(m, n) = sum_{k in split} A[m*lda + k] * B[n*ldb + k]
-// with both operands K-major (row-major M x K and N x K) and a functor
+// All-FP64 tile GEMM on the DMMA tensor path:
+//     value(m, n) = sum_{k in split} A(m, k) * B(n, k)
+// with each operand K-major (row-major M x K and N x K, the default "TN"
+// form) or, with TA / TB, MN-major (stored K x M / K x N), and a functor
 // epilogue, so one kernel serves the gradient's second contraction
-// (Gamma = 4 B_ov Tt^T), the DF-K half-transform and the DF-K rank update.
+// (Gamma = 4 B_ov Tt^T), the DF-K half-transform and rank update, the MP2
+// densities and the RI response products.
 //
 // Tile 128 x 64 x 16, 8 warps (4 x 2), each warp 32 x 32 = 4 x 4 DMMA tiles;
 // 3-stage cp.async pipeline; split-K over blockIdx.z.  Shared-memory rows are
@@ -15,11 +17,14 @@ namespace fc {
 constexpr int DG_BM = 128, DG_BN = 64, DG_BK = 16, DG_LDK = 20, DG_STAGES = 3;
 constexpr int DG_SMEM = DG_STAGES * (DG_BM + DG_BN) * DG_LDK * 8;
 
-template <class Epi>
-__global__ void __launch_bounds__(256) dgemm_tn_kernel(const double* __restrict__ A, int64_t lda,
-                                                       const double* __restrict__ B, int64_t ldb,
-                                                       int M, int N, int64_t K, int64_t k_per_split,
-                                                       int upper_only, Epi epi) {
+// The tile body.  A(m, k) = TA ? A[k*lda + m] : A[m*lda + k], and B(n, k) the
+// same with TB: a transposed (MN-major) operand is read with consecutive
+// threads on consecutive m (n), so its global loads stay coalesced.  The
+// epilogue gets `z` (the split or the batch index).
+template <class Epi, bool TA, bool TB>
+__device__ __forceinline__ void dgemm_tile(const double* __restrict__ A, int64_t lda, const double* __restrict__ B,
+                                           int64_t ldb, int M, int N, int64_t kbeg, int64_t kend, int upper_only,
+                                           const Epi& epi, int z) {
     extern __shared__ __align__(16) double dg_smem[];
     double* sA = dg_smem;                                   // [STAGES][BM][LDK]
     double* sB = dg_smem + DG_STAGES * DG_BM * DG_LDK;      // [STAGES][BN][LDK]
@@ -29,8 +34,6 @@ __global__ void __launch_bounds__(256) dgemm_tn_kernel(const double* __restrict_
     const int wm = warp & 3, wn = warp >> 2;
     const int m0 = blockIdx.y * DG_BM, n0 = blockIdx.x * DG_BN;
     if (upper_only && m0 > n0 + DG_BN - 1) return;  // tile strictly below the diagonal
-    const int64_t kbeg = (int64_t)blockIdx.z * k_per_split;
-    const int64_t kend = kbeg + k_per_split < K ? kbeg + k_per_split : K;
     if (kbeg >= kend) return;
     const int nk = (int)((kend - kbeg + DG_BK - 1) / DG_BK);
 
@@ -40,19 +43,21 @@ __global__ void __launch_bounds__(256) dgemm_tn_kernel(const double* __restrict_
         double* b = sB + stage * DG_BN * DG_LDK;
 #pragma unroll
         for (int e = 0; e < (DG_BM * DG_BK) / 256; ++e) {
-            const int idx = tid + 256 * e, row = idx >> 4, kk = idx & 15;
+            const int idx = tid + 256 * e;
+            const int row = TA ? idx % DG_BM : idx >> 4, kk = TA ? idx / DG_BM : idx & 15;
             const int gm = m0 + row;
             const int64_t gk = kb + kk;
             const bool ok = gm < M && gk < kend;
-            cp_async8(a + row * DG_LDK + kk, ok ? A + (int64_t)gm * lda + gk : A, ok);
+            cp_async8(a + row * DG_LDK + kk, ok ? (TA ? A + gk * lda + gm : A + (int64_t)gm * lda + gk) : A, ok);
         }
 #pragma unroll
         for (int e = 0; e < (DG_BN * DG_BK) / 256; ++e) {
-            const int idx = tid + 256 * e, row = idx >> 4, kk = idx & 15;
+            const int idx = tid + 256 * e;
+            const int row = TB ? idx % DG_BN : idx >> 4, kk = TB ? idx / DG_BN : idx & 15;
             const int gn = n0 + row;
             const int64_t gk = kb + kk;
             const bool ok = gn < N && gk < kend;
-            cp_async8(b + row * DG_LDK + kk, ok ? B + (int64_t)gn * ldb + gk : B, ok);
+            cp_async8(b + row * DG_LDK + kk, ok ? (TB ? B + gk * ldb + gn : B + (int64_t)gn * ldb + gk) : B, ok);
         }
     };
 
@@ -98,8 +103,27 @@ __global__ void __launch_bounds__(256) dgemm_tn_kernel(const double* __restrict_
             for (int h = 0; h < 2; ++h) {
                 const int m = m0 + wm * 32 + mt * 8 + g;
                 const int n = n0 + wn * 32 + nt * 8 + 2 * t + h;
-                if (m < M && n < N) epi(m, n, acc[mt][nt][h], (int)blockIdx.z);
+                if (m < M && n < N) epi(m, n, acc[mt][nt][h], z);
             }
+}
+
+template <class Epi, bool TA = false, bool TB = false>
+__global__ void __launch_bounds__(256) dgemm_tn_kernel(const double* __restrict__ A, int64_t lda,
+                                                       const double* __restrict__ B, int64_t ldb,
+                                                       int M, int N, int64_t K, int64_t k_per_split,
+                                                       int upper_only, Epi epi) {
+    const int64_t kbeg = (int64_t)blockIdx.z * k_per_split;
+    const int64_t kend = kbeg + k_per_split < K ? kbeg + k_per_split : K;
+    dgemm_tile<Epi, TA, TB>(A, lda, B, ldb, M, N, kbeg, kend, upper_only, epi, (int)blockIdx.z);
+}
+
+// Batched over blockIdx.z: operands z * sa and z * sb elements on, all of K.
+template <class Epi, bool TA = false, bool TB = false>
+__global__ void __launch_bounds__(256) dgemm_batched_kernel(const double* __restrict__ A, int64_t lda, int64_t sa,
+                                                            const double* __restrict__ B, int64_t ldb, int64_t sb,
+                                                            int M, int N, int64_t K, Epi epi) {
+    const int z = (int)blockIdx.z;
+    dgemm_tile<Epi, TA, TB>(A + z * sa, lda, B + z * sb, ldb, M, N, 0, K, 0, epi, z);
 }
 
 // value * alpha -> C[m*ldc + n]

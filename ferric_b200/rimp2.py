@@ -273,3 +273,54 @@ def rimp2_imat(x_ov, b_full, nocc, nvir, first_occ=0, precision="f64", stats=Non
     if stats is not None:
         stats.update(st.as_dict())
     return out
+
+
+def rimp2_response_2c(x_ov, b_ov, v_inv_sqrt, weight=2.0, stats=None):
+    """``(y_ov, gamma_2c)`` of the RI 3c/2c response for one channel
+    (ferric-mp2/src/gradient.rs:559-887): ``y_ov = V^{-1/2 T} x_ov`` and
+    ``gamma_2c = -w (V^{-1/2 T} b_ov) y_ov^T``, FP64."""
+    _lib.ensure_init()
+    naux, nov = int(x_ov.shape[0]), int(x_ov.shape[1])
+    st = FcStats()
+    if _is_torch_cuda(x_ov):
+        import torch
+        x, b, v = (t.contiguous() for t in (x_ov, b_ov, v_inv_sqrt))
+        y = torch.empty_like(x)
+        g = torch.empty((naux, naux), dtype=torch.float64, device=x.device)
+        check(_lib.lib.fc_rimp2_response_2c_dev(ptr(x), ptr(b), ptr(v), naux, nov, float(weight), ptr(y), ptr(g),
+                                                _stream_of(x), ctypes.byref(st)))
+    else:
+        x, b, v = (np.ascontiguousarray(t, dtype=np.float64) for t in (x_ov, b_ov, v_inv_sqrt))
+        y = np.empty_like(x)
+        g = np.empty((naux, naux))
+        check(_lib.lib.fc_rimp2_response_2c(ptr(x), ptr(b), ptr(v), naux, nov, float(weight), ptr(y), ptr(g),
+                                            ctypes.byref(st)))
+    if stats is not None:
+        stats.update(st.as_dict())
+    return y, g
+
+
+def rimp2_response_3c(y_ov, c_occ, c_vir, p0=0, np_=None, weight=2.0, stats=None):
+    """The 3-centre weight ``g3c[P] = w (G_P + G_P^T)``, ``G_P = C_occ Y_P
+    C_vir^T``, for the aux slab ``[p0, p0 + np_)`` (np_, nbf, nbf)
+    (ferric-mp2/src/gradient.rs:772-804), FP64."""
+    _lib.ensure_init()
+    naux = int(y_ov.shape[0])
+    nbf, nocc = int(c_occ.shape[0]), int(c_occ.shape[1])
+    nvir = int(c_vir.shape[1])
+    np_ = naux - p0 if np_ is None else int(np_)
+    st = FcStats()
+    if _is_torch_cuda(y_ov):
+        import torch
+        y, co, cv = (t.contiguous() for t in (y_ov, c_occ, c_vir))
+        out = torch.empty((np_, nbf, nbf), dtype=torch.float64, device=y.device)
+        check(_lib.lib.fc_rimp2_response_3c_dev(ptr(y), ptr(co), ptr(cv), naux, nocc, nvir, nbf, p0, np_,
+                                                float(weight), ptr(out), _stream_of(y), ctypes.byref(st)))
+    else:
+        y, co, cv = (np.ascontiguousarray(t, dtype=np.float64) for t in (y_ov, c_occ, c_vir))
+        out = np.empty((np_, nbf, nbf))
+        check(_lib.lib.fc_rimp2_response_3c(ptr(y), ptr(co), ptr(cv), naux, nocc, nvir, nbf, p0, np_, float(weight),
+                                            ptr(out), ctypes.byref(st)))
+    if stats is not None:
+        stats.update(st.as_dict())
+    return out

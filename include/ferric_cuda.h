@@ -220,6 +220,32 @@ fc_status fc_rimp2_imat_dev(const double* x_ov, const double* b_full, int64_t na
                             int64_t nvir, int64_t first_occ, int32_t precision, double* imat, void* stream,
                             fc_stats* stats);
 
+/* The GEMM-shaped part of the RI 3c/2c integral response of the RI-MP2
+ * gradient, for one channel of weight w (integral_response_gradient_3c2c /
+ * ri_response_gradient_channels, ferric-mp2/src/gradient.rs:559-887; w = 2
+ * closed shell, 1 per spin):
+ *   y_ov     = V^{-1/2 T} x_ov                          (naux x nov)
+ *   gamma_2c = -w (V^{-1/2 T} b_ov) y_ov^T               (naux x naux)
+ *   g3c[P]   = w (G_P + G_P^T), G_P = C_occ Y_P C_vir^T  (nbf x nbf)
+ * Y_P = row P of y_ov as nocc x nvir; v_inv_sqrt (naux x naux), c_occ
+ * (nbf x nocc), c_vir (nbf x nvir), all row-major FP64.  g3c is produced for
+ * the aux slab [p0, p0 + np) (np x nbf x nbf), as the reference builds it per
+ * aux shell for the derivative integrals, which stay with the caller.  FP64
+ * throughout (DMMA).  The _dev forms take device pointers and synchronise
+ * their stream before returning; the host form of _3c uploads only the rows
+ * [p0, p0 + np) of y_ov. */
+fc_status fc_rimp2_response_2c(const double* x_ov, const double* b_ov, const double* v_inv_sqrt, int64_t naux,
+                               int64_t nov, double weight, double* y_ov, double* gamma_2c, fc_stats* stats);
+fc_status fc_rimp2_response_2c_dev(const double* x_ov, const double* b_ov, const double* v_inv_sqrt, int64_t naux,
+                                   int64_t nov, double weight, double* y_ov, double* gamma_2c, void* stream,
+                                   fc_stats* stats);
+fc_status fc_rimp2_response_3c(const double* y_ov, const double* c_occ, const double* c_vir, int64_t naux,
+                               int64_t nocc, int64_t nvir, int64_t nbf, int64_t p0, int64_t np, double weight,
+                               double* g3c, fc_stats* stats);
+fc_status fc_rimp2_response_3c_dev(const double* y_ov, const double* c_occ, const double* c_vir, int64_t naux,
+                                   int64_t nocc, int64_t nvir, int64_t nbf, int64_t p0, int64_t np, double weight,
+                                   double* g3c, void* stream, fc_stats* stats);
+
 /* FP64 RI-MP2 energy that allocates no device memory.  No counterpart in the
  * reference: it is for callers that cannot call cudaMalloc -- callers whose
  * device memory belongs to another allocator (ferric's device-pool ledger

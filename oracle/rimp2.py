@@ -309,3 +309,24 @@ def imat_scalar(x_ov, b_full, nocc, nvir, first_occ=0):
                     want[q, nt + a] -= 2.0 * t2
                     absum[q, nt + a] += 2.0 * abs(t2)
     return want, absum
+
+
+def response_2c(x_ov, b_ov, v_inv_sqrt, weight=2.0):
+    """``(y_ov, gamma_2c)`` of one response channel: ``y_ov = V^{-1/2 T}
+    x_ov`` (ferric-mp2/src/gradient.rs:656-658) and ``gamma_2c = -w C_fit
+    y_ov^T`` with ``C_fit = V^{-1/2 T} b_ov`` (gradient.rs:881-887)."""
+    y = v_inv_sqrt.T @ x_ov
+    c_fit = v_inv_sqrt.T @ b_ov
+    return y, -weight * (c_fit @ y.T)
+
+
+def response_3c(y_ov, c_occ, c_vir, p0, np_, weight=2.0):
+    """The 3-centre weight of aux rows ``[p0, p0 + np_)``: ``w (G_P + G_P^T)``,
+    ``G_P = C_occ Y_P C_vir^T`` with ``Y_P`` row P of y_ov as (nocc, nvir)
+    (ferric-mp2/src/gradient.rs:772-804)."""
+    nocc, nvir = c_occ.shape[1], c_vir.shape[1]
+    out = np.empty((np_, c_occ.shape[0], c_occ.shape[0]))
+    for k in range(np_):
+        g = c_occ @ y_ov[p0 + k].reshape(nocc, nvir) @ c_vir.T
+        out[k] = weight * (g + g.T)
+    return out

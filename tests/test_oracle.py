@@ -182,3 +182,21 @@ def test_imat_gemm_matches_scalar_definition():
     assert np.all(np.abs(got - want) <= bar * absum)
     assert np.all(got[:, :fo] == 0.0)
     assert np.any(got != 0.0)
+
+
+def test_response_restatement_matches_scalar_definition():
+    """The oracle's 3c/2c response (gradient.rs:559-887) against the
+    definitions written as einsums: y = V^T x, gamma_2c = -w (V^T b) y^T,
+    g3c[P] = w (G_P + G_P^T), G_P[mu, nu] = sum_ia C_occ[mu, i] Y[P, ia] C_vir[nu, a]."""
+    from oracle import rimp2 as orc
+    rng = np.random.default_rng(3)
+    naux, nocc, nvir, nbf = 11, 3, 4, 6
+    x, b = rng.standard_normal((2, naux, nocc * nvir))
+    v = rng.standard_normal((naux, naux))
+    co, cv = rng.standard_normal((nbf, nocc)), rng.standard_normal((nbf, nvir))
+    y, g2 = orc.response_2c(x, b, v, 1.5)
+    assert np.allclose(y, np.einsum("qp,qk->pk", v, x), rtol=1e-13, atol=1e-13)
+    assert np.allclose(g2, -1.5 * np.einsum("qp,qk,rk->pr", v, b, y), rtol=1e-12, atol=1e-12)
+    g3 = orc.response_3c(y, co, cv, 2, 5, 1.5)
+    gp = np.einsum("mi,pia,na->pmn", co, y[2:7].reshape(5, nocc, nvir), cv)
+    assert np.allclose(g3, 1.5 * (gp + gp.transpose(0, 2, 1)), rtol=1e-12, atol=1e-12)
