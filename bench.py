@@ -464,6 +464,35 @@ def c5_leg(torch, dev, prec, steps=3):
     return out
 
 
+def dfjk_leg(torch, dev, prec, index, builds=20):
+    """One DF-JK build at config 2 (n 600, naux 2400, nocc 60) as the SCF runs
+    it, one build after another: the fused J + K call, mixed and FP64 plain,
+    each the median of `builds` device-timed calls after three warm-up calls,
+    with the SM clocks sampled during them.  The step's own DF-JK figure is
+    taken right after the RI-MP2 gradient, at the clock that part's power draw
+    sets; this leg gives the builds at the clock they run at on their own."""
+    from ferric_b200.dfjk import DfJK
+    inp = make_inputs(torch, dev, dict(naux=64, nocc=2, nvir=8), DFJK)
+    out = {"dfjk": DFJK, "builds": builds}
+    for p in (prec, "f64"):
+        jk = DfJK(inp["bjk"], layout="square", precision=p)
+        j, k = torch.empty_like(inp["d"]), torch.empty_like(inp["d"])
+        for _ in range(3):
+            jk.jk_from_occ(inp["c"], out=(j, k))
+        ms = []
+        with ClockSampler(index) as clk:
+            for _ in range(builds):
+                st = {}
+                jk.jk_from_occ(inp["c"], out=(j, k), stats=st)
+                ms.append(st["kernel_ms"])
+        out[p] = {"ms": statistics.median(ms), "min_ms": min(ms), "max_ms": max(ms), "clocks": clk.summary()}
+        jk.close()
+    out["speedup_mixed_vs_plain"] = out["f64"]["ms"] / out[prec]["ms"]
+    del inp
+    torch.cuda.empty_cache()
+    return out
+
+
 def dens_leg(torch, dev, prec):
     """The gradient call with the full unrelaxed densities P_oo / P_vv at the
     config-3 RI-MP2 shapes: device time against the gradient call alone (one
@@ -815,6 +844,11 @@ def main():
     if prec == "mixed" and args.size == "full" and not args.no_c5:
         c5 = c5_leg(torch, dev, prec)
 
+    # ---- DF-JK builds one after another, as the SCF runs them (config 2)
+    dfjk_alone = None
+    if prec == "mixed" and args.size == "full":
+        dfjk_alone = dfjk_leg(torch, dev, prec, local)
+
     # ---- the gradient with the full densities, config-3 RI-MP2 shapes
     dens = None
     if prec == "mixed" and args.size == "full" and not args.no_dens:
@@ -847,6 +881,7 @@ def main():
             "plain_f64": plain,
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
             "config4_batch": batch, "config5": c5, "mo_dressing": dress, "densities": dens,
+            "dfjk_builds": dfjk_alone,
         }
         print(json.dumps(out))
     if world > 1:

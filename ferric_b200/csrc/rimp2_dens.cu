@@ -61,31 +61,39 @@ __host__ __device__ inline void tile_pair(int x, int n, int* t1, int* t2) {
 // t from Tt within every tp x tp sub-block (i, k) of an amplitude block of
 // nk sub-blocks per row of sub-blocks (pitch ld):
 //     dst[a, b] = (2 src[a, b] + src[b, a]) / 3.
-// One CTA per 32 x 32 tile pair (ta <= tb) of a sub-block (blockIdx.y); both
-// tiles are read before either is written, so dst may be src.
+// One CTA per AT x AT tile pair (ta <= tb) of a sub-block (blockIdx.y); both
+// tiles are read before either is written, so dst may be src.  A warp reads
+// 64 consecutive elements of a row: the row pitch is the whole block's, so
+// shorter runs cost DRAM row switches (32 x 32 FP32 tiles ran at 2.2 TB/s);
+// FP64 tiles are 32 wide (two of 64 x 64 would pass the static shared limit).
+template <typename T>
+constexpr int amp_tile() { return sizeof(T) == 4 ? 64 : 32; }
 template <typename T>
 __global__ void __launch_bounds__(256) amp_from_tt_kernel(const T* src, T* dst, int64_t ld, int64_t tp, int nk,
                                                           int ntt) {
-    __shared__ double s1[32][33], s2[32][33];
+    constexpr int AT = amp_tile<T>(), RY = 256 / AT;  // tile side, rows per pass
+    __shared__ T s1[AT][AT + 1], s2[AT][AT + 1];
     int ta, tb;
     tile_pair((int)blockIdx.x, ntt, &ta, &tb);
     const int64_t sb = blockIdx.y;
     const int64_t r0 = (sb / nk) * tp, c0 = (sb % nk) * tp;
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    const int64_t a0 = (int64_t)ta * 32, b0 = (int64_t)tb * 32;
-    for (int r = ty; r < 32; r += 8) {
+    const int tx = threadIdx.x % AT, ty = threadIdx.x / AT;
+    const int64_t a0 = (int64_t)ta * AT, b0 = (int64_t)tb * AT;
+    for (int r = ty; r < AT; r += RY) {
         const int64_t a = a0 + r, b = b0 + tx;  // s1[r][tx] = src[a, b]
-        s1[r][tx] = (a < tp && b < tp) ? (double)src[(r0 + a) * ld + c0 + b] : 0.0;
+        s1[r][tx] = (a < tp && b < tp) ? src[(r0 + a) * ld + c0 + b] : (T)0;
         const int64_t a2 = b0 + r, b2 = a0 + tx;  // s2[r][tx] = src[a2, b2]
-        s2[r][tx] = (a2 < tp && b2 < tp) ? (double)src[(r0 + a2) * ld + c0 + b2] : 0.0;
+        s2[r][tx] = (a2 < tp && b2 < tp) ? src[(r0 + a2) * ld + c0 + b2] : (T)0;
     }
     __syncthreads();
-    for (int r = ty; r < 32; r += 8) {
+    for (int r = ty; r < AT; r += RY) {
         const int64_t a = a0 + r, b = b0 + tx;  // src[b, a] = s2[tx][r]
-        if (a < tp && b < tp) dst[(r0 + a) * ld + c0 + b] = (T)((2.0 * s1[r][tx] + s2[tx][r]) / 3.0);
+        if (a < tp && b < tp)
+            dst[(r0 + a) * ld + c0 + b] = (T)((2.0 * (double)s1[r][tx] + (double)s2[tx][r]) / 3.0);
         if (ta != tb) {
             const int64_t a2 = b0 + r, b2 = a0 + tx;  // src[b2, a2] = s1[tx][r]
-            if (a2 < tp && b2 < tp) dst[(r0 + a2) * ld + c0 + b2] = (T)((2.0 * s2[r][tx] + s1[tx][r]) / 3.0);
+            if (a2 < tp && b2 < tp)
+                dst[(r0 + a2) * ld + c0 + b2] = (T)((2.0 * (double)s2[r][tx] + (double)s1[tx][r]) / 3.0);
         }
     }
 }
@@ -100,7 +108,7 @@ __global__ void __launch_bounds__(256) dens_split_rows_kernel(const float* __res
 
 template <typename T>
 fc_status amp_from_tt(const T* src, T* dst, int64_t ld, int64_t tp, int64_t nr, int64_t nk, cudaStream_t st) {
-    const int ntt = (int)((tp + 31) / 32);
+    const int ntt = (int)((tp + amp_tile<T>() - 1) / amp_tile<T>());
     const int64_t nsub = nr * nk;
     if (nsub > 65535) return fail(FC_ERR_LAYOUT, "MP2 densities: too many amplitude sub-blocks in one block");
     amp_from_tt_kernel<T><<<dim3((unsigned)(ntt * (ntt + 1) / 2), (unsigned)nsub), 256, 0, st>>>(src, dst, ld, tp,

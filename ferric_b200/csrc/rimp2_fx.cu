@@ -91,7 +91,7 @@ constexpr int SCR_BYTES = 8192;
 static_assert((2 * PSTAGES + 4) * 8 + 8 * (2 * EPI_WARPS * 3 + (NCG - 1) * BM + 4 * NCG * HC) <= SCR_BYTES,
               "pair scratch");
 static_assert(HC % 32 == 0 && 4 * NCG == EPI_WARPS, "pair epilogue layout");
-constexpr int SMEM = PSTAGES * PSTAGE_BYTES + 1024 + SCR_BYTES + COL_BYTES;
+constexpr int SMEM = PSTAGES * PSTAGE_BYTES + 1024 + SCR_BYTES + 2 * COL_BYTES;  // two column sets
 constexpr uint32_t IDESC = tc::idesc_i8_s32(128, 128);
 constexpr double LW = 254.0, LW2INV = 1.0 / (254.0 * 254.0), LW3INV = 1.0 / (254.0 * 254.0 * 254.0);
 
@@ -374,7 +374,7 @@ struct PairFxArgs {
     int xt;        // exchange (one phase) on diagonal tiles
     int64_t items;
     double* part;  // [item][2]
-    double* scr;   // [grid][2][BM][BN] FP64 X and Y tiles of each CTA
+    double* scr;   // [grid][3][BM][BN] FP64 tiles of each CTA: X of two items, Y
     int* err;
     // failure-path test hook: the MMA warp's waits for operand stages give up
     // after wait_ns; with drop_load, CTA 0's producer issues no load for its
@@ -508,7 +508,7 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
     double* red = reinterpret_cast<double*>(bars + 2 * S + 4);  // [2][EPI_WARPS][3]
     double* rowsh = red + 2 * EPI_WARPS * 3;                     // [NCG - 1][BM] row sums of column groups 1..
     double* colsh = rowsh + (NCG - 1) * BM;                      // [4 quadrants][NCG][HC] column sums
-    double* colb = reinterpret_cast<double*>(base + S * PSTAGE_BYTES + SCR_BYTES);  // [3][BN]
+    double* colb = reinterpret_cast<double*>(base + S * PSTAGE_BYTES + SCR_BYTES);  // [2 items][3][BN]
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (tid == 0) {
@@ -620,91 +620,52 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
         // column group h = (warp - 2) / 4; each thread owns row `row`, columns
         // [HC h, HC h + HC).  A phase's four level accumulators fill TMEM, so
         // each phase is drained at once into the CTA's FP64 tiles in global
-        // scratch (X, then Y), which hands TMEM back to the MMA warp; the FP64
-        // terms then run from the tiles under the next item's X phase.
+        // scratch (X, then Y), which hands TMEM back to the MMA warp.  The FP64
+        // terms of an item run in two halves of its columns, software-pipelined
+        // against the next item's phases:
+        //     drain X_k | terms(k-1, 2nd half), finish(k-1) | drain Y_k | terms(k, 1st half)
+        // so the first half runs under X_{k+1}'s MMAs and the second under
+        // Y_{k+1}'s (the FP64 terms of a whole item outlast one MMA phase).  X
+        // tiles alternate by item (X_k is drained while X_{k-1} is still read);
+        // Y_k is drained after the last read of Y_{k-1}.
         const int q = warp & 3;
         const int h = (warp - 2) >> 2;
         const int row = q * 32 + lane;  // a within the tile
         const int et = tid - 64;        // 0 .. EPI_THREADS - 1
         const uint32_t tl = tmem_base + ((uint32_t)(q * 32) << 16) + h * HC;
-        double* const sxt = p.scr + (int64_t)blockIdx.x * (2 * BM * BN);  // X tile [row][col]
-        double* const syt = sxt + BM * BN;                                 // Y tile
-        double* const xrow = sxt + row * BN + h * HC;
+        double* const scr0 = p.scr + (int64_t)blockIdx.x * (3 * BM * BN);  // X tiles [2][row][col], Y tile
+        double* const syt = scr0 + 2 * BM * BN;
         double* const yrow = syt + row * BN + h * HC;
-        uint32_t li = 0, pc = 0;
-        for (int64_t k = blockIdx.x; k < p.items; k += gridDim.x, ++li) {
+        constexpr int HH = HC / 2;  // columns per half
+        // carried from an item's first half of terms to its second
+        double os = 0.0, ss = 0.0, oc = 0.0, rowc = 0.0;
+
+        // FP64 terms of columns [c_lo, c_lo + HH) of this thread's HC, item k
+        // (li parity lk): energy sums, derivative sums, amplitude stores, and the
+        // column terms of the mirrored tile reduced over the warp's 32 rows into
+        // colsh[q][h][c_lo ..].
+        auto terms = [&](int64_t k, uint32_t lk, int c_lo) {
             const ItemView v = item_view<BATCH>(p, k);
             const int i = v.i, j = v.j;
             const bool diag = i == j;
             const int ta = v.ta, tb = v.tb;
-            // tiles ta <= tb only: X_ba = Y_ab, so the mirrored tile (tb, ta) is this
-            // tile transposed: its energy terms equal this tile's (weight 2), and
-            // gradient mode writes its amplitudes (transposed) and derivative terms.
-            // Pairs are unordered (i <= j); for i < j the item also stands for the
-            // pair (j, i), whose amplitudes are this item's transposed:
-            // Tt_ji[b, a] = Tt_ij[a, b].
-            const double wt = ta < tb ? 2.0 : 1.0;
             const bool mir = GRAD && ta < tb;
             const bool both = GRAD && !diag;
             const int a = ta * BM + row;
             const bool va = a < v.nvir;
             const double dA = v.eo[i] + v.eo[j] - (va ? v.ev[a] : 0.0);
-            const double sxa = v.scl[(int64_t)i * v.a_pad + a];
-            const double sya = v.scl[(int64_t)j * v.a_pad + a];
             const int b0 = tb * BN + h * HC;  // first column of this thread
-            // the tile's columns (virtual energies, scales of (j, b) and (i, b)) in
-            // shared memory: every lane of a warp reads the same column (broadcast)
-            {
-                const int cb = tb * BN + (et & (BN - 1));
-                if (et < BN) {
-                    colb[et] = cb < v.nvir ? v.ev[cb] : 0.0;
-                    colb[BN + et] = v.scl[(int64_t)j * v.a_pad + cb];
-                } else if (et < 2 * BN) {
-                    colb[2 * BN + (et - BN)] = v.scl[(int64_t)i * v.a_pad + cb];
-                }
-            }
-            asm volatile("bar.sync 1, %0;" ::"n"(EPI_THREADS) : "memory");
-            const double* evb = colb + h * HC;
-            const double* sxb = colb + BN + h * HC;
-            const double* syb = colb + 2 * BN + h * HC;
-            const int bmax = v.nvir - b0;    // columns c < bmax are real virtuals
-            const bool xt = v.xt;            // the same for every thread of the CTA
-            const bool two = !diag && !xt;   // a Y phase follows in TMEM
-
-            // X phase -> X tile.  One thread waits (bounded); the epilogue
-            // threads leave together if it gave up, since named barriers follow.
-            if (!tc::bar_and<1, EPI_THREADS>(et != 0 || tc::mbar_wait(tfull, pc & 1, abort_flag, p.err))) break;
-            if (et != 0) tc::mbar_wait(tfull, pc & 1, abort_flag, p.err);  // phase complete: returns at once
-            tc::fence_after_sync();
-            {
-                // (ia|ia) on the diagonal of an i == j block's diagonal tile
-                const int gdv = (diag && ta == tb && va) ? row - h * HC : -1;
-                const double gval = gdv >= 0 ? v.gd[(int64_t)i * v.a_pad + a] : 0.0;
-                drain_levels(tl, sxa, sxb, xrow, (gdv >= 0 && gdv < HC) ? gdv : -1, gval);
-            }
-            tc::fence_before_sync();
-            tc::mbar_arrive(tempty);
-            ++pc;
-            if (two) {
-                // Y phase: (ib|ja) = G_ji[a, b] -> Y tile
-                if (!tc::bar_and<1, EPI_THREADS>(et != 0 || tc::mbar_wait(tfull, pc & 1, abort_flag, p.err))) break;
-                if (et != 0) tc::mbar_wait(tfull, pc & 1, abort_flag, p.err);
-                tc::fence_after_sync();
-                drain_levels(tl, sya, syb, yrow, -1, 0.0);
-                tc::fence_before_sync();
-                tc::mbar_arrive(tempty);  // the level columns are free for the next item
-                ++pc;
-            }
-            // an exchanged tile reads other threads' rows of X
-            if (xt) asm volatile("bar.sync 1, %0;" ::"n"(EPI_THREADS) : "memory");
-
-            // plain FP64 sums over this thread's HC terms (relative error <= HC u);
-            // the tile partials are summed compensated
-            double os = 0.0, ss = 0.0, oc = 0.0, rowc = 0.0;
+            const double* evb = colb + (lk & 1) * 3 * BN + h * HC;
+            const int bmax = v.nvir - b0;  // columns c < bmax are real virtuals
+            const bool xt = v.xt;
+            const bool two = !diag && !xt;
+            double* const sxt = scr0 + (lk & 1) * BM * BN;
+            const double* const xrow = sxt + row * BN + h * HC;
             constexpr int CW = 4;  // columns per step of the FP64 terms
-            float ck[HC];  // column terms of this thread's columns (gradient)
+            float ck[HH];          // column terms of this half's columns (gradient)
 #pragma unroll
-            for (int c0 = 0; c0 < HC; c0 += CW) {
+            for (int cs = 0; cs < HH; cs += CW) {
+                const int c0 = c_lo + cs;
                 double xv[CW], yv[CW];
                 {
                     const double2* x2 = reinterpret_cast<const double2*>(xrow + c0);
@@ -772,7 +733,7 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
                     }
                     tt8[cc] = tval;
                     mv8[cc] = mval;
-                    ck[c0 + cc] = colv;
+                    ck[cs + cc] = colv;
                 }
                 if (GRAD && a < v.tpad) {
                     // amplitude rows (i, a) and columns (j, b) at pitch tpad (>= nvir);
@@ -818,20 +779,13 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
                     }
                 }
             }
-            const double vo = warp_sum(os), vs = warp_sum(ss);
-            const double vc = GRAD ? warp_sum(oc) : 0.0;
-            double* rb = red + (li & 1) * (EPI_WARPS * 3);
-            if (lane == 0) {
-                rb[(warp - 2) * 3 + 0] = vo;
-                rb[(warp - 2) * 3 + 1] = vs;
-                rb[(warp - 2) * 3 + 2] = vc;
-            }
-            if (GRAD && h > 0) rowsh[(h - 1) * BM + row] = rowc;
             if ((mir || both) && !xt) {
                 // column sums of the mirrored terms over this warp's 32 rows: a
-                // reduce-scatter butterfly leaves columns (HC / 32) lane + u in ck[u]
+                // reduce-scatter butterfly over offsets 16 .. 2 leaves column
+                // lane / 2 of the half in ck[0] (lanes 2m and 2m + 1 hold the two
+                // halves of the rows' sum), then lane pairs add
 #pragma unroll
-                for (int half = HC / 2, off = 16; off > 0; half >>= 1, off >>= 1) {
+                for (int half = HH / 2, off = 16; off > 1; half >>= 1, off >>= 1) {
                     const bool up = (lane & off) != 0;
 #pragma unroll
                     for (int c = 0; c < half; ++c) {
@@ -840,9 +794,28 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
                         ck[c] = (up ? ck[c + half] : ck[c]) + recv;
                     }
                 }
-#pragma unroll
-                for (int u = 0; u < HC / 32; ++u) colsh[(q * NCG + h) * HC + (HC / 32) * lane + u] = (double)ck[u];
+                const float tot = ck[0] + __shfl_xor_sync(0xffffffffu, ck[0], 1);
+                if ((lane & 1) == 0) colsh[(q * NCG + h) * HC + c_lo + (lane >> 1)] = (double)tot;
             }
+        };
+
+        // the item's sums: partials of E_OS / E_SS / dE/deps (fixed order)
+        auto finish = [&](int64_t k, uint32_t lk) {
+            const ItemView v = item_view<BATCH>(p, k);
+            const bool diag = v.i == v.j;
+            const bool mir = GRAD && v.ta < v.tb;
+            const bool both = GRAD && !diag;
+            const bool xt = v.xt;
+            const double wt = v.ta < v.tb ? 2.0 : 1.0;
+            const double vo = warp_sum(os), vs = warp_sum(ss);
+            const double vc = GRAD ? warp_sum(oc) : 0.0;
+            double* rb = red + (lk & 1) * (EPI_WARPS * 3);
+            if (lane == 0) {
+                rb[(warp - 2) * 3 + 0] = vo;
+                rb[(warp - 2) * 3 + 1] = vs;
+                rb[(warp - 2) * 3 + 2] = vc;
+            }
+            if (GRAD && h > 0) rowsh[(h - 1) * BM + row] = rowc;
             asm volatile("bar.sync 1, %0;" ::"n"(EPI_THREADS) : "memory");
             if (GRAD && h == 0) {
                 double rs = rowc;
@@ -869,9 +842,85 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
                 p.part[2 * k + 1] = wt * sn.value();
                 if (GRAD) p.occ_part[k] = sc.value();
             }
-            // rowsh and the scratch tiles are rewritten next item only after every
+            os = ss = oc = rowc = 0.0;
+            // rowsh, colsh and the item's tiles are rewritten only after every
             // thread passed this barrier
             asm volatile("bar.sync 1, %0;" ::"n"(EPI_THREADS) : "memory");
+        };
+
+        uint32_t li = 0, pc = 0;
+        int64_t kprev = -1;  // the item whose second half of terms is pending
+        uint32_t lprev = 0;
+        for (int64_t k = blockIdx.x;; k += gridDim.x, ++li) {
+            const bool cur = k < p.items;
+            bool two = false, xt = false;
+            if (cur) {
+                const ItemView v = item_view<BATCH>(p, k);
+                const int i = v.i, j = v.j;
+                const bool diag = i == j;
+                const int ta = v.ta, tb = v.tb;
+                const int a = ta * BM + row;
+                const bool va = a < v.nvir;
+                const double sxa = v.scl[(int64_t)i * v.a_pad + a];
+                const double sya = v.scl[(int64_t)j * v.a_pad + a];
+                double* const cb_ = colb + (li & 1) * 3 * BN;
+                // the tile's columns (virtual energies, scales of (j, b) and (i, b)) in
+                // shared memory: every lane of a warp reads the same column (broadcast)
+                {
+                    const int cb = tb * BN + (et & (BN - 1));
+                    if (et < BN) {
+                        cb_[et] = cb < v.nvir ? v.ev[cb] : 0.0;
+                        cb_[BN + et] = v.scl[(int64_t)j * v.a_pad + cb];
+                    } else if (et < 2 * BN) {
+                        cb_[2 * BN + (et - BN)] = v.scl[(int64_t)i * v.a_pad + cb];
+                    }
+                }
+                asm volatile("bar.sync 1, %0;" ::"n"(EPI_THREADS) : "memory");
+                const double* sxb = cb_ + BN + h * HC;
+                const double* syb = cb_ + 2 * BN + h * HC;
+                xt = v.xt;
+                two = !diag && !xt;  // a Y phase follows in TMEM
+                // X phase -> X tile.  One thread waits (bounded); the epilogue
+                // threads leave together if it gave up, since named barriers follow.
+                if (!tc::bar_and<1, EPI_THREADS>(et != 0 || tc::mbar_wait(tfull, pc & 1, abort_flag, p.err))) break;
+                if (et != 0) tc::mbar_wait(tfull, pc & 1, abort_flag, p.err);  // phase complete: returns at once
+                tc::fence_after_sync();
+                {
+                    // (ia|ia) on the diagonal of an i == j block's diagonal tile
+                    const int gdv = (diag && ta == tb && va) ? row - h * HC : -1;
+                    const double gval = gdv >= 0 ? v.gd[(int64_t)i * v.a_pad + a] : 0.0;
+                    double* const xrow = scr0 + (li & 1) * BM * BN + row * BN + h * HC;
+                    drain_levels(tl, sxa, sxb, xrow, (gdv >= 0 && gdv < HC) ? gdv : -1, gval);
+                }
+                tc::fence_before_sync();
+                tc::mbar_arrive(tempty);
+                ++pc;
+                (void)syb;
+            }
+            if (kprev >= 0) {
+                terms(kprev, lprev, HH);
+                finish(kprev, lprev);
+                kprev = -1;
+            }
+            if (!cur) break;
+            if (two) {
+                const ItemView v = item_view<BATCH>(p, k);
+                const double sya = v.scl[(int64_t)v.j * v.a_pad + v.ta * BM + row];
+                const double* syb = colb + (li & 1) * 3 * BN + 2 * BN + h * HC;
+                // Y phase: (ib|ja) = G_ji[a, b] -> Y tile
+                if (!tc::bar_and<1, EPI_THREADS>(et != 0 || tc::mbar_wait(tfull, pc & 1, abort_flag, p.err))) break;
+                if (et != 0) tc::mbar_wait(tfull, pc & 1, abort_flag, p.err);
+                tc::fence_after_sync();
+                drain_levels(tl, sya, syb, yrow, -1, 0.0);
+                tc::fence_before_sync();
+                tc::mbar_arrive(tempty);  // the level columns are free for the next item
+                ++pc;
+            }
+            // an exchanged tile reads other threads' rows of X
+            if (xt) asm volatile("bar.sync 1, %0;" ::"n"(EPI_THREADS) : "memory");
+            terms(k, li, 0);
+            kprev = (int64_t)k;
+            lprev = li;
         }
     }
 
@@ -1536,7 +1585,7 @@ static void fx_test_hooks(PairFxArgs* a) {
 // FP64 X / Y tiles of the pair kernel's CTAs (global scratch, L2-resident).
 fc_status pair_scratch(int grid, double** out) {
     void* v;
-    FC_TRY(ws_get(WS_PSCR, (size_t)grid * 2 * fx::BM * fx::BN * sizeof(double), &v));
+    FC_TRY(ws_get(WS_PSCR, (size_t)grid * 3 * fx::BM * fx::BN * sizeof(double), &v));
     *out = (double*)v;
     return FC_OK;
 }
@@ -2257,7 +2306,7 @@ fc_status rimp2_batch_build_fx(fc_rimp2_batch* b, const std::vector<BatchMolIn>&
     FC_TRY(batch_alloc(b, (size_t)items * sizeof(int4), &vitems));
     FC_TRY(batch_alloc(b, (size_t)items * 16, &vpart));
     const int pgrid = (int)std::min<int64_t>(std::max<int64_t>(items, 1), c.sm_count);
-    FC_TRY(batch_alloc(b, (size_t)pgrid * 2 * fx::BM * fx::BN * sizeof(double), &vscr));
+    FC_TRY(batch_alloc(b, (size_t)pgrid * 3 * fx::BM * fx::BN * sizeof(double), &vscr));
     FC_CUDA(cudaMemset(vbt, 0, (size_t)rows * q_pad));
     void *vocc = nullptr, *vvir = nullptr, *vqs = nullptr, *vbq = nullptr, *vgws = nullptr;
     void *vgm = nullptr, *vmaps = nullptr, *vgit = nullptr;

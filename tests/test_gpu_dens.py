@@ -15,6 +15,7 @@ SHAPES = [
     (200, 7, 65),    # one past a 32-tile edge
     (300, 9, 140),   # two 128-tiles of virtuals
     (17, 1, 1),      # one occupied, one virtual
+    (160, 130, 9),   # two 128-tiles of occupied orbitals (P_oo tile pairs (0,0), (0,1), (1,1))
 ]
 
 
