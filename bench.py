@@ -561,6 +561,8 @@ def main():
     ap.add_argument("--no-dress", action="store_true", help="skip the MO-dressing leg")
     ap.add_argument("--no-c5", action="store_true", help="skip the config-5 leg")
     ap.add_argument("--no-dens", action="store_true", help="skip the densities leg")
+    ap.add_argument("--leg", choices=["dfjk", "dens"], default=None,
+                    help="run only this side leg at --size's shapes and print its JSON (profiling cases)")
     ap.add_argument("--size", choices=["full", "small", "c5"], default="full",
                     help="small: naux 2400, nocc 60, nvir 550 + n 300, naux 1200, nocc 30 "
                          "(the profiling case; inputs still larger than L2); c5: the shapes of "
@@ -578,6 +580,15 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.leg:
+        from ferric_b200 import _lib
+        dev = torch.device("cuda", local)
+        torch.cuda.set_device(dev)
+        _lib.init(local)
+        prec = "mixed" if args.precision == "auto" else args.precision
+        leg = dfjk_leg(torch, dev, prec, local, builds=3) if args.leg == "dfjk" else dens_leg(torch, dev, prec)
+        print(json.dumps({"leg": args.leg, "size": args.size, **leg}))
+        return
     flops = step_flops()
     config = {"workload": f"synthetic RI-MP2 E+grad (naux {RIMP2['naux']}, nocc {RIMP2['nocc']}, "
                           f"nvir {RIMP2['nvir']}) + DF-JK build (n {DFJK['n']}, naux {DFJK['naux']}, "

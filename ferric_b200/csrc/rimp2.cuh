@@ -83,6 +83,8 @@ struct DensFx {
     int8_t* as;                    // [3][rows][ld] slices of t
     double* tsc;                   // [rows] row scales of ts
     double* asc;                   // [rows] row scales of as
+    double* tscT;                  // [nvir][nocc] ts scales, transposed (P_oo)
+    double* ascT;                  // [nvir][nocc] as scales, transposed
     double* part_vv;               // [grid_vv][128 x 128] partial P_vv tiles
     double* part_oo;               // [grid_oo][128 x 128] partial P_oo tiles
     int4* items;                   // per-slab work items (P_vv, then P_oo)

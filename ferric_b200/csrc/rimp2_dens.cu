@@ -133,33 +133,66 @@ struct EpiDensVV {
         const int b0 = (int)(it.y - i * tp) + col0;
         const double s = sa[it.x + row];
         double* pc = part + (int64_t)blockIdx.x * DT2 + (int64_t)col0 * DT + row;
+        // eight partials and scales loaded together, then updated (one chain
+        // of eight loads in flight instead of 32 dependent read-modify-writes)
 #pragma unroll
-        for (int c = 0; c < 32; ++c)
-            if (b0 + c < nvir) pc[c * DT] += s * st[it.y + col0 + c] * acc[c];
+        for (int c0 = 0; c0 < 32; c0 += 8) {
+            double sv[8], pv[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const bool ok = b0 + c0 + u < nvir;
+                sv[u] = ok ? __ldg(st + it.y + col0 + c0 + u) : 0.0;
+                pv[u] = ok ? pc[(c0 + u) * DT] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (b0 + c0 + u < nvir) pc[(c0 + u) * DT] = pv[u] + s * sv[u] * acc[c0 + u];
+        }
     }
 };
 
 // P_oo item (LdPlanes): planes (occupied i) it.x 128 .. of the t slab and
-// it.y 128 .. of the Tt slab, row a = it.z of each plane.
+// it.y 128 .. of the Tt slab, row a = it.z of each plane.  The row scales
+// come transposed (saT[a nocc + i], stT[a nocc + j]): a thread's 32
+// columns are then 32 consecutive scales.
 struct EpiDensOO {
-    const double* sa;
-    const double* st;
+    const double* saT;
+    const double* stT;
     double* part;
-    int64_t tp;
     int nocc;
     __device__ __forceinline__ void operator()(int64_t, int4 it, int row, int col0, const double (&acc)[32]) const {
         if (it.w == 0) return;
         const int i = it.x * DT + row;
         if (i >= nocc) return;
         const int64_t a = it.z;
-        const double s = -sa[i * tp + a];
+        const double s = -saT[a * nocc + i];
         const int j0 = it.y * DT + col0;
+        const double* sj = stT + a * nocc + j0;
         double* pc = part + (int64_t)blockIdx.x * DT2 + (int64_t)col0 * DT + row;
 #pragma unroll
-        for (int c = 0; c < 32; ++c)
-            if (j0 + c < nocc) pc[c * DT] += s * st[(int64_t)(j0 + c) * tp + a] * acc[c];
+        for (int c0 = 0; c0 < 32; c0 += 8) {
+            double sv[8], pv[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const bool ok = j0 + c0 + u < nocc;
+                sv[u] = ok ? __ldg(sj + c0 + u) : 0.0;
+                pv[u] = ok ? pc[(c0 + u) * DT] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (j0 + c0 + u < nocc) pc[(c0 + u) * DT] = pv[u] + s * sv[u] * acc[c0 + u];
+        }
     }
 };
+
+// sT[a nocc + i] = s[i tp + a] for a < nvir, i < nocc (the P_oo scales)
+__global__ void __launch_bounds__(256) scale_t_kernel(const double* __restrict__ s, int64_t nocc, int64_t nvir,
+                                                      int64_t tp, double* __restrict__ sT) {
+    const int64_t e = (int64_t)blockIdx.x * 256 + threadIdx.x;
+    if (e >= nocc * nvir) return;
+    const int64_t a = e / nocc, i = e % nocc;
+    sT[e] = s[i * tp + a];
+}
 
 // out (n x n, row-major) from the partial tiles: slot g ntp + x holds tile
 // pair x of group g; summed over g in order; pairs t1 < t2 mirrored, tiles
@@ -263,10 +296,13 @@ fc_status dens_fx_alloc(int64_t nocc, int64_t nvir, int64_t tp, int64_t cc, cuda
     o->as = o->ts + slab;
     const size_t nvv = (size_t)o->ntp_vv * o->g_vv * DT2, noo = (size_t)o->ntp_oo * o->g_oo * DT2;
     const size_t nitems = (size_t)items_per_slab(*o);
-    FC_TRY(ws_get(WS_DPART, (2 * o->rows + nvv + noo) * 8 + nitems * sizeof(int4), &vp));
+    const size_t nt = (size_t)nocc * nvir;
+    FC_TRY(ws_get(WS_DPART, (2 * o->rows + 2 * nt + nvv + noo) * 8 + nitems * sizeof(int4), &vp));
     o->tsc = (double*)vp;
     o->asc = o->tsc + o->rows;
-    o->part_vv = o->asc + o->rows;
+    o->tscT = o->asc + o->rows;
+    o->ascT = o->tscT + nt;
+    o->part_vv = o->ascT + nt;
     o->part_oo = o->part_vv + nvv;
     o->items = (int4*)(o->part_oo + noo);
     FC_CUDA(cudaMemsetAsync(o->part_vv, 0, (nvv + noo) * 8, st));
@@ -324,8 +360,12 @@ fc_status dens_fx_slab(const DensFx& o, int64_t nk, cudaStream_t st, int* err, i
         FC_TRY(check_launch("xgemm_kernel<P_vv>"));
     }
     {
+        const int64_t nt = o.nocc * o.nvir;
+        scale_t_kernel<<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(o.asc, o.nocc, o.nvir, o.tp, o.ascT);
+        scale_t_kernel<<<(unsigned)((nt + 255) / 256), 256, 0, st>>>(o.tsc, o.nocc, o.nvir, o.tp, o.tscT);
+        *nl += 2;
         XArgs a{o.items + nvv_items, (int64_t)(it.size() - nvv_items), (int)o.nocc, (int)o.nocc, err};
-        EpiDensOO epi{o.asc, o.tsc, o.part_oo, o.tp, (int)o.nocc};
+        EpiDensOO epi{o.ascT, o.tscT, o.part_oo, (int)o.nocc};
         xgemm_kernel<128, EpiDensOO, true, LdPlanes>
             <<<goo, xg::Cfg<128, true>::THREADS, xg::Cfg<128, true>::SMEM, st>>>(pa, pt, a, epi);
         FC_TRY(check_launch("xgemm_kernel<P_oo>"));
