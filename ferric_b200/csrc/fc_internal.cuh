@@ -77,6 +77,7 @@ enum WsSlot {
     WS_JD,         // fused DF-JK: d_P and J's pass-2 partials
     WS_DSLAB,      // MP2 densities: amplitude slabs (t and Tt)
     WS_DPART,      // MP2 densities: row scales, partial tiles, work items
+    WS_DSTORE,     // MP2 densities: FP32 amplitude blocks kept for a later column chunk
     WS_COUNT
 };
 

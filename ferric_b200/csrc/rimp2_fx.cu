@@ -1752,15 +1752,40 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
     // chunk pair (min, max) -- T (rows of its first chunk) when I <= K, T2
     // otherwise; the energy and dE/deps terms of a chunk pair are taken at
     // its I <= K visit.  The slab of K is complete after its last step.
+    //
+    // Densities kept without recomputation (the store form, when the blocks
+    // above the diagonal fit 8 chunk budgets; FERRIC_CUDA_DENS_STORE=0 forces
+    // the recomputing form): column chunk K runs chunk pairs (K, I), I >= K,
+    // once each -- T2 = block (I, K) goes to K's slab, T = block (K, I), I > K,
+    // is kept in FP32 until column I, whose slab takes it first (its Tt and t
+    // slices; its adjoint ran when it was made).
     struct Step {
         int64_t x;
-        int blk;    // 0: T, 1: T2, 2: both
+        int blk;    // 0: T, 1: T2, 2: both (store form: both, T2 to the slab, T to the store)
         bool sums;  // take the chunk pair's energy and dE/deps terms
         bool last;  // last block of the column chunk
+        int64_t col = -1;  // store form: the column chunk (the pair's first chunk)
     };
     std::vector<Step> steps;
+    std::vector<int64_t> store_off;  // [I][K], I < K: element offset of block (I, K) in the store
+    size_t store_elems = 0;
+    bool store = false;
+    if (dens) {
+        store_off.assign((size_t)(nch * nch), -1);
+        for (int64_t I = 0; I < nch; ++I)
+            for (int64_t K = I + 1; K < nch; ++K) {
+                store_off[(size_t)(I * nch + K)] = (int64_t)store_elems;
+                store_elems += (size_t)(std::min(cc, nocc - I * cc) * tp) * (size_t)(std::min(cc, nocc - K * cc) * tp);
+            }
+        const char* e = std::getenv("FERRIC_CUDA_DENS_STORE");
+        store = !(e && e[0] == '0') && store_elems * 4 <= (size_t)(8 * d.chunk_bytes);
+    }
     if (!dens) {
         for (int64_t x = 0; x < ncp; ++x) steps.push_back({x, 2, true, false});
+    } else if (store) {
+        for (int64_t K = 0; K < nch; ++K)
+            for (int64_t I = K; I < nch; ++I)
+                steps.push_back({cp_index[(size_t)(K * nch + I)], 2, true, I == nch - 1, K});
     } else {
         for (int64_t K = 0; K < nch; ++K)
             for (int64_t I = 0; I < nch; ++I)
@@ -1768,7 +1793,13 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
                                  I == nch - 1});
     }
     DensFx dx{};
+    float* dstore = nullptr;
     if (dens) FC_TRY(dens_fx_alloc(nocc, nvir, tp, cc, st, &dx));
+    if (store && store_elems) {
+        void* vs;
+        FC_TRY(ws_get(WS_DSTORE, store_elems * 4, &vs));
+        dstore = (float*)vs;
+    }
 
     void *vbq, *vtab, *vT, *vTs, *vpart;
     const size_t tab_bytes = ((pairs.size() * sizeof(int2) + 255) / 256) * 256;
@@ -1852,15 +1883,15 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
     // Gamma[:, rows] += 4 Bq[:, cols] T^T for one amplitude block
     // (with densities the slices go to the block's rows of the column chunk's
     // slab, slices nocc tp rows apart, and stay there for the density terms)
-    auto adjoint = [&](float* T, int64_t r0, int64_t nr, int64_t k0, int64_t nk) -> fc_status {
+    auto adjoint = [&](float* T, int64_t r0, int64_t nr, int64_t k0, int64_t nk, bool to_slab) -> fc_status {
         const int64_t ldk = nk * tp, rows = nr * tp, mp = (rows + 127) / 128 * 128;
-        const int64_t sstride = dens ? dx.rows : mp;  // rows between slices
-        int8_t* sl = dens ? dx.ts + r0 * tp * ldk : (int8_t*)vTs;
-        double* rsc = dens ? dx.tsc + r0 * tp : ts;
+        const int64_t sstride = to_slab ? dx.rows : mp;  // rows between slices
+        int8_t* sl = to_slab ? dx.ts + r0 * tp * ldk : (int8_t*)vTs;
+        double* rsc = to_slab ? dx.tsc + r0 * tp : ts;
         split_fx_rows_f32_kernel<<<(unsigned)rows, 256, 0, st>>>(T, ldk, sstride, rsc, sl);
         ++nl;
         CUtensorMap tmTs;
-        FC_TRY(make_tmap_i8_2d(&tmTs, sl, ldk, 3 * sstride - (dens ? r0 * tp : 0), ldk, fx::KT, 128));
+        FC_TRY(make_tmap_i8_2d(&tmTs, sl, ldk, 3 * sstride - (to_slab ? r0 * tp : 0), ldk, fx::KT, 128));
         GemmFxArgs g{};
         g.rs = rsc;
         g.cs = qs + (k0 / cc) * q_rows;  // the Q-row scales of the column chunk
@@ -1906,6 +1937,19 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
         const int64_t x = step.x;
         const CP& cp = cps[x];
         const bool same = cp.i0 == cp.j0;
+        if (store && same) {
+            // column chunk K starts: its slab rows of chunks I < K come from the store
+            const int64_t K = step.col, nk = std::min(cc, nocc - K * cc), ldk = nk * tp;
+            for (int64_t I = 0; I < K; ++I) {
+                float* blk = dstore + store_off[(size_t)(I * nch + K)];
+                const int64_t nr = std::min(cc, nocc - I * cc), rows = nr * tp;
+                split_fx_rows_f32_kernel<<<(unsigned)rows, 256, 0, st>>>(blk, ldk, dx.rows, dx.tsc + I * cc * tp,
+                                                                       dx.ts + I * cc * tp * ldk);
+                ++nl;
+                FC_TRY(check_launch("split_fx_rows_f32_kernel<store>"));
+                FC_TRY(dens_fx_block(dx, blk, I * cc * tp, nr, nk, st, &nl));
+            }
+        }
         if (owner[x] != d.shard) {
             if (stats) {
                 FC_CUDA(cudaEventRecord(ev[2 * sx], st));
@@ -1968,8 +2012,25 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
             nl += 4;  // the four reductions
         }
         ++nl;  // the pair kernel
-        if (step.blk != 1) FC_TRY(adjoint(T1, cp.i0, cp.ni, cp.j0, cp.nj));
-        if (step.blk != 0 && !same) FC_TRY(adjoint(T2, cp.j0, cp.nj, cp.i0, cp.ni));
+        if (store) {
+            // chunk pair (K, I), I >= K: T2 = block (I, K) of column K (the
+            // slab); T = block (K, I) of column I (the store), or the
+            // diagonal block (K, K) of column K
+            if (same) {
+                FC_TRY(adjoint(T1, cp.i0, cp.ni, cp.j0, cp.nj, true));
+                FC_TRY(dens_fx_block(dx, T1, cp.i0 * tp, cp.ni, cp.nj, st, &nl));
+            } else {
+                FC_TRY(adjoint(T1, cp.i0, cp.ni, cp.j0, cp.nj, false));
+                FC_CUDA(cudaMemcpyAsync(dstore + store_off[(size_t)((cp.i0 / cc) * nch + cp.j0 / cc)], T1,
+                                        (size_t)(cp.ni * tp) * (size_t)(cp.nj * tp) * 4, cudaMemcpyDeviceToDevice,
+                                        st));
+                FC_TRY(adjoint(T2, cp.j0, cp.nj, cp.i0, cp.ni, true));
+                FC_TRY(dens_fx_block(dx, T2, cp.j0 * tp, cp.nj, cp.ni, st, &nl));
+            }
+            if (step.last) FC_TRY(dens_fx_slab(dx, cp.ni, st, flags + 1, &nl));
+        } else {
+        if (step.blk != 1) FC_TRY(adjoint(T1, cp.i0, cp.ni, cp.j0, cp.nj, dens));
+        if (step.blk != 0 && !same) FC_TRY(adjoint(T2, cp.j0, cp.nj, cp.i0, cp.ni, dens));
         if (dens) {
             // the block (I, K) of the column chunk K: t and its slices, and
             // the slab's density terms once the column is complete
@@ -1977,6 +2038,7 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
             const int64_t r0 = t2 ? cp.j0 : cp.i0, nr = t2 ? cp.nj : cp.ni, nk = t2 ? cp.ni : cp.nj;
             FC_TRY(dens_fx_block(dx, t2 ? T2 : T1, r0 * tp, nr, nk, st, &nl));
             if (step.last) FC_TRY(dens_fx_slab(dx, nk, st, flags + 1, &nl));
+        }
         }
         // row I of the chunk pairs is done: Gamma's columns of chunk I are final
         if (!dens && sink && cp.j0 + cp.nj == nocc)

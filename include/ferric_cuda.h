@@ -144,12 +144,15 @@ fc_status fc_rimp2_energy_grad_dev(const double* b_ov, int64_t naux, int64_t noc
  * 1841-1883, with x_ov = gamma / 4):
  *   p_oo[i*nocc + j] = -sum_kab t_ik^ab (2 t_jk^ab - t_jk^ba)   (nocc x nocc)
  *   p_vv[a*nvir + b] =  sum_ijc t_ij^ac (2 t_ij^bc - t_ij^cb)   (nvir x nvir)
- * row-major and symmetric.  Amplitudes are still not stored: occupied-pair
- * blocks are recomputed per column chunk (the chunk pairs off the diagonal
- * twice) and each column's blocks are held as one slab (FC_PREC_MIXED: int8
- * slices of t and 2t - t^T, 6 B per element; FC_PREC_F64: 16 B per
- * element), at most four chunk budgets.  Otherwise as fc_rimp2_energy_grad /
- * _dev (gamma, de_docc, de_dvir as there). */
+ * row-major and symmetric.  The chunk pairs run by column chunk and each
+ * column's amplitude blocks are held as one slab (FC_PREC_MIXED: int8 slices
+ * of t and 2t - t^T, 6 B per element, at most four chunk budgets;
+ * FC_PREC_F64: 16 B per element).  FC_PREC_MIXED runs each chunk pair once
+ * and keeps the blocks above the diagonal in FP32 until their column (at
+ * most eight chunk budgets, else -- or with FERRIC_CUDA_DENS_STORE=0 -- the
+ * chunk pairs off the diagonal run once per column, as in FC_PREC_F64).
+ * Otherwise as fc_rimp2_energy_grad / _dev (gamma, de_docc, de_dvir as
+ * there). */
 fc_status fc_rimp2_energy_grad_dens(const double* b_ov, int64_t naux, int64_t nocc, int64_t nvir,
                                     const double* eps_occ, const double* eps_vir, int32_t precision,
                                     double* e_os, double* e_ss, double* gamma, double* de_docc,

@@ -97,14 +97,18 @@ def _f64_budget(nvir, chunk):
     return 2 * (chunk + 1) ** 2 * nvir * nvir * 8 - 1
 
 
-@pytest.mark.parametrize("prec", ["f64", "mixed"])
-def test_densities_chunked(fc, monkeypatch, prec):
+@pytest.mark.parametrize("prec,store", [("f64", "1"), ("mixed", "1"), ("mixed", "0")])
+def test_densities_chunked(fc, monkeypatch, prec, store):
     """Occupied chunks of 2 (the last shorter): every column chunk's slab
-    takes blocks from chunk pairs on both sides of the diagonal, and the
-    off-diagonal chunk pairs run once per column.  Energy, dE/deps and the
-    densities are those of one chunk (FP64 to summation order; mixed within
-    the slicing bound, the slab rows being split at their own maxima)."""
+    takes blocks from chunk pairs on both sides of the diagonal.  FP64 and
+    the recomputing mixed form run the off-diagonal chunk pairs once per
+    column (25 pair launches); the mixed store form runs each chunk pair once
+    (15) and keeps the blocks above the diagonal in FP32 until their column.
+    Energy, dE/deps and the densities are those of one chunk (FP64 to
+    summation order; mixed within the slicing bound, the slab rows being
+    split at their own maxima)."""
     from ferric_b200 import rimp2
+    monkeypatch.setenv("FERRIC_CUDA_DENS_STORE", store)
     naux, nocc, nvir = 160, 9, 40
     b, eo, ev = synthetic.rimp2_inputs(naux, nocc, nvir)
     t2, p_oo, p_vv = _ref(b, eo, ev)
@@ -113,7 +117,8 @@ def test_densities_chunked(fc, monkeypatch, prec):
     monkeypatch.setenv("FERRIC_CUDA_CHUNK_BYTES", str(budget))
     st = {}
     many = rimp2.rimp2_energy_grad_dens(b, eo, ev, precision=prec, stats=st)
-    assert st["main_launches"] == 25  # 5 column chunks x 5 blocks
+    # 5 column chunks: 5 x 5 blocks, or the 15 chunk pairs once
+    assert st["main_launches"] == (15 if prec == "mixed" and store == "1" else 25)
     assert abs(one[0].e_total - many[0].e_total) <= 1e-13 * abs(one[0].e_total)
     assert np.abs(one[2] - many[2]).max() <= 1e-13 * np.abs(one[2]).max()
     assert np.abs(one[3] - many[3]).max() <= 1e-13 * np.abs(one[3]).max()
@@ -125,6 +130,9 @@ def test_densities_chunked(fc, monkeypatch, prec):
         bo, bv = _mixed_bound(t2, nocc, nvir)
         assert np.all(np.abs(many[4] - p_oo) <= bo)
         assert np.all(np.abs(many[5] - p_vv) <= bv)
+        # Gamma as the chunked gradient call's: the same blocks, split alike
+        g = rimp2.rimp2_energy_grad(b, eo, ev, precision=prec)[1]
+        assert np.abs(many[1] - g).max() <= 1e-13 * np.abs(g).max()
     # the chunked gradient call (no densities) gives the same energy
     sc, *_ = rimp2.rimp2_energy_grad(b, eo, ev, precision=prec)
     assert abs(sc.e_total - many[0].e_total) <= 1e-13 * abs(sc.e_total)
