@@ -493,6 +493,20 @@ def dfjk_leg(torch, dev, prec, index, builds=20):
     return out
 
 
+def rimp2_leg(torch, dev, prec, calls=3):
+    """The RI-MP2 energy + gradient alone at --size's shapes: `calls` calls
+    (the first a warm-up), the library's stats of the last (profiling case)."""
+    from ferric_b200 import rimp2
+    inp = make_inputs(torch, dev, RIMP2, dict(n=16, naux=16, nocc=2))
+    st = {}
+    for _ in range(calls):
+        st = {}
+        sc, *_ = rimp2.rimp2_energy_grad(inp["b_ov"], inp["eo"], inp["ev"], precision=prec, stats=st)
+    return {"rimp2": RIMP2, "precision": prec, "kernel_ms": st["kernel_ms"], "pair_kernel_ms": st["main_ms"],
+            "pair_launches": st["main_launches"], "adjoint_ms": st["aux_ms"], "adjoint_launches": st["aux_launches"],
+            "e_total": sc.e_total}
+
+
 def dens_leg(torch, dev, prec):
     """The gradient call with the full unrelaxed densities P_oo / P_vv at the
     config-3 RI-MP2 shapes: device time against the gradient call alone (one
@@ -561,7 +575,7 @@ def main():
     ap.add_argument("--no-dress", action="store_true", help="skip the MO-dressing leg")
     ap.add_argument("--no-c5", action="store_true", help="skip the config-5 leg")
     ap.add_argument("--no-dens", action="store_true", help="skip the densities leg")
-    ap.add_argument("--leg", choices=["dfjk", "dens"], default=None,
+    ap.add_argument("--leg", choices=["dfjk", "dens", "rimp2"], default=None,
                     help="run only this side leg at --size's shapes and print its JSON (profiling cases)")
     ap.add_argument("--size", choices=["full", "small", "c5"], default="full",
                     help="small: naux 2400, nocc 60, nvir 550 + n 300, naux 1200, nocc 30 "
@@ -586,7 +600,12 @@ def main():
         torch.cuda.set_device(dev)
         _lib.init(local)
         prec = "mixed" if args.precision == "auto" else args.precision
-        leg = dfjk_leg(torch, dev, prec, local, builds=3) if args.leg == "dfjk" else dens_leg(torch, dev, prec)
+        if args.leg == "dfjk":
+            leg = dfjk_leg(torch, dev, prec, local, builds=3)
+        elif args.leg == "dens":
+            leg = dens_leg(torch, dev, prec)
+        else:
+            leg = rimp2_leg(torch, dev, prec)
         print(json.dumps({"leg": args.leg, "size": args.size, **leg}))
         return
     flops = step_flops()

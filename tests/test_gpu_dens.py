@@ -162,3 +162,18 @@ def test_ri_densities_shapes(fc):
     e_os, e_ss, gamma, _, _ = orc.energy_gamma_deps(b, eo, ev)
     assert abs(e - (e_os + e_ss)) <= 1e-10
     assert np.abs(x - gamma / 4.0).max() <= 1e-12 * np.abs(gamma).max()
+
+
+def test_densities_empty_and_refusals(fc):
+    """No virtuals: E = 0, P_oo = 0 (nocc x nocc), P_vv empty; a non-finite
+    B_ov element is refused by the mixed split (FC_ERR_RANGE), as in the
+    gradient call."""
+    from ferric_b200 import rimp2, _lib
+    b = np.zeros((10, 0))
+    sc, g, d_o, d_v, p_oo, p_vv = rimp2.rimp2_energy_grad_dens(b, np.array([-1.0, -0.5]), np.zeros(0))
+    assert sc.e_total == 0.0 and p_oo.shape == (2, 2) and not p_oo.any() and p_vv.shape == (0, 0)
+    b, eo, ev = synthetic.rimp2_inputs(40, 3, 9)
+    b[5, 7] = np.inf
+    with pytest.raises(_lib.FcError) as e:
+        rimp2.rimp2_energy_grad_dens(b, eo, ev, precision="mixed")
+    assert e.value.name == "FC_ERR_RANGE"

@@ -231,3 +231,28 @@ def test_rimp2_config3_densities(fc):
           f"E {sm.e_total - sf.e_total:.3e}")
     assert eo_rel <= 1e-6 and ev_rel <= 1e-6
     assert abs(sm.e_total - sf.e_total) <= 1e-6
+
+
+def test_rimp2_config5_mixed_against_fp64(fc):
+    """Config 5's RI-MP2 shapes (C20H42 def2-TZVP / def2-TZVP-RIFIT: naux 2150,
+    nocc 81, nvir 791), the config-3 distributions: the mixed energy within
+    1 uEh of the FP64 plain energy (the north star's bar), Gamma within 1e-5
+    and dE/deps within 1e-6 of their maxima."""
+    import torch
+    from ferric_b200 import rimp2
+    naux, nocc, nvir = 2150, 81, 791
+    g = torch.Generator(device="cuda")
+    g.manual_seed(3)
+    b = torch.randn((naux, nocc * nvir), generator=g, device="cuda", dtype=torch.float64)
+    b *= 0.02 * torch.exp(-torch.arange(naux, device="cuda", dtype=torch.float64) / (3000.0 * naux / 4800.0))[:, None]
+    r = np.random.default_rng(30)
+    eo = torch.from_numpy(np.sort(r.uniform(-20.0, -0.3, nocc))).cuda()
+    ev = torch.from_numpy(np.sort(r.uniform(0.05, 6.0, nvir))).cuda()
+    sm, gm, dom, dvm = rimp2.rimp2_energy_grad(b, eo, ev, precision="mixed")
+    sf, gf, dof, dvf = rimp2.rimp2_energy_grad(b, eo, ev, precision="f64")
+    err = sm.e_total - sf.e_total
+    print(f"config-5 shapes: mixed E error {err:.3e} Eh of {sf.e_total:.6f}")
+    assert abs(err) <= 1e-6
+    assert float((gm - gf).abs().max()) <= 1e-5 * float(gf.abs().max())
+    assert float((dom - dof).abs().max()) <= 1e-6 * float(dof.abs().max())
+    assert float((dvm - dvf).abs().max()) <= 1e-6 * float(dvf.abs().max())
