@@ -5,7 +5,9 @@
 // path of ferric-scf/src/df_k.rs:1409-1520, 1575-1660):
 //   once per handle  B rows (Q, mu) split into three int8 integer slices at a
 //                    power-of-two scale per row (fx_split.cuh): 3 bytes per
-//                    element, the bytes of the HBM-bound stage 1
+//                    element, the bytes of the HBM-bound stage 1, stored in
+//                    128-byte column blocks so each k-step's box is
+//                    contiguous
 //   per build        C^T rows (one per occupied orbital) split the same way
 //   stage 1          W[mu, (Q, i)] = sum_nu B[Q, mu, nu] C[nu, i]: int8
 //                    exact-slice GEMM (kind::i8, exact int32 levels),
@@ -33,11 +35,40 @@ namespace {
 
 int64_t rup(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
-// Row r = (Q, mu) of the square tensor -> int8 slices [3][rows][ldk], scale s[r].
-__global__ void __launch_bounds__(256) dfk_split_b_kernel(const double* __restrict__ b, int64_t n, int64_t ldk,
-                                                          int64_t rows, double* __restrict__ s,
-                                                          int8_t* __restrict__ bs) {
-    split_fx_qrows_body<SliceI8>(b, 1, n, ldk, ldk, rows, s, bs, blockIdx.x);
+// Row r = (Q, mu) of the square tensor -> int8 slices in k-blocks:
+// [3][nkb][rows][128] (column nu of row r at block nu / 128, byte nu % 128;
+// zero past n), scale s[r].  Stage 1 reads one 128-byte column block of 128
+// rows per k-step: contiguous 16 KB, not 128 bytes of each row at the row
+// pitch (DRAM pages stay open along a k-step's box).
+__global__ void __launch_bounds__(256) dfk_split_b_kblk_kernel(const double* __restrict__ b, int64_t n,
+                                                               int64_t nkb, int64_t rows, double* __restrict__ s,
+                                                               int8_t* __restrict__ bs) {
+    __shared__ double red[32];
+    const int64_t r = blockIdx.x;
+    const double* row = b + r * n;
+    double m = 0.0;
+    for (int64_t k = threadIdx.x; k < n; k += 256) m = fmax(m, fabs(row[k]));
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double t = threadIdx.x < 8 ? red[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) t = fmax(t, __shfl_xor_sync(0xffffffffu, t, o));
+        if (threadIdx.x == 0) red[0] = t;
+    }
+    __syncthreads();
+    const double sc = SliceI8::scale(red[0]);
+    if (threadIdx.x == 0) s[r] = sc;
+    const double inv = 1.0 / sc;
+    const int64_t ss = nkb * rows * 128;  // bytes between slices
+    for (int64_t k = threadIdx.x; k < nkb * 128; k += 256) {
+        int8_t c1 = 0, c2 = 0, c3 = 0;
+        if (k < n) fx_slices<SliceI8>(row[k], inv, c1, c2, c3);
+        const int64_t d = ((k >> 7) * rows + r) * 128 + (k & 127);
+        bs[d] = c1;
+        bs[ss + d] = c2;
+        bs[2 * ss + d] = c3;
+    }
 }
 
 // Column i of C (n x nocc) -> row i of the int8 C^T slices [3][npad][ldk], scale sc[i].
@@ -179,8 +210,8 @@ bool g_attr_done = false;
 
 fc_status xg_attrs() {
     if (g_attr_done) return FC_OK;
-    FC_CUDA(cudaFuncSetAttribute(xgemm_kernel<64, EpiW, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 xg::Cfg<64, true>::SMEM));
+    FC_CUDA(cudaFuncSetAttribute(xgemm_kernel<64, EpiW, true, LdKBlocksA>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, xg::Cfg<64, true>::SMEM));
     FC_CUDA(cudaFuncSetAttribute(xgemm_kernel<128, EpiPart, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  xg::Cfg<128, true>::SMEM));
     g_attr_done = true;
@@ -189,26 +220,26 @@ fc_status xg_attrs() {
 
 }  // namespace
 
-// Split of the square tensor for the tensor-core stages (mixed square handles).
+// Split of the square tensor for the tensor-core stages (mixed square
+// handles): three int8 slices per row (Q, mu) in 128-byte column blocks.
 fc_status dfk_prepare_split(fc_dfjk* h, cudaStream_t st) {
-    const int64_t rows = h->naux * h->n, ldk = rup(h->n, 16);  // 16-byte int8 rows for TMA
-    const size_t sbytes = (size_t)3 * rows * ldk, scl = (size_t)rows * 8;
+    const int64_t rows = h->naux * h->n, nkb = (h->n + 127) / 128;
+    const size_t sbytes = (size_t)3 * nkb * rows * 128, scl = (size_t)rows * 8;
     const size_t bytes = rup((int64_t)sbytes, 256) + scl;
+    if (rows > INT32_MAX || 3 * nkb * rows > INT32_MAX) return fail(FC_ERR_LAYOUT, "DF-K: naux*n too large");
     FC_TRY(pool_reserve(bytes));
     FC_CUDA(cudaMalloc(&h->sq_split, bytes));
     h->bytes += bytes;
     h->sq_scale = (double*)((char*)h->sq_split + rup((int64_t)sbytes, 256));
-    if (ldk != h->n) FC_CUDA(cudaMemsetAsync(h->sq_split, 0, sbytes, st));
-    if (rows > INT32_MAX) return fail(FC_ERR_LAYOUT, "DF-K: naux*n too large");
-    dfk_split_b_kernel<<<(unsigned)rows, 256, 0, st>>>(h->b_sq, h->n, ldk, rows, h->sq_scale,
-                                                       (int8_t*)h->sq_split);
-    return check_launch("dfk_split_b_kernel");
+    dfk_split_b_kblk_kernel<<<(unsigned)rows, 256, 0, st>>>(h->b_sq, h->n, nkb, rows, h->sq_scale,
+                                                            (int8_t*)h->sq_split);
+    return check_launch("dfk_split_b_kblk_kernel");
 }
 
 fc_status dfk_build_mixed(fc_dfjk* h, const double* c_occ, int64_t nocc, double* kout, cudaStream_t st,
                           fc_stats* stats, const JFork* jf) {
     if (!h->sq_split)
-        return fail(FC_ERR_KERNEL, "DF-K: handle has no split-BF16 copy (created with FC_PREC_F64)");
+        return fail(FC_ERR_KERNEL, "DF-K: handle has no int8 slice copy (created with FC_PREC_F64)");
     FC_TRY(xg_attrs());
     Context& cx = ctx();
     const int64_t n = h->n, naux = h->naux, ldk = rup(n, 16);
@@ -262,7 +293,8 @@ fc_status dfk_build_mixed(fc_dfjk* h, const double* c_occ, int64_t nocc, double*
     FC_CUDA(cudaMemsetAsync(vc, 0, cs_bytes, st));
 
     CUtensorMap tb, tcm, tw;
-    FC_TRY(make_tmap_i8_2d(&tb, h->sq_split, n, 3 * rows, ldk, 128, 128));
+    const int64_t nkb = (n + 127) / 128;  // k-blocks of the B slices
+    FC_TRY(make_tmap_i8_2d(&tb, h->sq_split, 128, 3 * nkb * rows, 128, 128, 128));
     FC_TRY(make_tmap_i8_2d(&tcm, vc, n, 3 * npad, ldk, 128, 64));
     FC_TRY(make_tmap_i8_2d(&tw, vws, ldw, 3 * mp, ldw, 128, 128));
 
@@ -275,11 +307,11 @@ fc_status dfk_build_mixed(fc_dfjk* h, const double* c_occ, int64_t nocc, double*
         FC_CUDA(cudaEventRecord(ev[0], st));
     }
     {
-        XArgs a{(const int4*)vtab, n1, (int)rows, (int)npad, flags + 1};
+        XArgs a{(const int4*)vtab, n1, (int)rows, (int)npad, flags + 1, (int)nkb};
         EpiW epi{h->sq_scale, sc, (float*)vw, ldw, rows, (int)n, (int)nocc, (int)nocc_p, wmax};
         const int grid = (int)std::min<int64_t>(n1, cx.sm_count);
-        xgemm_kernel<64, EpiW, true><<<grid, xg::Cfg<64, true>::THREADS, xg::Cfg<64, true>::SMEM, st>>>(tb, tcm, a,
-                                                                                                         epi);
+        xgemm_kernel<64, EpiW, true, LdKBlocksA>
+            <<<grid, xg::Cfg<64, true>::THREADS, xg::Cfg<64, true>::SMEM, st>>>(tb, tcm, a, epi);
     }
     if (stats) FC_CUDA(cudaEventRecord(ev[1], st));
     if (jf) {  // J: pass-1 vector from the FP32 W (each element rounded once), second pass forked off

@@ -76,6 +76,7 @@ struct XArgs {
     int64_t nitems;
     int Ma, Nb;  // rows (LdPlanes: planes) between the slices of the A and B tensor maps
     int* err;
+    int nka;     // LdKBlocksA: k-blocks of A per slice
 };
 
 struct LdTiles {
@@ -85,6 +86,19 @@ struct LdTiles {
     __device__ static void load(void* da, void* db, const CUtensorMap* ta, const CUtensorMap* tb, uint64_t* bar,
                                 const XArgs& p, int4 it, int kt, int sl) {
         tc::tma_load_2d(da, ta, bar, kt * KTE, sl * p.Ma + it.x * xg::BM);
+        tc::tma_load_2d(db, tb, bar, kt * KTE, sl * p.Nb + it.y * BN);
+    }
+};
+
+// A in 128-byte column blocks ([slice][k-block][Ma rows][128 B], a 2-D map
+// 128 bytes wide), B as LdTiles.
+struct LdKBlocksA {
+    static constexpr int KP = xg::KP;
+    __device__ static int k0(int4 it) { return it.z; }
+    template <int BN, int KTE>
+    __device__ static void load(void* da, void* db, const CUtensorMap* ta, const CUtensorMap* tb, uint64_t* bar,
+                                const XArgs& p, int4 it, int kt, int sl) {
+        tc::tma_load_2d(da, ta, bar, 0, (sl * p.nka + kt) * p.Ma + it.x * xg::BM);
         tc::tma_load_2d(db, tb, bar, kt * KTE, sl * p.Nb + it.y * BN);
     }
 };
