@@ -151,8 +151,9 @@ fc_status fc_rimp2_energy_grad_dev(const double* b_ov, int64_t naux, int64_t noc
  * and keeps the blocks above the diagonal in FP32 until their column (at
  * most eight chunk budgets, else -- or with FERRIC_CUDA_DENS_STORE=0 -- the
  * chunk pairs off the diagonal run once per column, as in FC_PREC_F64).
- * Otherwise as fc_rimp2_energy_grad / _dev (gamma, de_docc, de_dvir as
- * there). */
+ * Slabs and kept blocks are library workspace: they stay allocated for the
+ * next call until fc_release_workspace.  Otherwise as fc_rimp2_energy_grad /
+ * _dev (gamma, de_docc, de_dvir as there). */
 fc_status fc_rimp2_energy_grad_dens(const double* b_ov, int64_t naux, int64_t nocc, int64_t nvir,
                                     const double* eps_occ, const double* eps_vir, int32_t precision,
                                     double* e_os, double* e_ss, double* gamma, double* de_docc,
