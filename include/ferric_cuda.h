@@ -47,8 +47,10 @@ typedef int32_t fc_status;
                               /* slices, the 10 products of level <= 3 in 4 int32  */
                               /* sums (tcgen05 kind::i8), (ia|ia) of the i == j    */
                               /* blocks in FP64; adjoint: 3 int8 slices, 6         */
-                              /* products; DF-K, dressing, Imat: 3 bf16 slices,    */
-                              /* FP32 sums drained to FP64 before they could round */
+                              /* products; DF-K and the MP2 densities: 3 int8      */
+                              /* slices, int32 sums; dressing, Imat: 3 bf16        */
+                              /* slices, FP32 sums drained to FP64 before they     */
+                              /* could round                                       */
 #define FC_PREC_MIXED_FAST 2  /* split-BF16 hi+lo, 3 products, FP32 accumulation   */
                               /* (energy only; ~1e-5 relative, accumulation-bound) */
 
