@@ -93,6 +93,7 @@ static_assert((2 * PSTAGES + 4) * 8 + 8 * (2 * EPI_WARPS * 3 + (NCG - 1) * BM + 
 static_assert(HC % 32 == 0 && 4 * NCG == EPI_WARPS, "pair epilogue layout");
 constexpr int SMEM = PSTAGES * PSTAGE_BYTES + 1024 + SCR_BYTES + 2 * COL_BYTES;  // two column sets
 constexpr uint32_t IDESC = tc::idesc_i8_s32(128, 128);
+constexpr uint32_t IDESC2 = tc::idesc_i8_s32(128, 256);  // two stacked B slices
 constexpr double LW = 254.0, LW2INV = 1.0 / (254.0 * 254.0), LW3INV = 1.0 / (254.0 * 254.0 * 254.0);
 
 // s (L0 + L1 / 254 + L2 / 254^2) from the three int32 TMEM words of a level
@@ -295,51 +296,74 @@ __global__ void __launch_bounds__(256) split_fx_rows_f32_kernel(const float* __r
     split_fx_rows_f32_body<SliceI8>(T, K, K, slice_rows, ts, Ts, blockIdx.x);
 }
 
-// The 6 products of one k-step (4 MMAs of K = 32 each) from the stage whose
-// A slice 0 has descriptor `da`; the three A slices are A_BYTES apart and the
-// B slices start BOFS bytes after A slice 0.  Offsets are compile-time: the
-// descriptor start-address field is linear in the address.
-// PART 0 issues all six; PART 1 the four products of slices 0 and 1, PART 2
-// the two with a slice 2 (their operands may arrive later).  The int32 sums
-// are exact, so the order of the products does not change the result.
+// The 6 products of one k-step (KT / 32 MMAs of K = 32 per product) from
+// the stage whose A slice 0 has descriptor `da`; the three A slices are
+// A_BYTES apart and the B slices start BOFS bytes after A slice 0 (adjacent,
+// B_BYTES = 128 rows apart), and the level accumulators are adjacent in TMEM
+// (BN columns apart).  Offsets are compile-time: the descriptor start-address
+// field is linear in the address.  PART 1 issues the four products of slices
+// 0 and 1 as two N = 256 MMAs of an A slice with the stacked rows [B0; B1]
+// (A0 -> levels 0, 1; A1 -> levels 1, 2), except on the first K step of a
+// segment, where level 2 starts (A1 B1 is its first product) while level 1
+// accumulates, so A1 B0 and A1 B1 go as two N = 128 MMAs; PART 2 issues the
+// two with a slice 2 (their operands may arrive later); PART 0 both.  The
+// int32 sums are exact, so the order of the products does not change the
+// result.
 template <int BOFS, int PART = 0>
 __device__ __forceinline__ void issue_products(uint64_t da, uint32_t tmem_base, int kt) {
     using namespace fx;
-    constexpr int PA[6] = {0, 0, 1, 1, 0, 2};
-    constexpr int PB[6] = {0, 1, 0, 1, 2, 0};
-    constexpr int PL[6] = {0, 1, 1, 2, 2, 2};
-    constexpr int PF[6] = {1, 1, 0, 1, 0, 0};  // first product of its level
-    constexpr int P0 = PART == 2 ? 4 : 0, P1 = PART == 1 ? 4 : 6;
+    auto a_of = [&](int sl, int kk) { return da + (uint64_t)((sl * A_BYTES + kk * 32) >> 4); };
+    auto b_of = [&](int sl, int kk) { return da + (uint64_t)((BOFS + sl * B_BYTES + kk * 32) >> 4); };
+    if (PART != 2) {
 #pragma unroll
-    for (int pr = P0; pr < P1; ++pr) {
+        for (int kk = 0; kk < KT / 32; ++kk) {
+            const uint32_t acc = (kt > 0 || kk > 0) ? 1u : 0u;
+            tc::umma_i8(tmem_base, a_of(0, kk), b_of(0, kk), IDESC2, acc);
+            if (acc) {
+                tc::umma_i8(tmem_base + BN, a_of(1, kk), b_of(0, kk), IDESC2, 1u);
+            } else {
+                tc::umma_i8(tmem_base + BN, a_of(1, kk), b_of(0, kk), IDESC, 1u);
+                tc::umma_i8(tmem_base + 2 * BN, a_of(1, kk), b_of(1, kk), IDESC, 0u);
+            }
+        }
+    }
+    if (PART != 1) {
 #pragma unroll
-        for (int kk = 0; kk < KT / 32; ++kk)
-            tc::umma_i8(tmem_base + PL[pr] * BN, da + (uint64_t)((PA[pr] * A_BYTES + kk * 32) >> 4),
-                        da + (uint64_t)((BOFS + PB[pr] * B_BYTES + kk * 32) >> 4), IDESC,
-                        (kt > 0 || kk > 0 || !PF[pr]) ? 1u : 0u);
+        for (int kk = 0; kk < KT / 32; ++kk) {
+            tc::umma_i8(tmem_base + 2 * BN, a_of(0, kk), b_of(2, kk), IDESC, 1u);
+            tc::umma_i8(tmem_base + 2 * BN, a_of(2, kk), b_of(0, kk), IDESC, 1u);
+        }
     }
 }
 
 // ------------------------------------------------------------ pair kernel --
 
-// The 10 products of one k-step of the pair kernel (2 MMAs of K = 32 each)
-// from the stage whose A slice 0 has descriptor `da`; the four A slices are
-// PA_BYTES apart and the B slices start BOFS bytes after A slice 0.  Level
-// l = k + m collects the products c_k c'_m of slices k and m, l <= 3.
+// The 10 products of one k-step of the pair kernel (K = 32 per MMA, PKT / 32
+// MMAs per product) from the stage whose A slice 0 has descriptor `da`; the
+// four A slices are PA_BYTES apart and the B slices start BOFS bytes after A
+// slice 0.  Level l = k + m collects the products c_k c'_m of slices k and m,
+// l <= 3.  The B slices are adjacent in shared memory (PB_BYTES = 128 rows
+// apart) and the level accumulators adjacent in TMEM (BN columns apart), so
+// one N = 256 MMA of A slice k with the stacked rows [B_m; B_m+1] adds
+// c_k c'_m to level k + m and c_k c'_m+1 to level k + m + 1: six MMAs (four
+// of N = 256, two of N = 128) issue the ten products, and each A slice is
+// read from shared memory once per 256 columns.  The ten 128 x 128 MMAs they
+// replace were bound by shared-memory reads (8 KiB per 64-cycle MMA, with
+// the TMA writes beside them).
 template <int BOFS>
 __device__ __forceinline__ void issue_products4(uint64_t da, uint32_t tmem_base, int kt) {
     using namespace fx;
-    constexpr int PA[10] = {0, 0, 1, 0, 1, 2, 0, 1, 2, 3};
-    constexpr int PB[10] = {0, 1, 0, 2, 1, 0, 3, 2, 1, 0};
-    constexpr int PL[10] = {0, 1, 1, 2, 2, 2, 3, 3, 3, 3};
-    constexpr int PF[10] = {1, 1, 0, 1, 0, 0, 1, 0, 0, 0};  // first product of its level
+    constexpr int PA[6] = {0, 0, 1, 1, 2, 3};  // A slice
+    constexpr int PB[6] = {0, 2, 0, 2, 0, 0};  // first B slice; the MMA writes levels PA + PB (+ 1)
+    constexpr int PW[6] = {1, 1, 0, 0, 0, 0};  // first write of its levels
+    constexpr bool P2[6] = {true, true, true, false, true, false};  // two B slices (N = 256)
 #pragma unroll
-    for (int pr = 0; pr < 10; ++pr) {
+    for (int pr = 0; pr < 6; ++pr) {
 #pragma unroll
         for (int kk = 0; kk < PKT / 32; ++kk)
-            tc::umma_i8(tmem_base + PL[pr] * BN, da + (uint64_t)((PA[pr] * PA_BYTES + kk * 32) >> 4),
-                        da + (uint64_t)((BOFS + PB[pr] * PB_BYTES + kk * 32) >> 4), IDESC,
-                        (kt > 0 || kk > 0 || !PF[pr]) ? 1u : 0u);
+            tc::umma_i8(tmem_base + (PA[pr] + PB[pr]) * BN, da + (uint64_t)((PA[pr] * PA_BYTES + kk * 32) >> 4),
+                        da + (uint64_t)((BOFS + PB[pr] * PB_BYTES + kk * 32) >> 4), P2[pr] ? IDESC2 : IDESC,
+                        (kt > 0 || kk > 0 || !PW[pr]) ? 1u : 0u);
     }
 }
 
@@ -862,7 +886,6 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
                 const int a = ta * BM + row;
                 const bool va = a < v.nvir;
                 const double sxa = v.scl[(int64_t)i * v.a_pad + a];
-                const double sya = v.scl[(int64_t)j * v.a_pad + a];
                 double* const cb_ = colb + (li & 1) * 3 * BN;
                 // the tile's columns (virtual energies, scales of (j, b) and (i, b)) in
                 // shared memory: every lane of a warp reads the same column (broadcast)

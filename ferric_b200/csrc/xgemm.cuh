@@ -47,11 +47,6 @@ constexpr int BM = 128, KT = 64, KP = 8;
 constexpr double L1W = 1.0 / 256.0, L2W = 1.0 / 65536.0;
 constexpr double I8L1W = 1.0 / 254.0, I8L2W = 1.0 / (254.0 * 254.0);
 
-// products: (A slice, B slice, level)
-static __constant__ int8_t kPA[6] = {0, 0, 1, 0, 1, 2};
-static __constant__ int8_t kPB[6] = {0, 1, 0, 2, 1, 0};
-static __constant__ int8_t kPL[6] = {0, 1, 1, 2, 2, 2};
-static __constant__ int8_t kPFirst[6] = {1, 1, 0, 1, 0, 0};
 
 template <int BN, bool I8 = false>
 struct Cfg {
@@ -67,6 +62,7 @@ struct Cfg {
     static constexpr int TCOLS = NSET * 3 * BN <= 256 ? 256 : 512;
     static constexpr int SMEM = STAGES * STAGE + 1024 + 256;
     static constexpr uint32_t IDESC = I8 ? tc::idesc_i8_s32(128, BN) : tc::idesc_bf16_f32(128, BN);
+    static constexpr uint32_t IDESC2 = I8 ? tc::idesc_i8_s32(128, 2 * BN) : tc::idesc_bf16_f32(128, 2 * BN);
 };
 
 }  // namespace xg
@@ -218,19 +214,25 @@ __global__ void __launch_bounds__(xg::Cfg<BN, I8>::THREADS, 1)
                         const uint32_t uu = g / S;
                         if (!tc::mbar_wait(&full[s], uu & 1, abort_flag, p.err)) goto mma_done;
                         tc::fence_after_sync();
+                        // four MMAs: A0 B0 (level 0), A0 [B1; B2] (levels 1, 2: the B
+                        // slices are adjacent, BN rows apart, and so are the levels in
+                        // TMEM, so one N = 2 BN MMA reads A0 once for both), A1 [B0; B1]
+                        // (levels 1, 2), A2 B0 (level 2); the first two start the levels
+                        constexpr int kXA[4] = {0, 0, 1, 2}, kXB[4] = {0, 1, 0, 0};
 #pragma unroll
-                        for (int pr = 0; pr < 6; ++pr) {
-                            const uint32_t a0 = sa(s, kPA[pr]), b0 = sb(s, kPB[pr]);
-                            const uint32_t dcol = dset + kPL[pr] * BN;
+                        for (int pr = 0; pr < 4; ++pr) {
+                            const uint32_t a0 = sa(s, kXA[pr]), b0 = sb(s, kXB[pr]);
+                            const uint32_t dcol = dset + (kXA[pr] + kXB[pr]) * BN;
 #pragma unroll
                             for (int kk = 0; kk < 4; ++kk) {  // 32 bytes of K per MMA
-                                const uint32_t acc = (kq > k0 || kk > 0 || !kPFirst[pr]) ? 1u : 0u;
+                                const uint32_t acc = (kq > k0 || kk > 0 || pr > 1) ? 1u : 0u;
+                                const uint32_t id = (pr == 1 || pr == 2) ? C::IDESC2 : C::IDESC;
                                 if constexpr (I8)
                                     tc::umma_i8(dcol, tc::sdesc_k128(a0 + kk * 32), tc::sdesc_k128(b0 + kk * 32),
-                                                C::IDESC, acc);
+                                                id, acc);
                                 else
                                     tc::umma_bf16(dcol, tc::sdesc_k128(a0 + kk * 32), tc::sdesc_k128(b0 + kk * 32),
-                                                  C::IDESC, acc);
+                                                  id, acc);
                             }
                         }
                         tc::umma_commit(&empty[s]);
