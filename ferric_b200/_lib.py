@@ -32,6 +32,7 @@ SIGNATURES = {
     "fc_init": (_I32, [_I32, _c.c_uint64]),
     "fc_release_workspace": (_I32, []),
     "fc_pool_used": (_c.c_uint64, []),
+    "fc_check_recip": (_I32, [_P, _I64, _P]),
     "fc_last_error": (_c.c_size_t, [_c.c_char_p, _c.c_size_t]),
     "fc_version": (_c.c_char_p, []),
     "fc_rimp2_energy": (_I32, [_P, _I64, _I64, _I64, _P, _P, _I32, _D, _I32, _DP, _DP, _P]),

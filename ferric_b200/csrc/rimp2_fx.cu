@@ -103,13 +103,26 @@ __device__ __forceinline__ double level_value(float w0, float w1, float w2, doub
     return v * (s * LW2INV);
 }
 
-// s (L0 + L1 / 254 + L2 / 254^2 + L3 / 254^3) from the four int32 TMEM words
-// of the pair kernel's level set: ((L0 254 + L1) 254 + L2) 254 + L3 is an
-// integer below 2^53 while K <= 33286, so it is exact in FP64.
-__device__ __forceinline__ double level_value4(float w0, float w1, float w2, float w3, double s) {
+// 1 / d in FP64 by the Newton-Raphson iteration for the reciprocal, taken
+// to third order from an FP32 seed: with rf = (1 / d)(1 + delta) and
+// e = 1 - d rf = -delta (one FMA), rf (1 + e + e^2) = (1 / d)(1 - delta^3).
+// |delta| <= 2^-23 (the FP32 roundings of d and of the seed), so the result
+// is 1 / d to within the final FP64 rounding.  For normal FP32 magnitudes of
+// d (the orbital-energy denominators are far inside them).
+__device__ __forceinline__ double recip_nr(double d) {
+    const double rf = (double)__frcp_rn(__double2float_rn(d));
+    const double e = fma(-d, rf, 1.0);
+    return fma(fma(e, e, e), rf, rf);
+}
+
+// s (L0 + L1 / 254 + L2 / 254^2 + L3 / 254^3) = s3 (((L0 254 + L1) 254 + L2)
+// 254 + L3) for s3 = s / 254^3, from the four int32 TMEM words of the pair
+// kernel's level set; the integer combination is below 2^53 while
+// K <= 33286, so it is exact in FP64.
+__device__ __forceinline__ double level_value4(float w0, float w1, float w2, float w3, double s3) {
     const double v =
         ((tc::i32_to_f64(w0) * LW + tc::i32_to_f64(w1)) * LW + tc::i32_to_f64(w2)) * LW + tc::i32_to_f64(w3);
-    return v * (s * LW3INV);
+    return v * s3;
 }
 
 }  // namespace fx
@@ -491,6 +504,7 @@ __device__ __forceinline__ ItemView item_view(const PairFxArgs& p, int64_t k) {
 __device__ __forceinline__ void drain_levels(uint32_t tl, double sr, const double* __restrict__ sc, double* dst,
                                              int gdv, double gval) {
     using namespace fx;
+    const double sr3 = sr * LW3INV;
 #pragma unroll
     for (int c0 = 0; c0 < HC; c0 += 8) {
         float l0[8], l1[8], l2[8], l3[8];
@@ -502,7 +516,7 @@ __device__ __forceinline__ void drain_levels(uint32_t tl, double sr, const doubl
         double x[8];
 #pragma unroll
         for (int cc = 0; cc < 8; ++cc) {
-            x[cc] = level_value4(l0[cc], l1[cc], l2[cc], l3[cc], sr * sc[c0 + cc]);
+            x[cc] = level_value4(l0[cc], l1[cc], l2[cc], l3[cc], sr3 * sc[c0 + cc]);
             if (c0 + cc == gdv) x[cc] = gval;
         }
         double2* d2 = reinterpret_cast<double2*>(dst + c0);
@@ -723,12 +737,14 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
                     const double y = yv[cc];
                     float tval = 0.f, mval = 0.f, colv = 0.f;
                     if (va && c0 + cc < bmax) {
-                        const double r = 1.0 / (dA - evb[c0 + cc]);
+                        const double r = recip_nr(dA - evb[c0 + cc]);
+                        const double xr = x * r;
+                        const double yr = diag ? xr : y * r;
                         if (diag) {
-                            os += x * x * r;
+                            os = fma(x, xr, os);
                         } else {
-                            os += (x * x + y * y) * r;
-                            ss += (x - y) * (x - y) * r;
+                            os = fma(y, yr, fma(x, xr, os));
+                            ss = fma(x - y, xr - yr, ss);
                         }
                         if (GRAD) {
                             // t Tt summed over a pair's elements is the pair's share of
@@ -737,21 +753,25 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
                             // on b (its row index); the mirrored tile the other way round.
                             // On an exchanged diagonal tile the thread of row a also
                             // holds (b, a)'s term and puts it on a directly.
-                            const double tt = (2.0 * x - y) * r;   // Tt_ij[a, b]
-                            const double cd = x * r * tt;          // t Tt at (a, b)
-                            double cm = 0.0;
+                            const double tt = fma(2.0, xr, -yr);  // Tt_ij[a, b]
+                            const double cd = xr * tt;            // t Tt at (a, b)
                             tval = (float)tt;
-                            if (mir) {
-                                const double tm = (2.0 * y - x) * r;  // Tt_ij[b, a]
-                                cm = y * r * tm;                      // t Tt at (b, a)
-                                mval = (float)tm;
-                            }
-                            oc += cd + cm;
-                            if (xt) {
-                                rowc += cd + y * r * ((2.0 * y - x) * r);  // t Tt at (b, a)
+                            if (mir || xt) {
+                                const double tm = fma(2.0, yr, -xr);  // Tt_ij[b, a]
+                                const double cm = yr * tm;            // t Tt at (b, a)
+                                const double cs = cd + cm;
+                                if (mir) {
+                                    mval = (float)tm;
+                                    oc += cs;
+                                } else {
+                                    oc += cd;
+                                }
+                                rowc += (both || xt) ? cs : cd;
+                                if (!xt) colv = (float)(both ? cs : cm);
                             } else {
-                                rowc += both ? cd + cm : cd;
-                                colv = (float)(both ? cd + cm : cm);
+                                oc += cd;
+                                rowc += cd;
+                                colv = both ? (float)cd : 0.f;
                             }
                         }
                     }
@@ -2576,3 +2596,34 @@ fc_status rimp2_batch_build_fx(fc_rimp2_batch* b, const std::vector<BatchMolIn>&
 }
 
 }  // namespace fc
+
+// ------------------------------------------------------------ self-check --
+
+namespace fc {
+namespace {
+__global__ void recip_check_kernel(const double* __restrict__ d, int64_t n, double* __restrict__ out) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) out[k] = fx::recip_nr(d[k]);
+}
+}  // namespace
+}  // namespace fc
+
+extern "C" fc_status fc_check_recip(const double* d, int64_t n, double* out) {
+    using namespace fc;
+    if (n < 0 || (n > 0 && (!d || !out))) return fail(FC_ERR_INVALID, "fc_check_recip: bad arguments");
+    if (n == 0) return FC_OK;
+    FC_TRY(require_init());
+    double* dd = nullptr;
+    FC_CUDA(cudaMalloc(&dd, 2 * (size_t)n * sizeof(double)));
+    fc_status st = FC_OK;
+    cudaError_t e = cudaMemcpy(dd, d, (size_t)n * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        recip_check_kernel<<<(unsigned)((n + 255) / 256), 256>>>(dd, n, dd + n);
+        st = check_launch("recip_check_kernel");
+        if (st == FC_OK) e = cudaMemcpy(out, dd + n, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost);
+    }
+    cudaFree(dd);
+    if (st != FC_OK) return st;
+    if (e != cudaSuccess) return cuda_fail(e, "fc_check_recip copy");
+    return FC_OK;
+}

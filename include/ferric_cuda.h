@@ -413,6 +413,12 @@ fc_status fc_dfjk_build_occ_dev(fc_dfjk* h, const double* c_occ, int64_t nocc, d
 fc_status fc_dfjk_set_precision(fc_dfjk* h, int32_t precision);
 fc_status fc_dfjk_destroy(fc_dfjk* h);
 
+/* Self-check: out[k] = the mixed pair epilogue's FP64 reciprocal of d[k]
+ * (host arrays, n <= 2^31), evaluated on the device: an FP32 seed refined by
+ * the third-order Newton-Raphson step, which the tests hold to the
+ * correctly rounded 1 / d (CUDA's FP64 division) within 1 ulp. */
+fc_status fc_check_recip(const double* d, int64_t n, double* out);
+
 #ifdef __cplusplus
 }
 #endif

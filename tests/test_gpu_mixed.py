@@ -326,3 +326,19 @@ def test_gamma_streamed_to_pinned_host(fc, monkeypatch, precision):
                                        L.ptr(do), L.ptr(dv), None))
     assert np.array_equal(g.numpy(), ref[1])
     assert np.array_equal(do, ref[2]) and np.array_equal(dv, ref[3])
+
+
+def test_epilogue_reciprocal_within_one_ulp(fc):
+    """The pair epilogue's 1 / D (an FP32 seed and a third-order
+    Newton-Raphson step) against the correctly rounded FP64 quotient (CUDA's
+    and NumPy's division), over denominators of both signs from 1e-30 to 1e30
+    and a dense sample of the orbital-energy range."""
+    from ferric_b200 import _lib
+    rng = np.random.default_rng(5)
+    mag = np.concatenate([rng.uniform(0.05, 200.0, 200000), np.logspace(-30, 30, 6001),
+                          1.0 + np.arange(-50, 51) * 2.0 ** -52, [1.0, 2.0, 0.5, 3.0, 1.0 / 3.0]])
+    d = np.ascontiguousarray(np.concatenate([-mag, mag]))
+    out = np.empty_like(d)
+    _lib.check(_lib.lib.fc_check_recip(_lib.ptr(d), len(d), _lib.ptr(out)))
+    ref = 1.0 / d
+    assert np.all(np.abs(out - ref) <= np.spacing(np.abs(ref)))
