@@ -496,8 +496,9 @@ __device__ __forceinline__ ItemView item_view(const PairFxArgs& p, int64_t k) {
 }
 
 // This thread's HC columns of a phase's four level accumulators -> FP64
-// values s_r s_c (L0 + L1/254 + L2/254^2 + L3/254^3), stored at dst (its row
-// of the CTA's tile in global scratch, L2 only).  gdv >= 0 is the column (of
+// values s_r s_c (L0 + L1/254 + L2/254^2 + L3/254^3), stored at dst + c BM
+// for its column c (the CTA's column-major tile in global scratch, L2 only;
+// dst is its row of the first of its columns).  gdv >= 0 is the column (of
 // these HC) on the tile diagonal a == b of an i == j block: it takes the
 // exact (ia|ia) instead, whose dropped level-4 products (the slice c3 c3' of
 // a row with itself) are one-signed.
@@ -519,9 +520,9 @@ __device__ __forceinline__ void drain_levels(uint32_t tl, double sr, const doubl
             x[cc] = level_value4(l0[cc], l1[cc], l2[cc], l3[cc], sr3 * sc[c0 + cc]);
             if (c0 + cc == gdv) x[cc] = gval;
         }
-        double2* d2 = reinterpret_cast<double2*>(dst + c0);
+        // column-major tile: the warp's 32 rows of a column are one 256-byte run
 #pragma unroll
-        for (int u = 0; u < 4; ++u) __stcg(d2 + u, make_double2(x[2 * u], x[2 * u + 1]));
+        for (int cc = 0; cc < 8; ++cc) __stcg(dst + (c0 + cc) * BM, x[cc]);
     }
 }
 
@@ -671,9 +672,11 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
         const int row = q * 32 + lane;  // a within the tile
         const int et = tid - 64;        // 0 .. EPI_THREADS - 1
         const uint32_t tl = tmem_base + ((uint32_t)(q * 32) << 16) + h * HC;
-        double* const scr0 = p.scr + (int64_t)blockIdx.x * (3 * BM * BN);  // X tiles [2][row][col], Y tile
+        // X tiles [2][col][row], Y tile [col][row]: column-major, so a warp's
+        // stores and loads of one column cover its 32 consecutive rows
+        double* const scr0 = p.scr + (int64_t)blockIdx.x * (3 * BM * BN);
         double* const syt = scr0 + 2 * BM * BN;
-        double* const yrow = syt + row * BN + h * HC;
+        double* const ycol = syt + h * HC * BM + row;  // this thread's first column, its row
         constexpr int HH = HC / 2;  // columns per half
         // carried from an item's first half of terms to its second
         double os = 0.0, ss = 0.0, oc = 0.0, rowc = 0.0;
@@ -698,34 +701,27 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
             const bool xt = v.xt;
             const bool two = !diag && !xt;
             double* const sxt = scr0 + (lk & 1) * BM * BN;
-            const double* const xrow = sxt + row * BN + h * HC;
+            const double* const xcol = sxt + h * HC * BM + row;
             constexpr int CW = 4;  // columns per step of the FP64 terms
             float ck[HH];          // column terms of this half's columns (gradient)
 #pragma unroll
             for (int cs = 0; cs < HH; cs += CW) {
                 const int c0 = c_lo + cs;
                 double xv[CW], yv[CW];
-                {
-                    const double2* x2 = reinterpret_cast<const double2*>(xrow + c0);
+#pragma unroll
+                for (int cc = 0; cc < CW; ++cc) xv[cc] = __ldcg(xcol + (c0 + cc) * BM);
+                if (two) {
+#pragma unroll
+                    for (int cc = 0; cc < CW; ++cc) yv[cc] = __ldcg(ycol + (c0 + cc) * BM);
+                } else if (xt) {
+                    // Y[a, b] = X[b, a]: column a of X, this thread's columns b as rows
+                    const double2* x2 = reinterpret_cast<const double2*>(sxt + row * BM + h * HC + c0);
 #pragma unroll
                     for (int u = 0; u < CW / 2; ++u) {
                         const double2 t = __ldcg(x2 + u);
-                        xv[2 * u] = t.x;
-                        xv[2 * u + 1] = t.y;
-                    }
-                }
-                if (two) {
-                    const double2* y2 = reinterpret_cast<const double2*>(yrow + c0);
-#pragma unroll
-                    for (int u = 0; u < CW / 2; ++u) {
-                        const double2 t = __ldcg(y2 + u);
                         yv[2 * u] = t.x;
                         yv[2 * u + 1] = t.y;
                     }
-                } else if (xt) {
-                    // Y[a, b] = X[b, a]: lanes hold consecutive a, so each load is coalesced
-#pragma unroll
-                    for (int cc = 0; cc < CW; ++cc) yv[cc] = __ldcg(sxt + (h * HC + c0 + cc) * BN + row);
                 } else {
 #pragma unroll
                     for (int cc = 0; cc < CW; ++cc) yv[cc] = xv[cc];  // i == j: Y = X
@@ -932,8 +928,8 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
                     // (ia|ia) on the diagonal of an i == j block's diagonal tile
                     const int gdv = (diag && ta == tb && va) ? row - h * HC : -1;
                     const double gval = gdv >= 0 ? v.gd[(int64_t)i * v.a_pad + a] : 0.0;
-                    double* const xrow = scr0 + (li & 1) * BM * BN + row * BN + h * HC;
-                    drain_levels(tl, sxa, sxb, xrow, (gdv >= 0 && gdv < HC) ? gdv : -1, gval);
+                    double* const xcol = scr0 + (li & 1) * BM * BN + h * HC * BM + row;
+                    drain_levels(tl, sxa, sxb, xcol, (gdv >= 0 && gdv < HC) ? gdv : -1, gval);
                 }
                 tc::fence_before_sync();
                 tc::mbar_arrive(tempty);
@@ -954,7 +950,7 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
                 if (!tc::bar_and<1, EPI_THREADS>(et != 0 || tc::mbar_wait(tfull, pc & 1, abort_flag, p.err))) break;
                 if (et != 0) tc::mbar_wait(tfull, pc & 1, abort_flag, p.err);
                 tc::fence_after_sync();
-                drain_levels(tl, sya, syb, yrow, -1, 0.0);
+                drain_levels(tl, sya, syb, ycol, -1, 0.0);
                 tc::fence_before_sync();
                 tc::mbar_arrive(tempty);  // the level columns are free for the next item
                 ++pc;
