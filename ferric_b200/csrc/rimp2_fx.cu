@@ -1046,8 +1046,15 @@ __device__ __forceinline__ GemmView gemm_view(const GemmFxArgs& p, const CUtenso
         v.cs = p.cs;
         v.out = p.out;
         v.nov = p.nov;
-        v.tm = (int)(t / p.nTn);
-        v.tn = (int)(t % p.nTn);
+        // groups of GM m-tiles, n-major within a group: a wave of 148 CTAs
+        // covers ~12 x 12 tiles, so each A and each B tile of the wave is read
+        // by ~12 CTAs at about the same K (n-fastest order swept every B tile
+        // in every wave and read ~2x the bytes from DRAM)
+        constexpr int GM = 12;
+        const int64_t g = t / ((int64_t)GM * p.nTn), r = t % ((int64_t)GM * p.nTn);
+        const int gm = (int)(p.nTm - g * GM < GM ? p.nTm - g * GM : GM);
+        v.tm = (int)(g * GM + r % gm);
+        v.tn = (int)(r / gm);
         v.M = p.M;
         v.N = p.N;
         v.nk = p.nk;
