@@ -309,6 +309,88 @@ __global__ void __launch_bounds__(256) split_fx_rows_f32_kernel(const float* __r
     split_fx_rows_f32_body<SliceI8>(T, K, K, slice_rows, ts, Ts, blockIdx.x);
 }
 
+// Column maxima of |T| over the rows [0, R) of the FP32 block T[R][ldt] for
+// the columns [0, C) (C and ldt multiples of 4): cmax[c] takes the FP32 bits
+// (ordered like the values for non-negative floats) by atomicMax and starts
+// at 0.  A warp covers 128 columns (a float4 a lane); the eight warps and
+// blockIdx.y split the rows.
+__global__ void __launch_bounds__(256) colmax_f32_kernel(const float* __restrict__ T, int64_t R, int64_t C,
+                                                         int64_t ldt, int64_t rows_per_split,
+                                                         unsigned* __restrict__ cmax) {
+    __shared__ float4 red[8][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t c = (int64_t)blockIdx.x * 128 + lane * 4;
+    const int64_t r0 = (int64_t)blockIdx.y * rows_per_split;
+    const int64_t r1 = r0 + rows_per_split < R ? r0 + rows_per_split : R;
+    float4 m = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (c < C) {
+        for (int64_t r = r0 + w; r < r1; r += 8) {
+            const float4 v = *reinterpret_cast<const float4*>(T + r * ldt + c);
+            m.x = fmaxf(m.x, fabsf(v.x));
+            m.y = fmaxf(m.y, fabsf(v.y));
+            m.z = fmaxf(m.z, fabsf(v.z));
+            m.w = fmaxf(m.w, fabsf(v.w));
+        }
+    }
+    red[w][lane] = m;
+    __syncthreads();
+    if (w == 0 && c < C) {
+#pragma unroll
+        for (int k = 1; k < 8; ++k) {
+            const float4 v = red[k][lane];
+            m.x = fmaxf(m.x, v.x);
+            m.y = fmaxf(m.y, v.y);
+            m.z = fmaxf(m.z, v.z);
+            m.w = fmaxf(m.w, v.w);
+        }
+        atomicMax(cmax + c, __float_as_uint(m.x));
+        atomicMax(cmax + c + 1, __float_as_uint(m.y));
+        atomicMax(cmax + c + 2, __float_as_uint(m.z));
+        atomicMax(cmax + c + 3, __float_as_uint(m.w));
+    }
+}
+
+// Three int8 slices of T^T: row c of the output is column c of T[R][ldt]
+// (c < C) at the power-of-two scale of its maximum cmax[c]; Ts[s][c][r]
+// (pitch R, slices slice_rows rows apart), ts[c] = the scale: the same
+// values and scales as splitting the rows of a stored transpose.  64 x 64
+// tiles of T pass through shared memory; R and C are multiples of 16.
+__global__ void __launch_bounds__(256) split_cols_f32_kernel(const float* __restrict__ T, int64_t R, int64_t C,
+                                                             int64_t ldt, const unsigned* __restrict__ cmax,
+                                                             int64_t slice_rows, double* __restrict__ ts,
+                                                             int8_t* __restrict__ Ts) {
+    __shared__ float tile[64][65];
+    const int t = threadIdx.x;
+    const int64_t r0 = (int64_t)blockIdx.y * 64, c0 = (int64_t)blockIdx.x * 64;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int rr = (t >> 4) + 16 * k, cc = (t & 15) * 4;
+        const int64_t r = r0 + rr, c = c0 + cc;
+        const float4 v = (r < R && c < C) ? *reinterpret_cast<const float4*>(T + r * ldt + c)
+                                          : make_float4(0.f, 0.f, 0.f, 0.f);
+        tile[rr][cc] = v.x;
+        tile[rr][cc + 1] = v.y;
+        tile[rr][cc + 2] = v.z;
+        tile[rr][cc + 3] = v.w;
+    }
+    __syncthreads();
+    const int cc = t >> 2, rq = (t & 3) * 16;  // output row c0 + cc, its 16 columns from r0 + rq
+    const int64_t c = c0 + cc, r = r0 + rq;
+    if (c >= C || r >= R) return;
+    const double s = SliceI8::scale((double)__uint_as_float(cmax[c]));
+    if (blockIdx.y == 0 && rq == 0) ts[c] = s;
+    const double inv = 1.0 / s;
+    struct alignas(16) Q16 { int8_t e[16]; };
+    Q16 p0, p1, p2;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) fx_slices<SliceI8>(tile[rq + k][cc], inv, p0.e[k], p1.e[k], p2.e[k]);
+    const int64_t ss = slice_rows * R;
+    int8_t* o = Ts + c * R + r;
+    *reinterpret_cast<Q16*>(o) = p0;
+    *reinterpret_cast<Q16*>(o + ss) = p1;
+    *reinterpret_cast<Q16*>(o + 2 * ss) = p2;
+}
+
 // The 6 products of one k-step (KT / 32 MMAs of K = 32 per product) from
 // the stage whose A slice 0 has descriptor `da`; the three A slices are
 // A_BYTES apart and the B slices start BOFS bytes after A slice 0 (adjacent,
@@ -423,6 +505,7 @@ struct PairFxArgs {
     float* T2;       // amplitude rows of J: [|J| a_pad][ldt2 = |I| a_pad] (T when I == J)
     int64_t ldt, ldt2;
     int i0, j0;
+    int no_t2;         // T2 (a buffer of its own) is not written: its slices come from T transposed
     double* occ_part;  // [item]
     double* vir_part;  // [item][2][128]: row-virtual and column-virtual sums
 };
@@ -798,7 +881,7 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
                         for (int cc = 0; cc < CW; ++cc)  // lanes hold consecutive a: coalesced
                             if (cc < bw) trow[(int64_t)(b0 + c0 + cc) * v.ldt + a] = mv8[cc];
                     }
-                    if (both) {
+                    if (both && (BATCH || !p.no_t2)) {
                         float* t2 = v.T2 + ((int64_t)(j - v.j0) * v.tpad) * v.ldt2 + (int64_t)(i - v.i0) * v.tpad;
 #pragma unroll
                         for (int cc = 0; cc < CW; ++cc)  // Tt_ji[b, a] = Tt_ij[a, b]
@@ -1929,13 +2012,29 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
     // Gamma[:, rows] += 4 Bq[:, cols] T^T for one amplitude block
     // (with densities the slices go to the block's rows of the column chunk's
     // slab, slices nocc tp rows apart, and stay there for the density terms)
-    auto adjoint = [&](float* T, int64_t r0, int64_t nr, int64_t k0, int64_t nk, bool to_slab) -> fc_status {
+    // (from_t: T holds the block transposed, [nk tp][nr tp], as T1 of the
+    // chunk pair whose T2 was not written; its column maxima go to the T2
+    // buffer and a tiled transpose writes the slices of its columns)
+    auto adjoint = [&](float* T, int64_t r0, int64_t nr, int64_t k0, int64_t nk, bool to_slab,
+                       bool from_t = false) -> fc_status {
         const int64_t ldk = nk * tp, rows = nr * tp, mp = (rows + 127) / 128 * 128;
         const int64_t sstride = to_slab ? dx.rows : mp;  // rows between slices
         int8_t* sl = to_slab ? dx.ts + r0 * tp * ldk : (int8_t*)vTs;
         double* rsc = to_slab ? dx.tsc + r0 * tp : ts;
-        split_fx_rows_f32_kernel<<<(unsigned)rows, 256, 0, st>>>(T, ldk, sstride, rsc, sl);
-        ++nl;
+        if (from_t) {
+            unsigned* cmax = reinterpret_cast<unsigned*>(T2);
+            constexpr int64_t kSplit = 8;  // row ranges of the column maxima
+            FC_CUDA(cudaMemsetAsync(cmax, 0, (size_t)rows * sizeof(unsigned), st));
+            colmax_f32_kernel<<<dim3((unsigned)((rows + 127) / 128), (unsigned)kSplit), 256, 0, st>>>(
+                T, ldk, rows, rows, (ldk + kSplit - 1) / kSplit, cmax);
+            split_cols_f32_kernel<<<dim3((unsigned)((rows + 63) / 64), (unsigned)((ldk + 63) / 64)), 256, 0, st>>>(
+                T, ldk, rows, rows, cmax, sstride, rsc, sl);
+            FC_TRY(check_launch("split_cols_f32_kernel"));
+            nl += 2;
+        } else {
+            split_fx_rows_f32_kernel<<<(unsigned)rows, 256, 0, st>>>(T, ldk, sstride, rsc, sl);
+            ++nl;
+        }
         CUtensorMap tmTs;
         FC_TRY(make_tmap_i8_2d(&tmTs, sl, ldk, 3 * sstride - (to_slab ? r0 * tp : 0), ldk, fx::KT, 128));
         GemmFxArgs g{};
@@ -2030,6 +2129,9 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
         a.ldt = cp.nj * tp;
         a.T2 = same ? T1 : T2;
         a.ldt2 = same ? a.ldt : cp.ni * tp;
+        // without densities T2 only feeds the J rows' adjoint, whose slices
+        // come from T by a tiled transpose: the pair kernel skips its stores
+        a.no_t2 = (!dens && !same) ? 1 : 0;
         a.i0 = (int)cp.i0;
         a.j0 = (int)cp.j0;
         a.occ_part = occ_part;
@@ -2076,7 +2178,12 @@ fc_status rimp2_grad_fx(const Rimp2Dev& d, cudaStream_t st, double* e_os, double
             if (step.last) FC_TRY(dens_fx_slab(dx, cp.ni, st, flags + 1, &nl));
         } else {
         if (step.blk != 1) FC_TRY(adjoint(T1, cp.i0, cp.ni, cp.j0, cp.nj, dens));
-        if (step.blk != 0 && !same) FC_TRY(adjoint(T2, cp.j0, cp.nj, cp.i0, cp.ni, dens));
+        if (step.blk != 0 && !same) {
+            if (a.no_t2)
+                FC_TRY(adjoint(T1, cp.j0, cp.nj, cp.i0, cp.ni, false, true));
+            else
+                FC_TRY(adjoint(T2, cp.j0, cp.nj, cp.i0, cp.ni, dens));
+        }
         if (dens) {
             // the block (I, K) of the column chunk K: t and its slices, and
             // the slab's density terms once the column is complete
