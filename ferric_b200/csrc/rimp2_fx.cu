@@ -502,7 +502,8 @@ struct PairFxArgs {
     int drop_load;
     // gradient mode: pairs (i, j), i in chunk I (from i0), j in chunk J (from j0)
     float* T;        // amplitude rows of I: [|I| a_pad][ldt = |J| a_pad]
-    float* T2;       // amplitude rows of J: [|J| a_pad][ldt2 = |I| a_pad] (T when I == J)
+    float* T2;       // amplitude rows of J: [|J| a_pad][ldt2 = |I| a_pad] (T when I == J; not
+                     // written with no_t2)
     int64_t ldt, ldt2;
     int i0, j0;
     int no_t2;         // T2 (a buffer of its own) is not written: its slices come from T transposed
