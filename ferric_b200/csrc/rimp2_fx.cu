@@ -462,6 +462,28 @@ __device__ __forceinline__ void issue_products4(uint64_t da, uint32_t tmem_base,
     }
 }
 
+// The ten products one by one, N = n (a multiple of 16, idesc encodes it):
+// the last virtual tile of a pair operand, whose columns past n are
+// padding.  Ten MMAs of N = n issue n / 128 of the stacked form's work when
+// n <= 64; the accumulator columns from n on keep stale integers, which the
+// epilogue never reads as amplitudes (they are columns b >= nvir).
+template <int BOFS>
+__device__ __forceinline__ void issue_products4_n(uint64_t da, uint32_t tmem_base, int kt, uint32_t idesc) {
+    using namespace fx;
+    constexpr int PA[10] = {0, 0, 1, 0, 1, 2, 0, 1, 2, 3};
+    constexpr int PB[10] = {0, 1, 0, 2, 1, 0, 3, 2, 1, 0};
+    constexpr int PL[10] = {0, 1, 1, 2, 2, 2, 3, 3, 3, 3};
+    constexpr int PF[10] = {1, 1, 0, 1, 0, 0, 1, 0, 0, 0};  // first product of its level
+#pragma unroll
+    for (int pr = 0; pr < 10; ++pr) {
+#pragma unroll
+        for (int kk = 0; kk < PKT / 32; ++kk)
+            tc::umma_i8(tmem_base + PL[pr] * BN, da + (uint64_t)((PA[pr] * PA_BYTES + kk * 32) >> 4),
+                        da + (uint64_t)((BOFS + PB[pr] * PB_BYTES + kk * 32) >> 4), idesc,
+                        (kt > 0 || kk > 0 || !PF[pr]) ? 1u : 0u);
+    }
+}
+
 // One molecule of a batch (operand rows row0 .. row0 + 4*nocc*a_pad of the
 // concatenated slice buffer, slice-major).
 struct BatchMol {
@@ -711,6 +733,11 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
             for (int64_t k = blockIdx.x; k < p.items && !*abort_flag; k += gridDim.x) {
                 const ItemView v = item_view<BATCH>(p, k);
                 const int nph = (v.i == v.j || v.xt) ? 1 : 2;
+                // the last virtual tile of B: its first nt columns (rounded to 16) hold virtuals
+                const int rem = v.nvir - v.tb * BN;
+                const int nt = rem >= BN ? BN : (rem + 15) / 16 * 16;
+                const bool trim = nt <= 64;
+                const uint32_t idt = tc::idesc_i8_s32(128, nt);
                 for (int ph = 0; ph < nph; ++ph, ++pc) {
                     if (!tc::mbar_wait(tempty, (pc & 1) ^ 1, abort_flag, p.err)) goto mma_done;
                     tc::fence_after_sync();
@@ -725,7 +752,10 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
 #pragma unroll
                         for (int t = 1; t < S; ++t)
                             if (s == t) d = da[t];
-                        issue_products4<PSL * PA_BYTES>(d, tmem_base, kt);
+                        if (trim)
+                            issue_products4_n<PSL * PA_BYTES>(d, tmem_base, kt, idt);
+                        else
+                            issue_products4<PSL * PA_BYTES>(d, tmem_base, kt);
                         tc::umma_commit(&empty[s]);
                     }
                     tc::umma_commit(tfull);
