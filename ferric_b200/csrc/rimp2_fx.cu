@@ -30,18 +30,23 @@
 //
 // Pair kernel (this file): item = (pair, a-tile 128, b-tile 128); the X phase
 // accumulates (ia|jb) into the four level accumulators (all 512 TMEM
-// columns); the epilogue drains them into the CTA's FP64 X tile in global
+// columns; the ten products go as six MMAs, four of them over two stacked B
+// slices, or as ten narrower ones on a last virtual tile of <= 64 columns);
+// the epilogue drains them into the CTA's column-major FP64 X tile in global
 // scratch (L2-resident) and hands TMEM back; the Y phase accumulates
 // (ib|ja) = G_ji[a, b] and is drained into the Y tile; the FP64 terms then
-// run from the tiles under the next item's X phase.  16 epilogue warps, each
-// thread one row and 32 columns of the tile.  Energy mode: unordered pairs,
+// run from the tiles in two halves, under the next item's two phases.  16
+// epilogue warps, each thread one row and 32 columns of the tile.  Energy
+// mode: unordered pairs,
 // E_OS += (X^2 + Y^2)/D, E_SS += (X - Y)^2/D (i == j: X phase only, E_SS = 0),
 // the reference pair loop of ferric-mp2/src/rimp2.rs:1399-1544 over both
 // orderings.  Gradient mode: unordered pairs of an occupied chunk pair
 // (I, J); the item writes Tt_ij = (2X - Y)/D (FP32) into the rows of i and
-// Tt_ji = Tt_ij^T into the rows of j, and the dE/deps partials of both
-// orderings; the adjoint contraction Gamma[:, I] += 4 Bq[:, J] Tt_IJ^T runs
-// in gemm_fx_kernel.  Diagonal tiles (ta == tb, i != j) run in one phase,
+// (where the density terms need it, or I == J) Tt_ji = Tt_ij^T into the
+// rows of j, and the dE/deps partials of both orderings; the adjoint
+// contraction Gamma[:, I] += 4 Bq[:, J] Tt_IJ^T runs in gemm_fx_kernel, its
+// J-side operand sliced from Tt_IJ by a tiled transpose when Tt_JI is not
+// stored.  Diagonal tiles (ta == tb, i != j) run in one phase,
 // Y = X^T read back transposed from the X tile (the exchange schedule).
 #include <algorithm>
 #include <cstdlib>
