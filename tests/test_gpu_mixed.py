@@ -89,7 +89,10 @@ def energy_from_g(g, eo, ev, b=None):
     return e_os, e_ss
 
 
-SHAPES = [(96, 5, 23), (84, 5, 19), (200, 7, 65), (300, 4, 130), (130, 3, 128), (480, 12, 110)]
+# nvir 190 and 192: the last virtual tile trimmed to 64 columns (its limit);
+# 193: 80 columns, the stacked form
+SHAPES = [(96, 5, 23), (84, 5, 19), (200, 7, 65), (300, 4, 130), (130, 3, 128), (480, 12, 110),
+          (260, 4, 190), (260, 3, 193)]
 
 
 @pytest.mark.parametrize("xt", ["0", "1"])
@@ -111,7 +114,8 @@ def test_mixed_energy_matches_oracle_and_emulation(fc, monkeypatch, naux, nocc, 
 
 
 @pytest.mark.parametrize("xt", ["0", "1"])
-@pytest.mark.parametrize("naux,nocc,nvir", [(96, 5, 23), (200, 7, 65), (300, 4, 130), (520, 6, 300)])
+@pytest.mark.parametrize("naux,nocc,nvir", [(96, 5, 23), (200, 7, 65), (300, 4, 130), (520, 6, 300),
+                                            (260, 4, 192)])
 def test_mixed_gradient_matches_oracle(fc, monkeypatch, naux, nocc, nvir, xt):
     from ferric_b200 import rimp2
     monkeypatch.setenv("FERRIC_CUDA_XT", xt)
