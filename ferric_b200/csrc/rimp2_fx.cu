@@ -826,24 +826,28 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
 #pragma unroll
             for (int cs = 0; cs < HH; cs += CW) {
                 const int c0 = c_lo + cs;
-                double xv[CW], yv[CW];
+                double xv[CW] = {}, yv[CW] = {};
+                // columns wholly past the last virtual read nothing (their tile
+                // columns were not drained; their amplitudes are zeros)
+                if (c0 < bmax) {
 #pragma unroll
-                for (int cc = 0; cc < CW; ++cc) xv[cc] = __ldcg(xcol + (c0 + cc) * BM);
-                if (two) {
+                    for (int cc = 0; cc < CW; ++cc) xv[cc] = __ldcg(xcol + (c0 + cc) * BM);
+                    if (two) {
 #pragma unroll
-                    for (int cc = 0; cc < CW; ++cc) yv[cc] = __ldcg(ycol + (c0 + cc) * BM);
-                } else if (xt) {
-                    // Y[a, b] = X[b, a]: column a of X, this thread's columns b as rows
-                    const double2* x2 = reinterpret_cast<const double2*>(sxt + row * BM + h * HC + c0);
+                        for (int cc = 0; cc < CW; ++cc) yv[cc] = __ldcg(ycol + (c0 + cc) * BM);
+                    } else if (xt) {
+                        // Y[a, b] = X[b, a]: column a of X, this thread's columns b as rows
+                        const double2* x2 = reinterpret_cast<const double2*>(sxt + row * BM + h * HC + c0);
 #pragma unroll
-                    for (int u = 0; u < CW / 2; ++u) {
-                        const double2 t = __ldcg(x2 + u);
-                        yv[2 * u] = t.x;
-                        yv[2 * u + 1] = t.y;
+                        for (int u = 0; u < CW / 2; ++u) {
+                            const double2 t = __ldcg(x2 + u);
+                            yv[2 * u] = t.x;
+                            yv[2 * u + 1] = t.y;
+                        }
+                    } else {
+#pragma unroll
+                        for (int cc = 0; cc < CW; ++cc) yv[cc] = xv[cc];  // i == j: Y = X
                     }
-                } else {
-#pragma unroll
-                    for (int cc = 0; cc < CW; ++cc) yv[cc] = xv[cc];  // i == j: Y = X
                 }
                 float tt8[CW], mv8[CW];
 #pragma unroll
@@ -1048,7 +1052,9 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
                     const int gdv = (diag && ta == tb && va) ? row - h * HC : -1;
                     const double gval = gdv >= 0 ? v.gd[(int64_t)i * v.a_pad + a] : 0.0;
                     double* const xcol = scr0 + (li & 1) * BM * BN + h * HC * BM + row;
-                    drain_levels(tl, sxa, sxb, xcol, (gdv >= 0 && gdv < HC) ? gdv : -1, gval);
+                    // a column group wholly past the last virtual is never read
+                    if (h * HC < v.nvir - tb * BN)
+                        drain_levels(tl, sxa, sxb, xcol, (gdv >= 0 && gdv < HC) ? gdv : -1, gval);
                 }
                 tc::fence_before_sync();
                 tc::mbar_arrive(tempty);
@@ -1069,7 +1075,7 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
                 if (!tc::bar_and<1, EPI_THREADS>(et != 0 || tc::mbar_wait(tfull, pc & 1, abort_flag, p.err))) break;
                 if (et != 0) tc::mbar_wait(tfull, pc & 1, abort_flag, p.err);
                 tc::fence_after_sync();
-                drain_levels(tl, sya, syb, ycol, -1, 0.0);
+                if (h * HC < v.nvir - v.tb * BN) drain_levels(tl, sya, syb, ycol, -1, 0.0);
                 tc::fence_before_sync();
                 tc::mbar_arrive(tempty);  // the level columns are free for the next item
                 ++pc;
