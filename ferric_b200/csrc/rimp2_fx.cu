@@ -827,9 +827,9 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
             for (int cs = 0; cs < HH; cs += CW) {
                 const int c0 = c_lo + cs;
                 double xv[CW] = {}, yv[CW] = {};
-                // columns wholly past the last virtual read nothing (their tile
-                // columns were not drained; their amplitudes are zeros)
-                if (c0 < bmax) {
+                // rows and columns past the last virtual read nothing (those tile
+                // entries may not have been drained; their amplitudes are zeros)
+                if (va && c0 < bmax) {
 #pragma unroll
                     for (int cc = 0; cc < CW; ++cc) xv[cc] = __ldcg(xcol + (c0 + cc) * BM);
                     if (two) {
@@ -1052,8 +1052,9 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
                     const int gdv = (diag && ta == tb && va) ? row - h * HC : -1;
                     const double gval = gdv >= 0 ? v.gd[(int64_t)i * v.a_pad + a] : 0.0;
                     double* const xcol = scr0 + (li & 1) * BM * BN + h * HC * BM + row;
-                    // a column group wholly past the last virtual is never read
-                    if (h * HC < v.nvir - tb * BN)
+                    // a warp whose columns or rows lie wholly past the last virtual
+                    // drains nothing: those tile entries are never read
+                    if (h * HC < v.nvir - tb * BN && q * 32 < v.nvir - ta * BM)
                         drain_levels(tl, sxa, sxb, xcol, (gdv >= 0 && gdv < HC) ? gdv : -1, gval);
                 }
                 tc::fence_before_sync();
@@ -1075,7 +1076,8 @@ __global__ void __launch_bounds__(fx::PAIR_THREADS, 1)
                 if (!tc::bar_and<1, EPI_THREADS>(et != 0 || tc::mbar_wait(tfull, pc & 1, abort_flag, p.err))) break;
                 if (et != 0) tc::mbar_wait(tfull, pc & 1, abort_flag, p.err);
                 tc::fence_after_sync();
-                if (h * HC < v.nvir - v.tb * BN) drain_levels(tl, sya, syb, ycol, -1, 0.0);
+                if (h * HC < v.nvir - v.tb * BN && q * 32 < v.nvir - v.ta * BM)
+                    drain_levels(tl, sya, syb, ycol, -1, 0.0);
                 tc::fence_before_sync();
                 tc::mbar_arrive(tempty);  // the level columns are free for the next item
                 ++pc;
